@@ -1,0 +1,845 @@
+// Host driver of the B200 stochastic block partitioner and the C ABI of
+// include/sbp.h.
+//
+// The loop is GSAP's partition() (partition.hpp:852-954): start from B = N,
+// then repeat { merge step; nodal sweeps until the moving-average dS test
+// stops them; golden-section bookkeeping over B } until the bracket closes.
+// Differences in how it runs on the device:
+//   * one device arena per job (GSAP: four slabs plus separate buffers and
+//     per-call allocations inside bb_segsort / mgpu / thrust);
+//   * every kernel on one stream; the host synchronises once per nodal sweep
+//     (to read the sweep's dS sum and the MDL) and once per merge step (to
+//     apply the merges), where GSAP synchronises after every batch and inside
+//     every rebuild;
+//   * golden-section snapshots keep only the labels; the blockmodel of a
+//     restored point is rebuilt from them (exactly the same matrix);
+//   * merges are applied with a union-find pass over the ranked blocks, the
+//     same result as GSAP's O(B * B_to_merge) relabel loop
+//     (partition.hpp:41-56).
+#include "../../include/sbp.h"
+#include "common.cuh"
+#include "kernels.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace sbp {
+
+static thread_local std::string g_last_error;
+
+static sbp_status fail(sbp_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+sbp_status host_fail(sbp_status st, const char* msg) { return fail(st, msg); }
+
+#define SBP_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e__ = (call);                                                           \
+    if (e__ != cudaSuccess)                                                             \
+      return fail(SBP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+// ------------------------------------------------------------ validation --
+static sbp_status validate_graph(const sbp_graph_csr* g) {
+  if (!g) return fail(SBP_ERR_INVALID, "graph is NULL");
+  if (g->N < 1 || g->E < 0) return fail(SBP_ERR_INVALID, "need N >= 1 and E >= 0");
+  if (!g->out_ptr || !g->in_ptr || !g->deg_out || !g->deg_in)
+    return fail(SBP_ERR_INVALID, "graph arrays are NULL");
+  if (g->E > 0 && (!g->out_idx || !g->out_w || !g->in_idx || !g->in_w))
+    return fail(SBP_ERR_INVALID, "graph arrays are NULL");
+  const int32_t* ptrs[2] = {g->out_ptr, g->in_ptr};
+  const int32_t* idxs[2] = {g->out_idx, g->in_idx};
+  const uint32_t* ws[2] = {g->out_w, g->in_w};
+  const uint32_t* degs[2] = {g->deg_out, g->deg_in};
+  for (int d = 0; d < 2; ++d) {
+    if (ptrs[d][0] != 0 || ptrs[d][g->N] != g->E)
+      return fail(SBP_ERR_INVALID, "row pointers must start at 0 and end at E");
+    for (int32_t v = 0; v < g->N; ++v) {
+      if (ptrs[d][v + 1] < ptrs[d][v]) return fail(SBP_ERR_INVALID, "row pointers decrease");
+      uint64_t s = 0;
+      for (int32_t j = ptrs[d][v]; j < ptrs[d][v + 1]; ++j) {
+        if (idxs[d][j] < 0 || idxs[d][j] >= g->N)
+          return fail(SBP_ERR_INVALID, "vertex id out of range");
+        if (ws[d][j] == 0u) return fail(SBP_ERR_INVALID, "edge weights must be >= 1");
+        s += ws[d][j];
+      }
+      if (s != degs[d][v])
+        return fail(SBP_ERR_INVALID, "node degree differs from the sum of its edge weights");
+    }
+  }
+  return SBP_OK;
+}
+
+static sbp_status validate_part(const int32_t* part, int32_t N, int32_t B) {
+  if (!part) return fail(SBP_ERR_INVALID, "labels are NULL");
+  if (B < 1 || B > N) return fail(SBP_ERR_INVALID, "need 1 <= B <= N");
+  for (int32_t v = 0; v < N; ++v)
+    if (part[v] < 0 || part[v] >= B) return fail(SBP_ERR_INVALID, "label out of [0, B)");
+  return SBP_OK;
+}
+
+// ----------------------------------------------------------------- arena --
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, off = 0;
+  template <typename T>
+  T* take(size_t n) {
+    size_t bytes = ((n * sizeof(T)) + 255) & ~size_t(255);
+    if (off + bytes > cap) return nullptr;
+    T* p = (T*)(base + off);
+    off += bytes;
+    return p;
+  }
+};
+
+// Everything one partition job keeps in HBM.
+struct Job {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int32_t N = 0, E = 0, np = 10, max_itr = 100;
+  void* mem = nullptr;
+  size_t mem_bytes = 0;
+  DevGraph g;
+  DevBM m;
+  RebuildScratch rs;
+  int32_t *part = nullptr, *newlab = nullptr, *props = nullptr, *best = nullptr, *map = nullptr;
+  int32_t* snap[3] = {nullptr, nullptr, nullptr};
+  double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
+  double* dsum = nullptr;       // per nodal iteration: sum of recorded dS
+  double* dataS = nullptr;      // per nodal iteration: MDL data term
+  long long* acc = nullptr;     // per nodal iteration: applied moves
+  // pinned host mirrors
+  int32_t* h_best = nullptr;
+  double* h_best_dS = nullptr;
+  int32_t* h_map = nullptr;
+  double* h_scal = nullptr;     // dsum, dataS of one iteration
+  long long* h_acc = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> bev;  // per-batch timing events of one sweep
+
+  ~Job() { release(); }
+
+  void release() {
+    if (mem) {
+      int cur = 0;
+      cudaGetDevice(&cur);
+      cudaSetDevice(device);
+      if (st) cudaStreamSynchronize(st);
+      cudaFree(mem);
+      for (auto& e : ev)
+        if (e) cudaEventDestroy(e), e = nullptr;
+      for (auto& e : bev) cudaEventDestroy(e);
+      bev.clear();
+      if (st) cudaStreamDestroy(st);
+      cudaFreeHost(h_best);
+      cudaFreeHost(h_best_dS);
+      cudaFreeHost(h_map);
+      cudaFreeHost(h_scal);
+      cudaFreeHost(h_acc);
+      cudaSetDevice(cur);
+      mem = nullptr;
+      st = nullptr;
+    }
+  }
+};
+
+static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t tiles) {
+  size_t n1 = (size_t)N + 1, e = (size_t)E > 0 ? (size_t)E : 1;
+  size_t b = 0;
+  auto add = [&](size_t elems, size_t sz) { b += ((elems * sz) + 255) & ~size_t(255); };
+  // graph
+  add(n1, 4); add(n1, 4); add(e, 4); add(e, 4); add(e, 4); add(e, 4); add(e, 4); add(e, 4);
+  add(N, 4); add(N, 4);
+  // labels, snapshots, map
+  for (int i = 0; i < 6; ++i) add(n1, 4);
+  // blockmodel
+  add(n1, 4); add(n1, 4); add(e, 4); add(e, 4); add(e, 4); add(e, 4); add(N, 4); add(N, 4);
+  for (int i = 0; i < 6; ++i) add(N, 8);
+  add(N, 4); add(N, 1);
+  // rebuild scratch
+  for (int d = 0; d < 2; ++d) {
+    add(n1, 4); add(n1, 4); add(N, 4); add(e, 4); add(e, 4); add(e, 4); add(e, 4); add(n1, 4);
+    add(N, 4);
+  }
+  add(2, 4);
+  add((size_t)tiles, 4);
+  // nodal / merge
+  add(N, 8);
+  add((size_t)N * np, 4);
+  add((size_t)N * np, 8);
+  add(N, 8);
+  add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
+  return b + 4096;
+}
+
+static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np,
+                             int32_t max_itr) {
+  J.device = device;
+  J.N = N;
+  J.E = E;
+  J.np = np;
+  J.max_itr = max_itr;
+  SBP_CUDA(cudaSetDevice(device));
+  static std::once_flag once[64];
+  if (device >= 0 && device < 64) std::call_once(once[device], [] { init_kernel_attributes(); });
+  int32_t tiles = 2 * (2 * ((N + 1) / 2048 + 2) + 2);
+  J.mem_bytes = job_bytes(N, E, np, max_itr, tiles);
+  if (cudaMalloc(&J.mem, J.mem_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    J.mem = nullptr;
+    return fail(SBP_ERR_NOMEM, "device arena of " + std::to_string(J.mem_bytes) + " bytes");
+  }
+  SBP_CUDA(cudaStreamCreateWithFlags(&J.st, cudaStreamNonBlocking));
+  for (auto& e : J.ev) SBP_CUDA(cudaEventCreate(&e));
+  SBP_CUDA(cudaMallocHost(&J.h_best, sizeof(int32_t) * (size_t)N));
+  SBP_CUDA(cudaMallocHost(&J.h_best_dS, sizeof(double) * (size_t)N));
+  SBP_CUDA(cudaMallocHost(&J.h_map, sizeof(int32_t) * ((size_t)N + 1)));
+  SBP_CUDA(cudaMallocHost(&J.h_scal, sizeof(double) * 4));
+  SBP_CUDA(cudaMallocHost(&J.h_acc, sizeof(long long) * 2));
+  Arena A{(char*)J.mem, J.mem_bytes, 0};
+  size_t n1 = (size_t)N + 1, e = (size_t)E > 0 ? (size_t)E : 1;
+  DevGraph& g = J.g;
+  g.N = N;
+  g.E = E;
+  g.optr = A.take<int32_t>(n1); g.iptr = A.take<int32_t>(n1);
+  g.oidx = A.take<int32_t>(e); g.iidx = A.take<int32_t>(e);
+  g.ow = A.take<uint32_t>(e); g.iw = A.take<uint32_t>(e);
+  g.osrc = A.take<int32_t>(e); g.isrc = A.take<int32_t>(e);
+  g.kdo = A.take<uint32_t>(N); g.kdi = A.take<uint32_t>(N);
+  J.part = A.take<int32_t>(n1); J.newlab = A.take<int32_t>(n1); J.map = A.take<int32_t>(n1);
+  for (int i = 0; i < 3; ++i) J.snap[i] = A.take<int32_t>(n1);
+  DevBM& m = J.m;
+  m.optr = A.take<int32_t>(n1); m.iptr = A.take<int32_t>(n1);
+  m.ocol = A.take<int32_t>(e); m.icol = A.take<int32_t>(e);
+  m.ocnt = A.take<uint32_t>(e); m.icnt = A.take<uint32_t>(e);
+  m.d_out = A.take<uint32_t>(N); m.d_in = A.take<uint32_t>(N);
+  m.ld_out = A.take<double>(N); m.ld_in = A.take<double>(N);
+  m.dSout = A.take<double>(N); m.ambout = A.take<double>(N);
+  m.ambin = A.take<double>(N); m.sinfull = A.take<double>(N);
+  m.nbr_s = A.take<int32_t>(N); m.use_rand = A.take<uint8_t>(N);
+  for (int d = 0; d < 2; ++d) {
+    RebuildDir& r = J.rs.d[d];
+    r.cnt = A.take<int32_t>(n1); r.seg = A.take<int32_t>(n1); r.vofs = A.take<int32_t>(N);
+    r.tcol = A.take<int32_t>(e); r.tw = A.take<uint32_t>(e);
+    r.ucol = A.take<int32_t>(e); r.uw = A.take<uint32_t>(e);
+    r.uniq = A.take<int32_t>(n1); r.big = A.take<int32_t>(N);
+  }
+  J.rs.big_count = A.take<int32_t>(2);
+  J.rs.tile = A.take<int32_t>(tiles);
+  J.rs.tile_cap = tiles;
+  J.rec = A.take<double>(N);
+  J.props = A.take<int32_t>((size_t)N * np);
+  J.mdS = A.take<double>((size_t)N * np);
+  J.best = J.newlab;  // merge and nodal phases never overlap
+  J.best_dS = A.take<double>(N);
+  J.dsum = A.take<double>(max_itr);
+  J.dataS = A.take<double>(max_itr);
+  J.acc = (long long*)A.take<double>(max_itr);
+  if (!J.acc) return fail(SBP_ERR_INTERNAL, "arena sizing");
+  return SBP_OK;
+}
+
+__global__ void fill_src_kernel(const int32_t* __restrict__ ptr, int32_t N, int32_t* src) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  for (int32_t j = ptr[v]; j < ptr[v + 1]; ++j) src[j] = v;
+}
+
+__global__ void iota_kernel(int32_t* p, int32_t N) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < N) p[v] = v;
+}
+
+static sbp_status job_upload(Job& J, const sbp_graph_csr* h) {
+  DevGraph& g = J.g;
+  size_t n1 = (size_t)J.N + 1, E = (size_t)J.E;
+  cudaStream_t st = J.st;
+  SBP_CUDA(cudaMemcpyAsync(g.optr, h->out_ptr, 4 * n1, cudaMemcpyHostToDevice, st));
+  SBP_CUDA(cudaMemcpyAsync(g.iptr, h->in_ptr, 4 * n1, cudaMemcpyHostToDevice, st));
+  if (E) {
+    SBP_CUDA(cudaMemcpyAsync(g.oidx, h->out_idx, 4 * E, cudaMemcpyHostToDevice, st));
+    SBP_CUDA(cudaMemcpyAsync(g.iidx, h->in_idx, 4 * E, cudaMemcpyHostToDevice, st));
+    SBP_CUDA(cudaMemcpyAsync(g.ow, h->out_w, 4 * E, cudaMemcpyHostToDevice, st));
+    SBP_CUDA(cudaMemcpyAsync(g.iw, h->in_w, 4 * E, cudaMemcpyHostToDevice, st));
+  }
+  SBP_CUDA(cudaMemcpyAsync(g.kdo, h->deg_out, 4 * (size_t)J.N, cudaMemcpyHostToDevice, st));
+  SBP_CUDA(cudaMemcpyAsync(g.kdi, h->deg_in, 4 * (size_t)J.N, cudaMemcpyHostToDevice, st));
+  fill_src_kernel<<<(J.N + 255) / 256, 256, 0, st>>>(g.optr, J.N, g.osrc);
+  fill_src_kernel<<<(J.N + 255) / 256, 256, 0, st>>>(g.iptr, J.N, g.isrc);
+  SBP_CUDA(cudaGetLastError());
+  return SBP_OK;
+}
+
+static int resolve_device(int32_t d) {
+  if (d >= 0) return d;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  return cur;
+}
+
+// ------------------------------------------------------------ merge apply --
+// carry_out_best_merges (partition.hpp:26-78).  Blocks are ranked by their
+// best dS (ascending, ties by block id: thrust::sort_by_key's stable radix
+// sort over an id sequence, partition.hpp:442-447; NaN last); then in that
+// order each block merges into the current label of its best target unless
+// that label is itself.  Union-find gives the same labels as the reference's
+// relabel-all loop.  Surviving labels are renumbered in ascending order
+// (std::set, :58-68).  Returns the new block count.
+static int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
+                                 const double* best_dS, int32_t* map_out) {
+  std::vector<std::pair<uint64_t, int32_t>> key(B);
+  for (int32_t b = 0; b < B; ++b) {
+    double x = best_dS[b];
+    uint64_t k;
+    if (std::isnan(x)) {
+      k = ~0ull;
+    } else {
+      if (x == 0.0) x = 0.0;  // -0 ranks with +0
+      uint64_t u;
+      std::memcpy(&u, &x, 8);
+      k = (u >> 63) ? ~u : (u | (1ull << 63));
+    }
+    key[b] = {k, b};
+  }
+  std::sort(key.begin(), key.end());
+  std::vector<int32_t> parent(B);
+  std::iota(parent.begin(), parent.end(), 0);
+  auto find = [&](int32_t x) {
+    int32_t r = x;
+    while (parent[r] != r) r = parent[r];
+    while (parent[x] != r) {
+      int32_t n = parent[x];
+      parent[x] = r;
+      x = n;
+    }
+    return r;
+  };
+  int32_t merged = 0;
+  for (int32_t c = 0; c < B && merged < B_to_merge; ++c) {
+    int32_t from = key[c].second;
+    int32_t to = find(best[from]);
+    if (to != from) {
+      parent[from] = to;
+      ++merged;
+    }
+  }
+  std::vector<int32_t> rootid(B, -1);
+  int32_t next = 0;
+  for (int32_t b = 0; b < B; ++b)
+    if (find(b) == b) rootid[b] = next++;
+  for (int32_t b = 0; b < B; ++b) map_out[b] = rootid[find(b)];
+  return next;
+}
+
+static double model_S(int32_t B, int32_t N, int32_t E) {
+  // partition.hpp:696-699 (Q6)
+  double b = (double)B;
+  double x = b * b / (double)E;
+  return (double)E * (1.0 + x) * std::log(1.0 + x) - x * std::log(x) + (double)N * std::log(b);
+}
+
+struct Timer {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+        .count();
+  }
+};
+
+static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t seed, uint32_t seq,
+                             bool keep_dS) {
+  cudaStream_t st = J.st;
+  block_terms(J.m, B, 0, seed, 0, st);
+  merge_proposals(J.m, B, J.np, seed, seq, J.props, st);
+  merge_delta(J.m, B, J.np, J.props, keep_dS ? J.mdS : nullptr, J.best, J.best_dS, st);
+  SBP_CUDA(cudaMemcpyAsync(J.h_best, J.best, 4 * (size_t)B, cudaMemcpyDeviceToHost, st));
+  SBP_CUDA(cudaMemcpyAsync(J.h_best_dS, J.best_dS, 8 * (size_t)B, cudaMemcpyDeviceToHost, st));
+  SBP_CUDA(cudaStreamSynchronize(st));
+  int32_t nb = apply_merges_host(B, B_to_merge, J.h_best, J.h_best_dS, J.h_map);
+  SBP_CUDA(cudaMemcpyAsync(J.map, J.h_map, 4 * (size_t)B, cudaMemcpyHostToDevice, st));
+  relabel(J.part, J.N, J.map, st);
+  B = nb;
+  return SBP_OK;
+}
+
+struct Bracket {
+  int32_t B = 0;
+  int32_t B_to_merge = 0;
+  double S = std::numeric_limits<double>::infinity();
+  int slot = -1;  // snapshot buffer holding its labels
+};
+
+static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_out,
+                                sbp_report* rep) {
+  Timer total;
+  sbp_report R;
+  std::memset(&R, 0, sizeof(R));
+  cudaStream_t st = J.st;
+  const int32_t N = J.N, E = J.E;
+  iota_kernel<<<(N + 255) / 256, 256, 0, st>>>(J.part, N);
+  int32_t B = N;
+  int32_t B_to_merge = (int32_t)((float)B * o.reduction_rate);
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+  uint32_t seq = 0;
+  Bracket large, med, small;
+  // three snapshot buffers of labels; each bracket point owns one
+  bool optimal = false;
+  double S = 0.0;
+  int32_t BS = N / o.num_batches;
+  std::vector<double> itr_dS(o.max_nodal_itr);
+  float ms = 0.f;
+  while ((int)J.bev.size() < 2 * o.num_batches + 1) {
+    cudaEvent_t e;
+    SBP_CUDA(cudaEventCreate(&e));
+    J.bev.push_back(e);
+  }
+  while (!optimal) {
+    if (++R.outer_steps > o.max_outer) {
+      R.status = SBP_ERR_INTERNAL;
+      break;
+    }
+    // merge phase (partition.hpp:900-904)
+    SBP_CUDA(cudaEventRecord(J.ev[0], st));
+    sbp_status s = merge_step(J, B, B_to_merge, o.seed, seq++, false);
+    if (s != SBP_OK) return s;
+    SBP_CUDA(cudaEventRecord(J.ev[1], st));
+    rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+    SBP_CUDA(cudaEventRecord(J.ev[2], st));
+    // nodal phase (partition.hpp:906-935)
+    std::fill(itr_dS.begin(), itr_dS.end(), 0.0);
+    SBP_CUDA(cudaMemsetAsync(J.dsum, 0, sizeof(double) * o.max_nodal_itr, st));
+    SBP_CUDA(cudaMemsetAsync(J.acc, 0, sizeof(long long) * o.max_nodal_itr, st));
+    SBP_CUDA(cudaEventSynchronize(J.ev[2]));
+    SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[0], J.ev[1]));
+    R.ms_merge += ms;
+    SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[1], J.ev[2]));
+    R.ms_rebuild += ms;
+    for (int32_t itr = 0; itr < o.max_nodal_itr; ++itr) {
+      // events: bev[0] sweep start, bev[2b+1] after batch b's nodal kernels,
+      // bev[2b+2] after its rebuild; read at the sweep's one synchronisation
+      SBP_CUDA(cudaEventRecord(J.bev[0], st));
+      for (int32_t b = 0; b < o.num_batches; ++b) {
+        block_terms(J.m, B, 1, o.seed, seq, st);
+        nodal_batch_sample(J.g, J.part, J.m, B, o.seed, seq, b * BS, BS, J.newlab, J.rec, nullptr,
+                           st);
+        nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, st);
+        ++seq;
+        SBP_CUDA(cudaEventRecord(J.bev[2 * b + 1], st));
+        rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+        SBP_CUDA(cudaEventRecord(J.bev[2 * b + 2], st));
+        R.nodal_proposals += BS;
+      }
+      block_terms(J.m, B, 0, o.seed, 0, st);
+      mdl_data_sum(J.m, B, J.dataS + itr, st);
+      SBP_CUDA(cudaMemcpyAsync(J.h_scal, J.dsum + itr, 8, cudaMemcpyDeviceToHost, st));
+      SBP_CUDA(cudaMemcpyAsync(J.h_scal + 1, J.dataS + itr, 8, cudaMemcpyDeviceToHost, st));
+      SBP_CUDA(cudaMemcpyAsync(J.h_acc, J.acc + itr, 8, cudaMemcpyDeviceToHost, st));
+      SBP_CUDA(cudaStreamSynchronize(st));
+      SBP_CUDA(cudaGetLastError());
+      for (int32_t b = 0; b < o.num_batches; ++b) {
+        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[2 * b], J.bev[2 * b + 1]));
+        R.ms_nodal += ms;
+        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[2 * b + 1], J.bev[2 * b + 2]));
+        R.ms_rebuild += ms;
+      }
+      ++R.nodal_itrs;
+      itr_dS[itr] = J.h_scal[0];
+      R.accepted_moves += J.h_acc[0];
+      S = model_S(B, N, E) - J.h_scal[1];
+      if (itr >= o.window - 1) {
+        bool isf = std::isfinite(large.S) && std::isfinite(med.S) && std::isfinite(small.S);
+        double mean = 0.0;
+        for (int32_t i = itr - o.window + 1; i < itr; ++i) mean += itr_dS[i];
+        mean /= (double)(o.window - 1);
+        if (!isf) {
+          if (-mean < (double)o.threshold1 * S) break;
+        } else {
+          if (-mean < (double)o.threshold2 * S) break;
+        }
+      }
+    }
+    if (o.verbose)
+      std::fprintf(stderr, "[sbp] step %d B=%d S=%.6f itrs=%d\n", R.outer_steps, B, S,
+                   R.nodal_itrs);
+    // golden section (prepare_for_partition_next, partition.hpp:80-322)
+    Bracket P;
+    P.B = B;
+    P.B_to_merge = B_to_merge;
+    P.S = S;
+    auto take_slot = [&](Bracket& x) {
+      // the slot of whichever bracket point is being replaced is reused
+      bool used[3] = {false, false, false};
+      for (Bracket* q : {&large, &med, &small})
+        if (q != &x && q->slot >= 0) used[q->slot] = true;
+      for (int i = 0; i < 3; ++i)
+        if (!used[i]) return i;
+      return -1;
+    };
+    if (P.S <= med.S) {
+      if (med.B > P.B) large = med;
+      else small = med;
+      med = P;
+      med.slot = take_slot(med);
+      SBP_CUDA(cudaMemcpyAsync(J.snap[med.slot], J.part, 4 * (size_t)N, cudaMemcpyDeviceToDevice,
+                               st));
+    } else {
+      Bracket& tgt = med.B > P.B ? small : large;
+      tgt = P;
+      tgt.slot = take_slot(tgt);
+      SBP_CUDA(cudaMemcpyAsync(J.snap[tgt.slot], J.part, 4 * (size_t)N, cudaMemcpyDeviceToDevice,
+                               st));
+    }
+    const Bracket* restore = nullptr;
+    if (std::isinf(small.S)) {
+      restore = &med;
+      B_to_merge = (int32_t)((float)med.B * o.reduction_rate);
+      if (B_to_merge == 0) optimal = true;
+    } else if (large.B - small.B == 2) {
+      optimal = true;
+      restore = &med;
+    } else if ((large.B - med.B) >= (med.B - small.B)) {
+      int32_t next_B = med.B + (int32_t)std::round((large.B - med.B) * 0.618);
+      restore = &large;
+      B_to_merge = large.B - next_B;
+    } else {
+      int32_t next_B = small.B + (int32_t)std::round((med.B - small.B) * 0.618);
+      restore = &med;
+      B_to_merge = med.B - next_B;
+    }
+    if (restore->slot < 0) return fail(SBP_ERR_INTERNAL, "bracket point without a snapshot");
+    SBP_CUDA(cudaMemcpyAsync(J.part, J.snap[restore->slot], 4 * (size_t)N,
+                             cudaMemcpyDeviceToDevice, st));
+    B = restore->B;
+    S = restore->S;
+    SBP_CUDA(cudaEventRecord(J.ev[0], st));
+    rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+    SBP_CUDA(cudaEventRecord(J.ev[1], st));
+    SBP_CUDA(cudaEventSynchronize(J.ev[1]));
+    SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[0], J.ev[1]));
+    R.ms_rebuild += ms;
+  }
+  if (labels_out) {
+    SBP_CUDA(cudaMemcpyAsync(labels_out, J.part, 4 * (size_t)N, cudaMemcpyDeviceToHost, st));
+  }
+  SBP_CUDA(cudaStreamSynchronize(st));
+  SBP_CUDA(cudaGetLastError());
+  R.B = B;
+  R.S = S;
+  R.ms_total = total.ms();
+  if (rep) *rep = R;
+  return R.status == 0 ? SBP_OK : (sbp_status)R.status;
+}
+
+// A job with the graph uploaded, for the one-shot entry points.
+static sbp_status job_for(Job& J, const sbp_graph_csr* g, int device, int32_t np, int32_t max_itr) {
+  sbp_status s = validate_graph(g);
+  if (s != SBP_OK) return s;
+  s = job_create(J, resolve_device(device), g->N, g->E, np, max_itr);
+  if (s != SBP_OK) return s;
+  return job_upload(J, g);
+}
+
+static sbp_status set_part(Job& J, const int32_t* part, int32_t B) {
+  sbp_status s = validate_part(part, J.N, B);
+  if (s != SBP_OK) return s;
+  SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, J.st));
+  return SBP_OK;
+}
+
+}  // namespace sbp
+
+struct sbp_graph_dev {
+  sbp::Job job;
+  sbp_graph_csr shape;
+};
+
+using namespace sbp;
+
+extern "C" {
+
+void sbp_default_options(sbp_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->seed = 0;
+  o->num_proposals = 10;
+  o->reduction_rate = 0.35f;
+  o->max_nodal_itr = 100;
+  o->num_batches = 4;
+  o->threshold1 = 5e-4f;
+  o->threshold2 = 1e-4f;
+  o->window = 3;
+  o->max_outer = 1000;
+  o->device = -1;
+  o->use_graphs = 0;
+  o->verbose = 0;
+}
+
+const char* sbp_status_string(sbp_status s) {
+  switch (s) {
+    case SBP_OK: return "ok";
+    case SBP_ERR_INVALID: return "invalid argument";
+    case SBP_ERR_CUDA: return "CUDA error";
+    case SBP_ERR_NOMEM: return "out of memory";
+    case SBP_ERR_BUDGET: return "HBM budget exceeded";
+    case SBP_ERR_TIMEOUT: return "timed out";
+    case SBP_ERR_INTERNAL: return "internal error";
+    case SBP_ERR_BUSY: return "busy";
+    case SBP_ERR_NOT_FOUND: return "not found";
+    case SBP_ERR_CANCELLED: return "cancelled";
+  }
+  return "unknown status";
+}
+
+const char* sbp_last_error(void) { return g_last_error.c_str(); }
+
+static sbp_status check_options(const sbp_options* o) {
+  if (!o) return fail(SBP_ERR_INVALID, "options are NULL");
+  if (o->num_proposals < 1 || o->num_proposals > 32)
+    return fail(SBP_ERR_INVALID, "num_proposals must be in [1, 32]");
+  if (o->num_batches < 1 || o->max_nodal_itr < 1 || o->window < 2 || o->max_outer < 1)
+    return fail(SBP_ERR_INVALID, "bad loop options");
+  if (!(o->reduction_rate > 0.f && o->reduction_rate < 1.f))
+    return fail(SBP_ERR_INVALID, "reduction_rate must be in (0, 1)");
+  return SBP_OK;
+}
+
+sbp_status sbp_graph_upload(const sbp_graph_csr* g, int32_t device, sbp_graph_dev** out) {
+  if (!out) return fail(SBP_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  sbp_graph_dev* h = new (std::nothrow) sbp_graph_dev();
+  if (!h) return fail(SBP_ERR_NOMEM, "host allocation");
+  sbp_status s = job_for(h->job, g, device, 10, 100);
+  if (s != SBP_OK) {
+    delete h;
+    return s;
+  }
+  h->shape = *g;
+  cudaError_t e = cudaStreamSynchronize(h->job.st);
+  if (e != cudaSuccess) {
+    delete h;
+    return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
+  }
+  *out = h;
+  return SBP_OK;
+}
+
+sbp_status sbp_graph_release(sbp_graph_dev* g) {
+  delete g;
+  return SBP_OK;
+}
+
+sbp_status sbp_partition_resident(sbp_graph_dev* gd, const sbp_options* o, int32_t* labels_out,
+                                  sbp_report* report) {
+  if (!gd) return fail(SBP_ERR_INVALID, "graph handle is NULL");
+  sbp_status s = check_options(o);
+  if (s != SBP_OK) return s;
+  Job& J = gd->job;
+  if (o->num_proposals > J.np || o->max_nodal_itr > J.max_itr) {
+    // grow the job's arena for these options; the graph is uploaded again
+    int dev = J.device;
+    J.release();
+    J.bev.clear();
+    s = job_for(J, &gd->shape, dev, std::max(o->num_proposals, J.np),
+                std::max(o->max_nodal_itr, J.max_itr));
+    if (s != SBP_OK) return s;
+  }
+  SBP_CUDA(cudaSetDevice(J.device));
+  return run_partition(J, *o, labels_out, report);
+}
+
+sbp_status sbp_partition(const sbp_graph_csr* g, const sbp_options* o, int32_t* labels_out,
+                         sbp_report* report) {
+  sbp_status s = check_options(o);
+  if (s != SBP_OK) return s;
+  Timer t;
+  Job J;
+  s = job_for(J, g, o->device, o->num_proposals, o->max_nodal_itr);
+  if (s != SBP_OK) return s;
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  double up = t.ms();
+  s = run_partition(J, *o, labels_out, report);
+  if (report) {
+    report->ms_h2d = up;
+    report->ms_total += up;
+  }
+  return s;
+}
+
+sbp_status sbp_build_blockmodel(const sbp_graph_csr* g, const int32_t* part, int32_t B,
+                                int32_t* out_ptr, int32_t* out_col, uint32_t* out_cnt,
+                                int32_t* in_ptr, int32_t* in_col, uint32_t* in_cnt,
+                                uint32_t* d_out, uint32_t* d_in, int64_t* nnz) {
+  Job J;
+  sbp_status s = job_for(J, g, -1, 1, 1);
+  if (s != SBP_OK) return s;
+  s = set_part(J, part, B);
+  if (s != SBP_OK) return s;
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  int32_t n = 0;
+  SBP_CUDA(cudaMemcpyAsync(&n, J.m.optr + B, 4, cudaMemcpyDeviceToHost, J.st));
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  SBP_CUDA(cudaGetLastError());
+  size_t b1 = (size_t)B + 1;
+  if (out_ptr) SBP_CUDA(cudaMemcpy(out_ptr, J.m.optr, 4 * b1, cudaMemcpyDeviceToHost));
+  if (in_ptr) SBP_CUDA(cudaMemcpy(in_ptr, J.m.iptr, 4 * b1, cudaMemcpyDeviceToHost));
+  if (n > 0) {
+    if (out_col) SBP_CUDA(cudaMemcpy(out_col, J.m.ocol, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+    if (out_cnt) SBP_CUDA(cudaMemcpy(out_cnt, J.m.ocnt, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+    if (in_col) SBP_CUDA(cudaMemcpy(in_col, J.m.icol, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+    if (in_cnt) SBP_CUDA(cudaMemcpy(in_cnt, J.m.icnt, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+  }
+  if (d_out) SBP_CUDA(cudaMemcpy(d_out, J.m.d_out, 4 * (size_t)B, cudaMemcpyDeviceToHost));
+  if (d_in) SBP_CUDA(cudaMemcpy(d_in, J.m.d_in, 4 * (size_t)B, cudaMemcpyDeviceToHost));
+  if (nnz) *nnz = n;
+  return SBP_OK;
+}
+
+sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t nv,
+                               const int32_t* verts, const int32_t* props, double* dS) {
+  if (nv < 0 || (nv > 0 && (!verts || !props || !dS)))
+    return fail(SBP_ERR_INVALID, "bad vertex/proposal arrays");
+  for (int32_t i = 0; i < nv; ++i) {
+    if (verts[i] < 0 || verts[i] >= g->N) return fail(SBP_ERR_INVALID, "vertex out of range");
+    if (props[i] < 0 || props[i] >= B) return fail(SBP_ERR_INVALID, "proposal out of [0, B)");
+  }
+  Job J;
+  sbp_status s = job_for(J, g, -1, 1, 1);
+  if (s != SBP_OK) return s;
+  s = set_part(J, part, B);
+  if (s != SBP_OK) return s;
+  int32_t *dv = nullptr, *dp = nullptr;
+  double* dd = nullptr;
+  size_t n = (size_t)(nv > 0 ? nv : 1);
+  SBP_CUDA(cudaMalloc(&dv, 4 * n));
+  SBP_CUDA(cudaMalloc(&dp, 4 * n));
+  SBP_CUDA(cudaMalloc(&dd, 8 * n));
+  cudaMemcpyAsync(dv, verts, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
+  cudaMemcpyAsync(dp, props, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  block_terms(J.m, B, 0, 0, 0, J.st);
+  nodal_delta_given(J.g, J.part, J.m, B, nv, dv, dp, dd, J.st);
+  cudaMemcpyAsync(dS, dd, 8 * (size_t)nv, cudaMemcpyDeviceToHost, J.st);
+  cudaError_t e = cudaStreamSynchronize(J.st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaFree(dv);
+  cudaFree(dp);
+  cudaFree(dd);
+  if (e != cudaSuccess) return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
+  return SBP_OK;
+}
+
+sbp_status sbp_delta_mdl_merge(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
+                               const int32_t* props, double* dS, int32_t* best, double* best_dS) {
+  if (np < 1 || np > 32 || !props) return fail(SBP_ERR_INVALID, "bad proposals");
+  for (int64_t t = 0; t < (int64_t)B * np; ++t)
+    if (props[t] < 0 || props[t] >= B) return fail(SBP_ERR_INVALID, "proposal out of [0, B)");
+  Job J;
+  sbp_status s = job_for(J, g, -1, np, 1);
+  if (s != SBP_OK) return s;
+  s = set_part(J, part, B);
+  if (s != SBP_OK) return s;
+  size_t nt = (size_t)B * np;
+  SBP_CUDA(cudaMemcpyAsync(J.props, props, 4 * nt, cudaMemcpyHostToDevice, J.st));
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  block_terms(J.m, B, 0, 0, 0, J.st);
+  merge_delta(J.m, B, np, J.props, J.mdS, J.best, J.best_dS, J.st);
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  SBP_CUDA(cudaGetLastError());
+  if (dS) SBP_CUDA(cudaMemcpy(dS, J.mdS, 8 * nt, cudaMemcpyDeviceToHost));
+  if (best) SBP_CUDA(cudaMemcpy(best, J.best, 4 * (size_t)B, cudaMemcpyDeviceToHost));
+  if (best_dS) SBP_CUDA(cudaMemcpy(best_dS, J.best_dS, 8 * (size_t)B, cudaMemcpyDeviceToHost));
+  return SBP_OK;
+}
+
+sbp_status sbp_merge_proposals(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
+                               uint64_t seed, uint32_t seq, int32_t* props) {
+  if (np < 1 || np > 32 || !props) return fail(SBP_ERR_INVALID, "bad proposal buffer");
+  Job J;
+  sbp_status s = job_for(J, g, -1, np, 1);
+  if (s != SBP_OK) return s;
+  s = set_part(J, part, B);
+  if (s != SBP_OK) return s;
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  merge_proposals(J.m, B, np, seed, seq, J.props, J.st);
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  SBP_CUDA(cudaGetLastError());
+  SBP_CUDA(cudaMemcpy(props, J.props, 4 * (size_t)B * np, cudaMemcpyDeviceToHost));
+  return SBP_OK;
+}
+
+sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
+                           uint32_t seq, int32_t lo, int32_t hi, double* dS_rec, int32_t* props,
+                           double* sum) {
+  if (!g || lo < 0 || hi < lo || hi > g->N) return fail(SBP_ERR_INVALID, "bad batch range");
+  Job J;
+  sbp_status s = job_for(J, g, -1, 1, 1);
+  if (s != SBP_OK) return s;
+  s = set_part(J, part, B);
+  if (s != SBP_OK) return s;
+  int32_t cnt = hi - lo;
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  block_terms(J.m, B, 1, seed, seq, J.st);
+  SBP_CUDA(cudaMemsetAsync(J.dsum, 0, 8, J.st));
+  SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8, J.st));
+  nodal_batch_sample(J.g, J.part, J.m, B, seed, seq, lo, cnt, J.newlab, J.rec, J.props, J.st);
+  nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, J.st);
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  SBP_CUDA(cudaGetLastError());
+  SBP_CUDA(cudaMemcpy(part, J.part, 4 * (size_t)J.N, cudaMemcpyDeviceToHost));
+  if (dS_rec && cnt) SBP_CUDA(cudaMemcpy(dS_rec, J.rec, 8 * (size_t)cnt, cudaMemcpyDeviceToHost));
+  if (props && cnt) SBP_CUDA(cudaMemcpy(props, J.props, 4 * (size_t)cnt, cudaMemcpyDeviceToHost));
+  if (sum) SBP_CUDA(cudaMemcpy(sum, J.dsum, 8, cudaMemcpyDeviceToHost));
+  return SBP_OK;
+}
+
+sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int32_t B_to_merge,
+                          int32_t np, uint64_t seed, uint32_t seq, int32_t* best, double* best_dS,
+                          int32_t* B_new) {
+  if (np < 1 || np > 32) return fail(SBP_ERR_INVALID, "bad np");
+  Job J;
+  sbp_status s = job_for(J, g, -1, np, 1);
+  if (s != SBP_OK) return s;
+  s = set_part(J, part, B);
+  if (s != SBP_OK) return s;
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  int32_t b = B;
+  s = merge_step(J, b, B_to_merge, seed, seq, false);
+  if (s != SBP_OK) return s;
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  if (best) std::memcpy(best, J.h_best, 4 * (size_t)B);
+  if (best_dS) std::memcpy(best_dS, J.h_best_dS, 8 * (size_t)B);
+  SBP_CUDA(cudaMemcpy(part, J.part, 4 * (size_t)J.N, cudaMemcpyDeviceToHost));
+  if (B_new) *B_new = b;
+  return SBP_OK;
+}
+
+sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, double* S,
+                   double* data_S) {
+  Job J;
+  sbp_status s = job_for(J, g, -1, 1, 1);
+  if (s != SBP_OK) return s;
+  s = set_part(J, part, B);
+  if (s != SBP_OK) return s;
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  block_terms(J.m, B, 0, 0, 0, J.st);
+  mdl_data_sum(J.m, B, J.dataS, J.st);
+  double ds = 0.0;
+  SBP_CUDA(cudaMemcpyAsync(&ds, J.dataS, 8, cudaMemcpyDeviceToHost, J.st));
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  SBP_CUDA(cudaGetLastError());
+  if (data_S) *data_S = ds;
+  if (S) *S = model_S(B, g->N, g->E) - ds;
+  return SBP_OK;
+}
+
+}  // extern "C"

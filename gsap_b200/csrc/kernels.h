@@ -1,0 +1,91 @@
+// Host-side declarations of the partitioner's kernels and the device state
+// they work on.  All launches go to one stream; nothing here synchronises.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sbp {
+
+// The graph in HBM (uploaded once per job).
+struct DevGraph {
+  int32_t N = 0, E = 0;
+  int32_t *optr = nullptr, *oidx = nullptr, *iptr = nullptr, *iidx = nullptr;
+  uint32_t *ow = nullptr, *iw = nullptr, *kdo = nullptr, *kdi = nullptr;
+  int32_t *osrc = nullptr, *isrc = nullptr;  // owning vertex of each CSR entry
+};
+
+// Blockmodel M (out CSR rows = source block, in CSR rows = destination
+// block), weighted block degrees and their log2, and the per-block sums the
+// dS kernels start from.  Capacities: rows N+1, entries E.
+struct DevBM {
+  int32_t *optr = nullptr, *ocol = nullptr, *iptr = nullptr, *icol = nullptr;
+  uint32_t *ocnt = nullptr, *icnt = nullptr, *d_out = nullptr, *d_in = nullptr;
+  double *ld_out = nullptr, *ld_in = nullptr;
+  double *dSout = nullptr;    // sum over out-row b of M (log2 M - log2 d_out[b] - log2 d_in[c])
+  double *ambout = nullptr;   // sum over out-row b of M log2 M - M log2 d_in[c]
+  double *ambin = nullptr;    // sum over in-row b of M log2 M - M log2 d_out[c]
+  double *sinfull = nullptr;  // ambin[b] - d_in[b] log2 d_in[b]
+  int32_t* nbr_s = nullptr;   // per-block second-hop sample of a nodal batch
+  uint8_t* use_rand = nullptr;
+};
+
+// Scratch of one rebuild direction.
+struct RebuildDir {
+  int32_t *cnt = nullptr, *seg = nullptr, *vofs = nullptr, *tcol = nullptr, *uniq = nullptr;
+  uint32_t* tw = nullptr;
+  int32_t* ucol = nullptr;
+  uint32_t* uw = nullptr;
+  int32_t* big = nullptr;
+};
+
+struct RebuildScratch {
+  RebuildDir d[2];
+  int32_t* big_count = nullptr;  // 2 ints
+  int32_t* tile = nullptr;       // scan tile sums (capacity >= 2 * tiles)
+  int32_t tile_cap = 0;
+};
+
+// Opt-in shared-memory sizes; call once per device before the first launch.
+cudaError_t init_kernel_attributes();
+
+// Exclusive scan of n int32 counts into out[0..n] (out[n] = total).
+void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, cudaStream_t st);
+
+// calculate_new_csr (partition.hpp:707-849): rebuild M from the labels.
+void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
+                        RebuildScratch& rs, cudaStream_t st);
+
+// Per-block sums (dSout, ambout, ambin, sinfull).  With draws != 0, also the
+// per-block draws of nodal batch `seq` (choose_neighbored_block and the
+// per-block uniform, kernels.hpp:942-997, 1024).
+void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cudaStream_t st);
+
+// data_S = sum of dSout over blocks, written to *out (deterministic order).
+void mdl_data_sum(const DevBM& m, int32_t B, double* out, cudaStream_t st);
+
+// Nodal batch of vertices [lo, lo+count): proposal, dS, accept flag.
+// newlab[i] = new label of vertex lo+i, rec[i] = recorded dS (0 if rejected),
+// props[i] (optional) = proposal.
+void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
+                        uint64_t seed, uint32_t seq, int32_t lo, int32_t count, int32_t* newlab,
+                        double* rec, int32_t* props, cudaStream_t st);
+// dS of given (vertex, proposal) pairs, no accept.
+void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
+                       int32_t nv, const int32_t* verts, const int32_t* props, double* dS,
+                       cudaStream_t st);
+// Apply a batch: part[lo+i] = newlab[i]; slot_sum[0] += sum(rec) in a fixed
+// order, slot_acc[0] += number of moves.
+void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
+                  const double* rec, double* slot_sum, long long* slot_acc, cudaStream_t st);
+
+// Merge proposals (kernels.hpp:726-856) and their dS with the per-block best
+// (kernels.hpp:143-491).
+void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
+                     int32_t* props, cudaStream_t st);
+void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
+                 int32_t* best, double* best_dS, cudaStream_t st);
+// part[v] = map[part[v]] (update_partitions, kernels.hpp:1728-1740).
+void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st);
+
+}  // namespace sbp

@@ -1,0 +1,236 @@
+// Merge phase: proposals, merge dS and the best proposal of each block.
+//
+// GSAP draws proposals with three curand kernels and a float running-sum
+// scan (kernels.hpp:645-856), computes dS with four kernels that each walk
+// whole rows per proposal thread (kernels.hpp:143-449, grid sized from nnz,
+// Q16) and reduces with find_best_warp (kernels.hpp:452-491).
+//
+// Here: one thread per proposal draws it (Philox, exact integer picks); one
+// warp per block computes its proposals' dS, walking only the shorter of the
+// two rows being merged and looking the other up by binary search, with the
+// unchanged remainder taken from the per-block sums; lanes 0..np-1 then hold
+// the proposals' dS and run the same 32-lane halving argmin as
+// find_best_warp, ties going to the lane further up.  FP64 throughout.
+#include "common.cuh"
+#include "kernels.h"
+
+#include <cfloat>
+
+namespace sbp {
+
+namespace {
+
+struct MergeArgs {
+  const int32_t *optr, *ocol, *iptr, *icol;
+  const uint32_t *ocnt, *icnt, *d_out, *d_in;
+  const double *ld_out, *ld_in, *dSout, *ambout, *ambin, *sinfull;
+  int32_t B, np;
+  uint64_t seed;
+  uint32_t seq;
+  const int32_t* props_in;
+  int32_t* props;
+  double* dS;
+  int32_t* best;
+  double* best_dS;
+};
+
+// First index k of out-row ++ in-row of block b with running count > t.
+__device__ int pick_serial(const MergeArgs& a, int b, uint64_t t) {
+  uint64_t acc = 0;
+  int o0 = a.optr[b], o1 = a.optr[b + 1];
+  for (int i = o0; i < o1; ++i) {
+    acc += a.ocnt[i];
+    if (acc > t) return i - o0;
+  }
+  int i0 = a.iptr[b], i1 = a.iptr[b + 1];
+  for (int i = i0; i < i1; ++i) {
+    acc += a.icnt[i];
+    if (acc > t) return (o1 - o0) + (i - i0);
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int col_at(const MergeArgs& a, int b, int k) {
+  int o0 = a.optr[b], no = a.optr[b + 1] - o0;
+  return k < no ? a.ocol[o0 + k] : a.icol[a.iptr[b] + k - no];
+}
+
+// choose_neighbors + propose_blocks (kernels.hpp:726-856) for one proposal.
+__global__ void merge_props_kernel(MergeArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)a.B * a.np) return;
+  int r = (int)(t / a.np);
+  P4 x = draw(a.seed, kRngMerge, a.seq, (uint32_t)t);
+  uint32_t B = (uint32_t)a.B;
+  int rnd = (int)(x.v[0] % B);
+  uint64_t deg_r = (uint64_t)a.d_out[r] + a.d_in[r];
+  int s;
+  if (deg_r == 0) {
+    s = rnd;
+  } else {
+    int k = pick_serial(a, r, scale_draw(x.v[1], deg_r));
+    int u = k >= 0 ? col_at(a, r, k) : 0;
+    uint64_t deg_u = (uint64_t)a.d_out[u] + a.d_in[u];
+    if (accept_random(x.v[2], deg_u, B)) {
+      s = rnd;
+    } else {
+      s = 0;
+      int k2 = pick_serial(a, u, scale_draw(x.v[3], deg_u));
+      int n = (a.optr[u + 1] - a.optr[u]) + (a.iptr[u + 1] - a.iptr[u]);
+      for (; k2 >= 0 && k2 < n; ++k2) {
+        int c = col_at(a, u, k2);
+        if (c != r) { s = c; break; }
+      }
+    }
+  }
+  a.props[t] = s;
+}
+
+__device__ __forceinline__ double gterm(uint32_t x, double ld) {
+  return x == 0u ? 0.0 : (double)x * log2((double)x) - (double)x * ld;
+}
+__device__ __forceinline__ double fterm(uint32_t m, double a, double b) {
+  return m == 0u ? 0.0 : (double)m * (log2((double)m) - (a + b));
+}
+
+// Merge dS of block r with s (calculate_dS_overall, kernels.hpp:417-449),
+// s2 = the k-th proposal of block s (its in-term leaves out s2, Q1).
+__device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) {
+  // merged out-rows (calculate_dS_new_out, kernels.hpp:233-320)
+  double acc_o = 0.0, acc_i = 0.0;
+  const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s], ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
+  const uint32_t Mrr = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], r);
+  const uint32_t Mrs = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], s);
+  const uint32_t Msr = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], r);
+  const uint32_t Mss = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], s);
+  if (r == s) {
+    for (int i = a.optr[r] + lane; i < a.optr[r + 1]; i += 32)
+      acc_o += gterm(2u * a.ocnt[i], a.ld_in[a.ocol[i]]);
+    for (int i = a.iptr[r] + lane; i < a.iptr[r + 1]; i += 32) {
+      int c = a.icol[i];
+      if (c != r) acc_i += gterm(2u * a.icnt[i], a.ld_out[c]);
+    }
+  } else {
+    int x = r, y = s;
+    if (a.optr[s + 1] - a.optr[s] < a.optr[r + 1] - a.optr[r]) { x = s; y = r; }
+    int y0 = a.optr[y], y1 = a.optr[y + 1];
+    for (int i = a.optr[x] + lane; i < a.optr[x + 1]; i += 32) {
+      int c = a.ocol[i];
+      double ld = a.ld_in[c];
+      uint32_t my = row_lookup(a.ocol, a.ocnt, y0, y1, c);
+      acc_o += gterm(a.ocnt[i] + my, ld) - gterm(my, ld);
+    }
+    if (lane == 0) acc_o += a.ambout[y];
+    x = r; y = s;
+    if (a.iptr[s + 1] - a.iptr[s] < a.iptr[r + 1] - a.iptr[r]) { x = s; y = r; }
+    y0 = a.iptr[y]; y1 = a.iptr[y + 1];
+    for (int i = a.iptr[x] + lane; i < a.iptr[x + 1]; i += 32) {
+      int c = a.icol[i];
+      if (c == r || c == s) continue;
+      double ld = a.ld_out[c];
+      uint32_t my = row_lookup(a.icol, a.icnt, y0, y1, c);
+      acc_i += gterm(a.icnt[i] + my, ld) - gterm(my, ld);
+    }
+    if (lane == 0) {
+      // in-row y's own terms at columns r and s stay out
+      uint32_t yr = y == r ? Mrr : Mrs;  // M[r][y]
+      uint32_t ys = y == r ? Msr : Mss;  // M[s][y]
+      acc_i += a.ambin[y] - gterm(yr, ldo_r) - gterm(ys, ldo_s);
+    }
+  }
+  acc_o = warp_sum(acc_o);
+  acc_i = warp_sum(acc_i);
+  const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
+  long long mass_o = (long long)dor + (long long)dos;
+  long long mass_i = r == s ? 2LL * ((long long)dir - (long long)Mrr)
+                            : (long long)dir + (long long)dis - (long long)Mrr - (long long)Msr -
+                                  (long long)Mrs - (long long)Mss;
+  double new_out = -acc_o;
+  if (mass_o != 0) new_out += log2((double)(uint32_t)(dos + dor)) * (double)mass_o;
+  double new_in = -acc_i;
+  if (mass_i != 0) new_in += log2((double)(uint32_t)(dis + dir)) * (double)mass_i;
+  // old in-rows (calculate_dS_in, kernels.hpp:185-231): row r without r, s;
+  // row s without s, s2
+  double in_r = a.sinfull[r] - fterm(Mrr, ldo_r, ldi_r) - (s != r ? fterm(Msr, ldo_s, ldi_r) : 0.0);
+  uint32_t Ms2s = s2 == s ? 0u : row_lookup(a.ocol, a.ocnt, a.optr[s2], a.optr[s2 + 1], s);
+  double in_s = a.sinfull[s] - fterm(Mss, ldo_s, ldi_s) - fterm(Ms2s, a.ld_out[s2], ldi_s);
+  return a.dSout[r] + a.dSout[s] + in_r + in_s + new_out + new_in;
+}
+
+constexpr int kMergeWarps = 8;
+
+__global__ void __launch_bounds__(kMergeWarps * 32) merge_delta_kernel(MergeArgs a) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int r = blockIdx.x * kMergeWarps + wid; r < a.B; r += gridDim.x * kMergeWarps) {
+    double mine = DBL_MAX;
+    int who = 0;
+    for (int k = 0; k < a.np; ++k) {
+      int s = a.props_in[(long long)r * a.np + k];
+      int s2 = a.props_in[(long long)s * a.np + k];
+      double d = merge_one(a, r, s, s2, lane);
+      if (lane == k) {
+        mine = d;
+        who = s;
+      }
+      if (lane == 0 && a.dS) a.dS[(long long)r * a.np + k] = d;
+    }
+    // find_best_warp's reduction
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_down_sync(kFull, mine, o);
+      int ow = __shfl_down_sync(kFull, who, o);
+      mine = fmin(mine, ov);
+      if (mine == ov) who = ow;
+    }
+    if (lane == 0) {
+      a.best[r] = who;
+      a.best_dS[r] = mine;
+    }
+  }
+}
+
+__global__ void relabel_kernel(int32_t* part, int32_t N, const int32_t* __restrict__ map) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < N) part[v] = map[part[v]];
+}
+
+MergeArgs make_args(const DevBM& m, int32_t B, int32_t np) {
+  MergeArgs a{};
+  a.optr = m.optr; a.ocol = m.ocol; a.iptr = m.iptr; a.icol = m.icol;
+  a.ocnt = m.ocnt; a.icnt = m.icnt; a.d_out = m.d_out; a.d_in = m.d_in;
+  a.ld_out = m.ld_out; a.ld_in = m.ld_in; a.dSout = m.dSout; a.ambout = m.ambout;
+  a.ambin = m.ambin; a.sinfull = m.sinfull;
+  a.B = B;
+  a.np = np;
+  return a;
+}
+
+}  // namespace
+
+void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
+                     int32_t* props, cudaStream_t st) {
+  MergeArgs a = make_args(m, B, np);
+  a.seed = seed;
+  a.seq = seq;
+  a.props = props;
+  long long n = (long long)B * np;
+  if (n > 0) merge_props_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(a);
+}
+
+void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
+                 int32_t* best, double* best_dS, cudaStream_t st) {
+  MergeArgs a = make_args(m, B, np);
+  a.props_in = props;
+  a.dS = dS;
+  a.best = best;
+  a.best_dS = best_dS;
+  int g = (B + kMergeWarps - 1) / kMergeWarps;
+  if (g > 148 * 32) g = 148 * 32;
+  if (B > 0) merge_delta_kernel<<<g, kMergeWarps * 32, 0, st>>>(a);
+}
+
+void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st) {
+  if (N > 0) relabel_kernel<<<(N + 255) / 256, 256, 0, st>>>(part, N, map);
+}
+
+}  // namespace sbp

@@ -1,0 +1,211 @@
+/*
+ * sbp.h - C ABI of the B200-native stochastic block partitioner.
+ *
+ * This is the drop-in boundary for the SBP path of GSAP
+ * (chih-chun-chang/GSAP).  GSAP's entry point is the header template
+ *     template <typename T, typename V, typename W>
+ *     void partition(Graph<T, V, W>& g);          // GSAP/partition.hpp:852-954
+ * instantiated with <int, int, unsigned> (GSAP.cu:20,25).  include/partition.hpp
+ * keeps that template and forwards to sbp_partition() below.  Everything
+ * crosses this boundary as plain pointers and sizes.
+ *
+ * Graph convention: CSR with an N+1 entry row pointer (GSAP keeps N entries
+ * and uses adj_node.size() as the end of the last row, load.hpp:96-116),
+ * int32 vertex ids, uint32 edge weights >= 1, node degrees = weighted sums
+ * (load.hpp:106,112).  Labels are int32 in [0, B).
+ *
+ * Errors: every call returns an sbp_status; sbp_last_error() gives a message
+ * for the calling thread.  No call aborts the process.  (GSAP returns void
+ * and ignores CUDA errors, partition.hpp:852.)
+ */
+#ifndef SBP_H
+#define SBP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum sbp_status {
+  SBP_OK = 0,
+  SBP_ERR_INVALID = 1,   /* malformed input or option */
+  SBP_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  SBP_ERR_NOMEM = 3,     /* device or host allocation failed */
+  SBP_ERR_BUDGET = 4,    /* the HBM budget of a server/batch is exceeded */
+  SBP_ERR_TIMEOUT = 5,   /* a bounded device wait or a job deadline ran out */
+  SBP_ERR_INTERNAL = 6,  /* an internal consistency check failed */
+  SBP_ERR_BUSY = 7,      /* queue full / job still running */
+  SBP_ERR_NOT_FOUND = 8, /* unknown job id */
+  SBP_ERR_CANCELLED = 9  /* the job was cancelled */
+} sbp_status;
+
+/* A directed weighted graph in CSR, both directions (GSAP/graph.hpp:32-45). */
+typedef struct sbp_graph_csr {
+  int32_t N;                /* vertices */
+  int32_t E;                /* edges (entries of each CSR) */
+  const int32_t* out_ptr;   /* N+1 */
+  const int32_t* out_idx;   /* E: destination of each out-edge */
+  const uint32_t* out_w;    /* E */
+  const int32_t* in_ptr;    /* N+1 */
+  const int32_t* in_idx;    /* E: source of each in-edge */
+  const uint32_t* in_w;     /* E */
+  const uint32_t* deg_out;  /* N: weighted out-degree (node_deg_out) */
+  const uint32_t* deg_in;   /* N: weighted in-degree (node_deg_in) */
+} sbp_graph_csr;
+
+/* Hyper-parameters of partition.hpp:855-861 plus what the reference fixes
+ * implicitly (RNG seed, device). */
+typedef struct sbp_options {
+  uint64_t seed;           /* Philox key; the reference seeds curand with clock64() */
+  int32_t num_proposals;   /* merge proposals per block, 10 (:855) */
+  float reduction_rate;    /* 0.35 (:856) */
+  int32_t max_nodal_itr;   /* 100 (:857) */
+  int32_t num_batches;     /* Jacobi batches per nodal sweep, 4 (:858) */
+  float threshold1;        /* 5e-4, bracket incomplete (:859) */
+  float threshold2;        /* 1e-4, bracket complete (:860) */
+  int32_t window;          /* moving-average window, 3 (:861) */
+  int32_t max_outer;       /* cap on merge/golden-section steps (no reference counterpart) */
+  int32_t device;          /* CUDA device ordinal, -1 = current device */
+  int32_t use_graphs;      /* capture each nodal sweep in a CUDA graph */
+  int32_t verbose;         /* 1: one line per outer step on stderr */
+} sbp_options;
+
+/* What one partition run did.  Timings are CUDA-event milliseconds on the
+ * run's stream except ms_total (host steady clock around the whole call). */
+typedef struct sbp_report {
+  int32_t B;                /* final number of blocks */
+  double S;                 /* final MDL (partition.hpp:696-701, FP64) */
+  int32_t outer_steps;      /* merge + golden-section steps */
+  int32_t nodal_itrs;       /* nodal sweeps (each = num_batches batches) */
+  int64_t nodal_proposals;  /* vertex moves evaluated */
+  int64_t accepted_moves;   /* vertex moves applied */
+  double ms_total;
+  double ms_merge;          /* proposals, merge dS, merge application */
+  double ms_nodal;          /* nodal batches (proposal, dS, accept) */
+  double ms_rebuild;        /* blockmodel rebuilds and per-block terms */
+  double ms_h2d;            /* graph upload (sbp_partition only) */
+  double bytes_nodal;       /* algorithmic bytes, per the roofline model */
+  double bytes_rebuild;
+  double bytes_merge;
+  int32_t status;
+} sbp_report;
+
+void sbp_default_options(sbp_options* o);
+const char* sbp_status_string(sbp_status s);
+const char* sbp_last_error(void);
+
+/* ---------------------------------------------------------------- partition
+ * Replaces partition(g) (GSAP/partition.hpp:852-954): host graph in, host
+ * labels out (N int32).  Uploads the graph, runs the merge / nodal /
+ * golden-section loop on the GPU, downloads the labels. */
+sbp_status sbp_partition(const sbp_graph_csr* g, const sbp_options* o, int32_t* labels_out,
+                         sbp_report* report);
+
+/* The same with the graph already resident in HBM (allocate_device.hpp:
+ * 184-191 does this upload inside every partition call). */
+typedef struct sbp_graph_dev sbp_graph_dev;
+sbp_status sbp_graph_upload(const sbp_graph_csr* g, int32_t device, sbp_graph_dev** out);
+sbp_status sbp_graph_release(sbp_graph_dev* g);
+sbp_status sbp_partition_resident(sbp_graph_dev* g, const sbp_options* o, int32_t* labels_out,
+                                  sbp_report* report);
+
+/* ---------------------------------------------------- path pieces (parity)
+ * Each runs one phase of the loop on the GPU from host inputs. */
+
+/* calculate_new_csr (partition.hpp:707-849): the blockmodel of `part` as an
+ * out CSR (rows = source block) and an in CSR (rows = destination block),
+ * ascending columns, uint32 counts, and the weighted block degrees.  Row
+ * pointers have B+1 entries; column/count arrays need capacity E.  *nnz
+ * receives the number of nonzeros. */
+sbp_status sbp_build_blockmodel(const sbp_graph_csr* g, const int32_t* part, int32_t B,
+                                int32_t* out_ptr, int32_t* out_col, uint32_t* out_cnt,
+                                int32_t* in_ptr, int32_t* in_col, uint32_t* in_cnt,
+                                uint32_t* d_out, uint32_t* d_in, int64_t* nnz);
+
+/* dS of moving verts[i] to props[i] (kernels.hpp:494-643, 1153-1726), every
+ * move judged against the same `part` (one Jacobi batch without the accept). */
+sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t nv,
+                               const int32_t* verts, const int32_t* props, double* dS);
+
+/* Merge dS of B*np proposals (props[r*np+k] = target of block r's k-th
+ * proposal; kernels.hpp:143-449) and each block's best proposal and its dS
+ * (find_best_warp, kernels.hpp:452-491). */
+sbp_status sbp_delta_mdl_merge(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
+                               const int32_t* props, double* dS, int32_t* best, double* best_dS);
+
+/* Merge proposals (kernels.hpp:726-856) from the Philox stream (seed, seq). */
+sbp_status sbp_merge_proposals(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
+                               uint64_t seed, uint32_t seq, int32_t* props);
+
+/* One nodal batch over vertices [lo, hi) (propose_nodal_move,
+ * partition.hpp:456-662): proposals from the Philox stream (seed, seq), dS,
+ * accept if dS < 0, labels updated in place.  dS_rec[i] is the recorded dS
+ * (0 when rejected), props[i] the proposal; *sum = sum of dS_rec. */
+sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
+                           uint32_t seq, int32_t lo, int32_t hi, double* dS_rec, int32_t* props,
+                           double* sum);
+
+/* One merge step (propose_block_merge + carry_out_best_merges,
+ * partition.hpp:26-78, 324-454): labels updated in place; *B_new receives the
+ * new block count. */
+sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int32_t B_to_merge,
+                          int32_t np, uint64_t seed, uint32_t seq, int32_t* best, double* best_dS,
+                          int32_t* B_new);
+
+/* The MDL of a partition (compute_overall_entropy_cuda, partition.hpp:665-704). */
+sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, double* S,
+                   double* data_S);
+
+/* ----------------------------------------------------------- host utilities */
+
+/* Seeded directed DCSBM generator standing in for the GraphChallenge static
+ * graphs: Dirichlet(alpha) block sizes, truncated power-law out-degrees,
+ * in-block edges with probability p_in, destinations proportional to degree
+ * within the chosen block, no self-loops or repeated edges, unit weights. */
+typedef struct sbp_dcsbm_params {
+  int32_t N;
+  int32_t B;
+  double alpha;       /* Dirichlet concentration of block sizes */
+  double p_in;        /* probability an edge stays in its source block */
+  int32_t deg_min;    /* out-degree support [deg_min, deg_max] */
+  int32_t deg_max;
+  double exponent;    /* P(k) ~ k^-exponent */
+  uint64_t seed;
+} sbp_dcsbm_params;
+
+typedef struct sbp_edges sbp_edges;
+sbp_status sbp_dcsbm_generate(const sbp_dcsbm_params* p, sbp_edges** out);
+/* Sizes of an edge list; E may be NULL. */
+sbp_status sbp_edges_size(const sbp_edges* e, int32_t* N, int32_t* E);
+/* Copies the edge list (src, dst, w: E each) and the planted labels (N). Any
+ * pointer may be NULL. */
+sbp_status sbp_edges_copy(const sbp_edges* e, int32_t* src, int32_t* dst, uint32_t* w,
+                          int32_t* truth);
+void sbp_edges_free(sbp_edges* e);
+
+/* The CSR pair of an edge list the way load.hpp:86-117 builds it: out rows
+ * in edge order, in rows in edge order, weighted degrees. */
+sbp_status sbp_csr_from_edges(int32_t N, int32_t E, const int32_t* src, const int32_t* dst,
+                              const uint32_t* w, int32_t* out_ptr, int32_t* out_idx,
+                              uint32_t* out_w, int32_t* in_ptr, int32_t* in_idx, uint32_t* in_w,
+                              uint32_t* deg_out, uint32_t* deg_in);
+
+/* GraphChallenge TSV ("src\tdst\tweight", 1-based) as load.hpp:6-133 reads
+ * it, including its parse of a first field that holds a space (the first
+ * line of lowOverlap_lowBlockSizeVar/1k parses as a self-loop).  N is the
+ * largest source id, as in the reference.  truth_path (may be NULL) is the
+ * "_truePartition.tsv" file ("vertex\tblock", 1-based, load.hpp:119-130);
+ * without it the planted labels are -1. */
+sbp_status sbp_load_tsv(const char* path, const char* truth_path, sbp_edges** out);
+
+/* Pairwise recall, pairwise precision and NMI of `given` against `truth`
+ * (evaluate.hpp:18-265) with 64-bit pair counts.  truth[i] < 0 = unknown. */
+sbp_status sbp_evaluate(int32_t n, const int32_t* truth, const int32_t* given, double* recall,
+                        double* precision, double* nmi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBP_H */

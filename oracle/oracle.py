@@ -1,0 +1,197 @@
+"""ctypes view of the CPU oracle (oracle/sbp_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg as the checker, never by the partitioner.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "sbp_oracle.cpp")
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+def build(force=False):
+    if force or not os.path.exists(LIB) or os.path.getmtime(SRC) > os.path.getmtime(LIB):
+        tmp = LIB + ".tmp"
+        subprocess.run(["g++", "-std=c++17", "-O3", "-fPIC", "-shared", SRC, "-o", tmp],
+                       check=True)
+        os.replace(tmp, LIB)
+    return LIB
+
+
+build()
+_lib = C.CDLL(LIB)
+_vp = C.c_void_p
+
+
+class _G(C.Structure):
+    _fields_ = [("N", C.c_int32), ("E", C.c_int32)] + [
+        (k, C.c_void_p) for k in ("out_ptr", "out_idx", "out_w", "in_ptr", "in_idx", "in_w",
+                                  "deg_out", "deg_in")]
+
+
+class Options(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("num_proposals", C.c_int32),
+                ("reduction_rate", C.c_float), ("max_nodal_itr", C.c_int32),
+                ("num_batches", C.c_int32), ("threshold1", C.c_float),
+                ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32)]
+
+
+class Report(C.Structure):
+    _fields_ = [("B", C.c_int32), ("S", C.c_double), ("outer_steps", C.c_int32),
+                ("nodal_itrs", C.c_int32), ("nodal_proposals", C.c_int64),
+                ("accepted", C.c_int64), ("ms_total", C.c_double), ("ms_merge", C.c_double),
+                ("ms_nodal", C.c_double), ("ms_rebuild", C.c_double), ("status", C.c_int32)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+
+
+_GP = C.POINTER(_G)
+_sig("orc_philox", None, _vp, _vp, _vp)
+_sig("orc_build_blockmodel", C.c_int64, _GP, _vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+     _vp)
+_sig("orc_nodal_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
+_sig("orc_merge_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
+_sig("orc_mdl", C.c_double, _GP, _vp, C.c_int32, C.POINTER(C.c_double))
+_sig("orc_merge_proposals", None, _GP, _vp, C.c_int32, C.c_int32, C.c_uint64, C.c_uint32, _vp)
+_sig("orc_nodal_batch", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_uint32, C.c_int32,
+     C.c_int32, _vp, _vp)
+_sig("orc_merge_step", C.c_int32, _GP, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
+     C.c_uint32, _vp, _vp)
+_sig("orc_apply_merges", C.c_int32, C.c_int32, _vp, C.c_int32, C.c_int32, _vp, _vp)
+_sig("orc_partition", C.c_int, _GP, C.POINTER(Options), _vp, C.POINTER(Report))
+_sig("orc_time_nodal", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_int32, C.c_int32)
+_sig("orc_evaluate", None, C.c_int32, _vp, _vp, _vp)
+
+
+def _p(a):
+    return a.ctypes.data_as(_vp)
+
+
+def _g(g):
+    s = _G()
+    s.N, s.E = g.N, g.E
+    for k in ("out_ptr", "out_idx", "out_w", "in_ptr", "in_idx", "in_w", "deg_out", "deg_in"):
+        setattr(s, k, _p(getattr(g, k)))
+    return s
+
+
+def philox(ctr, key):
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    o = np.zeros(4, np.uint32)
+    _lib.orc_philox(_p(c), _p(k), _p(o))
+    return o
+
+
+def build_blockmodel(g, part, B):
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    cap = max(g.E, 1)
+    out = dict(optr=np.zeros(B + 1, np.int32), ocol=np.zeros(cap, np.int32),
+               ocnt=np.zeros(cap, np.uint32), iptr=np.zeros(B + 1, np.int32),
+               icol=np.zeros(cap, np.int32), icnt=np.zeros(cap, np.uint32),
+               d_out=np.zeros(B, np.uint32), d_in=np.zeros(B, np.uint32))
+    n = _lib.orc_build_blockmodel(C.byref(_g(g)), _p(part), B, *[_p(out[k]) for k in (
+        "optr", "ocol", "ocnt", "iptr", "icol", "icnt", "d_out", "d_in")])
+    for k in ("ocol", "ocnt", "icol", "icnt"):
+        out[k] = out[k][:n]
+    return out
+
+
+def nodal_delta(g, part, B, verts, props):
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    verts = np.ascontiguousarray(verts, dtype=np.int32)
+    props = np.ascontiguousarray(props, dtype=np.int32)
+    dS = np.zeros(max(verts.size, 1))
+    q3 = np.zeros(max(verts.size, 1), np.uint8)
+    _lib.orc_nodal_delta(C.byref(_g(g)), _p(part), B, verts.size, _p(verts), _p(props), _p(dS),
+                         _p(q3))
+    return dS[:verts.size], q3[:verts.size].astype(bool)
+
+
+def merge_delta(g, part, B, props, np_=10):
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    props = np.ascontiguousarray(props, dtype=np.int32)
+    dS = np.zeros(B * np_)
+    best = np.zeros(B, np.int32)
+    bds = np.zeros(B)
+    _lib.orc_merge_delta(C.byref(_g(g)), _p(part), B, np_, _p(props), _p(dS), _p(best), _p(bds))
+    return dS, best, bds
+
+
+def mdl(g, part, B):
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    d = C.c_double()
+    S = _lib.orc_mdl(C.byref(_g(g)), _p(part), B, C.byref(d))
+    return S, d.value
+
+
+def merge_proposals(g, part, B, seed, seq, np_=10):
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    props = np.zeros(B * np_, np.int32)
+    _lib.orc_merge_proposals(C.byref(_g(g)), _p(part), B, np_, seed, seq, _p(props))
+    return props
+
+
+def nodal_batch(g, part, B, seed, seq, lo, hi):
+    part = np.array(part, dtype=np.int32, copy=True)
+    n = max(hi - lo, 1)
+    dS = np.zeros(n)
+    props = np.zeros(n, np.int32)
+    tot = _lib.orc_nodal_batch(C.byref(_g(g)), _p(part), B, seed, seq, lo, hi, _p(dS), _p(props))
+    return part, dS[:hi - lo], props[:hi - lo], tot
+
+
+def merge_step(g, part, B, B_to_merge, seed, seq, np_=10):
+    part = np.array(part, dtype=np.int32, copy=True)
+    best = np.zeros(B, np.int32)
+    bds = np.zeros(B)
+    nb = _lib.orc_merge_step(C.byref(_g(g)), _p(part), B, B_to_merge, np_, seed, seq, _p(best),
+                             _p(bds))
+    return part, nb, best, bds
+
+
+def apply_merges(part, B, B_to_merge, best, best_dS):
+    part = np.array(part, dtype=np.int32, copy=True)
+    best = np.ascontiguousarray(best, dtype=np.int32)
+    best_dS = np.ascontiguousarray(best_dS, dtype=np.float64)
+    nb = _lib.orc_apply_merges(part.size, _p(part), B, B_to_merge, _p(best), _p(best_dS))
+    return part, nb
+
+
+def default_options(**kw):
+    o = Options(seed=0, num_proposals=10, reduction_rate=0.35, max_nodal_itr=100, num_batches=4,
+                threshold1=5e-4, threshold2=1e-4, window=3, max_outer=1000)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def partition(g, **kw):
+    o = default_options(**kw)
+    lab = np.zeros(g.N, np.int32)
+    r = Report()
+    st = _lib.orc_partition(C.byref(_g(g)), C.byref(o), _p(lab), C.byref(r))
+    return lab, {k: getattr(r, k) for k, _ in r._fields_}, st
+
+
+def time_nodal(g, part, B, seed, batches, num_batches=4):
+    part = np.array(part, dtype=np.int32, copy=True)
+    ms = _lib.orc_time_nodal(C.byref(_g(g)), _p(part), B, seed, batches, num_batches)
+    return ms, part
+
+
+def evaluate(truth, given):
+    t = np.ascontiguousarray(truth, dtype=np.int32)
+    g = np.ascontiguousarray(given, dtype=np.int32)
+    o = np.zeros(3)
+    _lib.orc_evaluate(t.size, _p(t), _p(g), _p(o))
+    return tuple(o)

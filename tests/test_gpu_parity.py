@@ -1,0 +1,137 @@
+"""GPU path vs the CPU oracle, through the C ABI.
+
+Bars: blockmodels, proposals, accepted moves and merge labels bit-exact;
+dS within 1e-9 relative (|gpu - oracle| <= 1e-9 * max(|oracle|, 1 bit)),
+the FP64 tolerance of the entropy terms.
+"""
+import numpy as np
+import pytest
+
+import graphs
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-9
+
+
+def close(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b) <= REL * np.maximum(np.abs(b), 1.0)
+
+
+def cases():
+    out = []
+    for name, g in (("LL1k", graphs.dcsbm("LL", 1000, 11, 0)),
+                    ("HH1k", graphs.dcsbm("HH", 1000, 11, 1)),
+                    ("weighted", graphs.weighted_graph())):
+        for pname, p, B in graphs.partitions(g):
+            out.append((f"{name}-{pname}", g, p, B))
+    g = graphs.dcsbm("LH", 1000, 11, 2)
+    p = np.random.default_rng(5).integers(0, 30, g.N).astype(np.int32)
+    out.append(("LH1k-empty-blocks", g, p, 40))  # blocks 30..39 empty
+    return out
+
+
+CASES = cases()
+IDS = [c[0] for c in CASES]
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_blockmodel_bit_exact(sbp, orc, case):
+    _, g, p, B = case
+    a = sbp.build_blockmodel(g, p, B)
+    b = orc.build_blockmodel(g, p, B)
+    for k in ("optr", "ocol", "ocnt", "iptr", "icol", "icnt", "d_out", "d_in"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_blockmodel_long_rows(sbp, orc):
+    # rows longer than one warp's buffer and than one CTA's (B > 16384)
+    g = graphs.hub_graph()
+    for p, B in ((np.arange(g.N, dtype=np.int32), g.N),
+                 (g.true_partitions, int(g.true_partitions.max()) + 1)):
+        a = sbp.build_blockmodel(g, p, B)
+        b = orc.build_blockmodel(g, p, B)
+        for k in ("optr", "ocol", "ocnt", "iptr", "icol", "icnt", "d_out", "d_in"):
+            assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_nodal_delta(sbp, orc, case):
+    _, g, p, B = case
+    rng = np.random.default_rng(11)
+    verts = np.arange(g.N, dtype=np.int32)
+    props = rng.integers(0, B, g.N).astype(np.int32)
+    # a share of the proposals go to neighbouring blocks, as the sampler does
+    src, dst, _ = g.edges()
+    pick = rng.integers(0, g.E, g.N)
+    near = p[dst[pick]]
+    props = np.where(rng.random(g.N) < 0.5, near, props).astype(np.int32)
+    got = sbp.delta_mdl_nodal(g, p, B, verts, props)
+    want, _ = orc.nodal_delta(g, p, B, verts, props)
+    ok = close(got, want)
+    assert ok.all(), (np.flatnonzero(~ok)[:5], got[~ok][:5], want[~ok][:5])
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_merge_delta(sbp, orc, case):
+    _, g, p, B = case
+    props = orc.merge_proposals(g, p, B, seed=3, seq=7)
+    d1, b1, bd1 = sbp.delta_mdl_merge(g, p, B, props)
+    d2, b2, bd2 = orc.merge_delta(g, p, B, props)
+    assert close(d1, d2).all()
+    assert close(bd1, bd2).all()
+    assert np.array_equal(b1, b2)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_merge_proposals_identical(sbp, orc, case):
+    _, g, p, B = case
+    a = sbp.merge_proposals(g, p, B, seed=9, seq=2)
+    b = orc.merge_proposals(g, p, B, seed=9, seq=2)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_nodal_batch_identical(sbp, orc, case):
+    _, g, p, B = case
+    BS = g.N // 4
+    for b in range(4):
+        pa, da, xa, ta = sbp.nodal_batch(g, p, B, 21, 100 + b, b * BS, (b + 1) * BS)
+        pb, db, xb, tb = orc.nodal_batch(g, p, B, 21, 100 + b, b * BS, (b + 1) * BS)
+        assert np.array_equal(xa, xb), "proposals differ"
+        assert close(da, db).all()
+        assert np.array_equal(pa, pb), "accepted moves differ"
+        assert abs(ta - tb) <= REL * max(abs(tb), 1.0)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_merge_step_identical(sbp, orc, case):
+    _, g, p, B = case
+    k = max(1, int(B * 0.35))
+    pa, nba, ba, bda = sbp.merge_step(g, p, B, k, seed=4, seq=1)
+    pb, nbb, bb, bdb = orc.merge_step(g, p, B, k, seed=4, seq=1)
+    assert np.array_equal(ba, bb)
+    assert close(bda, bdb).all()
+    assert nba == nbb
+    assert np.array_equal(pa, pb)
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_mdl(sbp, orc, case):
+    _, g, p, B = case
+    S1, d1 = sbp.mdl(g, p, B)
+    S2, d2 = orc.mdl(g, p, B)
+    assert close(S1, S2) and close(d1, d2)
+
+
+@pytest.mark.parametrize("variant,seed", [("LL", 0), ("HH", 1), ("LH", 2), ("HL", 3)])
+def test_partition_matches_oracle(sbp, orc, variant, seed):
+    g = graphs.dcsbm(variant, 1000, 11, seed)
+    rep = sbp.partition(g, seed=seed)
+    lab_o, rep_o, st = orc.partition(g, seed=seed)
+    assert st == 0 and rep["status"] == 0
+    assert rep["B"] == rep_o["B"]
+    assert close(rep["S"], rep_o["S"])
+    assert np.array_equal(g.partitions, lab_o)
