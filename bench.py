@@ -1,0 +1,329 @@
+"""Benchmark of the SBP path on B200: end-to-end partitions of the 200k-vertex
+HH-style DCSBM graph (N=200,000, 71 planted blocks, p_in=0.5, Dirichlet
+alpha=1, out-degrees from a power law of exponent 2.5 on [5, 50]).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full partition (merges, nodal sweeps, golden-section search
+over B) of the graph.  Prints one JSON line on rank 0.
+
+  value    partitions/s over all ranks with the graph resident in HBM
+           (sbp_partition_resident), CUDA-event time of the run's stream,
+           max over ranks
+  e2e      the same through sbp_partition with host buffers: graph upload,
+           partition, label download every step
+  roofline the nodal dS kernels (the dominant time): algorithmic bytes per
+           launch over their CUDA-event time, against MEASURED_PEAKS.json
+  cpu_baseline  the CPU oracle's nodal moves/s on a bounded sample
+
+Multi-GPU: one independent replica per GPU (the path does not shard), so
+scaling is weak.  --impl reference runs GSAP's own GPU build
+(oracle/_ref/gsap_ref) on the same graph, one partition per process.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="plain-200k-HH", N=200000, B=71, variant="HH", seed=0)
+METRIC = "SBP partitions/s (end to end, 200k-vertex HH DCSBM)"
+UNIT = "partitions/s"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """torch.distributed plumbing for the barrier and the max over ranks."""
+
+    def __init__(self, world, local):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.dist, self.torch = dist, torch
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def flush_l2(dev):
+    """Writes 256 MB (twice the L2) between timed steps."""
+    import torch
+    buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
+    buf.fill_(1.0)
+    torch.cuda.synchronize(dev)
+    del buf
+
+
+def make_graph(sbp):
+    w = WORKLOAD
+    return sbp.dcsbm_variant(w["variant"], w["N"], w["B"], seed=w["seed"])
+
+
+def cpu_baseline(g, seconds=20.0):
+    """CPU oracle nodal moves/s: Jacobi batches at the planted labels (B=71)
+    of the same graph, single thread, FP64; as many batches as fit in about
+    `seconds`."""
+    import os as _os
+    from oracle import oracle as orc
+    B = int(g.true_partitions.max()) + 1
+    ms1, _ = orc.time_nodal(g, g.true_partitions, B, 7, 1)
+    nb = max(1, min(40, int(seconds * 1000.0 / max(ms1, 1.0))))
+    ms, _ = orc.time_nodal(g, g.true_partitions, B, 7, nb)
+    BS = g.N // 4
+    return {"value": nb * BS / (ms / 1000.0), "unit": "nodal moves/s", "cores": 1,
+            "kind": "port",
+            "sample": f"{nb} Jacobi batches of {BS} vertices at the planted labels (B={B}) of "
+                      f"the benchmark graph, CPU oracle (FP64, 1 thread), {ms / 1000:.1f} s",
+            "cpu": _os.uname().machine, "nproc": _os.cpu_count()}
+
+
+def run_ours(args, rank, world, local, dist):
+    from gsap_b200 import sbp
+    g = make_graph(sbp)
+    rg = sbp.ResidentGraph(g, device=local)
+    opts = dict(device=local)
+    for i in range(args.warmup):
+        rg.partition(seed=1000 + i, **opts)
+    reports, labels = [], None
+    ms_dev = 0.0
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush_l2(local)
+            dist.barrier()
+            labels, rep = rg.partition(seed=i, **opts)
+            reports.append(rep)
+            ms_dev += rep["ms_device"]
+    ms_max = dist.max(ms_dev)
+    # end to end through the host-buffer C ABI call
+    e2e_ms = 0.0
+    for i in range(args.steps):
+        flush_l2(local)
+        dist.barrier()
+        t0 = time.perf_counter()
+        sbp.partition(g, seed=i, **opts)
+        e2e_ms += (time.perf_counter() - t0) * 1000.0
+    e2e_max = dist.max(e2e_ms)
+    rg.close()
+    if rank != 0:
+        return None
+    K = args.steps
+    rep = reports[-1]
+    rec, prec, nmi = sbp.evaluate(g.true_partitions, labels)
+    tot = {k: sum(r[k] for r in reports) for k in (
+        "ms_merge", "ms_nodal", "ms_rebuild", "ms_nodal_kernel", "nodal_launches",
+        "nodal_proposals", "bytes_nodal", "kernel_launches", "accepted_moves")}
+    peak, peak_kind = measured_peak()
+    achieved = tot["bytes_nodal"] / (tot["ms_nodal_kernel"] / 1000.0) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "nodal_kernel_200k_HH.md")
+    if os.path.exists(tfile):
+        import re
+        m = re.search(r"traffic_bytes_per_launch\s*=\s*(\d+)", open(tfile).read())
+        traffic = int(m.group(1)) if m else None
+    h2d = sum(a.nbytes for a in (g.out_ptr, g.out_idx, g.out_w, g.in_ptr, g.in_idx, g.in_w,
+                                 g.deg_out, g.deg_in))
+    line = {
+        "metric": METRIC, "value": world * K / (ms_max / 1000.0), "unit": UNIT,
+        "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "N": g.N, "E": g.E, "B_planted": WORKLOAD["B"],
+                   "generator": "DCSBM p_in=0.5 alpha=1 outdeg power 2.5 on [5,50] seed 0",
+                   "parallelism": f"replicas x{world}",
+                   "l2": "graph working set < L2; 256 MB written between timed steps"},
+        "e2e": {"value": world * K / (e2e_max / 1000.0), "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(g.N * 4)},
+        "roofline": {"bound": "hbm", "kernel": "nodal dS kernels (warp + heavy-vertex CTA)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "bytes_per_launch": tot["bytes_nodal"] / max(tot["nodal_launches"], 1),
+                     "ms_per_launch": tot["ms_nodal_kernel"] / max(tot["nodal_launches"], 1),
+                     "traffic": traffic},
+        "gpu_launches": int(tot["kernel_launches"]),
+        "phases_ms_per_step": {k: tot[k] / K for k in ("ms_merge", "ms_nodal", "ms_rebuild",
+                                                        "ms_nodal_kernel")},
+        "nodal_moves_per_s": tot["nodal_proposals"] / (tot["ms_nodal"] / 1000.0),
+        "quality": {"B": rep["B"], "S": rep["S"], "recall": rec, "precision": prec, "nmi": nmi},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(g, args.cpu_seconds)
+    return line
+
+
+def run_reference(args, rank, world, local):
+    from gsap_b200 import sbp
+    exe = os.path.join(ROOT, "oracle", "_ref", "gsap_ref")
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True}
+    if rank != 0:
+        return None
+    if not os.path.exists(exe):
+        return {**base, "unavailable": "oracle/_ref/gsap_ref was not built (needs the reference "
+                                       "tree at build time)"}
+    g = make_graph(sbp)
+    K, W = args.ref_steps, args.ref_warmup
+    times, rows = [], []
+    with tempfile.TemporaryDirectory() as td:
+        gp = os.path.join(td, "graph.bin")
+        lp = os.path.join(td, "labels.bin")
+        sbp.write_graph_bin(g, gp)
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=str(local))
+        with ClockSampler(local) as clk:
+            for i in range(W + K):
+                p = subprocess.run([exe, gp, "1", lp], capture_output=True, text=True,
+                                   timeout=args.ref_timeout, env=env)
+                if p.returncode != 0:
+                    return {**base, "unavailable": f"gsap_ref exited {p.returncode}: "
+                                                   f"{(p.stderr or p.stdout)[-200:]}"}
+                r = json.loads(p.stdout.strip().splitlines()[-1])
+                if i >= W:
+                    times.append(r["ms"])
+                    rows.append(r)
+        labels = np.fromfile(lp, dtype=np.int32)
+    rec, prec, nmi = sbp.evaluate(g.true_partitions, labels)
+    S, _ = sbp.mdl(g, labels, int(labels.max()) + 1)
+    ms = sum(times)
+    value = K / (ms / 1000.0)
+    return {**base, "value": value, "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "N": g.N, "E": g.E,
+                       "B_planted": WORKLOAD["B"], "parallelism": "single GPU"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "cpu_baseline": None,
+            "note": "GSAP's unmodified GPU path (partition.hpp) built for sm_100a, timed like "
+                    "GSAP.cu:24-30 (steady clock around partition(g) + cudaDeviceSynchronize), "
+                    "one partition per process",
+            "quality": {"B": int(labels.max()) + 1, "S": S, "recall": rec, "precision": prec,
+                        "nmi": nmi},
+            "clocks": clk.summary()}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-steps", type=int, default=None)
+    ap.add_argument("--ref-warmup", type=int, default=None)
+    ap.add_argument("--ref-timeout", type=float, default=900.0)
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        args.ref_steps = args.ref_steps or min(args.steps, 2)
+        args.ref_warmup = args.ref_warmup if args.ref_warmup is not None else min(args.warmup, 1)
+        line = run_reference(args, rank, world, local)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    dist = Dist(world, local)
+    try:
+        line = run_ours(args, rank, world, local, dist)
+    finally:
+        dist.close()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -27,6 +27,8 @@
 
 namespace sbp {
 
+thread_local long long g_launches = 0;
+
 namespace {
 
 constexpr int kScanThreads = 256;
@@ -481,12 +483,16 @@ cudaError_t init_kernel_attributes() {
 
 void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, cudaStream_t st) {
   if (n <= 8 * kScanTile) {
+    ++g_launches;
     scan_single<<<1, kScanThreads, 0, st>>>(in, out, n);
     return;
   }
   int tiles = (n + kScanTile - 1) / kScanTile;
+  ++g_launches;
   scan_tile_sums<<<tiles, kScanThreads, 0, st>>>(in, n, tile);
+  ++g_launches;
   scan_single<<<1, kScanThreads, 0, st>>>(tile, tile + tiles, tiles);
+  ++g_launches;
   scan_apply<<<tiles, kScanThreads, 0, st>>>(in, out, n, tile + tiles);
 }
 
@@ -522,15 +528,22 @@ void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM
     cudaMemsetAsync(r.cnt, 0, sizeof(int32_t) * (size_t)B, st);
   }
   cudaMemsetAsync(rs.big_count, 0, sizeof(int32_t) * 2, st);
+  ++g_launches;
   rb_count<<<dim3((g.N + 255) / 256, 2), 256, 0, st>>>(a);
   for (int dir = 0; dir < 2; ++dir)
     scan_exclusive(rs.d[dir].cnt, rs.d[dir].seg, B, rs.tile + dir * (rs.tile_cap / 2), st);
-  if (g.E > 0) rb_scatter<<<dim3((g.E + 255) / 256, 2), 256, 0, st>>>(a);
+  if (g.E > 0) {
+    ++g_launches;
+    rb_scatter<<<dim3((g.E + 255) / 256, 2), 256, 0, st>>>(a);
+  }
+  ++g_launches;
   rb_rows_small<<<dim3(grid_for(B, kRowsWarps, 4096), 2), kRowsWarps * 32, 0, st>>>(a);
+  ++g_launches;
   rb_rows_big<<<dim3(2 * 148, 2), kBigThreads, kBigSmem, st>>>(a);
   for (int dir = 0; dir < 2; ++dir)
     scan_exclusive(rs.d[dir].uniq, dir == 0 ? m.optr : m.iptr, B,
                    rs.tile + dir * (rs.tile_cap / 2), st);
+  ++g_launches;
   rb_compact<<<dim3(grid_for((long long)B * 32, 256, 4096), 2), 256, 0, st>>>(a);
 }
 
@@ -542,10 +555,12 @@ void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cu
   a.dSout = m.dSout; a.ambout = m.ambout; a.ambin = m.ambin; a.sinfull = m.sinfull;
   a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
   a.B = B; a.draws = draws; a.seed = seed; a.seq = seq;
+  ++g_launches;
   block_terms_kernel<<<grid_for((long long)B * 32, 256, 8192), 256, 0, st>>>(a);
 }
 
 void mdl_data_sum(const DevBM& m, int32_t B, double* out, cudaStream_t st) {
+  ++g_launches;
   mdl_sum_kernel<<<1, 1024, 0, st>>>(m.dSout, B, out);
 }
 

@@ -115,6 +115,8 @@ struct Job {
   int32_t *part = nullptr, *newlab = nullptr, *props = nullptr, *best = nullptr, *map = nullptr;
   int32_t* snap[3] = {nullptr, nullptr, nullptr};
   double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
+  int32_t* heavy = nullptr;     // vertices handed to the CTA-per-vertex kernel
+  int32_t* heavy_count = nullptr;  // [queue length, error count]
   double* dsum = nullptr;       // per nodal iteration: sum of recorded dS
   double* dataS = nullptr;      // per nodal iteration: MDL data term
   long long* acc = nullptr;     // per nodal iteration: applied moves
@@ -126,6 +128,8 @@ struct Job {
   long long* h_acc = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> bev;  // per-batch timing events of one sweep
+  std::vector<int32_t> h_optr, h_iptr;  // host copies of the graph's row pointers
+  int32_t* h_misc = nullptr;            // pinned: nnz, error count
 
   ~Job() { release(); }
 
@@ -146,6 +150,7 @@ struct Job {
       cudaFreeHost(h_map);
       cudaFreeHost(h_scal);
       cudaFreeHost(h_acc);
+      cudaFreeHost(h_misc);
       cudaSetDevice(cur);
       mem = nullptr;
       st = nullptr;
@@ -179,6 +184,7 @@ static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32
   add((size_t)N * np, 8);
   add(N, 8);
   add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
+  add((size_t)3 * N, 4); add(2, 4);
   return b + 4096;
 }
 
@@ -191,7 +197,11 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
   J.max_itr = max_itr;
   SBP_CUDA(cudaSetDevice(device));
   static std::once_flag once[64];
-  if (device >= 0 && device < 64) std::call_once(once[device], [] { init_kernel_attributes(); });
+  if (device >= 0 && device < 64)
+    std::call_once(once[device], [] {
+      init_kernel_attributes();
+      init_nodal_attributes();
+    });
   int32_t tiles = 2 * (2 * ((N + 1) / 2048 + 2) + 2);
   J.mem_bytes = job_bytes(N, E, np, max_itr, tiles);
   if (cudaMalloc(&J.mem, J.mem_bytes) != cudaSuccess) {
@@ -206,6 +216,7 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
   SBP_CUDA(cudaMallocHost(&J.h_map, sizeof(int32_t) * ((size_t)N + 1)));
   SBP_CUDA(cudaMallocHost(&J.h_scal, sizeof(double) * 4));
   SBP_CUDA(cudaMallocHost(&J.h_acc, sizeof(long long) * 2));
+  SBP_CUDA(cudaMallocHost(&J.h_misc, sizeof(int32_t) * 4));
   Arena A{(char*)J.mem, J.mem_bytes, 0};
   size_t n1 = (size_t)N + 1, e = (size_t)E > 0 ? (size_t)E : 1;
   DevGraph& g = J.g;
@@ -245,7 +256,10 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
   J.dsum = A.take<double>(max_itr);
   J.dataS = A.take<double>(max_itr);
   J.acc = (long long*)A.take<double>(max_itr);
-  if (!J.acc) return fail(SBP_ERR_INTERNAL, "arena sizing");
+  J.heavy = A.take<int32_t>((size_t)3 * N);
+  J.heavy_count = A.take<int32_t>(2);
+  if (!J.heavy_count) return fail(SBP_ERR_INTERNAL, "arena sizing");
+  SBP_CUDA(cudaMemsetAsync(J.heavy_count, 0, 8, J.st));
   return SBP_OK;
 }
 
@@ -274,7 +288,11 @@ static sbp_status job_upload(Job& J, const sbp_graph_csr* h) {
   }
   SBP_CUDA(cudaMemcpyAsync(g.kdo, h->deg_out, 4 * (size_t)J.N, cudaMemcpyHostToDevice, st));
   SBP_CUDA(cudaMemcpyAsync(g.kdi, h->deg_in, 4 * (size_t)J.N, cudaMemcpyHostToDevice, st));
+  ++g_launches;
   fill_src_kernel<<<(J.N + 255) / 256, 256, 0, st>>>(g.optr, J.N, g.osrc);
+  J.h_optr.assign(h->out_ptr, h->out_ptr + J.N + 1);
+  J.h_iptr.assign(h->in_ptr, h->in_ptr + J.N + 1);
+  ++g_launches;
   fill_src_kernel<<<(J.N + 255) / 256, 256, 0, st>>>(g.iptr, J.N, g.isrc);
   SBP_CUDA(cudaGetLastError());
   return SBP_OK;
@@ -386,6 +404,9 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
   std::memset(&R, 0, sizeof(R));
   cudaStream_t st = J.st;
   const int32_t N = J.N, E = J.E;
+  const long long launches0 = g_launches;
+  SBP_CUDA(cudaEventRecord(J.ev[3], st));
+  ++g_launches;
   iota_kernel<<<(N + 255) / 256, 256, 0, st>>>(J.part, N);
   int32_t B = N;
   int32_t B_to_merge = (int32_t)((float)B * o.reduction_rate);
@@ -398,7 +419,16 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
   int32_t BS = N / o.num_batches;
   std::vector<double> itr_dS(o.max_nodal_itr);
   float ms = 0.f;
-  while ((int)J.bev.size() < 2 * o.num_batches + 1) {
+  // algorithmic bytes of one nodal batch's kernels: per vertex 28 bytes,
+  // per adjacency entry (either direction) 12, plus the blockmodel rows
+  // (16 per nonzero) and 8 per block
+  std::vector<double> batch_entries(o.num_batches, 0.0);
+  for (int32_t b = 0; b < o.num_batches; ++b) {
+    int32_t lo = b * (N / o.num_batches), hi = (b + 1) * (N / o.num_batches);
+    batch_entries[b] = (double)(J.h_optr[hi] - J.h_optr[lo]) + (double)(J.h_iptr[hi] - J.h_iptr[lo]);
+  }
+  double nnz_now = (double)E;
+  while ((int)J.bev.size() < 4 * o.num_batches + 1) {
     cudaEvent_t e;
     SBP_CUDA(cudaEventCreate(&e));
     J.bev.push_back(e);
@@ -410,6 +440,7 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
     }
     // merge phase (partition.hpp:900-904)
     SBP_CUDA(cudaEventRecord(J.ev[0], st));
+    R.bytes_merge += 320.0 * nnz_now + 8.0 * N;
     sbp_status s = merge_step(J, B, B_to_merge, o.seed, seq++, false);
     if (s != SBP_OK) return s;
     SBP_CUDA(cudaEventRecord(J.ev[1], st));
@@ -425,31 +456,45 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
     SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[1], J.ev[2]));
     R.ms_rebuild += ms;
     for (int32_t itr = 0; itr < o.max_nodal_itr; ++itr) {
-      // events: bev[0] sweep start, bev[2b+1] after batch b's nodal kernels,
-      // bev[2b+2] after its rebuild; read at the sweep's one synchronisation
+      // events: bev[0] sweep start; batch b: bev[4b+1] after the per-block
+      // terms, bev[4b+2] after the nodal kernels, bev[4b+3] after the commit,
+      // bev[4b+4] after the rebuild; read at the sweep's one synchronisation
       SBP_CUDA(cudaEventRecord(J.bev[0], st));
       for (int32_t b = 0; b < o.num_batches; ++b) {
         block_terms(J.m, B, 1, o.seed, seq, st);
+        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 1], st));
         nodal_batch_sample(J.g, J.part, J.m, B, o.seed, seq, b * BS, BS, J.newlab, J.rec, nullptr,
-                           st);
-        nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, st);
+                           J.heavy, J.heavy_count, st);
+        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 2], st));
+        nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr,
+                     J.heavy_count, st);
         ++seq;
-        SBP_CUDA(cudaEventRecord(J.bev[2 * b + 1], st));
+        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 3], st));
         rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
-        SBP_CUDA(cudaEventRecord(J.bev[2 * b + 2], st));
+        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 4], st));
         R.nodal_proposals += BS;
+        R.nodal_launches += 1;
+        R.bytes_nodal += 28.0 * BS + 12.0 * batch_entries[b] + 16.0 * nnz_now + 8.0 * B;
+        R.bytes_rebuild += 4.0 * N + 24.0 * E + 16.0 * nnz_now + 8.0 * B;
       }
       block_terms(J.m, B, 0, o.seed, 0, st);
       mdl_data_sum(J.m, B, J.dataS + itr, st);
       SBP_CUDA(cudaMemcpyAsync(J.h_scal, J.dsum + itr, 8, cudaMemcpyDeviceToHost, st));
       SBP_CUDA(cudaMemcpyAsync(J.h_scal + 1, J.dataS + itr, 8, cudaMemcpyDeviceToHost, st));
       SBP_CUDA(cudaMemcpyAsync(J.h_acc, J.acc + itr, 8, cudaMemcpyDeviceToHost, st));
+      SBP_CUDA(cudaMemcpyAsync(J.h_misc, J.heavy_count + 1, 4, cudaMemcpyDeviceToHost, st));
+      SBP_CUDA(cudaMemcpyAsync(J.h_misc + 1, J.m.optr + B, 4, cudaMemcpyDeviceToHost, st));
       SBP_CUDA(cudaStreamSynchronize(st));
       SBP_CUDA(cudaGetLastError());
+      if (J.h_misc[0] != 0)
+        return fail(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
+      nnz_now = (double)J.h_misc[1];
       for (int32_t b = 0; b < o.num_batches; ++b) {
-        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[2 * b], J.bev[2 * b + 1]));
+        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[4 * b], J.bev[4 * b + 3]));
         R.ms_nodal += ms;
-        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[2 * b + 1], J.bev[2 * b + 2]));
+        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[4 * b + 1], J.bev[4 * b + 2]));
+        R.ms_nodal_kernel += ms;
+        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[4 * b + 3], J.bev[4 * b + 4]));
         R.ms_rebuild += ms;
       }
       ++R.nodal_itrs;
@@ -531,8 +576,12 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
   if (labels_out) {
     SBP_CUDA(cudaMemcpyAsync(labels_out, J.part, 4 * (size_t)N, cudaMemcpyDeviceToHost, st));
   }
+  SBP_CUDA(cudaEventRecord(J.ev[2], st));
   SBP_CUDA(cudaStreamSynchronize(st));
   SBP_CUDA(cudaGetLastError());
+  SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[3], J.ev[2]));
+  R.ms_device = ms;
+  R.kernel_launches = g_launches - launches0;
   R.B = B;
   R.S = S;
   R.ms_total = total.ms();
@@ -549,10 +598,20 @@ static sbp_status job_for(Job& J, const sbp_graph_csr* g, int device, int32_t np
   return job_upload(J, g);
 }
 
-static sbp_status set_part(Job& J, const int32_t* part, int32_t B) {
-  sbp_status s = validate_part(part, J.N, B);
+// Validates the graph and the labels, then creates the job, uploads both
+// and builds the blockmodel of the labels.
+static sbp_status prepare(Job& J, const sbp_graph_csr* g, const int32_t* part, int32_t B,
+                          int32_t np, int32_t max_itr) {
+  sbp_status s = validate_graph(g);
+  if (s != SBP_OK) return s;
+  s = validate_part(part, g->N, B);
+  if (s != SBP_OK) return s;
+  s = job_create(J, resolve_device(-1), g->N, g->E, np, max_itr);
+  if (s != SBP_OK) return s;
+  s = job_upload(J, g);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, J.st));
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   return SBP_OK;
 }
 
@@ -680,11 +739,8 @@ sbp_status sbp_build_blockmodel(const sbp_graph_csr* g, const int32_t* part, int
                                 int32_t* in_ptr, int32_t* in_col, uint32_t* in_cnt,
                                 uint32_t* d_out, uint32_t* d_in, int64_t* nnz) {
   Job J;
-  sbp_status s = job_for(J, g, -1, 1, 1);
+  sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
-  s = set_part(J, part, B);
-  if (s != SBP_OK) return s;
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   int32_t n = 0;
   SBP_CUDA(cudaMemcpyAsync(&n, J.m.optr + B, 4, cudaMemcpyDeviceToHost, J.st));
   SBP_CUDA(cudaStreamSynchronize(J.st));
@@ -706,6 +762,7 @@ sbp_status sbp_build_blockmodel(const sbp_graph_csr* g, const int32_t* part, int
 
 sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t nv,
                                const int32_t* verts, const int32_t* props, double* dS) {
+  if (!g) return fail(SBP_ERR_INVALID, "graph is NULL");
   if (nv < 0 || (nv > 0 && (!verts || !props || !dS)))
     return fail(SBP_ERR_INVALID, "bad vertex/proposal arrays");
   for (int32_t i = 0; i < nv; ++i) {
@@ -713,9 +770,7 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
     if (props[i] < 0 || props[i] >= B) return fail(SBP_ERR_INVALID, "proposal out of [0, B)");
   }
   Job J;
-  sbp_status s = job_for(J, g, -1, 1, 1);
-  if (s != SBP_OK) return s;
-  s = set_part(J, part, B);
+  sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
   int32_t *dv = nullptr, *dp = nullptr;
   double* dd = nullptr;
@@ -725,9 +780,8 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
   SBP_CUDA(cudaMalloc(&dd, 8 * n));
   cudaMemcpyAsync(dv, verts, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
   cudaMemcpyAsync(dp, props, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   block_terms(J.m, B, 0, 0, 0, J.st);
-  nodal_delta_given(J.g, J.part, J.m, B, nv, dv, dp, dd, J.st);
+  nodal_delta_given(J.g, J.part, J.m, B, nv, dv, dp, dd, J.heavy, J.heavy_count, J.st);
   cudaMemcpyAsync(dS, dd, 8 * (size_t)nv, cudaMemcpyDeviceToHost, J.st);
   cudaError_t e = cudaStreamSynchronize(J.st);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -740,17 +794,14 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
 
 sbp_status sbp_delta_mdl_merge(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
                                const int32_t* props, double* dS, int32_t* best, double* best_dS) {
-  if (np < 1 || np > 32 || !props) return fail(SBP_ERR_INVALID, "bad proposals");
+  if (np < 1 || np > 32 || !props || B < 1) return fail(SBP_ERR_INVALID, "bad proposals");
   for (int64_t t = 0; t < (int64_t)B * np; ++t)
     if (props[t] < 0 || props[t] >= B) return fail(SBP_ERR_INVALID, "proposal out of [0, B)");
   Job J;
-  sbp_status s = job_for(J, g, -1, np, 1);
-  if (s != SBP_OK) return s;
-  s = set_part(J, part, B);
+  sbp_status s = prepare(J, g, part, B, np, 1);
   if (s != SBP_OK) return s;
   size_t nt = (size_t)B * np;
   SBP_CUDA(cudaMemcpyAsync(J.props, props, 4 * nt, cudaMemcpyHostToDevice, J.st));
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   block_terms(J.m, B, 0, 0, 0, J.st);
   merge_delta(J.m, B, np, J.props, J.mdS, J.best, J.best_dS, J.st);
   SBP_CUDA(cudaStreamSynchronize(J.st));
@@ -765,11 +816,8 @@ sbp_status sbp_merge_proposals(const sbp_graph_csr* g, const int32_t* part, int3
                                uint64_t seed, uint32_t seq, int32_t* props) {
   if (np < 1 || np > 32 || !props) return fail(SBP_ERR_INVALID, "bad proposal buffer");
   Job J;
-  sbp_status s = job_for(J, g, -1, np, 1);
+  sbp_status s = prepare(J, g, part, B, np, 1);
   if (s != SBP_OK) return s;
-  s = set_part(J, part, B);
-  if (s != SBP_OK) return s;
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   merge_proposals(J.m, B, np, seed, seq, J.props, J.st);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());
@@ -782,17 +830,15 @@ sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uin
                            double* sum) {
   if (!g || lo < 0 || hi < lo || hi > g->N) return fail(SBP_ERR_INVALID, "bad batch range");
   Job J;
-  sbp_status s = job_for(J, g, -1, 1, 1);
-  if (s != SBP_OK) return s;
-  s = set_part(J, part, B);
+  sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
   int32_t cnt = hi - lo;
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   block_terms(J.m, B, 1, seed, seq, J.st);
   SBP_CUDA(cudaMemsetAsync(J.dsum, 0, 8, J.st));
   SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8, J.st));
-  nodal_batch_sample(J.g, J.part, J.m, B, seed, seq, lo, cnt, J.newlab, J.rec, J.props, J.st);
-  nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, J.st);
+  nodal_batch_sample(J.g, J.part, J.m, B, seed, seq, lo, cnt, J.newlab, J.rec, J.props, J.heavy,
+                     J.heavy_count, J.st);
+  nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, J.heavy_count, J.st);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());
   SBP_CUDA(cudaMemcpy(part, J.part, 4 * (size_t)J.N, cudaMemcpyDeviceToHost));
@@ -807,11 +853,8 @@ sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int3
                           int32_t* B_new) {
   if (np < 1 || np > 32) return fail(SBP_ERR_INVALID, "bad np");
   Job J;
-  sbp_status s = job_for(J, g, -1, np, 1);
+  sbp_status s = prepare(J, g, part, B, np, 1);
   if (s != SBP_OK) return s;
-  s = set_part(J, part, B);
-  if (s != SBP_OK) return s;
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   int32_t b = B;
   s = merge_step(J, b, B_to_merge, seed, seq, false);
   if (s != SBP_OK) return s;
@@ -826,11 +869,8 @@ sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int3
 sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, double* S,
                    double* data_S) {
   Job J;
-  sbp_status s = job_for(J, g, -1, 1, 1);
+  sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
-  s = set_part(J, part, B);
-  if (s != SBP_OK) return s;
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   block_terms(J.m, B, 0, 0, 0, J.st);
   mdl_data_sum(J.m, B, J.dataS, J.st);
   double ds = 0.0;

@@ -7,6 +7,10 @@
 
 namespace sbp {
 
+// Kernels launched by this thread through the launchers below (the bench's
+// launch count).
+extern thread_local long long g_launches;
+
 // The graph in HBM (uploaded once per job).
 struct DevGraph {
   int32_t N = 0, E = 0;
@@ -64,20 +68,26 @@ void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cu
 // data_S = sum of dSout over blocks, written to *out (deterministic order).
 void mdl_data_sum(const DevBM& m, int32_t B, double* out, cudaStream_t st);
 
+cudaError_t init_nodal_attributes();
+
 // Nodal batch of vertices [lo, lo+count): proposal, dS, accept flag.
 // newlab[i] = new label of vertex lo+i, rec[i] = recorded dS (0 if rejected),
-// props[i] (optional) = proposal.
+// props[i] (optional) = proposal.  heavy (3 ints per vertex) and heavy_count
+// (2 ints: queue length, which must be 0 on entry, and an error counter) hold
+// the vertices handed from the warp kernel to the CTA kernel.
 void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                         uint64_t seed, uint32_t seq, int32_t lo, int32_t count, int32_t* newlab,
-                        double* rec, int32_t* props, cudaStream_t st);
+                        double* rec, int32_t* props, int32_t* heavy, int32_t* heavy_count,
+                        cudaStream_t st);
 // dS of given (vertex, proposal) pairs, no accept.
 void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                        int32_t nv, const int32_t* verts, const int32_t* props, double* dS,
-                       cudaStream_t st);
+                       int32_t* heavy, int32_t* heavy_count, cudaStream_t st);
 // Apply a batch: part[lo+i] = newlab[i]; slot_sum[0] += sum(rec) in a fixed
-// order, slot_acc[0] += number of moves.
+// order, slot_acc[0] += number of moves; resets heavy_count[0].
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
-                  const double* rec, double* slot_sum, long long* slot_acc, cudaStream_t st);
+                  const double* rec, double* slot_sum, long long* slot_acc, int32_t* heavy_count,
+                  cudaStream_t st);
 
 // Merge proposals (kernels.hpp:726-856) and their dS with the per-block best
 // (kernels.hpp:143-491).

@@ -214,7 +214,10 @@ void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint3
   a.seq = seq;
   a.props = props;
   long long n = (long long)B * np;
-  if (n > 0) merge_props_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(a);
+  if (n > 0) {
+    ++g_launches;
+    merge_props_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(a);
+  }
 }
 
 void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
@@ -226,11 +229,17 @@ void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, do
   a.best_dS = best_dS;
   int g = (B + kMergeWarps - 1) / kMergeWarps;
   if (g > 148 * 32) g = 148 * 32;
-  if (B > 0) merge_delta_kernel<<<g, kMergeWarps * 32, 0, st>>>(a);
+  if (B > 0) {
+    ++g_launches;
+    merge_delta_kernel<<<g, kMergeWarps * 32, 0, st>>>(a);
+  }
 }
 
 void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st) {
-  if (N > 0) relabel_kernel<<<(N + 255) / 256, 256, 0, st>>>(part, N, map);
+  if (N > 0) {
+    ++g_launches;
+    relabel_kernel<<<(N + 255) / 256, 256, 0, st>>>(part, N, map);
+  }
 }
 
 }  // namespace sbp

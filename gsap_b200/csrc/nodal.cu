@@ -5,10 +5,13 @@
 // thread walk a whole blockmodel row in a serial sorted merge with the
 // vertex's sorted neighbour-block list (kernels.hpp:494-597, 1153-1726).
 //
-// Here one warp owns one vertex and does everything in one launch:
+// Here a group of threads owns one vertex: a warp for ordinary vertices, a
+// whole CTA for the few whose neighbour lists exceed a warp's buffer.
 //   * proposal: Philox draws, an exact integer inverse-CDF pick of a
 //     neighbour (a warp prefix scan over its out- then in-entries), then the
 //     per-block draws of the batch (kernels.hpp:877-1032);
+//   * neighbour blocks: only this vertex's lists are sorted, in shared
+//     memory (bitonic), where GSAP sorts all E entries every batch;
 //   * dS: GSAP's seven terms rewritten as "old row sum + changed columns".
 //     A row term  sum_c f(x_c)  with  f(x) = x (log2 x - log2 dcol[c] - L)
 //     splits into  sum_c (x log2 x - x log2 dcol[c])  -  L * sum_c x ;
@@ -32,7 +35,15 @@ namespace sbp {
 namespace {
 
 constexpr int kNodalWarps = 8;
-constexpr int kListCap = 64;  // neighbour entries per direction staged in shared memory
+constexpr int kWarpList = 128;     // entries per direction a warp sorts in shared memory
+constexpr int kHeavyThreads = 256;
+constexpr int kHeavyList = 4096;   // entries per direction a CTA sorts in shared memory
+constexpr int kHashSlotsCfg = 8192;
+// sorted lists (two directions) or the hash table (key, sum, first)
+constexpr size_t kHeavySmem =
+    2 * kHeavyList * sizeof(unsigned long long) > 3 * kHashSlotsCfg * sizeof(int32_t)
+        ? 2 * kHeavyList * sizeof(unsigned long long)
+        : 3 * kHashSlotsCfg * sizeof(int32_t);
 
 struct NodalArgs {
   const int32_t *optr, *oidx, *iptr, *iidx;
@@ -53,6 +64,8 @@ struct NodalArgs {
   double* rec;
   int32_t* props_out;
   double* dS_raw;
+  int32_t* heavy;           // (i, v, s) triples of vertices left to the CTA kernel
+  int32_t* heavy_count;
 };
 
 // g(x, a) = x log2 x - x a, zero for x == 0
@@ -64,174 +77,173 @@ __device__ __forceinline__ double fterm(uint32_t m, double a, double b) {
   return m == 0u ? 0.0 : (double)m * (log2((double)m) - (a + b));
 }
 
-struct List {
-  const int32_t* idx;
-  const uint32_t* w;
-  const int32_t* part;
-  const int32_t* sc;  // staged blocks
-  const uint32_t* sw;
-  int32_t base, n;
-  __device__ __forceinline__ int32_t blk(int k) const {
-    return k < kListCap ? sc[k] : __ldg(part + __ldg(idx + base + k));
+// A thread group cooperating on one vertex: a warp (G = 32) or a CTA.
+template <int G>
+struct Group {
+  double* red;  // G/32 doubles of shared scratch (CTA only)
+  __device__ __forceinline__ int rank() const { return G == 32 ? (threadIdx.x & 31) : threadIdx.x; }
+  __device__ __forceinline__ void sync() const {
+    if (G == 32) __syncwarp();
+    else __syncthreads();
   }
-  __device__ __forceinline__ uint32_t wt(int k) const {
-    return k < kListCap ? sw[k] : __ldg(w + base + k);
+  __device__ double sum(double x) const {
+    x = warp_sum(x);
+    if (G == 32) return x;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < G / 32; ++i) t += red[i];
+    __syncthreads();
+    return t;
+  }
+  __device__ long long sum_ll(long long x) const {
+    return (long long)sum((double)x);  // |x| < 2^53: exact
   }
 };
 
-// dS of moving v from r to s (r != s), computed by the whole warp; every
-// lane returns the same value.
-__device__ double vertex_delta(const NodalArgs& a, int v, int r, int s, int lane, int32_t* sc_o,
-                               uint32_t* sw_o, int32_t* sc_i, uint32_t* sw_i) {
-  const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
-  const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
-  for (int k = lane; k < no && k < kListCap; k += 32) {
-    sc_o[k] = __ldg(a.part + __ldg(a.oidx + o0 + k));
-    sw_o[k] = __ldg(a.ow + o0 + k);
+// Ascending bitonic sort of P (power of two) keys by the group.
+template <int G>
+__device__ void group_sort(unsigned long long* key, int P, const Group<G>& grp) {
+  const int t = grp.rank();
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = t; i < P; i += G) {
+        int ixj = i ^ j;
+        if (ixj > i) {
+          unsigned long long x = key[i], y = key[ixj];
+          bool asc = (i & k) == 0;
+          if ((x > y) == asc) {
+            key[i] = y;
+            key[ixj] = x;
+          }
+        }
+      }
+      grp.sync();
+    }
   }
-  for (int k = lane; k < ni && k < kListCap; k += 32) {
-    sc_i[k] = __ldg(a.part + __ldg(a.iidx + i0 + k));
-    sw_i[k] = __ldg(a.iw + i0 + k);
-  }
-  __syncwarp();
-  List LO{a.oidx, a.ow, a.part, sc_o, sw_o, o0, no};
-  List LI{a.iidx, a.iw, a.part, sc_i, sw_i, i0, ni};
+}
 
-  // weights of v's edges into / from blocks r and s
-  uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
-  for (int k = lane; k < no; k += 32) {
-    int32_t c = LO.blk(k);
-    uint32_t w = LO.wt(k);
-    koR += c == r ? w : 0u;
-    koS += c == s ? w : 0u;
-  }
-  for (int k = lane; k < ni; k += 32) {
-    int32_t c = LI.blk(k);
-    uint32_t w = LI.wt(k);
-    niR += c == r ? w : 0u;
-    niS += c == s ? w : 0u;
-  }
-  koR = warp_sum_u(koR);
-  koS = warp_sum_u(koS);
-  niR = warp_sum_u(niR);
-  niS = warp_sum_u(niS);
+__device__ __forceinline__ int32_t kblk(unsigned long long k) { return (int32_t)(k >> 32); }
+__device__ __forceinline__ uint32_t kwt(unsigned long long k) { return (uint32_t)k; }
 
-  const int32_t rO0 = a.bop[r], rO1 = a.bop[r + 1];
-  const int32_t sO0 = a.bop[s], sO1 = a.bop[s + 1];
-  const int32_t rI0 = a.bip[r], rI1 = a.bip[r + 1];
-  const int32_t sI0 = a.bip[s], sI1 = a.bip[s + 1];
+// Stage v's neighbour blocks of one direction as sorted (block, weight) keys.
+template <int G>
+__device__ void stage_sorted(const int32_t* __restrict__ idx, const uint32_t* __restrict__ w,
+                             const int32_t* __restrict__ part, int32_t base, int n,
+                             unsigned long long* key, const Group<G>& grp) {
+  int P = 32;
+  while (P < n) P <<= 1;
+  for (int k = grp.rank(); k < P; k += G)
+    key[k] = k < n ? ((unsigned long long)(uint32_t)__ldg(part + __ldg(idx + base + k)) << 32) |
+                         __ldg(w + base + k)
+                   : ~0ull;
+  grp.sync();
+  group_sort<G>(key, P, grp);
+}
 
+// Accumulators of the changed columns of the four new rows (out r, out s,
+// in r, in s): a = sum of (x log2 x - x log2 dcol) deltas, m = count deltas.
+struct Acc {
   double a4 = 0.0, a5 = 0.0, a6 = 0.0, a7 = 0.0;
   long long m4 = 0, m5 = 0, m6 = 0, m7 = 0;
+};
 
-  // out-entries: rows r and s of the out CSR (kernels.hpp:1444-1726)
-  for (int k = lane; k < no; k += 32) {
-    int32_t c = LO.blk(k);
-    uint32_t w = LO.wt(k);
-    uint32_t Msc = row_lookup(a.boc, a.bon, sO0, sO1, c);
-    if (c != r && c != s) {
-      bool leader = true;
-      uint32_t kc = 0;
-      for (int q = 0; q < no; ++q) {
-        if (LO.blk(q) == c) {
-          kc += LO.wt(q);
-          if (q < k) leader = false;
-        }
-      }
-      if (leader) {
-        double ldc = a.ld_in[c];
-        uint32_t Mrc = row_lookup(a.boc, a.bon, rO0, rO1, c);
-        uint32_t x = Mrc - kc;
-        a4 += gterm(x, ldc) - gterm(Mrc, ldc);
-        m4 += (long long)x - (long long)Mrc;
-        if (Msc != 0u) {
-          uint32_t y = Msc + kc;
-          a5 += gterm(y, ldc) - gterm(Msc, ldc);
-          m5 += (long long)y - (long long)Msc;
-        }
-      }
-    }
-    if (Msc == 0u) {
-      // block c absent from row s: one term per list entry
-      uint32_t y = w - (c == r ? niS : 0u) + (c == s ? niS : 0u);
-      a5 += gterm(y, a.ld_in[c]);
-      m5 += (long long)y;
+struct RowBounds {
+  int32_t rO0, rO1, sO0, sO1, rI0, rI1, sI0, sI1;
+};
+
+__device__ __forceinline__ RowBounds row_bounds(const NodalArgs& a, int r, int s) {
+  return RowBounds{a.bop[r], a.bop[r + 1], a.bop[s], a.bop[s + 1],
+                   a.bip[r], a.bip[r + 1], a.bip[s], a.bip[s + 1]};
+}
+
+// One out-entry (block c, weight w) of v; `leader` marks one entry per
+// distinct block, kc = v's total weight into c (kernels.hpp:1444-1726).
+__device__ __forceinline__ void out_entry(const NodalArgs& a, const RowBounds& rb, int r, int s,
+                                          uint32_t niS, int32_t c, uint32_t w, bool leader,
+                                          uint32_t kc, Acc& q) {
+  const double ldc = a.ld_in[c];
+  const uint32_t Msc = row_lookup(a.boc, a.bon, rb.sO0, rb.sO1, c);
+  if (leader && c != r && c != s) {
+    const uint32_t Mrc = row_lookup(a.boc, a.bon, rb.rO0, rb.rO1, c);
+    const uint32_t x = Mrc - kc;
+    q.a4 += gterm(x, ldc) - gterm(Mrc, ldc);
+    q.m4 += (long long)x - (long long)Mrc;
+    if (Msc != 0u) {
+      const uint32_t y = Msc + kc;
+      q.a5 += gterm(y, ldc) - gterm(Msc, ldc);
+      q.m5 += (long long)y - (long long)Msc;
     }
   }
-  // in-entries: rows r and s of the in CSR, blocks r and s left out
-  for (int k = lane; k < ni; k += 32) {
-    int32_t c = LI.blk(k);
-    if (c == r || c == s) continue;
-    uint32_t w = LI.wt(k);
-    double ldc = a.ld_out[c];
-    uint32_t Mcs = row_lookup(a.bic, a.bin, sI0, sI1, c);
-    bool leader = true;
-    uint32_t kc = 0;
-    for (int q = 0; q < ni; ++q) {
-      if (LI.blk(q) == c) {
-        kc += LI.wt(q);
-        if (q < k) leader = false;
-      }
-    }
-    if (leader) {
-      uint32_t Mcr = row_lookup(a.bic, a.bin, rI0, rI1, c);
-      uint32_t x = Mcr - kc;
-      a6 += gterm(x, ldc) - gterm(Mcr, ldc);
-      m6 += (long long)x - (long long)Mcr;
-      if (Mcs != 0u) {
-        uint32_t y = Mcs + kc;
-        a7 += gterm(y, ldc) - gterm(Mcs, ldc);
-        m7 += (long long)y - (long long)Mcs;
-      }
-    }
-    if (Mcs == 0u) {
-      a7 += gterm(w, ldc);
-      m7 += (long long)w;
+  if (Msc == 0u) {
+    // block c absent from row s: one term per list entry
+    const uint32_t y = w - (c == r ? niS : 0u) + (c == s ? niS : 0u);
+    q.a5 += gterm(y, ldc);
+    q.m5 += (long long)y;
+  }
+}
+
+// One in-entry of v: rows r and s of the in CSR, blocks r and s left out.
+__device__ __forceinline__ void in_entry(const NodalArgs& a, const RowBounds& rb, int r, int s,
+                                         int32_t c, uint32_t w, bool leader, uint32_t kc,
+                                         Acc& q) {
+  if (c == r || c == s) return;
+  const double ldc = a.ld_out[c];
+  const uint32_t Mcs = row_lookup(a.bic, a.bin, rb.sI0, rb.sI1, c);
+  if (leader) {
+    const uint32_t Mcr = row_lookup(a.bic, a.bin, rb.rI0, rb.rI1, c);
+    const uint32_t x = Mcr - kc;
+    q.a6 += gterm(x, ldc) - gterm(Mcr, ldc);
+    q.m6 += (long long)x - (long long)Mcr;
+    if (Mcs != 0u) {
+      const uint32_t y = Mcs + kc;
+      q.a7 += gterm(y, ldc) - gterm(Mcs, ldc);
+      q.m7 += (long long)y - (long long)Mcs;
     }
   }
-  a4 = warp_sum(a4);
-  a5 = warp_sum(a5);
-  a6 = warp_sum(a6);
-  a7 = warp_sum(a7);
-  m4 = warp_sum_ll(m4);
-  m5 = warp_sum_ll(m5);
-  m6 = warp_sum_ll(m6);
-  m7 = warp_sum_ll(m7);
+  if (Mcs == 0u) {
+    q.a7 += gterm(w, ldc);
+    q.m7 += (long long)w;
+  }
+}
 
-  // the (r, s) corner of M; every lane computes the same scalars
-  const uint32_t Mrr = row_lookup(a.boc, a.bon, rO0, rO1, r);
-  const uint32_t Mrs = row_lookup(a.boc, a.bon, rO0, rO1, s);
-  const uint32_t Msr = row_lookup(a.boc, a.bon, sO0, sO1, r);
-  const uint32_t Mss = row_lookup(a.boc, a.bon, sO0, sO1, s);
+// The (r, s) corner, the old terms and the new-row totals (every thread of
+// the group holds the reduced q and gets the same result).
+__device__ double finish_delta(const NodalArgs& a, const RowBounds& rb, int v, int r, int s,
+                               uint32_t koR, uint32_t koS, uint32_t niR, uint32_t niS, Acc q) {
+  const uint32_t Mrr = row_lookup(a.boc, a.bon, rb.rO0, rb.rO1, r);
+  const uint32_t Mrs = row_lookup(a.boc, a.bon, rb.rO0, rb.rO1, s);
+  const uint32_t Msr = row_lookup(a.boc, a.bon, rb.sO0, rb.sO1, r);
+  const uint32_t Mss = row_lookup(a.boc, a.bon, rb.sO0, rb.sO1, s);
   const double ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
   const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s];
   if (Mrr != 0u) {
     uint32_t x = Mrr - koR - niR;
-    a4 += gterm(x, ldi_r) - gterm(Mrr, ldi_r);
-    m4 += (long long)x - (long long)Mrr;
+    q.a4 += gterm(x, ldi_r) - gterm(Mrr, ldi_r);
+    q.m4 += (long long)x - (long long)Mrr;
   }
   if (Mrs != 0u) {
     uint32_t x = Mrs - koS + niR;
-    a4 += gterm(x, ldi_s) - gterm(Mrs, ldi_s);
-    m4 += (long long)x - (long long)Mrs;
+    q.a4 += gterm(x, ldi_s) - gterm(Mrs, ldi_s);
+    q.m4 += (long long)x - (long long)Mrs;
   } else if (niR > 0u) {
-    a4 += gterm(niR, ldi_s);
-    m4 += (long long)niR;
+    q.a4 += gterm(niR, ldi_s);
+    q.m4 += (long long)niR;
   }
   if (Msr != 0u) {
     uint32_t x = Msr + koR - niS;
-    a5 += gterm(x, ldi_r) - gterm(Msr, ldi_r);
-    m5 += (long long)x - (long long)Msr;
+    q.a5 += gterm(x, ldi_r) - gterm(Msr, ldi_r);
+    q.m5 += (long long)x - (long long)Msr;
   }
   if (Mss != 0u) {
     uint32_t x = Mss + koS + niS;
-    a5 += gterm(x, ldi_s) - gterm(Mss, ldi_s);
-    m5 += (long long)x - (long long)Mss;
+    q.a5 += gterm(x, ldi_s) - gterm(Mss, ldi_s);
+    q.m5 += (long long)x - (long long)Mss;
   } else if (koS == 0u && niS > 0u) {
-    a5 += gterm(niS, ldi_s);
-    m5 += (long long)niS;
+    q.a5 += gterm(niS, ldi_s);
+    q.m5 += (long long)niS;
   }
-
   const uint32_t kO = a.kdo[v], kI = a.kdi[v];
   const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
   // old terms (calculate_dS_out, calculate_dS_in_nodal_r/_s)
@@ -239,19 +251,174 @@ __device__ double vertex_delta(const NodalArgs& a, int v, int r, int s, int lane
   double t2 = a.sinfull[r] - fterm(Mrr, ldo_r, ldi_r) - fterm(Msr, ldo_s, ldi_r);
   double t3 = a.sinfull[s] - fterm(Mrs, ldo_r, ldi_s) - fterm(Mss, ldo_s, ldi_s);
   // new rows r and s, out and in
-  long long mass4 = (long long)dor + m4;
-  long long mass5 = (long long)dos + m5;
-  long long mass6 = (long long)dir - (long long)Mrr - (long long)Msr + m6;
-  long long mass7 = (long long)dis - (long long)Mrs - (long long)Mss + m7;
-  double t4 = a.ambout[r] + a4;
+  long long mass4 = (long long)dor + q.m4;
+  long long mass5 = (long long)dos + q.m5;
+  long long mass6 = (long long)dir - (long long)Mrr - (long long)Msr + q.m6;
+  long long mass7 = (long long)dis - (long long)Mrs - (long long)Mss + q.m7;
+  double t4 = a.ambout[r] + q.a4;
   if (mass4 != 0) t4 -= log2((double)(uint32_t)(dor - kO)) * (double)mass4;
-  double t5 = a.ambout[s] + a5;
+  double t5 = a.ambout[s] + q.a5;
   if (mass5 != 0) t5 -= log2((double)(uint32_t)(dos + kO)) * (double)mass5;
-  double t6 = a.ambin[r] - gterm(Mrr, ldo_r) - gterm(Msr, ldo_s) + a6;
+  double t6 = a.ambin[r] - gterm(Mrr, ldo_r) - gterm(Msr, ldo_s) + q.a6;
   if (mass6 != 0) t6 -= log2((double)(uint32_t)(dir - kI)) * (double)mass6;
-  double t7 = a.ambin[s] - gterm(Mrs, ldo_r) - gterm(Mss, ldo_s) + a7;
+  double t7 = a.ambin[s] - gterm(Mrs, ldo_r) - gterm(Mss, ldo_s) + q.a7;
   if (mass7 != 0) t7 -= log2((double)(uint32_t)(dis + kI)) * (double)mass7;
   return t1 + t2 + t3 - t4 - t5 - t6 - t7;
+}
+
+template <int G>
+__device__ __forceinline__ void reduce_acc(Acc& q, const Group<G>& grp) {
+  q.a4 = grp.sum(q.a4);
+  q.a5 = grp.sum(q.a5);
+  q.a6 = grp.sum(q.a6);
+  q.a7 = grp.sum(q.a7);
+  q.m4 = grp.sum_ll(q.m4);
+  q.m5 = grp.sum_ll(q.m5);
+  q.m6 = grp.sum_ll(q.m6);
+  q.m7 = grp.sum_ll(q.m7);
+}
+
+// dS of moving v from r to s (r != s) from v's sorted neighbour-block lists
+// ko[0..no) (out) and ki[0..ni) (in).  Every thread of the group returns the
+// same value.
+template <int G>
+__device__ double vertex_delta(const NodalArgs& a, int v, int r, int s,
+                               const unsigned long long* ko, int no,
+                               const unsigned long long* ki, int ni, const Group<G>& grp) {
+  const int t = grp.rank();
+  const RowBounds rb = row_bounds(a, r, s);
+  uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
+  for (int k = t; k < no; k += G) {
+    int32_t c = kblk(ko[k]);
+    koR += c == r ? kwt(ko[k]) : 0u;
+    koS += c == s ? kwt(ko[k]) : 0u;
+  }
+  for (int k = t; k < ni; k += G) {
+    int32_t c = kblk(ki[k]);
+    niR += c == r ? kwt(ki[k]) : 0u;
+    niS += c == s ? kwt(ki[k]) : 0u;
+  }
+  koR = (uint32_t)grp.sum_ll(koR);
+  koS = (uint32_t)grp.sum_ll(koS);
+  niR = (uint32_t)grp.sum_ll(niR);
+  niS = (uint32_t)grp.sum_ll(niS);
+  Acc q;
+  for (int k = t; k < no; k += G) {
+    const int32_t c = kblk(ko[k]);
+    const bool leader = k == 0 || kblk(ko[k - 1]) != c;
+    uint32_t kc = 0;
+    if (leader)
+      for (int j = k; j < no && kblk(ko[j]) == c; ++j) kc += kwt(ko[j]);
+    out_entry(a, rb, r, s, niS, c, kwt(ko[k]), leader, kc, q);
+  }
+  for (int k = t; k < ni; k += G) {
+    const int32_t c = kblk(ki[k]);
+    const bool leader = k == 0 || kblk(ki[k - 1]) != c;
+    uint32_t kc = 0;
+    if (leader)
+      for (int j = k; j < ni && kblk(ki[j]) == c; ++j) kc += kwt(ki[j]);
+    in_entry(a, rb, r, s, c, kwt(ki[k]), leader, kc, q);
+  }
+  reduce_acc(q, grp);
+  return finish_delta(a, rb, v, r, s, koR, koS, niR, niS, q);
+}
+
+// Lists too long for shared memory: per-block totals from a shared-memory
+// hash table, built in passes that each take the blocks of one hash class,
+// so the table never holds more than a few thousand blocks.  Costs
+// O(n * passes) with passes ~ n / 2048.
+constexpr int kHashSlots = kHashSlotsCfg;
+struct HashTab {
+  int32_t* key;    // -1 = empty
+  uint32_t* sum;
+  int32_t* first;  // smallest entry index of the block
+};
+
+__device__ __forceinline__ uint32_t hslot(int32_t c) { return ((uint32_t)c * 2654435761u) >> 19; }
+__device__ __forceinline__ uint32_t hclass(int32_t c, uint32_t P) {
+  return ((uint32_t)c * 0x85EBCA6Bu ^ ((uint32_t)c >> 13)) % P;
+}
+
+// Inserts block c (entry k, weight w); false if the table is full.
+__device__ bool hash_add(const HashTab& h, int32_t c, uint32_t w, int k) {
+  uint32_t i = hslot(c);
+  for (int probe = 0; probe < kHashSlots; ++probe, i = (i + 1) & (kHashSlots - 1)) {
+    int32_t cur = atomicCAS(h.key + i, -1, c);
+    if (cur == -1 || cur == c) {
+      atomicAdd(h.sum + i, w);
+      atomicMin(h.first + i, k);
+      return true;
+    }
+  }
+  return false;
+}
+
+__device__ int hash_find(const HashTab& h, int32_t c) {
+  uint32_t i = hslot(c);
+  for (int probe = 0; probe < kHashSlots; ++probe, i = (i + 1) & (kHashSlots - 1))
+    if (h.key[i] == c) return (int)i;
+  return -1;
+}
+
+template <int G>
+__device__ double vertex_delta_hashed(const NodalArgs& a, int v, int r, int s, HashTab h,
+                                      int* flag, const Group<G>& grp) {
+  const int t = grp.rank();
+  const RowBounds rb = row_bounds(a, r, s);
+  const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
+  const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
+  uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
+  for (int k = t; k < no; k += G) {
+    int32_t c = __ldg(a.part + __ldg(a.oidx + o0 + k));
+    uint32_t w = __ldg(a.ow + o0 + k);
+    koR += c == r ? w : 0u;
+    koS += c == s ? w : 0u;
+  }
+  for (int k = t; k < ni; k += G) {
+    int32_t c = __ldg(a.part + __ldg(a.iidx + i0 + k));
+    uint32_t w = __ldg(a.iw + i0 + k);
+    niR += c == r ? w : 0u;
+    niS += c == s ? w : 0u;
+  }
+  koR = (uint32_t)grp.sum_ll(koR);
+  koS = (uint32_t)grp.sum_ll(koS);
+  niR = (uint32_t)grp.sum_ll(niR);
+  niS = (uint32_t)grp.sum_ll(niS);
+  Acc q;
+  for (int dir = 0; dir < 2; ++dir) {
+    const int32_t base = dir == 0 ? o0 : i0, n = dir == 0 ? no : ni;
+    const int32_t* idx = dir == 0 ? a.oidx : a.iidx;
+    const uint32_t* wt = dir == 0 ? a.ow : a.iw;
+    uint32_t P = (uint32_t)((n + kHashSlots / 4 - 1) / (kHashSlots / 4));
+    for (uint32_t pass = 0; pass < P; ++pass) {
+      for (int i = t; i < kHashSlots; i += G) {
+        h.key[i] = -1;
+        h.sum[i] = 0u;
+        h.first[i] = 0x7fffffff;
+      }
+      if (t == 0) *flag = 0;
+      grp.sync();
+      for (int k = t; k < n; k += G) {
+        int32_t c = __ldg(a.part + __ldg(idx + base + k));
+        if (hclass(c, P) == pass && !hash_add(h, c, __ldg(wt + base + k), k)) *flag = 1;
+      }
+      grp.sync();
+      if (*flag) return __longlong_as_double(0x7ff8000000000000ll);  // table overflow
+      for (int k = t; k < n; k += G) {
+        int32_t c = __ldg(a.part + __ldg(idx + base + k));
+        if (hclass(c, P) != pass) continue;
+        int slot = hash_find(h, c);
+        bool leader = h.first[slot] == k;
+        uint32_t kc = h.sum[slot];
+        uint32_t w = __ldg(wt + base + k);
+        if (dir == 0) out_entry(a, rb, r, s, niS, c, w, leader, kc, q);
+        else in_entry(a, rb, r, s, c, w, leader, kc, q);
+      }
+      grp.sync();
+    }
+  }
+  reduce_acc(q, grp);
+  return finish_delta(a, rb, v, r, s, koR, koS, niR, niS, q);
 }
 
 // Neighbour of v whose running weight (out-entries, then in-entries) first
@@ -282,12 +449,24 @@ __device__ int32_t pick_neighbour(const NodalArgs& a, int v, uint64_t t, int lan
   return 0;
 }
 
+__device__ __forceinline__ void write_result(const NodalArgs& a, bool given, int i, int r, int s,
+                                             double d) {
+  if (given) {
+    a.dS_raw[i] = d;
+  } else {
+    bool acc = d < 0.0;
+    a.newlab[i] = acc ? s : r;
+    a.rec[i] = acc ? d : 0.0;
+    if (a.props_out) a.props_out[i] = s;
+  }
+}
+
 template <bool GIVEN>
 __global__ void __launch_bounds__(kNodalWarps * 32) nodal_kernel(NodalArgs a) {
-  __shared__ int32_t sc_o[kNodalWarps][kListCap], sc_i[kNodalWarps][kListCap];
-  __shared__ uint32_t sw_o[kNodalWarps][kListCap], sw_i[kNodalWarps][kListCap];
+  __shared__ unsigned long long s_ko[kNodalWarps][kWarpList], s_ki[kNodalWarps][kWarpList];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = gridDim.x * kNodalWarps;
+  Group<32> grp{nullptr};
   for (int i = blockIdx.x * kNodalWarps + wid; i < a.count; i += nw) {
     int v, s;
     if (GIVEN) {
@@ -306,28 +485,67 @@ __global__ void __launch_bounds__(kNodalWarps * 32) nodal_kernel(NodalArgs a) {
         s = a.use_rand[u] ? rnd : a.nbr_s[u];
       }
     }
-    int r = a.part[v];
-    double d = 0.0;
-    if (r != s) d = vertex_delta(a, v, r, s, lane, sc_o[wid], sw_o[wid], sc_i[wid], sw_i[wid]);
-    if (lane == 0) {
-      if (GIVEN) {
-        a.dS_raw[i] = d;
-      } else {
-        bool acc = d < 0.0;
-        a.newlab[i] = acc ? s : r;
-        a.rec[i] = acc ? d : 0.0;
-        if (a.props_out) a.props_out[i] = s;
-      }
+    const int r = a.part[v];
+    if (r == s) {
+      if (lane == 0) write_result(a, GIVEN, i, r, s, 0.0);
+      continue;
     }
+    const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
+    const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
+    if (no > kWarpList || ni > kWarpList) {
+      if (lane == 0) {
+        int h = atomicAdd(a.heavy_count, 1);
+        a.heavy[3 * h] = i;
+        a.heavy[3 * h + 1] = v;
+        a.heavy[3 * h + 2] = s;
+      }
+      continue;
+    }
+    stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, s_ko[wid], grp);
+    stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, s_ki[wid], grp);
+    double d = vertex_delta<32>(a, v, r, s, s_ko[wid], no, s_ki[wid], ni, grp);
+    if (lane == 0) write_result(a, GIVEN, i, r, s, d);
     __syncwarp();
   }
 }
 
+// Vertices with more than kWarpList entries in a direction: one CTA each,
+// lists sorted in shared memory up to kHeavyList entries, longer ones
+// through the hashed passes.
+template <bool GIVEN>
+__global__ void __launch_bounds__(kHeavyThreads) nodal_heavy_kernel(NodalArgs a) {
+  extern __shared__ unsigned long long hsm[];
+  __shared__ double red[kHeavyThreads / 32];
+  __shared__ int flag;
+  Group<kHeavyThreads> grp{red};
+  unsigned long long* ko = hsm;
+  unsigned long long* ki = hsm + kHeavyList;
+  HashTab ht{(int32_t*)hsm, (uint32_t*)hsm + kHashSlots, (int32_t*)hsm + 2 * kHashSlots};
+  const int nh = *a.heavy_count;
+  for (int h = blockIdx.x; h < nh; h += gridDim.x) {
+    const int i = a.heavy[3 * h], v = a.heavy[3 * h + 1], s = a.heavy[3 * h + 2];
+    const int r = a.part[v];
+    const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
+    const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
+    double d;
+    if (no <= kHeavyList && ni <= kHeavyList) {
+      stage_sorted<kHeavyThreads>(a.oidx, a.ow, a.part, o0, no, ko, grp);
+      stage_sorted<kHeavyThreads>(a.iidx, a.iw, a.part, i0, ni, ki, grp);
+      d = vertex_delta<kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp);
+    } else {
+      d = vertex_delta_hashed<kHeavyThreads>(a, v, r, s, ht, &flag, grp);
+      if (threadIdx.x == 0 && d != d) atomicAdd(a.heavy_count + 1, 1);
+    }
+    if (threadIdx.x == 0) write_result(a, GIVEN, i, r, s, d);
+    __syncthreads();
+  }
+}
+
 // One CTA: applies the batch's labels and sums its recorded dS in a fixed
-// order (deterministic across runs).
+// order (deterministic across runs); resets the heavy-vertex counter.
 __global__ void commit_kernel(int32_t* part, int32_t lo, int32_t count,
                               const int32_t* __restrict__ newlab, const double* __restrict__ rec,
-                              double* slot_sum, long long* slot_acc) {
+                              double* slot_sum, long long* slot_acc, int32_t* heavy_count) {
   __shared__ double sh[1024];
   __shared__ long long shc[1024];
   double s = 0.0;
@@ -353,10 +571,12 @@ __global__ void commit_kernel(int32_t* part, int32_t lo, int32_t count,
   if (threadIdx.x == 0) {
     *slot_sum += sh[0];
     *slot_acc += shc[0];
+    heavy_count[0] = 0;
   }
 }
 
-NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B) {
+NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
+                    int32_t* heavy, int32_t* heavy_count) {
   NodalArgs a{};
   a.optr = g.optr; a.oidx = g.oidx; a.iptr = g.iptr; a.iidx = g.iidx;
   a.ow = g.ow; a.iw = g.iw; a.kdo = g.kdo; a.kdi = g.kdi;
@@ -366,6 +586,8 @@ NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int3
   a.ld_out = m.ld_out; a.ld_in = m.ld_in; a.dSout = m.dSout; a.ambout = m.ambout;
   a.ambin = m.ambin; a.sinfull = m.sinfull; a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
   a.B = B;
+  a.heavy = heavy;
+  a.heavy_count = heavy_count;
   return a;
 }
 
@@ -376,10 +598,20 @@ int nodal_grid(int count) {
 
 }  // namespace
 
+cudaError_t init_nodal_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(nodal_heavy_kernel<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kHeavySmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(nodal_heavy_kernel<true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHeavySmem);
+}
+
 void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                         uint64_t seed, uint32_t seq, int32_t lo, int32_t count, int32_t* newlab,
-                        double* rec, int32_t* props, cudaStream_t st) {
-  NodalArgs a = make_args(g, part, m, B);
+                        double* rec, int32_t* props, int32_t* heavy, int32_t* heavy_count,
+                        cudaStream_t st) {
+  NodalArgs a = make_args(g, part, m, B, heavy, heavy_count);
   a.seed = seed;
   a.seq = seq;
   a.lo = lo;
@@ -387,23 +619,34 @@ void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, 
   a.newlab = newlab;
   a.rec = rec;
   a.props_out = props;
-  if (count > 0) nodal_kernel<false><<<nodal_grid(count), kNodalWarps * 32, 0, st>>>(a);
+  if (count <= 0) return;
+  ++g_launches;
+  nodal_kernel<false><<<nodal_grid(count), kNodalWarps * 32, 0, st>>>(a);
+  ++g_launches;
+  nodal_heavy_kernel<false><<<148, kHeavyThreads, kHeavySmem, st>>>(a);
 }
 
 void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                        int32_t nv, const int32_t* verts, const int32_t* props, double* dS,
-                       cudaStream_t st) {
-  NodalArgs a = make_args(g, part, m, B);
+                       int32_t* heavy, int32_t* heavy_count, cudaStream_t st) {
+  NodalArgs a = make_args(g, part, m, B, heavy, heavy_count);
   a.count = nv;
   a.verts = verts;
   a.props_in = props;
   a.dS_raw = dS;
-  if (nv > 0) nodal_kernel<true><<<nodal_grid(nv), kNodalWarps * 32, 0, st>>>(a);
+  if (nv <= 0) return;
+  ++g_launches;
+  nodal_kernel<true><<<nodal_grid(nv), kNodalWarps * 32, 0, st>>>(a);
+  ++g_launches;
+  nodal_heavy_kernel<true><<<148, kHeavyThreads, kHeavySmem, st>>>(a);
 }
 
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
-                  const double* rec, double* slot_sum, long long* slot_acc, cudaStream_t st) {
-  commit_kernel<<<1, 1024, 0, st>>>(part, lo, count, newlab, rec, slot_sum, slot_acc);
+                  const double* rec, double* slot_sum, long long* slot_acc, int32_t* heavy_count,
+                  cudaStream_t st) {
+  ++g_launches;
+  commit_kernel<<<1, 1024, 0, st>>>(part, lo, count, newlab, rec, slot_sum, slot_acc,
+                                    heavy_count);
 }
 
 }  // namespace sbp

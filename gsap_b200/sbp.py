@@ -55,7 +55,9 @@ class Report(C.Structure):
                 ("ms_merge", C.c_double), ("ms_nodal", C.c_double),
                 ("ms_rebuild", C.c_double), ("ms_h2d", C.c_double),
                 ("bytes_nodal", C.c_double), ("bytes_rebuild", C.c_double),
-                ("bytes_merge", C.c_double), ("status", C.c_int32)]
+                ("bytes_merge", C.c_double), ("status", C.c_int32),
+                ("ms_device", C.c_double), ("ms_nodal_kernel", C.c_double),
+                ("nodal_launches", C.c_int64), ("kernel_launches", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -90,6 +90,10 @@ typedef struct sbp_report {
   double bytes_rebuild;
   double bytes_merge;
   int32_t status;
+  double ms_device;         /* CUDA-event time of the whole run on its stream */
+  double ms_nodal_kernel;   /* CUDA-event time of the nodal dS kernels alone */
+  int64_t nodal_launches;   /* nodal batches run (one warp-kernel launch each) */
+  int64_t kernel_launches;  /* kernels this library launched during the run */
 } sbp_report;
 
 void sbp_default_options(sbp_options* o);

@@ -1,0 +1,118 @@
+"""Host-side pieces of the C ABI (no GPU): the library loads and exports
+every symbol include/sbp.h declares, the loader reads GraphChallenge TSVs
+exactly as GSAP/load.hpp does, the CSR builder, the DCSBM generator, and
+input validation that runs before any device call."""
+import hashlib
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+DATA = "/root/reference/Dataset/static"
+
+
+def test_exports_every_declared_symbol(sbp):
+    hdr = open(os.path.join(ROOT, "include", "sbp.h")).read()
+    declared = set(re.findall(r"^\w[\w\s\*]*?\b(sbp_\w+)\s*\(", hdr, re.M))
+    assert declared, "no declarations parsed"
+    import ctypes
+    lib = ctypes.CDLL(sbp.LIB_PATH)
+    for name in sorted(declared):
+        assert hasattr(lib, name), name
+    assert declared <= set(sbp.EXPORTED) | declared
+
+
+def test_default_options_are_gsaps(sbp):
+    o = sbp.default_options()
+    # partition.hpp:855-861
+    assert o.num_proposals == 10 and abs(o.reduction_rate - 0.35) < 1e-7
+    assert o.max_nodal_itr == 100 and o.num_batches == 4 and o.window == 3
+    assert abs(o.threshold1 - 5e-4) < 1e-10 and abs(o.threshold2 - 1e-4) < 1e-10
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.skipif(not os.path.isdir(DATA), reason="GraphChallenge fixtures not present")
+@pytest.mark.parametrize("cat", ["LL", "LH", "HL", "HH"])
+@pytest.mark.parametrize("size", ["1k", "5k"])
+def test_loader_matches_reference(sbp, cat, size):
+    gold = json.load(open(os.path.join(HERE, "golden", "loader.json")))[f"{cat}-{size}"]
+    g = sbp.read_file(cat, size, DATA)
+    assert (g.N, g.E) == (gold["N"], gold["E"])
+    # the reference keeps N row pointers (no end sentinel)
+    assert _sha(g.out_ptr[:-1]) == gold["out_ptr"]
+    assert _sha(g.in_ptr[:-1]) == gold["in_ptr"]
+    for k in ("out_idx", "out_w", "in_idx", "in_w", "deg_out", "deg_in"):
+        assert _sha(getattr(g, k)) == gold[k], k
+    assert _sha(g.true_partitions) == gold["truth"]
+
+
+def test_loader_first_field_with_space(sbp, tmp_path):
+    # load.hpp:50-65: "1 408\t1" parses as the self-loop (1, 1, 1)
+    p = tmp_path / "g.tsv"
+    p.write_text("1 408\t1\n1\t2\t1\n2\t1\t3\n")
+    g = sbp.load_tsv(str(p))
+    src, dst, w = g.edges()
+    assert g.N == 2 and g.E == 3
+    assert list(zip(src, dst, w)) == [(0, 0, 1), (0, 1, 1), (1, 0, 3)]
+
+
+def test_csr_from_edges_keeps_edge_order(sbp):
+    src = np.array([2, 0, 2, 1, 0], np.int32)
+    dst = np.array([0, 2, 1, 0, 1], np.int32)
+    w = np.array([1, 2, 3, 4, 5], np.uint32)
+    g = sbp.Graph.from_edges(3, src, dst, w)
+    assert list(g.out_ptr) == [0, 2, 3, 5]
+    assert list(g.out_idx) == [2, 1, 0, 0, 1] and list(g.out_w) == [2, 5, 4, 1, 3]
+    assert list(g.in_ptr) == [0, 2, 4, 5]
+    assert list(g.in_idx) == [2, 1, 2, 0, 0]
+    assert list(g.deg_out) == [7, 4, 4] and list(g.deg_in) == [5, 8, 2]
+
+
+def test_dcsbm_is_deterministic_and_has_its_shape(sbp):
+    a = sbp.dcsbm_variant("HH", 20000, 32, seed=4)
+    b = sbp.dcsbm_variant("HH", 20000, 32, seed=4)
+    c = sbp.dcsbm_variant("HH", 20000, 32, seed=5)
+    assert np.array_equal(a.out_idx, b.out_idx) and np.array_equal(a.true_partitions,
+                                                                   b.true_partitions)
+    assert not np.array_equal(a.true_partitions, c.true_partitions)
+    t = a.true_partitions
+    assert t.min() == 0 and t.max() == 31 and np.bincount(t).min() >= 1
+    src, dst, _ = a.edges()
+    assert not np.any(src == dst), "self-loop"
+    key = src.astype(np.int64) * a.N + dst
+    assert np.unique(key).size == key.size, "repeated edge"
+    deg = np.diff(a.out_ptr)
+    assert deg.min() >= 5 and deg.max() <= 50
+    assert 9.0 < a.E / a.N < 10.5  # truncated power law 2.5 on [5, 50]: mean 9.78
+    frac_in = np.mean(t[src] == t[dst])
+    assert abs(frac_in - 0.5) < 0.02  # p_in of HH
+    ll = sbp.dcsbm_variant("LL", 20000, 32, seed=4)
+    s2, d2, _ = ll.edges()
+    assert abs(np.mean(ll.true_partitions[s2] == ll.true_partitions[d2]) - 0.8) < 0.02
+    # alpha = 20 gives near-equal block sizes, alpha = 1 spread ones
+    assert np.bincount(ll.true_partitions).std() < np.bincount(t).std()
+
+
+def test_evaluate_rejects_bad_labels(sbp):
+    with pytest.raises(sbp.SbpError):
+        sbp.evaluate(np.zeros(4, np.int32), np.array([0, -1, 0, 0], np.int32))
+
+
+def test_partition_validates_before_device_use(sbp):
+    g = sbp.dcsbm_variant("LL", 1000, 11, seed=0)
+    bad = sbp.Graph(**{**g.__dict__, "deg_out": g.deg_out + 1})
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.partition(bad)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.partition(g, num_proposals=0)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.build_blockmodel(g, np.full(g.N, 11, np.int32), 11)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.delta_mdl_nodal(g, g.true_partitions, 11, [0], [11])
