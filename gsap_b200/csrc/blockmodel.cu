@@ -454,6 +454,174 @@ __global__ void block_terms_kernel(BtArgs a) {
   }
 }
 
+
+// ------------------------------------------------------------ dense form --
+// For small B the blockmodel is kept as two B x B count matrices (rows and
+// columns of M both contiguous).  Built once per merge step / golden-section
+// restore; after each nodal batch only the edges of the moved vertices are
+// applied, with integer atomics (exact, order-independent).
+
+__global__ void dense_edges_kernel(const int32_t* __restrict__ osrc,
+                                   const int32_t* __restrict__ oidx,
+                                   const uint32_t* __restrict__ ow,
+                                   const int32_t* __restrict__ part, int32_t E, int32_t B,
+                                   uint32_t* Md, uint32_t* MTd) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= E) return;
+  int r = __ldg(part + __ldg(osrc + j)), c = __ldg(part + __ldg(oidx + j));
+  uint32_t w = __ldg(ow + j);
+  atomicAdd(Md + (size_t)r * B + c, w);
+  atomicAdd(MTd + (size_t)c * B + r, w);
+}
+
+__global__ void dense_degrees_kernel(const int32_t* __restrict__ part,
+                                     const uint32_t* __restrict__ kdo,
+                                     const uint32_t* __restrict__ kdi, int32_t N,
+                                     uint32_t* d_out, uint32_t* d_in) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  int b = part[v];
+  atomicAdd(d_out + b, kdo[v]);
+  atomicAdd(d_in + b, kdi[v]);
+}
+
+__global__ void dense_logs_kernel(const uint32_t* __restrict__ d_out,
+                                  const uint32_t* __restrict__ d_in, int32_t B, double* ld_out,
+                                  double* ld_in) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  ld_out[b] = log2((double)d_out[b]);
+  ld_in[b] = log2((double)d_in[b]);
+}
+
+// One warp per batch vertex that moves: its out-edges move from
+// (r, old block of w) to (s, new block of w); its in-edges from unmoved
+// sources move from (b(u), r) to (b(u), s).  Edges between two moved vertices
+// are handled once, from the source's out-edges.
+__global__ void dense_update_kernel(const int32_t* __restrict__ optr,
+                                    const int32_t* __restrict__ oidx,
+                                    const uint32_t* __restrict__ ow,
+                                    const int32_t* __restrict__ iptr,
+                                    const int32_t* __restrict__ iidx,
+                                    const uint32_t* __restrict__ iw,
+                                    const uint32_t* __restrict__ kdo,
+                                    const uint32_t* __restrict__ kdi,
+                                    const int32_t* __restrict__ part, int32_t lo, int32_t count,
+                                    const int32_t* __restrict__ newlab, int32_t B, uint32_t* Md,
+                                    uint32_t* MTd, uint32_t* d_out, uint32_t* d_in) {
+  const int lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = w0; i < count; i += nw) {
+    const int v = lo + i;
+    const int r = part[v], s = newlab[i];
+    if (r == s) continue;
+    if (lane == 0) {
+      atomicSub(d_out + r, kdo[v]);
+      atomicAdd(d_out + s, kdo[v]);
+      atomicSub(d_in + r, kdi[v]);
+      atomicAdd(d_in + s, kdi[v]);
+    }
+    for (int j = optr[v] + lane; j < optr[v + 1]; j += 32) {
+      const int x = __ldg(oidx + j);
+      const uint32_t wt = __ldg(ow + j);
+      const int bo = __ldg(part + x);
+      const int bn = (x >= lo && x < lo + count) ? newlab[x - lo] : bo;
+      atomicSub(Md + (size_t)r * B + bo, wt);
+      atomicSub(MTd + (size_t)bo * B + r, wt);
+      atomicAdd(Md + (size_t)s * B + bn, wt);
+      atomicAdd(MTd + (size_t)bn * B + s, wt);
+    }
+    for (int j = iptr[v] + lane; j < iptr[v + 1]; j += 32) {
+      const int u = __ldg(iidx + j);
+      const int bu = __ldg(part + u);
+      if (u >= lo && u < lo + count && newlab[u - lo] != bu) continue;  // moved source
+      const uint32_t wt = __ldg(iw + j);
+      atomicSub(Md + (size_t)bu * B + r, wt);
+      atomicSub(MTd + (size_t)r * B + bu, wt);
+      atomicAdd(Md + (size_t)bu * B + s, wt);
+      atomicAdd(MTd + (size_t)s * B + bu, wt);
+    }
+  }
+}
+
+// First column k of dense out-row ++ in-row of block b whose running count
+// exceeds t (zero columns never advance the count, so this is the same
+// entry as in the CSR rows); the whole warp returns it, or -1.
+__device__ int warp_pick_dense(const uint32_t* orow, const uint32_t* irow, int B, uint64_t t,
+                               int lane) {
+  uint64_t acc = 0;
+  for (int k0 = 0; k0 < 2 * B; k0 += 32) {
+    int k = k0 + lane;
+    uint64_t w = 0;
+    if (k < 2 * B) w = k < B ? orow[k] : irow[k - B];
+    uint64_t incl = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    unsigned hit = __ballot_sync(kFull, k < 2 * B && acc + incl > t);
+    if (hit) {
+      int kk = k0 + __ffs(hit) - 1;
+      return kk < B ? kk : kk - B;
+    }
+    acc += __shfl_sync(kFull, incl, 31);
+  }
+  return -1;
+}
+
+struct BtDenseArgs {
+  const uint32_t *Md, *MTd, *d_out, *d_in;
+  const double *ld_out, *ld_in;
+  double *dSout, *ambout, *ambin, *sinfull;
+  int32_t* nbr_s;
+  uint8_t* use_rand;
+  int32_t B;
+  int draws;
+  uint64_t seed;
+  uint32_t seq;
+};
+
+__global__ void block_terms_dense_kernel(BtDenseArgs a) {
+  int lane = threadIdx.x & 31;
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int nw = (gridDim.x * blockDim.x) >> 5;
+  const int B = a.B;
+  for (int b = w; b < B; b += nw) {
+    const uint32_t* orow = a.Md + (size_t)b * B;
+    const uint32_t* irow = a.MTd + (size_t)b * B;
+    double ao = 0.0, ai = 0.0;
+    for (int c = lane; c < B; c += 32) {
+      uint32_t mo = orow[c], mi = irow[c];
+      if (mo) ao += xlog2x(mo) - (double)mo * a.ld_in[c];
+      if (mi) ai += xlog2x(mi) - (double)mi * a.ld_out[c];
+    }
+    ao = warp_sum(ao);
+    ai = warp_sum(ai);
+    if (lane == 0) {
+      uint32_t dout = a.d_out[b], din = a.d_in[b];
+      a.ambout[b] = ao;
+      a.dSout[b] = ao - (dout ? (double)dout * a.ld_out[b] : 0.0);
+      a.ambin[b] = ai;
+      a.sinfull[b] = ai - (din ? (double)din * a.ld_in[b] : 0.0);
+    }
+    if (a.draws) {
+      P4 x = draw(a.seed, kRngNodalBlock, a.seq, (uint32_t)b);
+      uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
+      int nb = 0;
+      if (deg > 0) {
+        int c = warp_pick_dense(orow, irow, B, scale_draw(x.v[1], deg), lane);
+        nb = c >= 0 ? c : 0;
+      }
+      if (lane == 0) {
+        a.use_rand[b] = accept_random(x.v[0], deg, (uint64_t)B) ? 1 : 0;
+        a.nbr_s[b] = nb;
+      }
+    }
+  }
+}
+
 __global__ void mdl_sum_kernel(const double* __restrict__ dSout, int32_t B, double* out) {
   __shared__ double sh[1024];
   double s = 0.0;
@@ -557,6 +725,45 @@ void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cu
   a.B = B; a.draws = draws; a.seed = seed; a.seq = seq;
   ++g_launches;
   block_terms_kernel<<<grid_for((long long)B * 32, 256, 8192), 256, 0, st>>>(a);
+}
+
+void dense_build(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, cudaStream_t st) {
+  size_t bb = (size_t)B * B;
+  cudaMemsetAsync(m.Md, 0, bb * sizeof(uint32_t), st);
+  cudaMemsetAsync(m.MTd, 0, bb * sizeof(uint32_t), st);
+  cudaMemsetAsync(m.d_out, 0, (size_t)B * sizeof(uint32_t), st);
+  cudaMemsetAsync(m.d_in, 0, (size_t)B * sizeof(uint32_t), st);
+  if (g.E > 0) {
+    ++g_launches;
+    dense_edges_kernel<<<(g.E + 255) / 256, 256, 0, st>>>(g.osrc, g.oidx, g.ow, part, g.E, B,
+                                                          m.Md, m.MTd);
+  }
+  ++g_launches;
+  dense_degrees_kernel<<<(g.N + 255) / 256, 256, 0, st>>>(part, g.kdo, g.kdi, g.N, m.d_out,
+                                                          m.d_in);
+  ++g_launches;
+  dense_logs_kernel<<<(B + 255) / 256, 256, 0, st>>>(m.d_out, m.d_in, B, m.ld_out, m.ld_in);
+}
+
+void dense_update(const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
+                  const int32_t* newlab, int32_t B, DevBM& m, cudaStream_t st) {
+  if (count <= 0) return;
+  ++g_launches;
+  dense_update_kernel<<<grid_for((long long)count * 32, 256, 148 * 16), 256, 0, st>>>(
+      g.optr, g.oidx, g.ow, g.iptr, g.iidx, g.iw, g.kdo, g.kdi, part, lo, count, newlab, B, m.Md,
+      m.MTd, m.d_out, m.d_in);
+}
+
+void block_terms_dense(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq,
+                       cudaStream_t st) {
+  BtDenseArgs a;
+  a.Md = m.Md; a.MTd = m.MTd; a.d_out = m.d_out; a.d_in = m.d_in;
+  a.ld_out = m.ld_out; a.ld_in = m.ld_in;
+  a.dSout = m.dSout; a.ambout = m.ambout; a.ambin = m.ambin; a.sinfull = m.sinfull;
+  a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
+  a.B = B; a.draws = draws; a.seed = seed; a.seq = seq;
+  ++g_launches;
+  block_terms_dense_kernel<<<grid_for((long long)B * 32, 256, 8192), 256, 0, st>>>(a);
 }
 
 void mdl_data_sum(const DevBM& m, int32_t B, double* out, cudaStream_t st) {

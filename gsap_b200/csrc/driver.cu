@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <mutex>
@@ -115,8 +116,12 @@ struct Job {
   int32_t *part = nullptr, *newlab = nullptr, *props = nullptr, *best = nullptr, *map = nullptr;
   int32_t* snap[3] = {nullptr, nullptr, nullptr};
   double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
-  int32_t* heavy = nullptr;     // vertices handed to the CTA-per-vertex kernel
-  int32_t* heavy_count = nullptr;  // [queue length, error count]
+  int32_t* heavy = nullptr;     // batch indices of the CTA-per-vertex kernel
+  int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
+  int32_t dense_cap = 0;        // largest B the dense arrays can hold
+  int32_t dense_eff = 0;        // largest B kept in dense form in this run
+  cudaStream_t side = nullptr;  // heavy vertices run here, next to the warp kernel
+  cudaEvent_t fork = nullptr, join = nullptr;
   double* dsum = nullptr;       // per nodal iteration: sum of recorded dS
   double* dataS = nullptr;      // per nodal iteration: MDL data term
   long long* acc = nullptr;     // per nodal iteration: applied moves
@@ -144,6 +149,11 @@ struct Job {
         if (e) cudaEventDestroy(e), e = nullptr;
       for (auto& e : bev) cudaEventDestroy(e);
       bev.clear();
+      if (fork) cudaEventDestroy(fork);
+      if (join) cudaEventDestroy(join);
+      fork = join = nullptr;
+      if (side) cudaStreamDestroy(side);
+      side = nullptr;
       if (st) cudaStreamDestroy(st);
       cudaFreeHost(h_best);
       cudaFreeHost(h_best_dS);
@@ -158,7 +168,8 @@ struct Job {
   }
 };
 
-static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t tiles) {
+static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t tiles,
+                        int32_t dense_cap) {
   size_t n1 = (size_t)N + 1, e = (size_t)E > 0 ? (size_t)E : 1;
   size_t b = 0;
   auto add = [&](size_t elems, size_t sz) { b += ((elems * sz) + 255) & ~size_t(255); };
@@ -184,13 +195,16 @@ static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32
   add((size_t)N * np, 8);
   add(N, 8);
   add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
-  add((size_t)3 * N, 4); add(2, 4);
+  add((size_t)N, 4); add(2, 4);
+  add((size_t)dense_cap * dense_cap, 4); add((size_t)dense_cap * dense_cap, 4);
   return b + 4096;
 }
 
 static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np,
-                             int32_t max_itr) {
+                             int32_t max_itr, int32_t dense_max) {
   J.device = device;
+  J.dense_cap = std::max(0, std::min(N, dense_max));
+  J.dense_eff = J.dense_cap;
   J.N = N;
   J.E = E;
   J.np = np;
@@ -203,13 +217,16 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
       init_nodal_attributes();
     });
   int32_t tiles = 2 * (2 * ((N + 1) / 2048 + 2) + 2);
-  J.mem_bytes = job_bytes(N, E, np, max_itr, tiles);
+  J.mem_bytes = job_bytes(N, E, np, max_itr, tiles, J.dense_cap);
   if (cudaMalloc(&J.mem, J.mem_bytes) != cudaSuccess) {
     cudaGetLastError();
     J.mem = nullptr;
     return fail(SBP_ERR_NOMEM, "device arena of " + std::to_string(J.mem_bytes) + " bytes");
   }
   SBP_CUDA(cudaStreamCreateWithFlags(&J.st, cudaStreamNonBlocking));
+  SBP_CUDA(cudaStreamCreateWithFlags(&J.side, cudaStreamNonBlocking));
+  SBP_CUDA(cudaEventCreateWithFlags(&J.fork, cudaEventDisableTiming));
+  SBP_CUDA(cudaEventCreateWithFlags(&J.join, cudaEventDisableTiming));
   for (auto& e : J.ev) SBP_CUDA(cudaEventCreate(&e));
   SBP_CUDA(cudaMallocHost(&J.h_best, sizeof(int32_t) * (size_t)N));
   SBP_CUDA(cudaMallocHost(&J.h_best_dS, sizeof(double) * (size_t)N));
@@ -256,10 +273,14 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
   J.dsum = A.take<double>(max_itr);
   J.dataS = A.take<double>(max_itr);
   J.acc = (long long*)A.take<double>(max_itr);
-  J.heavy = A.take<int32_t>((size_t)3 * N);
-  J.heavy_count = A.take<int32_t>(2);
-  if (!J.heavy_count) return fail(SBP_ERR_INTERNAL, "arena sizing");
-  SBP_CUDA(cudaMemsetAsync(J.heavy_count, 0, 8, J.st));
+  J.heavy = A.take<int32_t>((size_t)N);
+  J.err = A.take<int32_t>(2);
+  if (J.dense_cap > 0) {
+    m.Md = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
+    m.MTd = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
+  }
+  if (!J.err || (J.dense_cap > 0 && !m.MTd)) return fail(SBP_ERR_INTERNAL, "arena sizing");
+  SBP_CUDA(cudaMemsetAsync(J.err, 0, 8, J.st));
   return SBP_OK;
 }
 
@@ -374,9 +395,42 @@ struct Timer {
   }
 };
 
+static bool is_dense(const Job& J, int32_t B) { return B <= J.dense_eff; }
+
+// The blockmodel of the current labels, in the form used at this B: dense
+// B x B matrices for small B, the CSR pair otherwise.
+static void build_model(Job& J, int32_t B, cudaStream_t st) {
+  if (is_dense(J, B)) dense_build(J.g, J.part, B, J.m, st);
+  else rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+}
+
+static void block_terms_any(Job& J, int32_t B, int draws, uint64_t seed, uint32_t seq,
+                            cudaStream_t st) {
+  if (is_dense(J, B)) block_terms_dense(J.m, B, draws, seed, seq, st);
+  else block_terms(J.m, B, draws, seed, seq, st);
+}
+
+static bool heavy_vertex(const Job& J, int32_t v) {
+  const int32_t t = nodal_heavy_threshold();
+  return J.h_optr[v + 1] - J.h_optr[v] > t || J.h_iptr[v + 1] - J.h_iptr[v] > t;
+}
+
+static NodalAux aux_for(Job& J, const int32_t* heavy, int32_t n) {
+  NodalAux a;
+  a.heavy = heavy;
+  a.nheavy = n;
+  a.err = J.err;
+  a.side = J.side;
+  a.fork = J.fork;
+  a.join = J.join;
+  return a;
+}
+
 static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t seed, uint32_t seq,
                              bool keep_dS) {
   cudaStream_t st = J.st;
+  // the merge kernels read the CSR form, stale after dense nodal sweeps
+  if (is_dense(J, B)) rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
   block_terms(J.m, B, 0, seed, 0, st);
   merge_proposals(J.m, B, J.np, seed, seq, J.props, st);
   merge_delta(J.m, B, J.np, J.props, keep_dS ? J.mdS : nullptr, J.best, J.best_dS, st);
@@ -408,9 +462,10 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
   SBP_CUDA(cudaEventRecord(J.ev[3], st));
   ++g_launches;
   iota_kernel<<<(N + 255) / 256, 256, 0, st>>>(J.part, N);
+  J.dense_eff = std::min(J.dense_cap, std::max(0, o.dense_max));
   int32_t B = N;
   int32_t B_to_merge = (int32_t)((float)B * o.reduction_rate);
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+  build_model(J, B, st);
   uint32_t seq = 0;
   Bracket large, med, small;
   // three snapshot buffers of labels; each bracket point owns one
@@ -423,10 +478,18 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
   // per adjacency entry (either direction) 12, plus the blockmodel rows
   // (16 per nonzero) and 8 per block
   std::vector<double> batch_entries(o.num_batches, 0.0);
+  // heavy vertices of each batch (static: they depend on degrees only)
+  std::vector<int32_t> heavy_all, heavy_off(o.num_batches + 1, 0);
   for (int32_t b = 0; b < o.num_batches; ++b) {
-    int32_t lo = b * (N / o.num_batches), hi = (b + 1) * (N / o.num_batches);
+    int32_t lo = b * BS, hi = (b + 1) * BS;
     batch_entries[b] = (double)(J.h_optr[hi] - J.h_optr[lo]) + (double)(J.h_iptr[hi] - J.h_iptr[lo]);
+    for (int32_t v = lo; v < hi; ++v)
+      if (heavy_vertex(J, v)) heavy_all.push_back(v - lo);
+    heavy_off[b + 1] = (int32_t)heavy_all.size();
   }
+  if (!heavy_all.empty())
+    SBP_CUDA(cudaMemcpyAsync(J.heavy, heavy_all.data(), 4 * heavy_all.size(),
+                             cudaMemcpyHostToDevice, st));
   double nnz_now = (double)E;
   while ((int)J.bev.size() < 4 * o.num_batches + 1) {
     cudaEvent_t e;
@@ -444,8 +507,10 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
     sbp_status s = merge_step(J, B, B_to_merge, o.seed, seq++, false);
     if (s != SBP_OK) return s;
     SBP_CUDA(cudaEventRecord(J.ev[1], st));
-    rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+    build_model(J, B, st);
     SBP_CUDA(cudaEventRecord(J.ev[2], st));
+    const bool dense = is_dense(J, B);
+    if (dense) nnz_now = std::min((double)E, (double)B * B);
     // nodal phase (partition.hpp:906-935)
     std::fill(itr_dS.begin(), itr_dS.end(), 0.0);
     SBP_CUDA(cudaMemsetAsync(J.dsum, 0, sizeof(double) * o.max_nodal_itr, st));
@@ -461,34 +526,44 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
       // bev[4b+4] after the rebuild; read at the sweep's one synchronisation
       SBP_CUDA(cudaEventRecord(J.bev[0], st));
       for (int32_t b = 0; b < o.num_batches; ++b) {
-        block_terms(J.m, B, 1, o.seed, seq, st);
+        block_terms_any(J, B, 1, o.seed, seq, st);
         SBP_CUDA(cudaEventRecord(J.bev[4 * b + 1], st));
-        nodal_batch_sample(J.g, J.part, J.m, B, o.seed, seq, b * BS, BS, J.newlab, J.rec, nullptr,
-                           J.heavy, J.heavy_count, st);
+        NodalAux aux = aux_for(J, J.heavy + heavy_off[b], heavy_off[b + 1] - heavy_off[b]);
+        nodal_batch_sample(J.g, J.part, J.m, B, dense, o.seed, seq, b * BS, BS, J.newlab, J.rec,
+                           nullptr, aux, st);
         SBP_CUDA(cudaEventRecord(J.bev[4 * b + 2], st));
-        nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr,
-                     J.heavy_count, st);
+        if (dense) {
+          // the moved vertices' edges, applied to the dense form before the
+          // labels change (it reads old and new labels)
+          dense_update(J.g, J.part, b * BS, BS, J.newlab, B, J.m, st);
+          nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, &J.m, B,
+                       st);
+        } else {
+          nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, nullptr,
+                       0, st);
+        }
         ++seq;
         SBP_CUDA(cudaEventRecord(J.bev[4 * b + 3], st));
-        rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+        if (!dense) rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
         SBP_CUDA(cudaEventRecord(J.bev[4 * b + 4], st));
         R.nodal_proposals += BS;
         R.nodal_launches += 1;
         R.bytes_nodal += 28.0 * BS + 12.0 * batch_entries[b] + 16.0 * nnz_now + 8.0 * B;
-        R.bytes_rebuild += 4.0 * N + 24.0 * E + 16.0 * nnz_now + 8.0 * B;
+        R.bytes_rebuild += dense ? 12.0 * batch_entries[b] + 8.0 * (double)B * B
+                                 : 4.0 * N + 24.0 * E + 16.0 * nnz_now + 8.0 * B;
       }
-      block_terms(J.m, B, 0, o.seed, 0, st);
+      block_terms_any(J, B, 0, o.seed, 0, st);
       mdl_data_sum(J.m, B, J.dataS + itr, st);
       SBP_CUDA(cudaMemcpyAsync(J.h_scal, J.dsum + itr, 8, cudaMemcpyDeviceToHost, st));
       SBP_CUDA(cudaMemcpyAsync(J.h_scal + 1, J.dataS + itr, 8, cudaMemcpyDeviceToHost, st));
       SBP_CUDA(cudaMemcpyAsync(J.h_acc, J.acc + itr, 8, cudaMemcpyDeviceToHost, st));
-      SBP_CUDA(cudaMemcpyAsync(J.h_misc, J.heavy_count + 1, 4, cudaMemcpyDeviceToHost, st));
+      SBP_CUDA(cudaMemcpyAsync(J.h_misc, J.err, 4, cudaMemcpyDeviceToHost, st));
       SBP_CUDA(cudaMemcpyAsync(J.h_misc + 1, J.m.optr + B, 4, cudaMemcpyDeviceToHost, st));
       SBP_CUDA(cudaStreamSynchronize(st));
       SBP_CUDA(cudaGetLastError());
       if (J.h_misc[0] != 0)
         return fail(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
-      nnz_now = (double)J.h_misc[1];
+      if (!dense) nnz_now = (double)J.h_misc[1];
       for (int32_t b = 0; b < o.num_batches; ++b) {
         SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[4 * b], J.bev[4 * b + 3]));
         R.ms_nodal += ms;
@@ -567,7 +642,7 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
     B = restore->B;
     S = restore->S;
     SBP_CUDA(cudaEventRecord(J.ev[0], st));
-    rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+    build_model(J, B, st);
     SBP_CUDA(cudaEventRecord(J.ev[1], st));
     SBP_CUDA(cudaEventSynchronize(J.ev[1]));
     SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[0], J.ev[1]));
@@ -590,10 +665,16 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
 }
 
 // A job with the graph uploaded, for the one-shot entry points.
-static sbp_status job_for(Job& J, const sbp_graph_csr* g, int device, int32_t np, int32_t max_itr) {
+static int32_t env_dense_max() {
+  const char* e = std::getenv("SBP_DENSE_MAX");
+  return e ? std::atoi(e) : 4096;
+}
+
+static sbp_status job_for(Job& J, const sbp_graph_csr* g, int device, int32_t np, int32_t max_itr,
+                          int32_t dense_max) {
   sbp_status s = validate_graph(g);
   if (s != SBP_OK) return s;
-  s = job_create(J, resolve_device(device), g->N, g->E, np, max_itr);
+  s = job_create(J, resolve_device(device), g->N, g->E, np, max_itr, dense_max);
   if (s != SBP_OK) return s;
   return job_upload(J, g);
 }
@@ -606,12 +687,13 @@ static sbp_status prepare(Job& J, const sbp_graph_csr* g, const int32_t* part, i
   if (s != SBP_OK) return s;
   s = validate_part(part, g->N, B);
   if (s != SBP_OK) return s;
-  s = job_create(J, resolve_device(-1), g->N, g->E, np, max_itr);
+  s = job_create(J, resolve_device(-1), g->N, g->E, np, max_itr, env_dense_max());
   if (s != SBP_OK) return s;
   s = job_upload(J, g);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, J.st));
   rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  if (is_dense(J, B)) dense_build(J.g, J.part, B, J.m, J.st);
   return SBP_OK;
 }
 
@@ -641,6 +723,7 @@ void sbp_default_options(sbp_options* o) {
   o->device = -1;
   o->use_graphs = 0;
   o->verbose = 0;
+  o->dense_max = 4096;
 }
 
 const char* sbp_status_string(sbp_status s) {
@@ -677,7 +760,7 @@ sbp_status sbp_graph_upload(const sbp_graph_csr* g, int32_t device, sbp_graph_de
   *out = nullptr;
   sbp_graph_dev* h = new (std::nothrow) sbp_graph_dev();
   if (!h) return fail(SBP_ERR_NOMEM, "host allocation");
-  sbp_status s = job_for(h->job, g, device, 10, 100);
+  sbp_status s = job_for(h->job, g, device, 10, 100, 4096);
   if (s != SBP_OK) {
     delete h;
     return s;
@@ -703,13 +786,15 @@ sbp_status sbp_partition_resident(sbp_graph_dev* gd, const sbp_options* o, int32
   sbp_status s = check_options(o);
   if (s != SBP_OK) return s;
   Job& J = gd->job;
-  if (o->num_proposals > J.np || o->max_nodal_itr > J.max_itr) {
+  const int32_t want_dense = std::min(gd->shape.N, std::max(0, o->dense_max));
+  if (o->num_proposals > J.np || o->max_nodal_itr > J.max_itr || want_dense > J.dense_cap) {
     // grow the job's arena for these options; the graph is uploaded again
     int dev = J.device;
+    int32_t np = std::max(o->num_proposals, J.np), mi = std::max(o->max_nodal_itr, J.max_itr);
+    int32_t dm = std::max(want_dense, J.dense_cap);
     J.release();
     J.bev.clear();
-    s = job_for(J, &gd->shape, dev, std::max(o->num_proposals, J.np),
-                std::max(o->max_nodal_itr, J.max_itr));
+    s = job_for(J, &gd->shape, dev, np, mi, dm);
     if (s != SBP_OK) return s;
   }
   SBP_CUDA(cudaSetDevice(J.device));
@@ -722,7 +807,7 @@ sbp_status sbp_partition(const sbp_graph_csr* g, const sbp_options* o, int32_t* 
   if (s != SBP_OK) return s;
   Timer t;
   Job J;
-  s = job_for(J, g, o->device, o->num_proposals, o->max_nodal_itr);
+  s = job_for(J, g, o->device, o->num_proposals, o->max_nodal_itr, o->dense_max);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaStreamSynchronize(J.st));
   double up = t.ms();
@@ -780,8 +865,17 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
   SBP_CUDA(cudaMalloc(&dd, 8 * n));
   cudaMemcpyAsync(dv, verts, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
   cudaMemcpyAsync(dp, props, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
-  block_terms(J.m, B, 0, 0, 0, J.st);
-  nodal_delta_given(J.g, J.part, J.m, B, nv, dv, dp, dd, J.heavy, J.heavy_count, J.st);
+  std::vector<int32_t> hv;
+  for (int32_t i = 0; i < nv; ++i)
+    if (heavy_vertex(J, verts[i])) hv.push_back(i);
+  if (!hv.empty())
+    cudaMemcpyAsync(J.heavy, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice, J.st);
+  block_terms_any(J, B, 0, 0, 0, J.st);
+  nodal_delta_given(J.g, J.part, J.m, B, is_dense(J, B), nv, dv, dp, dd,
+                    aux_for(J, J.heavy, (int32_t)hv.size()), J.st);
+  cudaStreamSynchronize(J.st);
+  int32_t err_h = 0;
+  cudaMemcpy(&err_h, J.err, 4, cudaMemcpyDeviceToHost);
   cudaMemcpyAsync(dS, dd, 8 * (size_t)nv, cudaMemcpyDeviceToHost, J.st);
   cudaError_t e = cudaStreamSynchronize(J.st);
   if (e == cudaSuccess) e = cudaGetLastError();
@@ -789,6 +883,7 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
   cudaFree(dp);
   cudaFree(dd);
   if (e != cudaSuccess) return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
+  if (err_h) return fail(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
   return SBP_OK;
 }
 
@@ -833,18 +928,80 @@ sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uin
   sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
   int32_t cnt = hi - lo;
-  block_terms(J.m, B, 1, seed, seq, J.st);
+  std::vector<int32_t> hv;
+  for (int32_t v = lo; v < hi; ++v)
+    if (heavy_vertex(J, v)) hv.push_back(v - lo);
+  if (!hv.empty())
+    SBP_CUDA(cudaMemcpyAsync(J.heavy, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice, J.st));
+  const bool dense = is_dense(J, B);
+  block_terms_any(J, B, 1, seed, seq, J.st);
   SBP_CUDA(cudaMemsetAsync(J.dsum, 0, 8, J.st));
   SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8, J.st));
-  nodal_batch_sample(J.g, J.part, J.m, B, seed, seq, lo, cnt, J.newlab, J.rec, J.props, J.heavy,
-                     J.heavy_count, J.st);
-  nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, J.heavy_count, J.st);
+  nodal_batch_sample(J.g, J.part, J.m, B, dense, seed, seq, lo, cnt, J.newlab, J.rec, J.props,
+                     aux_for(J, J.heavy, (int32_t)hv.size()), J.st);
+  nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, nullptr, 0, J.st);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());
   SBP_CUDA(cudaMemcpy(part, J.part, 4 * (size_t)J.N, cudaMemcpyDeviceToHost));
   if (dS_rec && cnt) SBP_CUDA(cudaMemcpy(dS_rec, J.rec, 8 * (size_t)cnt, cudaMemcpyDeviceToHost));
   if (props && cnt) SBP_CUDA(cudaMemcpy(props, J.props, 4 * (size_t)cnt, cudaMemcpyDeviceToHost));
   if (sum) SBP_CUDA(cudaMemcpy(sum, J.dsum, 8, cudaMemcpyDeviceToHost));
+  return SBP_OK;
+}
+
+sbp_status sbp_nodal_sweeps(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
+                            uint32_t seq0, int32_t num_batches, int32_t sweeps, int32_t dense_max,
+                            double* sums) {
+  if (!g || num_batches < 1 || sweeps < 1 || !sums) return fail(SBP_ERR_INVALID, "bad arguments");
+  sbp_status s = validate_graph(g);
+  if (s != SBP_OK) return s;
+  s = validate_part(part, g->N, B);
+  if (s != SBP_OK) return s;
+  const int32_t nb = num_batches * sweeps;
+  Job J;
+  s = job_create(J, resolve_device(-1), g->N, g->E, 1, nb, dense_max);
+  if (s != SBP_OK) return s;
+  s = job_upload(J, g);
+  if (s != SBP_OK) return s;
+  cudaStream_t st = J.st;
+  SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, st));
+  build_model(J, B, st);
+  const bool dense = is_dense(J, B);
+  const int32_t BS = J.N / num_batches;
+  std::vector<int32_t> heavy_all, heavy_off(num_batches + 1, 0);
+  for (int32_t b = 0; b < num_batches; ++b) {
+    for (int32_t v = b * BS; v < (b + 1) * BS; ++v)
+      if (heavy_vertex(J, v)) heavy_all.push_back(v - b * BS);
+    heavy_off[b + 1] = (int32_t)heavy_all.size();
+  }
+  if (!heavy_all.empty())
+    SBP_CUDA(cudaMemcpyAsync(J.heavy, heavy_all.data(), 4 * heavy_all.size(),
+                             cudaMemcpyHostToDevice, st));
+  SBP_CUDA(cudaMemsetAsync(J.dsum, 0, 8 * (size_t)nb, st));
+  SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8 * (size_t)nb, st));
+  uint32_t seq = seq0;
+  for (int32_t k = 0; k < nb; ++k) {
+    const int32_t b = k % num_batches;
+    block_terms_any(J, B, 1, seed, seq, st);
+    NodalAux aux = aux_for(J, J.heavy + heavy_off[b], heavy_off[b + 1] - heavy_off[b]);
+    nodal_batch_sample(J.g, J.part, J.m, B, dense, seed, seq, b * BS, BS, J.newlab, J.rec, nullptr,
+                       aux, st);
+    if (dense) {
+      dense_update(J.g, J.part, b * BS, BS, J.newlab, B, J.m, st);
+      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, &J.m, B, st);
+    } else {
+      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, nullptr, 0, st);
+      rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
+    }
+    ++seq;
+  }
+  SBP_CUDA(cudaStreamSynchronize(st));
+  SBP_CUDA(cudaGetLastError());
+  int32_t err_h = 0;
+  SBP_CUDA(cudaMemcpy(&err_h, J.err, 4, cudaMemcpyDeviceToHost));
+  if (err_h) return fail(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
+  SBP_CUDA(cudaMemcpy(part, J.part, 4 * (size_t)J.N, cudaMemcpyDeviceToHost));
+  SBP_CUDA(cudaMemcpy(sums, J.dsum, 8 * (size_t)nb, cudaMemcpyDeviceToHost));
   return SBP_OK;
 }
 

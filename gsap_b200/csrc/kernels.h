@@ -32,6 +32,9 @@ struct DevBM {
   double *sinfull = nullptr;  // ambin[b] - d_in[b] log2 d_in[b]
   int32_t* nbr_s = nullptr;   // per-block second-hop sample of a nodal batch
   uint8_t* use_rand = nullptr;
+  // dense form for small B: Md[r*B + c] = M[r][c], MTd[c*B + r] = M[r][c]
+  uint32_t* Md = nullptr;
+  uint32_t* MTd = nullptr;
 };
 
 // Scratch of one rebuild direction.
@@ -65,29 +68,53 @@ void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM
 // per-block uniform, kernels.hpp:942-997, 1024).
 void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cudaStream_t st);
 
+// Dense form (B*B counts and their transpose, degrees and their log2) of the
+// labels' blockmodel, built from scratch.
+void dense_build(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, cudaStream_t st);
+// Applies a batch's moves to the dense form: `part` still holds the old
+// labels, newlab[i] the new label of vertex lo+i.  Degrees are updated; their
+// log2 are refreshed by nodal_commit (dense mode).
+void dense_update(const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
+                  const int32_t* newlab, int32_t B, DevBM& m, cudaStream_t st);
+// block_terms for the dense form.
+void block_terms_dense(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq,
+                       cudaStream_t st);
+
 // data_S = sum of dSout over blocks, written to *out (deterministic order).
 void mdl_data_sum(const DevBM& m, int32_t B, double* out, cudaStream_t st);
 
 cudaError_t init_nodal_attributes();
+// Vertices with more than this many entries in a direction go to the
+// CTA-per-vertex kernel.
+int nodal_heavy_threshold();
+
+// Heavy-vertex list of a batch (indices into the batch) and the side stream
+// it runs on; err counts hash-table overflows (should stay 0).
+struct NodalAux {
+  const int32_t* heavy = nullptr;
+  int32_t nheavy = 0;
+  int32_t* err = nullptr;
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
 
 // Nodal batch of vertices [lo, lo+count): proposal, dS, accept flag.
 // newlab[i] = new label of vertex lo+i, rec[i] = recorded dS (0 if rejected),
-// props[i] (optional) = proposal.  heavy (3 ints per vertex) and heavy_count
-// (2 ints: queue length, which must be 0 on entry, and an error counter) hold
-// the vertices handed from the warp kernel to the CTA kernel.
+// props[i] (optional) = proposal.  dense: read M from its dense form.
 void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
-                        uint64_t seed, uint32_t seq, int32_t lo, int32_t count, int32_t* newlab,
-                        double* rec, int32_t* props, int32_t* heavy, int32_t* heavy_count,
+                        bool dense, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
+                        int32_t* newlab, double* rec, int32_t* props, const NodalAux& aux,
                         cudaStream_t st);
 // dS of given (vertex, proposal) pairs, no accept.
 void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
-                       int32_t nv, const int32_t* verts, const int32_t* props, double* dS,
-                       int32_t* heavy, int32_t* heavy_count, cudaStream_t st);
+                       bool dense, int32_t nv, const int32_t* verts, const int32_t* props,
+                       double* dS, const NodalAux& aux, cudaStream_t st);
 // Apply a batch: part[lo+i] = newlab[i]; slot_sum[0] += sum(rec) in a fixed
-// order, slot_acc[0] += number of moves; resets heavy_count[0].
+// order, slot_acc[0] += number of moves.  With dense_m, also recomputes the
+// log2 of its block degrees.
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
-                  const double* rec, double* slot_sum, long long* slot_acc, int32_t* heavy_count,
-                  cudaStream_t st);
+                  const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
+                  int32_t B, cudaStream_t st);
 
 // Merge proposals (kernels.hpp:726-856) and their dS with the per-block best
 // (kernels.hpp:143-491).

@@ -6,19 +6,22 @@
 // vertex's sorted neighbour-block list (kernels.hpp:494-597, 1153-1726).
 //
 // Here a group of threads owns one vertex: a warp for ordinary vertices, a
-// whole CTA for the few whose neighbour lists exceed a warp's buffer.
+// whole CTA for the few with more than kWarpList neighbours in a direction
+// (a static per-batch list, run on a second stream next to the warp kernel).
 //   * proposal: Philox draws, an exact integer inverse-CDF pick of a
 //     neighbour (a warp prefix scan over its out- then in-entries), then the
 //     per-block draws of the batch (kernels.hpp:877-1032);
-//   * neighbour blocks: only this vertex's lists are sorted, in shared
-//     memory (bitonic), where GSAP sorts all E entries every batch;
+//   * neighbour blocks grouped per distinct block: in registers with
+//     __match_any_sync / __reduce_add_sync when a list fits a warp, else
+//     sorted in shared memory (bitonic), else hashed in shared memory in
+//     passes; GSAP sorts all E entries every batch;
 //   * dS: GSAP's seven terms rewritten as "old row sum + changed columns".
 //     A row term  sum_c f(x_c)  with  f(x) = x (log2 x - log2 dcol[c] - L)
 //     splits into  sum_c (x log2 x - x log2 dcol[c])  -  L * sum_c x ;
 //     the first sum over the unchanged columns is the per-block sum computed
 //     once per batch (ambout / ambin), so only the columns the vertex touches
-//     are visited: O(deg(v) log(row)) per vertex instead of O(row nnz).  The
-//     changed counts are read with binary searches in the CSR rows.
+//     are visited.  Counts come from the dense B x B form (small B, O(1)) or
+//     by binary search in the CSR rows.
 //     Quirks of the reference kept: old column degrees (Q2), one term per
 //     list entry for blocks missing from the target row
 //     (kernels.hpp:1648-1652, 1314-1318), the r/s in-weight corrections and
@@ -51,6 +54,7 @@ struct NodalArgs {
   const int32_t* part;
   const int32_t *bop, *boc, *bip, *bic;
   const uint32_t *bon, *bin, *d_out, *d_in;
+  const uint32_t *Md, *MTd;
   const double *ld_out, *ld_in, *dSout, *ambout, *ambin, *sinfull;
   const int32_t* nbr_s;
   const uint8_t* use_rand;
@@ -64,8 +68,9 @@ struct NodalArgs {
   double* rec;
   int32_t* props_out;
   double* dS_raw;
-  int32_t* heavy;           // (i, v, s) triples of vertices left to the CTA kernel
-  int32_t* heavy_count;
+  const int32_t* heavy;     // batch indices handled by the CTA kernel
+  int32_t nheavy;
+  int32_t* err;             // error counter (hash table overflow)
 };
 
 // g(x, a) = x log2 x - x a, zero for x == 0
@@ -77,70 +82,36 @@ __device__ __forceinline__ double fterm(uint32_t m, double a, double b) {
   return m == 0u ? 0.0 : (double)m * (log2((double)m) - (a + b));
 }
 
-// A thread group cooperating on one vertex: a warp (G = 32) or a CTA.
-template <int G>
-struct Group {
-  double* red;  // G/32 doubles of shared scratch (CTA only)
-  __device__ __forceinline__ int rank() const { return G == 32 ? (threadIdx.x & 31) : threadIdx.x; }
-  __device__ __forceinline__ void sync() const {
-    if (G == 32) __syncwarp();
-    else __syncthreads();
-  }
-  __device__ double sum(double x) const {
-    x = warp_sum(x);
-    if (G == 32) return x;
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
-    __syncthreads();
-    double t = 0.0;
-    for (int i = 0; i < G / 32; ++i) t += red[i];
-    __syncthreads();
-    return t;
-  }
-  __device__ long long sum_ll(long long x) const {
-    return (long long)sum((double)x);  // |x| < 2^53: exact
-  }
+// The four rows a move from r to s reads: out-rows r and s, in-rows r and s.
+template <bool DENSE>
+struct Rows;
+
+template <>
+struct Rows<false> {
+  const int32_t *oc, *ic;
+  const uint32_t *on, *inn;
+  int32_t rO0, rO1, sO0, sO1, rI0, rI1, sI0, sI1;
+  __device__ Rows(const NodalArgs& a, int r, int s)
+      : oc(a.boc), ic(a.bic), on(a.bon), inn(a.bin), rO0(a.bop[r]), rO1(a.bop[r + 1]),
+        sO0(a.bop[s]), sO1(a.bop[s + 1]), rI0(a.bip[r]), rI1(a.bip[r + 1]), sI0(a.bip[s]),
+        sI1(a.bip[s + 1]) {}
+  __device__ __forceinline__ uint32_t out_r(int c) const { return row_lookup(oc, on, rO0, rO1, c); }
+  __device__ __forceinline__ uint32_t out_s(int c) const { return row_lookup(oc, on, sO0, sO1, c); }
+  __device__ __forceinline__ uint32_t in_r(int c) const { return row_lookup(ic, inn, rI0, rI1, c); }
+  __device__ __forceinline__ uint32_t in_s(int c) const { return row_lookup(ic, inn, sI0, sI1, c); }
 };
 
-// Ascending bitonic sort of P (power of two) keys by the group.
-template <int G>
-__device__ void group_sort(unsigned long long* key, int P, const Group<G>& grp) {
-  const int t = grp.rank();
-  for (int k = 2; k <= P; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = t; i < P; i += G) {
-        int ixj = i ^ j;
-        if (ixj > i) {
-          unsigned long long x = key[i], y = key[ixj];
-          bool asc = (i & k) == 0;
-          if ((x > y) == asc) {
-            key[i] = y;
-            key[ixj] = x;
-          }
-        }
-      }
-      grp.sync();
-    }
-  }
-}
-
-__device__ __forceinline__ int32_t kblk(unsigned long long k) { return (int32_t)(k >> 32); }
-__device__ __forceinline__ uint32_t kwt(unsigned long long k) { return (uint32_t)k; }
-
-// Stage v's neighbour blocks of one direction as sorted (block, weight) keys.
-template <int G>
-__device__ void stage_sorted(const int32_t* __restrict__ idx, const uint32_t* __restrict__ w,
-                             const int32_t* __restrict__ part, int32_t base, int n,
-                             unsigned long long* key, const Group<G>& grp) {
-  int P = 32;
-  while (P < n) P <<= 1;
-  for (int k = grp.rank(); k < P; k += G)
-    key[k] = k < n ? ((unsigned long long)(uint32_t)__ldg(part + __ldg(idx + base + k)) << 32) |
-                         __ldg(w + base + k)
-                   : ~0ull;
-  grp.sync();
-  group_sort<G>(key, P, grp);
-}
+template <>
+struct Rows<true> {
+  const uint32_t *orr, *ors, *irr, *irs;
+  __device__ Rows(const NodalArgs& a, int r, int s)
+      : orr(a.Md + (size_t)r * a.B), ors(a.Md + (size_t)s * a.B), irr(a.MTd + (size_t)r * a.B),
+        irs(a.MTd + (size_t)s * a.B) {}
+  __device__ __forceinline__ uint32_t out_r(int c) const { return __ldg(orr + c); }
+  __device__ __forceinline__ uint32_t out_s(int c) const { return __ldg(ors + c); }
+  __device__ __forceinline__ uint32_t in_r(int c) const { return __ldg(irr + c); }
+  __device__ __forceinline__ uint32_t in_s(int c) const { return __ldg(irs + c); }
+};
 
 // Accumulators of the changed columns of the four new rows (out r, out s,
 // in r, in s): a = sum of (x log2 x - x log2 dcol) deltas, m = count deltas.
@@ -149,24 +120,16 @@ struct Acc {
   long long m4 = 0, m5 = 0, m6 = 0, m7 = 0;
 };
 
-struct RowBounds {
-  int32_t rO0, rO1, sO0, sO1, rI0, rI1, sI0, sI1;
-};
-
-__device__ __forceinline__ RowBounds row_bounds(const NodalArgs& a, int r, int s) {
-  return RowBounds{a.bop[r], a.bop[r + 1], a.bop[s], a.bop[s + 1],
-                   a.bip[r], a.bip[r + 1], a.bip[s], a.bip[s + 1]};
-}
-
 // One out-entry (block c, weight w) of v; `leader` marks one entry per
 // distinct block, kc = v's total weight into c (kernels.hpp:1444-1726).
-__device__ __forceinline__ void out_entry(const NodalArgs& a, const RowBounds& rb, int r, int s,
+template <bool DENSE>
+__device__ __forceinline__ void out_entry(const NodalArgs& a, const Rows<DENSE>& R, int r, int s,
                                           uint32_t niS, int32_t c, uint32_t w, bool leader,
                                           uint32_t kc, Acc& q) {
   const double ldc = a.ld_in[c];
-  const uint32_t Msc = row_lookup(a.boc, a.bon, rb.sO0, rb.sO1, c);
+  const uint32_t Msc = R.out_s(c);
   if (leader && c != r && c != s) {
-    const uint32_t Mrc = row_lookup(a.boc, a.bon, rb.rO0, rb.rO1, c);
+    const uint32_t Mrc = R.out_r(c);
     const uint32_t x = Mrc - kc;
     q.a4 += gterm(x, ldc) - gterm(Mrc, ldc);
     q.m4 += (long long)x - (long long)Mrc;
@@ -185,14 +148,15 @@ __device__ __forceinline__ void out_entry(const NodalArgs& a, const RowBounds& r
 }
 
 // One in-entry of v: rows r and s of the in CSR, blocks r and s left out.
-__device__ __forceinline__ void in_entry(const NodalArgs& a, const RowBounds& rb, int r, int s,
+template <bool DENSE>
+__device__ __forceinline__ void in_entry(const NodalArgs& a, const Rows<DENSE>& R, int r, int s,
                                          int32_t c, uint32_t w, bool leader, uint32_t kc,
                                          Acc& q) {
   if (c == r || c == s) return;
   const double ldc = a.ld_out[c];
-  const uint32_t Mcs = row_lookup(a.bic, a.bin, rb.sI0, rb.sI1, c);
+  const uint32_t Mcs = R.in_s(c);
   if (leader) {
-    const uint32_t Mcr = row_lookup(a.bic, a.bin, rb.rI0, rb.rI1, c);
+    const uint32_t Mcr = R.in_r(c);
     const uint32_t x = Mcr - kc;
     q.a6 += gterm(x, ldc) - gterm(Mcr, ldc);
     q.m6 += (long long)x - (long long)Mcr;
@@ -210,12 +174,13 @@ __device__ __forceinline__ void in_entry(const NodalArgs& a, const RowBounds& rb
 
 // The (r, s) corner, the old terms and the new-row totals (every thread of
 // the group holds the reduced q and gets the same result).
-__device__ double finish_delta(const NodalArgs& a, const RowBounds& rb, int v, int r, int s,
+template <bool DENSE>
+__device__ double finish_delta(const NodalArgs& a, const Rows<DENSE>& R, int v, int r, int s,
                                uint32_t koR, uint32_t koS, uint32_t niR, uint32_t niS, Acc q) {
-  const uint32_t Mrr = row_lookup(a.boc, a.bon, rb.rO0, rb.rO1, r);
-  const uint32_t Mrs = row_lookup(a.boc, a.bon, rb.rO0, rb.rO1, s);
-  const uint32_t Msr = row_lookup(a.boc, a.bon, rb.sO0, rb.sO1, r);
-  const uint32_t Mss = row_lookup(a.boc, a.bon, rb.sO0, rb.sO1, s);
+  const uint32_t Mrr = R.out_r(r);
+  const uint32_t Mrs = R.out_r(s);
+  const uint32_t Msr = R.out_s(r);
+  const uint32_t Mss = R.out_s(s);
   const double ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
   const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s];
   if (Mrr != 0u) {
@@ -266,6 +231,31 @@ __device__ double finish_delta(const NodalArgs& a, const RowBounds& rb, int v, i
   return t1 + t2 + t3 - t4 - t5 - t6 - t7;
 }
 
+// A thread group cooperating on one vertex: a warp (G = 32) or a CTA.
+template <int G>
+struct Group {
+  double* red;  // G/32 doubles of shared scratch (CTA only)
+  __device__ __forceinline__ int rank() const { return G == 32 ? (threadIdx.x & 31) : threadIdx.x; }
+  __device__ __forceinline__ void sync() const {
+    if (G == 32) __syncwarp();
+    else __syncthreads();
+  }
+  __device__ double sum(double x) const {
+    x = warp_sum(x);
+    if (G == 32) return x;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < G / 32; ++i) t += red[i];
+    __syncthreads();
+    return t;
+  }
+  __device__ long long sum_ll(long long x) const {
+    return (long long)sum((double)x);  // |x| < 2^53: exact
+  }
+};
+
 template <int G>
 __device__ __forceinline__ void reduce_acc(Acc& q, const Group<G>& grp) {
   q.a4 = grp.sum(q.a4);
@@ -278,15 +268,53 @@ __device__ __forceinline__ void reduce_acc(Acc& q, const Group<G>& grp) {
   q.m7 = grp.sum_ll(q.m7);
 }
 
-// dS of moving v from r to s (r != s) from v's sorted neighbour-block lists
-// ko[0..no) (out) and ki[0..ni) (in).  Every thread of the group returns the
-// same value.
+// Ascending bitonic sort of P (power of two) keys by the group.
 template <int G>
-__device__ double vertex_delta(const NodalArgs& a, int v, int r, int s,
+__device__ void group_sort(unsigned long long* key, int P, const Group<G>& grp) {
+  const int t = grp.rank();
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = t; i < P; i += G) {
+        int ixj = i ^ j;
+        if (ixj > i) {
+          unsigned long long x = key[i], y = key[ixj];
+          bool asc = (i & k) == 0;
+          if ((x > y) == asc) {
+            key[i] = y;
+            key[ixj] = x;
+          }
+        }
+      }
+      grp.sync();
+    }
+  }
+}
+
+__device__ __forceinline__ int32_t kblk(unsigned long long k) { return (int32_t)(k >> 32); }
+__device__ __forceinline__ uint32_t kwt(unsigned long long k) { return (uint32_t)k; }
+
+// Stage v's neighbour blocks of one direction as sorted (block, weight) keys.
+template <int G>
+__device__ void stage_sorted(const int32_t* __restrict__ idx, const uint32_t* __restrict__ w,
+                             const int32_t* __restrict__ part, int32_t base, int n,
+                             unsigned long long* key, const Group<G>& grp) {
+  int P = 32;
+  while (P < n) P <<= 1;
+  for (int k = grp.rank(); k < P; k += G)
+    key[k] = k < n ? ((unsigned long long)(uint32_t)__ldg(part + __ldg(idx + base + k)) << 32) |
+                         __ldg(w + base + k)
+                   : ~0ull;
+  grp.sync();
+  group_sort<G>(key, P, grp);
+}
+
+// dS from v's sorted neighbour-block lists ko[0..no) (out), ki[0..ni) (in).
+template <bool DENSE, int G>
+__device__ double delta_sorted(const NodalArgs& a, int v, int r, int s,
                                const unsigned long long* ko, int no,
                                const unsigned long long* ki, int ni, const Group<G>& grp) {
   const int t = grp.rank();
-  const RowBounds rb = row_bounds(a, r, s);
+  const Rows<DENSE> R(a, r, s);
   uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
   for (int k = t; k < no; k += G) {
     int32_t c = kblk(ko[k]);
@@ -309,7 +337,7 @@ __device__ double vertex_delta(const NodalArgs& a, int v, int r, int s,
     uint32_t kc = 0;
     if (leader)
       for (int j = k; j < no && kblk(ko[j]) == c; ++j) kc += kwt(ko[j]);
-    out_entry(a, rb, r, s, niS, c, kwt(ko[k]), leader, kc, q);
+    out_entry<DENSE>(a, R, r, s, niS, c, kwt(ko[k]), leader, kc, q);
   }
   for (int k = t; k < ni; k += G) {
     const int32_t c = kblk(ki[k]);
@@ -317,10 +345,45 @@ __device__ double vertex_delta(const NodalArgs& a, int v, int r, int s,
     uint32_t kc = 0;
     if (leader)
       for (int j = k; j < ni && kblk(ki[j]) == c; ++j) kc += kwt(ki[j]);
-    in_entry(a, rb, r, s, c, kwt(ki[k]), leader, kc, q);
+    in_entry<DENSE>(a, R, r, s, c, kwt(ki[k]), leader, kc, q);
   }
   reduce_acc(q, grp);
-  return finish_delta(a, rb, v, r, s, koR, koS, niR, niS, q);
+  return finish_delta<DENSE>(a, R, v, r, s, koR, koS, niR, niS, q);
+}
+
+// dS when both lists fit in one warp: each lane holds one out- and one
+// in-entry; entries of the same block are grouped with __match_any_sync and
+// their weights summed with __reduce_add_sync.
+template <bool DENSE>
+__device__ double delta_registers(const NodalArgs& a, int v, int r, int s, int32_t o0, int no,
+                                  int32_t i0, int ni, int lane) {
+  const Rows<DENSE> R(a, r, s);
+  const bool vo = lane < no, vi = lane < ni;
+  const int32_t co = vo ? __ldg(a.part + __ldg(a.oidx + o0 + lane)) : -1 - lane;
+  const uint32_t wo = vo ? __ldg(a.ow + o0 + lane) : 0u;
+  const int32_t ci = vi ? __ldg(a.part + __ldg(a.iidx + i0 + lane)) : -1 - lane;
+  const uint32_t wi = vi ? __ldg(a.iw + i0 + lane) : 0u;
+  const unsigned po = __match_any_sync(kFull, co);
+  const unsigned pi = __match_any_sync(kFull, ci);
+  const uint32_t kco = __reduce_add_sync(po, wo);
+  const uint32_t kci = __reduce_add_sync(pi, wi);
+  const uint32_t koR = __reduce_add_sync(kFull, co == r ? wo : 0u);
+  const uint32_t koS = __reduce_add_sync(kFull, co == s ? wo : 0u);
+  const uint32_t niR = __reduce_add_sync(kFull, ci == r ? wi : 0u);
+  const uint32_t niS = __reduce_add_sync(kFull, ci == s ? wi : 0u);
+  Acc q;
+  if (vo) out_entry<DENSE>(a, R, r, s, niS, co, wo, lane == __ffs(po) - 1, kco, q);
+  if (vi) in_entry<DENSE>(a, R, r, s, ci, wi, lane == __ffs(pi) - 1, kci, q);
+  q.a4 = warp_sum(q.a4);
+  q.a5 = warp_sum(q.a5);
+  q.a6 = warp_sum(q.a6);
+  q.a7 = warp_sum(q.a7);
+  // per-lane count deltas are bounded by the vertex's degree: 32-bit sums
+  q.m4 = __reduce_add_sync(kFull, (int)q.m4);
+  q.m5 = __reduce_add_sync(kFull, (int)q.m5);
+  q.m6 = __reduce_add_sync(kFull, (int)q.m6);
+  q.m7 = __reduce_add_sync(kFull, (int)q.m7);
+  return finish_delta<DENSE>(a, R, v, r, s, koR, koS, niR, niS, q);
 }
 
 // Lists too long for shared memory: per-block totals from a shared-memory
@@ -360,11 +423,11 @@ __device__ int hash_find(const HashTab& h, int32_t c) {
   return -1;
 }
 
-template <int G>
-__device__ double vertex_delta_hashed(const NodalArgs& a, int v, int r, int s, HashTab h,
-                                      int* flag, const Group<G>& grp) {
+template <bool DENSE, int G>
+__device__ double delta_hashed(const NodalArgs& a, int v, int r, int s, HashTab h, int* flag,
+                               const Group<G>& grp) {
   const int t = grp.rank();
-  const RowBounds rb = row_bounds(a, r, s);
+  const Rows<DENSE> R(a, r, s);
   const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
   const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
   uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
@@ -411,14 +474,14 @@ __device__ double vertex_delta_hashed(const NodalArgs& a, int v, int r, int s, H
         bool leader = h.first[slot] == k;
         uint32_t kc = h.sum[slot];
         uint32_t w = __ldg(wt + base + k);
-        if (dir == 0) out_entry(a, rb, r, s, niS, c, w, leader, kc, q);
-        else in_entry(a, rb, r, s, c, w, leader, kc, q);
+        if (dir == 0) out_entry<DENSE>(a, R, r, s, niS, c, w, leader, kc, q);
+        else in_entry<DENSE>(a, R, r, s, c, w, leader, kc, q);
       }
       grp.sync();
     }
   }
   reduce_acc(q, grp);
-  return finish_delta(a, rb, v, r, s, koR, koS, niR, niS, q);
+  return finish_delta<DENSE>(a, R, v, r, s, koR, koS, niR, niS, q);
 }
 
 // Neighbour of v whose running weight (out-entries, then in-entries) first
@@ -449,6 +512,27 @@ __device__ int32_t pick_neighbour(const NodalArgs& a, int v, uint64_t t, int lan
   return 0;
 }
 
+// Vertex and proposal of batch item i (computed by one warp).
+template <bool GIVEN>
+__device__ __forceinline__ void item(const NodalArgs& a, int i, int lane, int& v, int& s) {
+  if (GIVEN) {
+    v = a.verts[i];
+    s = a.props_in[i];
+    return;
+  }
+  v = a.lo + i;
+  P4 x = draw(a.seed, kRngNodalVertex, a.seq, (uint32_t)v);
+  int rnd = (int)(x.v[0] % (uint32_t)a.B);
+  uint64_t deg = (uint64_t)a.kdo[v] + a.kdi[v];
+  if (deg == 0) {
+    s = rnd;
+  } else {
+    int32_t un = pick_neighbour(a, v, scale_draw(x.v[1], deg), lane);
+    int32_t u = a.part[un];
+    s = a.use_rand[u] ? rnd : a.nbr_s[u];
+  }
+}
+
 __device__ __forceinline__ void write_result(const NodalArgs& a, bool given, int i, int r, int s,
                                              double d) {
   if (given) {
@@ -461,49 +545,34 @@ __device__ __forceinline__ void write_result(const NodalArgs& a, bool given, int
   }
 }
 
-template <bool GIVEN>
-__global__ void __launch_bounds__(kNodalWarps * 32) nodal_kernel(NodalArgs a) {
+__device__ __forceinline__ bool is_heavy(int no, int ni) {
+  return no > kWarpList || ni > kWarpList;
+}
+
+template <bool GIVEN, bool DENSE>
+__global__ void __launch_bounds__(kNodalWarps * 32, 4) nodal_kernel(NodalArgs a) {
   __shared__ unsigned long long s_ko[kNodalWarps][kWarpList], s_ki[kNodalWarps][kWarpList];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = gridDim.x * kNodalWarps;
   Group<32> grp{nullptr};
   for (int i = blockIdx.x * kNodalWarps + wid; i < a.count; i += nw) {
+    const int vv = GIVEN ? a.verts[i] : a.lo + i;
+    const int32_t o0 = a.optr[vv], no = a.optr[vv + 1] - o0;
+    const int32_t i0 = a.iptr[vv], ni = a.iptr[vv + 1] - i0;
+    if (is_heavy(no, ni)) continue;  // the CTA kernel's
     int v, s;
-    if (GIVEN) {
-      v = a.verts[i];
-      s = a.props_in[i];
-    } else {
-      v = a.lo + i;
-      P4 x = draw(a.seed, kRngNodalVertex, a.seq, (uint32_t)v);
-      int rnd = (int)(x.v[0] % (uint32_t)a.B);
-      uint64_t deg = (uint64_t)a.kdo[v] + a.kdi[v];
-      if (deg == 0) {
-        s = rnd;
-      } else {
-        int32_t un = pick_neighbour(a, v, scale_draw(x.v[1], deg), lane);
-        int32_t u = a.part[un];
-        s = a.use_rand[u] ? rnd : a.nbr_s[u];
-      }
-    }
+    item<GIVEN>(a, i, lane, v, s);
     const int r = a.part[v];
-    if (r == s) {
-      if (lane == 0) write_result(a, GIVEN, i, r, s, 0.0);
-      continue;
-    }
-    const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
-    const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
-    if (no > kWarpList || ni > kWarpList) {
-      if (lane == 0) {
-        int h = atomicAdd(a.heavy_count, 1);
-        a.heavy[3 * h] = i;
-        a.heavy[3 * h + 1] = v;
-        a.heavy[3 * h + 2] = s;
+    double d = 0.0;
+    if (r != s) {
+      if (no <= 32 && ni <= 32) {
+        d = delta_registers<DENSE>(a, v, r, s, o0, no, i0, ni, lane);
+      } else {
+        stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, s_ko[wid], grp);
+        stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, s_ki[wid], grp);
+        d = delta_sorted<DENSE, 32>(a, v, r, s, s_ko[wid], no, s_ki[wid], ni, grp);
       }
-      continue;
     }
-    stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, s_ko[wid], grp);
-    stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, s_ki[wid], grp);
-    double d = vertex_delta<32>(a, v, r, s, s_ko[wid], no, s_ki[wid], ni, grp);
     if (lane == 0) write_result(a, GIVEN, i, r, s, d);
     __syncwarp();
   }
@@ -512,29 +581,40 @@ __global__ void __launch_bounds__(kNodalWarps * 32) nodal_kernel(NodalArgs a) {
 // Vertices with more than kWarpList entries in a direction: one CTA each,
 // lists sorted in shared memory up to kHeavyList entries, longer ones
 // through the hashed passes.
-template <bool GIVEN>
+template <bool GIVEN, bool DENSE>
 __global__ void __launch_bounds__(kHeavyThreads) nodal_heavy_kernel(NodalArgs a) {
   extern __shared__ unsigned long long hsm[];
   __shared__ double red[kHeavyThreads / 32];
-  __shared__ int flag;
+  __shared__ int flag, sh_v, sh_s;
   Group<kHeavyThreads> grp{red};
   unsigned long long* ko = hsm;
   unsigned long long* ki = hsm + kHeavyList;
   HashTab ht{(int32_t*)hsm, (uint32_t*)hsm + kHashSlots, (int32_t*)hsm + 2 * kHashSlots};
-  const int nh = *a.heavy_count;
-  for (int h = blockIdx.x; h < nh; h += gridDim.x) {
-    const int i = a.heavy[3 * h], v = a.heavy[3 * h + 1], s = a.heavy[3 * h + 2];
+  for (int h = blockIdx.x; h < a.nheavy; h += gridDim.x) {
+    const int i = a.heavy[h];
+    if (threadIdx.x < 32) {
+      int v, s;
+      item<GIVEN>(a, i, threadIdx.x, v, s);
+      if (threadIdx.x == 0) {
+        sh_v = v;
+        sh_s = s;
+      }
+    }
+    __syncthreads();
+    const int v = sh_v, s = sh_s;
     const int r = a.part[v];
     const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
     const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
-    double d;
-    if (no <= kHeavyList && ni <= kHeavyList) {
-      stage_sorted<kHeavyThreads>(a.oidx, a.ow, a.part, o0, no, ko, grp);
-      stage_sorted<kHeavyThreads>(a.iidx, a.iw, a.part, i0, ni, ki, grp);
-      d = vertex_delta<kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp);
-    } else {
-      d = vertex_delta_hashed<kHeavyThreads>(a, v, r, s, ht, &flag, grp);
-      if (threadIdx.x == 0 && d != d) atomicAdd(a.heavy_count + 1, 1);
+    double d = 0.0;
+    if (r != s) {
+      if (no <= kHeavyList && ni <= kHeavyList) {
+        stage_sorted<kHeavyThreads>(a.oidx, a.ow, a.part, o0, no, ko, grp);
+        stage_sorted<kHeavyThreads>(a.iidx, a.iw, a.part, i0, ni, ki, grp);
+        d = delta_sorted<DENSE, kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp);
+      } else {
+        d = delta_hashed<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp);
+        if (threadIdx.x == 0 && d != d) atomicAdd(a.err, 1);
+      }
     }
     if (threadIdx.x == 0) write_result(a, GIVEN, i, r, s, d);
     __syncthreads();
@@ -542,10 +622,13 @@ __global__ void __launch_bounds__(kHeavyThreads) nodal_heavy_kernel(NodalArgs a)
 }
 
 // One CTA: applies the batch's labels and sums its recorded dS in a fixed
-// order (deterministic across runs); resets the heavy-vertex counter.
+// order (deterministic across runs).  In dense mode it also refreshes the
+// log2 of the block degrees that dense_update changed.
 __global__ void commit_kernel(int32_t* part, int32_t lo, int32_t count,
                               const int32_t* __restrict__ newlab, const double* __restrict__ rec,
-                              double* slot_sum, long long* slot_acc, int32_t* heavy_count) {
+                              double* slot_sum, long long* slot_acc, int32_t B,
+                              const uint32_t* __restrict__ d_out,
+                              const uint32_t* __restrict__ d_in, double* ld_out, double* ld_in) {
   __shared__ double sh[1024];
   __shared__ long long shc[1024];
   double s = 0.0;
@@ -558,6 +641,11 @@ __global__ void commit_kernel(int32_t* part, int32_t lo, int32_t count,
     }
     s += rec[i];
   }
+  if (ld_out)
+    for (int b = threadIdx.x; b < B; b += blockDim.x) {
+      ld_out[b] = log2((double)d_out[b]);
+      ld_in[b] = log2((double)d_in[b]);
+    }
   sh[threadIdx.x] = s;
   shc[threadIdx.x] = c;
   __syncthreads();
@@ -571,23 +659,24 @@ __global__ void commit_kernel(int32_t* part, int32_t lo, int32_t count,
   if (threadIdx.x == 0) {
     *slot_sum += sh[0];
     *slot_acc += shc[0];
-    heavy_count[0] = 0;
   }
 }
 
 NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
-                    int32_t* heavy, int32_t* heavy_count) {
+                    const NodalAux& aux) {
   NodalArgs a{};
   a.optr = g.optr; a.oidx = g.oidx; a.iptr = g.iptr; a.iidx = g.iidx;
   a.ow = g.ow; a.iw = g.iw; a.kdo = g.kdo; a.kdi = g.kdi;
   a.part = part;
   a.bop = m.optr; a.boc = m.ocol; a.bip = m.iptr; a.bic = m.icol;
   a.bon = m.ocnt; a.bin = m.icnt; a.d_out = m.d_out; a.d_in = m.d_in;
+  a.Md = m.Md; a.MTd = m.MTd;
   a.ld_out = m.ld_out; a.ld_in = m.ld_in; a.dSout = m.dSout; a.ambout = m.ambout;
   a.ambin = m.ambin; a.sinfull = m.sinfull; a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
   a.B = B;
-  a.heavy = heavy;
-  a.heavy_count = heavy_count;
+  a.heavy = aux.heavy;
+  a.nheavy = aux.nheavy;
+  a.err = aux.err;
   return a;
 }
 
@@ -596,22 +685,45 @@ int nodal_grid(int count) {
   return g < 1 ? 1 : (g > 148 * 64 ? 148 * 64 : g);
 }
 
+template <bool GIVEN, bool DENSE>
+void launch_pair(const NodalArgs& a, const NodalAux& aux, cudaStream_t st) {
+  if (a.nheavy > 0) {
+    // heavy vertices on the side stream, next to the warp kernel
+    cudaEventRecord(aux.fork, st);
+    cudaStreamWaitEvent(aux.side, aux.fork, 0);
+    ++g_launches;
+    int grid = a.nheavy < 2 * 148 ? a.nheavy : 2 * 148;
+    nodal_heavy_kernel<GIVEN, DENSE><<<grid, kHeavyThreads, kHeavySmem, aux.side>>>(a);
+    cudaEventRecord(aux.join, aux.side);
+  }
+  ++g_launches;
+  nodal_kernel<GIVEN, DENSE><<<nodal_grid(a.count), kNodalWarps * 32, 0, st>>>(a);
+  if (a.nheavy > 0) cudaStreamWaitEvent(st, aux.join, 0);
+}
+
 }  // namespace
 
 cudaError_t init_nodal_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(nodal_heavy_kernel<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kHeavySmem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(nodal_heavy_kernel<true>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHeavySmem);
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* f) {
+    cudaError_t x = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kHeavySmem);
+    if (x != cudaSuccess) e = x;
+  };
+  set((const void*)nodal_heavy_kernel<false, false>);
+  set((const void*)nodal_heavy_kernel<false, true>);
+  set((const void*)nodal_heavy_kernel<true, false>);
+  set((const void*)nodal_heavy_kernel<true, true>);
+  return e;
 }
 
+int nodal_heavy_threshold() { return kWarpList; }
+
 void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
-                        uint64_t seed, uint32_t seq, int32_t lo, int32_t count, int32_t* newlab,
-                        double* rec, int32_t* props, int32_t* heavy, int32_t* heavy_count,
+                        bool dense, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
+                        int32_t* newlab, double* rec, int32_t* props, const NodalAux& aux,
                         cudaStream_t st) {
-  NodalArgs a = make_args(g, part, m, B, heavy, heavy_count);
+  NodalArgs a = make_args(g, part, m, B, aux);
   a.seed = seed;
   a.seq = seq;
   a.lo = lo;
@@ -620,33 +732,34 @@ void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, 
   a.rec = rec;
   a.props_out = props;
   if (count <= 0) return;
-  ++g_launches;
-  nodal_kernel<false><<<nodal_grid(count), kNodalWarps * 32, 0, st>>>(a);
-  ++g_launches;
-  nodal_heavy_kernel<false><<<148, kHeavyThreads, kHeavySmem, st>>>(a);
+  if (dense) launch_pair<false, true>(a, aux, st);
+  else launch_pair<false, false>(a, aux, st);
 }
 
 void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
-                       int32_t nv, const int32_t* verts, const int32_t* props, double* dS,
-                       int32_t* heavy, int32_t* heavy_count, cudaStream_t st) {
-  NodalArgs a = make_args(g, part, m, B, heavy, heavy_count);
+                       bool dense, int32_t nv, const int32_t* verts, const int32_t* props,
+                       double* dS, const NodalAux& aux, cudaStream_t st) {
+  NodalArgs a = make_args(g, part, m, B, aux);
   a.count = nv;
   a.verts = verts;
   a.props_in = props;
   a.dS_raw = dS;
   if (nv <= 0) return;
-  ++g_launches;
-  nodal_kernel<true><<<nodal_grid(nv), kNodalWarps * 32, 0, st>>>(a);
-  ++g_launches;
-  nodal_heavy_kernel<true><<<148, kHeavyThreads, kHeavySmem, st>>>(a);
+  if (dense) launch_pair<true, true>(a, aux, st);
+  else launch_pair<true, false>(a, aux, st);
 }
 
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
-                  const double* rec, double* slot_sum, long long* slot_acc, int32_t* heavy_count,
-                  cudaStream_t st) {
+                  const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
+                  int32_t B, cudaStream_t st) {
   ++g_launches;
-  commit_kernel<<<1, 1024, 0, st>>>(part, lo, count, newlab, rec, slot_sum, slot_acc,
-                                    heavy_count);
+  if (dense_m)
+    commit_kernel<<<1, 1024, 0, st>>>(part, lo, count, newlab, rec, slot_sum, slot_acc, B,
+                                      dense_m->d_out, dense_m->d_in, dense_m->ld_out,
+                                      dense_m->ld_in);
+  else
+    commit_kernel<<<1, 1024, 0, st>>>(part, lo, count, newlab, rec, slot_sum, slot_acc, 0,
+                                      nullptr, nullptr, nullptr, nullptr);
 }
 
 }  // namespace sbp

@@ -45,7 +45,8 @@ class Options(C.Structure):
                 ("reduction_rate", C.c_float), ("max_nodal_itr", C.c_int32),
                 ("num_batches", C.c_int32), ("threshold1", C.c_float),
                 ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32),
-                ("device", C.c_int32), ("use_graphs", C.c_int32), ("verbose", C.c_int32)]
+                ("device", C.c_int32), ("use_graphs", C.c_int32), ("verbose", C.c_int32),
+                ("dense_max", C.c_int32)]
 
 
 class Report(C.Structure):
@@ -94,6 +95,8 @@ _sig("sbp_merge_proposals", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_i
      C.c_uint32, _vp)
 _sig("sbp_nodal_batch", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint64, C.c_uint32,
      C.c_int32, C.c_int32, _vp, _vp, C.POINTER(C.c_double))
+_sig("sbp_nodal_sweeps", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint64, C.c_uint32,
+     C.c_int32, C.c_int32, C.c_int32, _vp)
 _sig("sbp_merge_step", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, C.c_int32,
      C.c_uint64, C.c_uint32, _vp, _vp, C.POINTER(C.c_int32))
 _sig("sbp_mdl", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.POINTER(C.c_double),
@@ -113,7 +116,7 @@ EXPORTED = [
     "sbp_default_options", "sbp_status_string", "sbp_last_error", "sbp_partition",
     "sbp_graph_upload", "sbp_graph_release", "sbp_partition_resident", "sbp_build_blockmodel",
     "sbp_delta_mdl_nodal", "sbp_delta_mdl_merge", "sbp_merge_proposals", "sbp_nodal_batch",
-    "sbp_merge_step", "sbp_mdl", "sbp_dcsbm_generate", "sbp_edges_size", "sbp_edges_copy",
+    "sbp_merge_step", "sbp_nodal_sweeps", "sbp_mdl", "sbp_dcsbm_generate", "sbp_edges_size", "sbp_edges_copy",
     "sbp_edges_free", "sbp_csr_from_edges", "sbp_load_tsv", "sbp_evaluate",
 ]
 
@@ -336,6 +339,16 @@ def nodal_batch(g: Graph, part, B, seed, seq, lo, hi):
     _check(_lib.sbp_nodal_batch(C.byref(g.csr()), _p(part), B, seed, seq, lo, hi, _p(dS),
                                 _p(props), C.byref(tot)))
     return part, dS[:hi - lo], props[:hi - lo], tot.value
+
+
+def nodal_sweeps(g: Graph, part, B, seed, seq0, num_batches=4, sweeps=1, dense_max=4096):
+    """`sweeps` nodal sweeps as the nodal phase runs them; returns the new
+    labels and the recorded dS sum of every batch."""
+    part = np.array(part, dtype=np.int32, copy=True)
+    sums = np.zeros(num_batches * sweeps, np.float64)
+    _check(_lib.sbp_nodal_sweeps(C.byref(g.csr()), _p(part), B, seed, seq0, num_batches, sweeps,
+                                 dense_max, _p(sums)))
+    return part, sums
 
 
 def merge_step(g: Graph, part, B, B_to_merge, seed, seq, np_=10):

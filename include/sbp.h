@@ -70,6 +70,8 @@ typedef struct sbp_options {
   int32_t device;          /* CUDA device ordinal, -1 = current device */
   int32_t use_graphs;      /* capture each nodal sweep in a CUDA graph */
   int32_t verbose;         /* 1: one line per outer step on stderr */
+  int32_t dense_max;       /* keep M as dense B x B matrices while B <= dense_max
+                              (default 4096; 0 = always CSR) */
 } sbp_options;
 
 /* What one partition run did.  Timings are CUDA-event milliseconds on the
@@ -150,6 +152,16 @@ sbp_status sbp_merge_proposals(const sbp_graph_csr* g, const int32_t* part, int3
 sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
                            uint32_t seq, int32_t lo, int32_t hi, double* dS_rec, int32_t* props,
                            double* sum);
+
+/* `sweeps` nodal sweeps of `num_batches` Jacobi batches each, as the nodal
+ * phase of partition() runs them (partition.hpp:912-916): batch k uses the
+ * Philox stream (seed, seq0 + k).  The blockmodel is kept dense while
+ * B <= dense_max (updated from the moved vertices' edges after each batch),
+ * else rebuilt as CSR.  Labels updated in place; sums[k] = recorded dS sum
+ * of batch k (sweeps * num_batches entries). */
+sbp_status sbp_nodal_sweeps(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
+                            uint32_t seq0, int32_t num_batches, int32_t sweeps, int32_t dense_max,
+                            double* sums);
 
 /* One merge step (propose_block_merge + carry_out_best_merges,
  * partition.hpp:26-78, 324-454): labels updated in place; *B_new receives the
