@@ -374,6 +374,7 @@ __global__ void rb_compact(RbArgs a) {
 
 // ------------------------------------------------------------ block terms --
 struct BtArgs {
+  const double* xlx;
   const int32_t *optr, *ocol, *iptr, *icol;
   const uint32_t *ocnt, *icnt, *d_out, *d_in;
   const double *ld_out, *ld_in;
@@ -422,13 +423,13 @@ __global__ void block_terms_kernel(BtArgs a) {
     double acc = 0.0;
     for (int i = a.optr[b] + lane; i < a.optr[b + 1]; i += 32) {
       uint32_t m = a.ocnt[i];
-      acc += xlog2x(m) - (double)m * a.ld_in[a.ocol[i]];
+      acc += xlx(a.xlx, m) - (double)m * a.ld_in[a.ocol[i]];
     }
     double ao = warp_sum(acc);
     acc = 0.0;
     for (int i = a.iptr[b] + lane; i < a.iptr[b + 1]; i += 32) {
       uint32_t m = a.icnt[i];
-      acc += xlog2x(m) - (double)m * a.ld_out[a.icol[i]];
+      acc += xlx(a.xlx, m) - (double)m * a.ld_out[a.icol[i]];
     }
     double ai = warp_sum(acc);
     if (lane == 0) {
@@ -572,6 +573,7 @@ __device__ int warp_pick_dense(const uint32_t* orow, const uint32_t* irow, int B
 }
 
 struct BtDenseArgs {
+  const double* xlx;
   const uint32_t *Md, *MTd, *d_out, *d_in;
   const double *ld_out, *ld_in;
   double *dSout, *ambout, *ambin, *sinfull;
@@ -594,8 +596,8 @@ __global__ void block_terms_dense_kernel(BtDenseArgs a) {
     double ao = 0.0, ai = 0.0;
     for (int c = lane; c < B; c += 32) {
       uint32_t mo = orow[c], mi = irow[c];
-      if (mo) ao += xlog2x(mo) - (double)mo * a.ld_in[c];
-      if (mi) ai += xlog2x(mi) - (double)mi * a.ld_out[c];
+      if (mo) ao += xlx(a.xlx, mo) - (double)mo * a.ld_in[c];
+      if (mi) ai += xlx(a.xlx, mi) - (double)mi * a.ld_out[c];
     }
     ao = warp_sum(ao);
     ai = warp_sum(ai);
@@ -620,6 +622,11 @@ __global__ void block_terms_dense_kernel(BtDenseArgs a) {
       }
     }
   }
+}
+
+__global__ void fill_xlx_kernel(double* tab) {
+  uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x < kXlxTable) tab[x] = xlog2x(x);
 }
 
 __global__ void mdl_sum_kernel(const double* __restrict__ dSout, int32_t B, double* out) {
@@ -717,6 +724,7 @@ void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM
 
 void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cudaStream_t st) {
   BtArgs a;
+  a.xlx = m.xlx;
   a.optr = m.optr; a.ocol = m.ocol; a.iptr = m.iptr; a.icol = m.icol;
   a.ocnt = m.ocnt; a.icnt = m.icnt; a.d_out = m.d_out; a.d_in = m.d_in;
   a.ld_out = m.ld_out; a.ld_in = m.ld_in;
@@ -725,6 +733,11 @@ void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cu
   a.B = B; a.draws = draws; a.seed = seed; a.seq = seq;
   ++g_launches;
   block_terms_kernel<<<grid_for((long long)B * 32, 256, 8192), 256, 0, st>>>(a);
+}
+
+void fill_xlx_table(double* tab, cudaStream_t st) {
+  ++g_launches;
+  fill_xlx_kernel<<<kXlxTable / 256, 256, 0, st>>>(tab);
 }
 
 void dense_build(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, cudaStream_t st) {
@@ -757,6 +770,7 @@ void dense_update(const DevGraph& g, const int32_t* part, int32_t lo, int32_t co
 void block_terms_dense(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq,
                        cudaStream_t st) {
   BtDenseArgs a;
+  a.xlx = m.xlx;
   a.Md = m.Md; a.MTd = m.MTd; a.d_out = m.d_out; a.d_in = m.d_in;
   a.ld_out = m.ld_out; a.ld_in = m.ld_in;
   a.dSout = m.dSout; a.ambout = m.ambout; a.ambin = m.ambin; a.sinfull = m.sinfull;

@@ -116,6 +116,16 @@ __device__ __forceinline__ double xlog2x(uint32_t w) {
   return w == 0u ? 0.0 : (double)w * log2((double)w);
 }
 
+// x*log2(x) of small counts from a table (tab[x] holds exactly
+// xlog2x(x), filled on the device), larger ones computed.
+constexpr uint32_t kXlxTable = 1u << 16;
+static __device__ __forceinline__ double xlog2x_big(uint32_t w) {
+  return (double)w * log2((double)w);
+}
+__device__ __forceinline__ double xlx(const double* __restrict__ tab, uint32_t w) {
+  return w < kXlxTable ? __ldg(tab + w) : xlog2x_big(w);
+}
+
 // Binary search of column c in the CSR row [lo, hi); its count, or 0.
 __device__ __forceinline__ uint32_t row_lookup(const int32_t* __restrict__ col,
                                                const uint32_t* __restrict__ cnt, int32_t lo,

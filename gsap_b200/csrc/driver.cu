@@ -118,6 +118,7 @@ struct Job {
   double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
   int32_t* heavy = nullptr;     // batch indices of the CTA-per-vertex kernel
   int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
+  CommitScratch cs;
   int32_t dense_cap = 0;        // largest B the dense arrays can hold
   int32_t dense_eff = 0;        // largest B kept in dense form in this run
   cudaStream_t side = nullptr;  // heavy vertices run here, next to the warp kernel
@@ -197,6 +198,7 @@ static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32
   add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
   add((size_t)N, 4); add(2, 4);
   add((size_t)dense_cap * dense_cap, 4); add((size_t)dense_cap * dense_cap, 4);
+  add(kXlxTable, 8); add(kCommitCtas, 8); add(kCommitCtas, 8); add(1, 4);
   return b + 4096;
 }
 
@@ -279,8 +281,14 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
     m.Md = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
     m.MTd = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
   }
-  if (!J.err || (J.dense_cap > 0 && !m.MTd)) return fail(SBP_ERR_INTERNAL, "arena sizing");
+  m.xlx = A.take<double>(kXlxTable);
+  J.cs.part_sum = A.take<double>(kCommitCtas);
+  J.cs.part_cnt = A.take<long long>(kCommitCtas);
+  J.cs.ticket = A.take<unsigned>(1);
+  if (!J.cs.ticket || (J.dense_cap > 0 && !m.MTd)) return fail(SBP_ERR_INTERNAL, "arena sizing");
   SBP_CUDA(cudaMemsetAsync(J.err, 0, 8, J.st));
+  SBP_CUDA(cudaMemsetAsync(J.cs.ticket, 0, 4, J.st));
+  fill_xlx_table(m.xlx, J.st);
   return SBP_OK;
 }
 
@@ -537,10 +545,10 @@ static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_ou
           // labels change (it reads old and new labels)
           dense_update(J.g, J.part, b * BS, BS, J.newlab, B, J.m, st);
           nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, &J.m, B,
-                       st);
+                       J.cs, st);
         } else {
           nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, nullptr,
-                       0, st);
+                       0, J.cs, st);
         }
         ++seq;
         SBP_CUDA(cudaEventRecord(J.bev[4 * b + 3], st));
@@ -939,7 +947,7 @@ sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uin
   SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8, J.st));
   nodal_batch_sample(J.g, J.part, J.m, B, dense, seed, seq, lo, cnt, J.newlab, J.rec, J.props,
                      aux_for(J, J.heavy, (int32_t)hv.size()), J.st);
-  nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, nullptr, 0, J.st);
+  nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, nullptr, 0, J.cs, J.st);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());
   SBP_CUDA(cudaMemcpy(part, J.part, 4 * (size_t)J.N, cudaMemcpyDeviceToHost));
@@ -988,9 +996,9 @@ sbp_status sbp_nodal_sweeps(const sbp_graph_csr* g, int32_t* part, int32_t B, ui
                        aux, st);
     if (dense) {
       dense_update(J.g, J.part, b * BS, BS, J.newlab, B, J.m, st);
-      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, &J.m, B, st);
+      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, &J.m, B, J.cs, st);
     } else {
-      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, nullptr, 0, st);
+      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, nullptr, 0, J.cs, st);
       rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
     }
     ++seq;

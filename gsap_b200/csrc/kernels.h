@@ -35,7 +35,20 @@ struct DevBM {
   // dense form for small B: Md[r*B + c] = M[r][c], MTd[c*B + r] = M[r][c]
   uint32_t* Md = nullptr;
   uint32_t* MTd = nullptr;
+  // xlx[x] = x log2 x for x < kXlxTable (filled by fill_xlx_table)
+  double* xlx = nullptr;
 };
+
+// Fills the x log2 x table of a job.
+void fill_xlx_table(double* tab, cudaStream_t st);
+
+// Scratch of the multi-CTA commit (partial sums of each CTA, a ticket).
+struct CommitScratch {
+  double* part_sum = nullptr;
+  long long* part_cnt = nullptr;
+  unsigned* ticket = nullptr;  // must be 0 between commits
+};
+constexpr int kCommitCtas = 64;
 
 // Scratch of one rebuild direction.
 struct RebuildDir {
@@ -114,7 +127,7 @@ void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, i
 // log2 of its block degrees.
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                   const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
-                  int32_t B, cudaStream_t st);
+                  int32_t B, const CommitScratch& cs, cudaStream_t st);
 
 // Merge proposals (kernels.hpp:726-856) and their dS with the per-block best
 // (kernels.hpp:143-491).

@@ -21,6 +21,7 @@ namespace sbp {
 namespace {
 
 struct MergeArgs {
+  const double* xlx;
   const int32_t *optr, *ocol, *iptr, *icol;
   const uint32_t *ocnt, *icnt, *d_out, *d_in;
   const double *ld_out, *ld_in, *dSout, *ambout, *ambin, *sinfull;
@@ -86,11 +87,11 @@ __global__ void merge_props_kernel(MergeArgs a) {
   a.props[t] = s;
 }
 
-__device__ __forceinline__ double gterm(uint32_t x, double ld) {
-  return x == 0u ? 0.0 : (double)x * log2((double)x) - (double)x * ld;
+__device__ __forceinline__ double gterm(const double* tab, uint32_t x, double ld) {
+  return x == 0u ? 0.0 : xlx(tab, x) - (double)x * ld;
 }
-__device__ __forceinline__ double fterm(uint32_t m, double a, double b) {
-  return m == 0u ? 0.0 : (double)m * (log2((double)m) - (a + b));
+__device__ __forceinline__ double fterm(const double* tab, uint32_t m, double a, double b) {
+  return m == 0u ? 0.0 : xlx(tab, m) - (double)m * (a + b);
 }
 
 // Merge dS of block r with s (calculate_dS_overall, kernels.hpp:417-449),
@@ -105,10 +106,10 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) 
   const uint32_t Mss = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], s);
   if (r == s) {
     for (int i = a.optr[r] + lane; i < a.optr[r + 1]; i += 32)
-      acc_o += gterm(2u * a.ocnt[i], a.ld_in[a.ocol[i]]);
+      acc_o += gterm(a.xlx, 2u * a.ocnt[i], a.ld_in[a.ocol[i]]);
     for (int i = a.iptr[r] + lane; i < a.iptr[r + 1]; i += 32) {
       int c = a.icol[i];
-      if (c != r) acc_i += gterm(2u * a.icnt[i], a.ld_out[c]);
+      if (c != r) acc_i += gterm(a.xlx, 2u * a.icnt[i], a.ld_out[c]);
     }
   } else {
     int x = r, y = s;
@@ -118,7 +119,7 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) 
       int c = a.ocol[i];
       double ld = a.ld_in[c];
       uint32_t my = row_lookup(a.ocol, a.ocnt, y0, y1, c);
-      acc_o += gterm(a.ocnt[i] + my, ld) - gterm(my, ld);
+      acc_o += gterm(a.xlx, a.ocnt[i] + my, ld) - gterm(a.xlx, my, ld);
     }
     if (lane == 0) acc_o += a.ambout[y];
     x = r; y = s;
@@ -129,13 +130,13 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) 
       if (c == r || c == s) continue;
       double ld = a.ld_out[c];
       uint32_t my = row_lookup(a.icol, a.icnt, y0, y1, c);
-      acc_i += gterm(a.icnt[i] + my, ld) - gterm(my, ld);
+      acc_i += gterm(a.xlx, a.icnt[i] + my, ld) - gterm(a.xlx, my, ld);
     }
     if (lane == 0) {
       // in-row y's own terms at columns r and s stay out
       uint32_t yr = y == r ? Mrr : Mrs;  // M[r][y]
       uint32_t ys = y == r ? Msr : Mss;  // M[s][y]
-      acc_i += a.ambin[y] - gterm(yr, ldo_r) - gterm(ys, ldo_s);
+      acc_i += a.ambin[y] - gterm(a.xlx, yr, ldo_r) - gterm(a.xlx, ys, ldo_s);
     }
   }
   acc_o = warp_sum(acc_o);
@@ -151,9 +152,9 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) 
   if (mass_i != 0) new_in += log2((double)(uint32_t)(dis + dir)) * (double)mass_i;
   // old in-rows (calculate_dS_in, kernels.hpp:185-231): row r without r, s;
   // row s without s, s2
-  double in_r = a.sinfull[r] - fterm(Mrr, ldo_r, ldi_r) - (s != r ? fterm(Msr, ldo_s, ldi_r) : 0.0);
+  double in_r = a.sinfull[r] - fterm(a.xlx, Mrr, ldo_r, ldi_r) - (s != r ? fterm(a.xlx, Msr, ldo_s, ldi_r) : 0.0);
   uint32_t Ms2s = s2 == s ? 0u : row_lookup(a.ocol, a.ocnt, a.optr[s2], a.optr[s2 + 1], s);
-  double in_s = a.sinfull[s] - fterm(Mss, ldo_s, ldi_s) - fterm(Ms2s, a.ld_out[s2], ldi_s);
+  double in_s = a.sinfull[s] - fterm(a.xlx, Mss, ldo_s, ldi_s) - fterm(a.xlx, Ms2s, a.ld_out[s2], ldi_s);
   return a.dSout[r] + a.dSout[s] + in_r + in_s + new_out + new_in;
 }
 
@@ -196,6 +197,7 @@ __global__ void relabel_kernel(int32_t* part, int32_t N, const int32_t* __restri
 
 MergeArgs make_args(const DevBM& m, int32_t B, int32_t np) {
   MergeArgs a{};
+  a.xlx = m.xlx;
   a.optr = m.optr; a.ocol = m.ocol; a.iptr = m.iptr; a.icol = m.icol;
   a.ocnt = m.ocnt; a.icnt = m.icnt; a.d_out = m.d_out; a.d_in = m.d_in;
   a.ld_out = m.ld_out; a.ld_in = m.ld_in; a.dSout = m.dSout; a.ambout = m.ambout;

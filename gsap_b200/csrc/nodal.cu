@@ -49,6 +49,7 @@ constexpr size_t kHeavySmem =
         : 3 * kHashSlotsCfg * sizeof(int32_t);
 
 struct NodalArgs {
+  const double* xlx;        // x log2 x table
   const int32_t *optr, *oidx, *iptr, *iidx;
   const uint32_t *ow, *iw, *kdo, *kdi;
   const int32_t* part;
@@ -74,12 +75,8 @@ struct NodalArgs {
 };
 
 // g(x, a) = x log2 x - x a, zero for x == 0
-__device__ __forceinline__ double gterm(uint32_t x, double a) {
-  return x == 0u ? 0.0 : (double)x * log2((double)x) - (double)x * a;
-}
-// f(M; a, b) = M (log2 M - (a + b)), zero for M == 0 (one old term)
-__device__ __forceinline__ double fterm(uint32_t m, double a, double b) {
-  return m == 0u ? 0.0 : (double)m * (log2((double)m) - (a + b));
+__device__ __forceinline__ double gterm(const double* tab, uint32_t x, double a) {
+  return x == 0u ? 0.0 : xlx(tab, x) - (double)x * a;
 }
 
 // The four rows a move from r to s reads: out-rows r and s, in-rows r and s.
@@ -131,18 +128,18 @@ __device__ __forceinline__ void out_entry(const NodalArgs& a, const Rows<DENSE>&
   if (leader && c != r && c != s) {
     const uint32_t Mrc = R.out_r(c);
     const uint32_t x = Mrc - kc;
-    q.a4 += gterm(x, ldc) - gterm(Mrc, ldc);
+    q.a4 += gterm(a.xlx, x, ldc) - gterm(a.xlx, Mrc, ldc);
     q.m4 += (long long)x - (long long)Mrc;
     if (Msc != 0u) {
       const uint32_t y = Msc + kc;
-      q.a5 += gterm(y, ldc) - gterm(Msc, ldc);
+      q.a5 += gterm(a.xlx, y, ldc) - gterm(a.xlx, Msc, ldc);
       q.m5 += (long long)y - (long long)Msc;
     }
   }
   if (Msc == 0u) {
     // block c absent from row s: one term per list entry
     const uint32_t y = w - (c == r ? niS : 0u) + (c == s ? niS : 0u);
-    q.a5 += gterm(y, ldc);
+    q.a5 += gterm(a.xlx, y, ldc);
     q.m5 += (long long)y;
   }
 }
@@ -158,76 +155,116 @@ __device__ __forceinline__ void in_entry(const NodalArgs& a, const Rows<DENSE>& 
   if (leader) {
     const uint32_t Mcr = R.in_r(c);
     const uint32_t x = Mcr - kc;
-    q.a6 += gterm(x, ldc) - gterm(Mcr, ldc);
+    q.a6 += gterm(a.xlx, x, ldc) - gterm(a.xlx, Mcr, ldc);
     q.m6 += (long long)x - (long long)Mcr;
     if (Mcs != 0u) {
       const uint32_t y = Mcs + kc;
-      q.a7 += gterm(y, ldc) - gterm(Mcs, ldc);
+      q.a7 += gterm(a.xlx, y, ldc) - gterm(a.xlx, Mcs, ldc);
       q.m7 += (long long)y - (long long)Mcs;
     }
   }
   if (Mcs == 0u) {
-    q.a7 += gterm(w, ldc);
+    q.a7 += gterm(a.xlx, w, ldc);
     q.m7 += (long long)w;
   }
 }
 
-// The (r, s) corner, the old terms and the new-row totals (every thread of
-// the group holds the reduced q and gets the same result).
+// The (r, s) corner, the old terms and the new-row totals.  Every thread
+// of the group holds the reduced q and returns the same value; the dozen
+// logarithms involved are computed once each, spread over the lanes of each
+// warp and broadcast with shuffles.
 template <bool DENSE>
 __device__ double finish_delta(const NodalArgs& a, const Rows<DENSE>& R, int v, int r, int s,
                                uint32_t koR, uint32_t koS, uint32_t niR, uint32_t niS, Acc q) {
-  const uint32_t Mrr = R.out_r(r);
-  const uint32_t Mrs = R.out_r(s);
-  const uint32_t Msr = R.out_s(r);
-  const uint32_t Mss = R.out_s(s);
+  const int lane = threadIdx.x & 31;
+  uint32_t m = 0u;
+  if (lane == 0) m = R.out_r(r);
+  else if (lane == 1) m = R.out_r(s);
+  else if (lane == 2) m = R.out_s(r);
+  else if (lane == 3) m = R.out_s(s);
+  const uint32_t Mrr = __shfl_sync(kFull, m, 0), Mrs = __shfl_sync(kFull, m, 1);
+  const uint32_t Msr = __shfl_sync(kFull, m, 2), Mss = __shfl_sync(kFull, m, 3);
+  const uint32_t kO = a.kdo[v], kI = a.kdi[v];
+  const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
+  // new counts of the corner cells (kernels.hpp:1506-1510, 1573-1578,
+  // 1663-1669, 1718-1723); when Mrs (Mss) is 0 the extra column term holds
+  // niR (niS)
+  const uint32_t xrr = Mrr - koR - niR;
+  const uint32_t xrs = Mrs != 0u ? Mrs - koS + niR : niR;
+  const uint32_t xsr = Msr + koR - niS;
+  const uint32_t xss = Mss != 0u ? Mss + koS + niS : niS;
+  uint32_t arg = 0u;
+  switch (lane) {
+    case 0: arg = Mrr; break;
+    case 1: arg = Mrs; break;
+    case 2: arg = Msr; break;
+    case 3: arg = Mss; break;
+    case 4: arg = xrr; break;
+    case 5: arg = xrs; break;
+    case 6: arg = xsr; break;
+    case 7: arg = xss; break;
+    case 8: arg = dor - kO; break;
+    case 9: arg = dos + kO; break;
+    case 10: arg = dir - kI; break;
+    case 11: arg = dis + kI; break;
+    default: break;
+  }
+  double val = 0.0;
+  if (lane < 8) val = arg == 0u ? 0.0 : xlx(a.xlx, arg);
+  else if (lane < 12) val = log2((double)arg);
+  const double XMrr = __shfl_sync(kFull, val, 0), XMrs = __shfl_sync(kFull, val, 1);
+  const double XMsr = __shfl_sync(kFull, val, 2), XMss = __shfl_sync(kFull, val, 3);
+  const double Xrr = __shfl_sync(kFull, val, 4), Xrs = __shfl_sync(kFull, val, 5);
+  const double Xsr = __shfl_sync(kFull, val, 6), Xss = __shfl_sync(kFull, val, 7);
+  const double L4 = __shfl_sync(kFull, val, 8), L5 = __shfl_sync(kFull, val, 9);
+  const double L6 = __shfl_sync(kFull, val, 10), L7 = __shfl_sync(kFull, val, 11);
   const double ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
   const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s];
+  // g(x, a) = x log2 x - x a from the broadcast x log2 x
+  auto g = [](double xl, uint32_t x, double ld) { return x == 0u ? 0.0 : xl - (double)x * ld; };
+  // f(M; a, b) = M log2 M - M (a + b)
+  auto f = [](double xl, uint32_t x, double l1, double l2) {
+    return x == 0u ? 0.0 : xl - (double)x * (l1 + l2);
+  };
   if (Mrr != 0u) {
-    uint32_t x = Mrr - koR - niR;
-    q.a4 += gterm(x, ldi_r) - gterm(Mrr, ldi_r);
-    q.m4 += (long long)x - (long long)Mrr;
+    q.a4 += g(Xrr, xrr, ldi_r) - g(XMrr, Mrr, ldi_r);
+    q.m4 += (long long)xrr - (long long)Mrr;
   }
   if (Mrs != 0u) {
-    uint32_t x = Mrs - koS + niR;
-    q.a4 += gterm(x, ldi_s) - gterm(Mrs, ldi_s);
-    q.m4 += (long long)x - (long long)Mrs;
+    q.a4 += g(Xrs, xrs, ldi_s) - g(XMrs, Mrs, ldi_s);
+    q.m4 += (long long)xrs - (long long)Mrs;
   } else if (niR > 0u) {
-    q.a4 += gterm(niR, ldi_s);
+    q.a4 += g(Xrs, niR, ldi_s);
     q.m4 += (long long)niR;
   }
   if (Msr != 0u) {
-    uint32_t x = Msr + koR - niS;
-    q.a5 += gterm(x, ldi_r) - gterm(Msr, ldi_r);
-    q.m5 += (long long)x - (long long)Msr;
+    q.a5 += g(Xsr, xsr, ldi_r) - g(XMsr, Msr, ldi_r);
+    q.m5 += (long long)xsr - (long long)Msr;
   }
   if (Mss != 0u) {
-    uint32_t x = Mss + koS + niS;
-    q.a5 += gterm(x, ldi_s) - gterm(Mss, ldi_s);
-    q.m5 += (long long)x - (long long)Mss;
+    q.a5 += g(Xss, xss, ldi_s) - g(XMss, Mss, ldi_s);
+    q.m5 += (long long)xss - (long long)Mss;
   } else if (koS == 0u && niS > 0u) {
-    q.a5 += gterm(niS, ldi_s);
+    q.a5 += g(Xss, niS, ldi_s);
     q.m5 += (long long)niS;
   }
-  const uint32_t kO = a.kdo[v], kI = a.kdi[v];
-  const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
   // old terms (calculate_dS_out, calculate_dS_in_nodal_r/_s)
   double t1 = a.dSout[r] + a.dSout[s];
-  double t2 = a.sinfull[r] - fterm(Mrr, ldo_r, ldi_r) - fterm(Msr, ldo_s, ldi_r);
-  double t3 = a.sinfull[s] - fterm(Mrs, ldo_r, ldi_s) - fterm(Mss, ldo_s, ldi_s);
+  double t2 = a.sinfull[r] - f(XMrr, Mrr, ldo_r, ldi_r) - f(XMsr, Msr, ldo_s, ldi_r);
+  double t3 = a.sinfull[s] - f(XMrs, Mrs, ldo_r, ldi_s) - f(XMss, Mss, ldo_s, ldi_s);
   // new rows r and s, out and in
   long long mass4 = (long long)dor + q.m4;
   long long mass5 = (long long)dos + q.m5;
   long long mass6 = (long long)dir - (long long)Mrr - (long long)Msr + q.m6;
   long long mass7 = (long long)dis - (long long)Mrs - (long long)Mss + q.m7;
   double t4 = a.ambout[r] + q.a4;
-  if (mass4 != 0) t4 -= log2((double)(uint32_t)(dor - kO)) * (double)mass4;
+  if (mass4 != 0) t4 -= L4 * (double)mass4;
   double t5 = a.ambout[s] + q.a5;
-  if (mass5 != 0) t5 -= log2((double)(uint32_t)(dos + kO)) * (double)mass5;
-  double t6 = a.ambin[r] - gterm(Mrr, ldo_r) - gterm(Msr, ldo_s) + q.a6;
-  if (mass6 != 0) t6 -= log2((double)(uint32_t)(dir - kI)) * (double)mass6;
-  double t7 = a.ambin[s] - gterm(Mrs, ldo_r) - gterm(Mss, ldo_s) + q.a7;
-  if (mass7 != 0) t7 -= log2((double)(uint32_t)(dis + kI)) * (double)mass7;
+  if (mass5 != 0) t5 -= L5 * (double)mass5;
+  double t6 = a.ambin[r] - g(XMrr, Mrr, ldo_r) - g(XMsr, Msr, ldo_s) + q.a6;
+  if (mass6 != 0) t6 -= L6 * (double)mass6;
+  double t7 = a.ambin[s] - g(XMrs, Mrs, ldo_r) - g(XMss, Mss, ldo_s) + q.a7;
+  if (mass7 != 0) t7 -= L7 * (double)mass7;
   return t1 + t2 + t3 - t4 - t5 - t6 - t7;
 }
 
@@ -550,7 +587,7 @@ __device__ __forceinline__ bool is_heavy(int no, int ni) {
 }
 
 template <bool GIVEN, bool DENSE>
-__global__ void __launch_bounds__(kNodalWarps * 32, 4) nodal_kernel(NodalArgs a) {
+__global__ void __launch_bounds__(kNodalWarps * 32, 3) nodal_kernel(NodalArgs a) {
   __shared__ unsigned long long s_ko[kNodalWarps][kWarpList], s_ki[kNodalWarps][kWarpList];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = gridDim.x * kNodalWarps;
@@ -582,7 +619,7 @@ __global__ void __launch_bounds__(kNodalWarps * 32, 4) nodal_kernel(NodalArgs a)
 // lists sorted in shared memory up to kHeavyList entries, longer ones
 // through the hashed passes.
 template <bool GIVEN, bool DENSE>
-__global__ void __launch_bounds__(kHeavyThreads) nodal_heavy_kernel(NodalArgs a) {
+__global__ void __launch_bounds__(kHeavyThreads, 2) nodal_heavy_kernel(NodalArgs a) {
   extern __shared__ unsigned long long hsm[];
   __shared__ double red[kHeavyThreads / 32];
   __shared__ int flag, sh_v, sh_s;
@@ -621,19 +658,25 @@ __global__ void __launch_bounds__(kHeavyThreads) nodal_heavy_kernel(NodalArgs a)
   }
 }
 
-// One CTA: applies the batch's labels and sums its recorded dS in a fixed
-// order (deterministic across runs).  In dense mode it also refreshes the
-// log2 of the block degrees that dense_update changed.
-__global__ void commit_kernel(int32_t* part, int32_t lo, int32_t count,
-                              const int32_t* __restrict__ newlab, const double* __restrict__ rec,
-                              double* slot_sum, long long* slot_acc, int32_t B,
-                              const uint32_t* __restrict__ d_out,
-                              const uint32_t* __restrict__ d_in, double* ld_out, double* ld_in) {
-  __shared__ double sh[1024];
-  __shared__ long long shc[1024];
+// Applies the batch's labels and sums its recorded dS.  Each CTA sums a fixed
+// slice in a fixed order into its own partial; the last CTA to finish (a
+// ticket, no waiting) adds the partials in CTA order, so the result does
+// not depend on scheduling.  In dense mode the CTAs also refresh the log2 of
+// the block degrees that dense_update changed.
+constexpr int kCommitThreads = 512;
+
+__global__ void __launch_bounds__(kCommitThreads) commit_kernel(
+    int32_t* part, int32_t lo, int32_t count, const int32_t* __restrict__ newlab,
+    const double* __restrict__ rec, double* slot_sum, long long* slot_acc, int32_t B,
+    const uint32_t* __restrict__ d_out, const uint32_t* __restrict__ d_in, double* ld_out,
+    double* ld_in, double* part_sum, long long* part_cnt, unsigned* ticket) {
+  __shared__ double sh[kCommitThreads];
+  __shared__ long long shc[kCommitThreads];
+  __shared__ bool last;
+  const int tid = threadIdx.x;
   double s = 0.0;
   long long c = 0;
-  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+  for (int i = blockIdx.x * kCommitThreads + tid; i < count; i += gridDim.x * kCommitThreads) {
     int32_t nl = newlab[i];
     if (part[lo + i] != nl) {
       part[lo + i] = nl;
@@ -642,29 +685,45 @@ __global__ void commit_kernel(int32_t* part, int32_t lo, int32_t count,
     s += rec[i];
   }
   if (ld_out)
-    for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    for (int b = blockIdx.x * kCommitThreads + tid; b < B; b += gridDim.x * kCommitThreads) {
       ld_out[b] = log2((double)d_out[b]);
       ld_in[b] = log2((double)d_in[b]);
     }
-  sh[threadIdx.x] = s;
-  shc[threadIdx.x] = c;
+  sh[tid] = s;
+  shc[tid] = c;
   __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) {
-      sh[threadIdx.x] += sh[threadIdx.x + o];
-      shc[threadIdx.x] += shc[threadIdx.x + o];
+  for (int o = kCommitThreads / 2; o > 0; o >>= 1) {
+    if (tid < o) {
+      sh[tid] += sh[tid + o];
+      shc[tid] += shc[tid + o];
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    *slot_sum += sh[0];
-    *slot_acc += shc[0];
+  if (tid == 0) {
+    part_sum[blockIdx.x] = sh[0];
+    part_cnt[blockIdx.x] = shc[0];
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && tid == 0) {
+    __threadfence();
+    double t = 0.0;
+    long long n = 0;
+    for (int k = 0; k < (int)gridDim.x; ++k) {
+      t += ((volatile double*)part_sum)[k];
+      n += ((volatile long long*)part_cnt)[k];
+    }
+    *slot_sum += t;
+    *slot_acc += n;
+    *ticket = 0u;
   }
 }
 
 NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                     const NodalAux& aux) {
   NodalArgs a{};
+  a.xlx = m.xlx;
   a.optr = g.optr; a.oidx = g.oidx; a.iptr = g.iptr; a.iidx = g.iidx;
   a.ow = g.ow; a.iw = g.iw; a.kdo = g.kdo; a.kdi = g.kdi;
   a.part = part;
@@ -751,15 +810,13 @@ void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, i
 
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                   const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
-                  int32_t B, cudaStream_t st) {
+                  int32_t B, const CommitScratch& cs, cudaStream_t st) {
   ++g_launches;
-  if (dense_m)
-    commit_kernel<<<1, 1024, 0, st>>>(part, lo, count, newlab, rec, slot_sum, slot_acc, B,
-                                      dense_m->d_out, dense_m->d_in, dense_m->ld_out,
-                                      dense_m->ld_in);
-  else
-    commit_kernel<<<1, 1024, 0, st>>>(part, lo, count, newlab, rec, slot_sum, slot_acc, 0,
-                                      nullptr, nullptr, nullptr, nullptr);
+  commit_kernel<<<kCommitCtas, kCommitThreads, 0, st>>>(
+      part, lo, count, newlab, rec, slot_sum, slot_acc, dense_m ? B : 0,
+      dense_m ? dense_m->d_out : nullptr, dense_m ? dense_m->d_in : nullptr,
+      dense_m ? dense_m->ld_out : nullptr, dense_m ? dense_m->ld_in : nullptr, cs.part_sum,
+      cs.part_cnt, cs.ticket);
 }
 
 }  // namespace sbp
