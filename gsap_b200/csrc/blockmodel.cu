@@ -420,6 +420,7 @@ __global__ void block_terms_kernel(BtArgs a) {
   int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int nw = (gridDim.x * blockDim.x) >> 5;
   for (int b = w; b < a.B; b += nw) {
+   if (a.draws != 1) {
     double acc = 0.0;
     for (int i = a.optr[b] + lane; i < a.optr[b + 1]; i += 32) {
       uint32_t m = a.ocnt[i];
@@ -439,6 +440,7 @@ __global__ void block_terms_kernel(BtArgs a) {
       a.ambin[b] = ai;
       a.sinfull[b] = ai - (din ? (double)din * a.ld_in[b] : 0.0);
     }
+   }
     if (a.draws) {
       P4 x = draw(a.seed, kRngNodalBlock, a.seq, (uint32_t)b);
       uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
@@ -593,6 +595,7 @@ __global__ void block_terms_dense_kernel(BtDenseArgs a) {
   for (int b = w; b < B; b += nw) {
     const uint32_t* orow = a.Md + (size_t)b * B;
     const uint32_t* irow = a.MTd + (size_t)b * B;
+   if (a.draws != 1) {
     double ao = 0.0, ai = 0.0;
     for (int c = lane; c < B; c += 32) {
       uint32_t mo = orow[c], mi = irow[c];
@@ -608,6 +611,7 @@ __global__ void block_terms_dense_kernel(BtDenseArgs a) {
       a.ambin[b] = ai;
       a.sinfull[b] = ai - (din ? (double)din * a.ld_in[b] : 0.0);
     }
+   }
     if (a.draws) {
       P4 x = draw(a.seed, kRngNodalBlock, a.seq, (uint32_t)b);
       uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];

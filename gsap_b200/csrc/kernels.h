@@ -76,9 +76,10 @@ void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, c
 void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
                         RebuildScratch& rs, cudaStream_t st);
 
-// Per-block sums (dSout, ambout, ambin, sinfull).  With draws != 0, also the
-// per-block draws of nodal batch `seq` (choose_neighbored_block and the
-// per-block uniform, kernels.hpp:942-997, 1024).
+// Per-block work: draws == 0 computes the per-block sums (dSout, ambout,
+// ambin, sinfull; the MDL and the merge phase read them), draws == 1 only
+// the per-block draws of nodal batch `seq` (choose_neighbored_block and the
+// per-block uniform, kernels.hpp:942-997, 1024), draws == 2 both.
 void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cudaStream_t st);
 
 // Dense form (B*B counts and their transpose, degrees and their log2) of the

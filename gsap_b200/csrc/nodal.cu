@@ -15,13 +15,13 @@
 //     __match_any_sync / __reduce_add_sync when a list fits a warp, else
 //     sorted in shared memory (bitonic), else hashed in shared memory in
 //     passes; GSAP sorts all E entries every batch;
-//   * dS: GSAP's seven terms rewritten as "old row sum + changed columns".
+//   * dS: GSAP's seven terms rewritten as "changed cells + row degrees".
 //     A row term  sum_c f(x_c)  with  f(x) = x (log2 x - log2 dcol[c] - L)
 //     splits into  sum_c (x log2 x - x log2 dcol[c])  -  L * sum_c x ;
-//     the first sum over the unchanged columns is the per-block sum computed
-//     once per batch (ambout / ambin), so only the columns the vertex touches
-//     are visited.  Counts come from the dense B x B form (small B, O(1)) or
-//     by binary search in the CSR rows.
+//     between the old and the new rows the first sums over unchanged columns
+//     cancel, so only the columns the vertex touches and the four rows'
+//     degree terms remain (see Acc below).  Counts come from the dense B x B
+//     form (small B, O(1)) or by binary search in the CSR rows.
 //     Quirks of the reference kept: old column degrees (Q2), one term per
 //     list entry for blocks missing from the target row
 //     (kernels.hpp:1648-1652, 1314-1318), the r/s in-weight corrections and
@@ -56,7 +56,7 @@ struct NodalArgs {
   const int32_t *bop, *boc, *bip, *bic;
   const uint32_t *bon, *bin, *d_out, *d_in;
   const uint32_t *Md, *MTd;
-  const double *ld_out, *ld_in, *dSout, *ambout, *ambin, *sinfull;
+  const double *ld_out, *ld_in;
   const int32_t* nbr_s;
   const uint8_t* use_rand;
   int32_t B;
@@ -110,162 +110,113 @@ struct Rows<true> {
   __device__ __forceinline__ uint32_t in_s(int c) const { return __ldg(irs + c); }
 };
 
-// Accumulators of the changed columns of the four new rows (out r, out s,
-// in r, in s): a = sum of (x log2 x - x log2 dcol) deltas, m = count deltas.
+// Per-thread partial of a move's dS.  GSAP's seven terms (kernels.hpp:143-182,
+// 494-597, 1153-1726) combine, after the per-block row sums cancel, into
+//   dS = - sum_X d_X log2 d_X  +  sum_X L_X mass_X
+//        - sum over changed cells (g(new) - g(old))  + corner cells
+// where X runs over the old/new out- and in-rows of r and s, d_X the old row
+// degree, L_X = log2 of the new row degree and mass_X the new row's total
+// count; g(x, a) = x log2 x - x a with a = log2 of the old column degree (Q2).
+// `acc` collects this thread's terms, m4..m7 the count changes of the new
+// out-row r, out-row s, in-row r and in-row s.
 struct Acc {
-  double a4 = 0.0, a5 = 0.0, a6 = 0.0, a7 = 0.0;
-  long long m4 = 0, m5 = 0, m6 = 0, m7 = 0;
+  double acc = 0.0;
+  int m4 = 0, m5 = 0, m6 = 0, m7 = 0;
 };
 
-// One out-entry (block c, weight w) of v; `leader` marks one entry per
-// distinct block, kc = v's total weight into c (kernels.hpp:1444-1726).
+// One neighbour entry of v (block c, weight w) in direction `in` (false =
+// out-edge, true = in-edge); `leader` marks one entry per distinct block of
+// that direction and kc is v's total weight to/from c
+// (kernels.hpp:1444-1726 for out, 1153-1362 for in).
 template <bool DENSE>
-__device__ __forceinline__ void out_entry(const NodalArgs& a, const Rows<DENSE>& R, int r, int s,
-                                          uint32_t niS, int32_t c, uint32_t w, bool leader,
-                                          uint32_t kc, Acc& q) {
-  const double ldc = a.ld_in[c];
-  const uint32_t Msc = R.out_s(c);
+__device__ __forceinline__ void entry(const NodalArgs& a, const Rows<DENSE>& R, int r, int s,
+                                      uint32_t niS, bool in, int32_t c, uint32_t w, bool leader,
+                                      uint32_t kc, Acc& q) {
+  if (in && (c == r || c == s)) return;  // in-rows leave out blocks r and s
+  const double ldc = in ? a.ld_out[c] : a.ld_in[c];
+  const uint32_t Mt = in ? R.in_s(c) : R.out_s(c);
+  int dmo = 0, dmt = 0;
   if (leader && c != r && c != s) {
-    const uint32_t Mrc = R.out_r(c);
-    const uint32_t x = Mrc - kc;
-    q.a4 += gterm(a.xlx, x, ldc) - gterm(a.xlx, Mrc, ldc);
-    q.m4 += (long long)x - (long long)Mrc;
-    if (Msc != 0u) {
-      const uint32_t y = Msc + kc;
-      q.a5 += gterm(a.xlx, y, ldc) - gterm(a.xlx, Msc, ldc);
-      q.m5 += (long long)y - (long long)Msc;
+    const uint32_t Mo = in ? R.in_r(c) : R.out_r(c);
+    const uint32_t x = Mo - kc;
+    q.acc -= gterm(a.xlx, x, ldc) - gterm(a.xlx, Mo, ldc);
+    dmo = (int)((long long)x - (long long)Mo);
+    if (Mt != 0u) {
+      const uint32_t y = Mt + kc;
+      q.acc -= gterm(a.xlx, y, ldc) - gterm(a.xlx, Mt, ldc);
+      dmt = (int)((long long)y - (long long)Mt);
     }
   }
-  if (Msc == 0u) {
-    // block c absent from row s: one term per list entry
-    const uint32_t y = w - (c == r ? niS : 0u) + (c == s ? niS : 0u);
-    q.a5 += gterm(a.xlx, y, ldc);
-    q.m5 += (long long)y;
+  if (Mt == 0u) {
+    // block c absent from the target row: one term per list entry
+    // (kernels.hpp:1648-1652, 1696-1713; 1314-1318, 1348-1358)
+    const uint32_t y = in ? w : w - (c == r ? niS : 0u) + (c == s ? niS : 0u);
+    q.acc -= gterm(a.xlx, y, ldc);
+    dmt += (int)y;
+  }
+  if (in) {
+    q.m6 += dmo;
+    q.m7 += dmt;
+  } else {
+    q.m4 += dmo;
+    q.m5 += dmt;
   }
 }
 
-// One in-entry of v: rows r and s of the in CSR, blocks r and s left out.
+// Adds the corner cells (r,r), (r,s), (s,r), (s,s) of M and the row-degree
+// terms to lanes 0..12 of the calling warp (call it from one warp of the
+// group, after m4..m7 hold the group totals).  kernels.hpp:1506-1510,
+// 1573-1578, 1663-1669, 1718-1723 give the new corner counts.
 template <bool DENSE>
-__device__ __forceinline__ void in_entry(const NodalArgs& a, const Rows<DENSE>& R, int r, int s,
-                                         int32_t c, uint32_t w, bool leader, uint32_t kc,
-                                         Acc& q) {
-  if (c == r || c == s) return;
-  const double ldc = a.ld_out[c];
-  const uint32_t Mcs = R.in_s(c);
-  if (leader) {
-    const uint32_t Mcr = R.in_r(c);
-    const uint32_t x = Mcr - kc;
-    q.a6 += gterm(a.xlx, x, ldc) - gterm(a.xlx, Mcr, ldc);
-    q.m6 += (long long)x - (long long)Mcr;
-    if (Mcs != 0u) {
-      const uint32_t y = Mcs + kc;
-      q.a7 += gterm(a.xlx, y, ldc) - gterm(a.xlx, Mcs, ldc);
-      q.m7 += (long long)y - (long long)Mcs;
-    }
-  }
-  if (Mcs == 0u) {
-    q.a7 += gterm(a.xlx, w, ldc);
-    q.m7 += (long long)w;
-  }
-}
-
-// The (r, s) corner, the old terms and the new-row totals.  Every thread
-// of the group holds the reduced q and returns the same value; the dozen
-// logarithms involved are computed once each, spread over the lanes of each
-// warp and broadcast with shuffles.
-template <bool DENSE>
-__device__ double finish_delta(const NodalArgs& a, const Rows<DENSE>& R, int v, int r, int s,
-                               uint32_t koR, uint32_t koS, uint32_t niR, uint32_t niS, Acc q) {
+__device__ __forceinline__ void corner_terms(const NodalArgs& a, const Rows<DENSE>& R, int v,
+                                             int r, int s, uint32_t koR, uint32_t koS,
+                                             uint32_t niR, uint32_t niS, Acc& q) {
   const int lane = threadIdx.x & 31;
-  uint32_t m = 0u;
-  if (lane == 0) m = R.out_r(r);
-  else if (lane == 1) m = R.out_r(s);
-  else if (lane == 2) m = R.out_s(r);
-  else if (lane == 3) m = R.out_s(s);
-  const uint32_t Mrr = __shfl_sync(kFull, m, 0), Mrs = __shfl_sync(kFull, m, 1);
-  const uint32_t Msr = __shfl_sync(kFull, m, 2), Mss = __shfl_sync(kFull, m, 3);
-  const uint32_t kO = a.kdo[v], kI = a.kdi[v];
-  const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
-  // new counts of the corner cells (kernels.hpp:1506-1510, 1573-1578,
-  // 1663-1669, 1718-1723); when Mrs (Mss) is 0 the extra column term holds
-  // niR (niS)
+  uint32_t mm = 0u;
+  if (lane == 0) mm = R.out_r(r);
+  else if (lane == 1) mm = R.out_r(s);
+  else if (lane == 2) mm = R.out_s(r);
+  else if (lane == 3) mm = R.out_s(s);
+  const uint32_t Mrr = __shfl_sync(kFull, mm, 0), Mrs = __shfl_sync(kFull, mm, 1);
+  const uint32_t Msr = __shfl_sync(kFull, mm, 2), Mss = __shfl_sync(kFull, mm, 3);
   const uint32_t xrr = Mrr - koR - niR;
   const uint32_t xrs = Mrs != 0u ? Mrs - koS + niR : niR;
   const uint32_t xsr = Msr + koR - niS;
   const uint32_t xss = Mss != 0u ? Mss + koS + niS : niS;
-  uint32_t arg = 0u;
-  switch (lane) {
-    case 0: arg = Mrr; break;
-    case 1: arg = Mrs; break;
-    case 2: arg = Msr; break;
-    case 3: arg = Mss; break;
-    case 4: arg = xrr; break;
-    case 5: arg = xrs; break;
-    case 6: arg = xsr; break;
-    case 7: arg = xss; break;
-    case 8: arg = dor - kO; break;
-    case 9: arg = dos + kO; break;
-    case 10: arg = dir - kI; break;
-    case 11: arg = dis + kI; break;
-    default: break;
-  }
-  double val = 0.0;
-  if (lane < 8) val = arg == 0u ? 0.0 : xlx(a.xlx, arg);
-  else if (lane < 12) val = log2((double)arg);
-  const double XMrr = __shfl_sync(kFull, val, 0), XMrs = __shfl_sync(kFull, val, 1);
-  const double XMsr = __shfl_sync(kFull, val, 2), XMss = __shfl_sync(kFull, val, 3);
-  const double Xrr = __shfl_sync(kFull, val, 4), Xrs = __shfl_sync(kFull, val, 5);
-  const double Xsr = __shfl_sync(kFull, val, 6), Xss = __shfl_sync(kFull, val, 7);
-  const double L4 = __shfl_sync(kFull, val, 8), L5 = __shfl_sync(kFull, val, 9);
-  const double L6 = __shfl_sync(kFull, val, 10), L7 = __shfl_sync(kFull, val, 11);
+  const bool use_rs = Mrs != 0u || niR > 0u;                       // cell or extra term
+  const bool use_ss = Mss != 0u || (koS == 0u && niS > 0u);
+  const long long m4 = q.m4 + (Mrr ? (long long)xrr - Mrr : 0) +
+                       (use_rs ? (long long)xrs - (long long)Mrs : 0);
+  const long long m5 = q.m5 + (Msr ? (long long)xsr - Msr : 0) +
+                       (use_ss ? (long long)xss - (long long)Mss : 0);
+  const uint32_t kO = a.kdo[v], kI = a.kdi[v];
+  const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
+  const long long mass4 = (long long)dor + m4;
+  const long long mass5 = (long long)dos + m5;
+  const long long mass6 = (long long)dir - (long long)Mrr - (long long)Msr + q.m6;
+  const long long mass7 = (long long)dis - (long long)Mrs - (long long)Mss + q.m7;
   const double ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
   const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s];
-  // g(x, a) = x log2 x - x a from the broadcast x log2 x
-  auto g = [](double xl, uint32_t x, double ld) { return x == 0u ? 0.0 : xl - (double)x * ld; };
-  // f(M; a, b) = M log2 M - M (a + b)
-  auto f = [](double xl, uint32_t x, double l1, double l2) {
-    return x == 0u ? 0.0 : xl - (double)x * (l1 + l2);
-  };
-  if (Mrr != 0u) {
-    q.a4 += g(Xrr, xrr, ldi_r) - g(XMrr, Mrr, ldi_r);
-    q.m4 += (long long)xrr - (long long)Mrr;
+  double t = 0.0;
+  // lanes 0-3: old corner cells, + M log2 M; lanes 4-7: new corner cells,
+  // - g(x); lanes 8-11: + L mass of the four new rows; lane 12: old degrees
+  if (lane < 4) {
+    const uint32_t M = lane == 0 ? Mrr : lane == 1 ? Mrs : lane == 2 ? Msr : Mss;
+    if (M != 0u) t = xlx(a.xlx, M);
+  } else if (lane < 8) {
+    const bool on = lane == 4 ? Mrr != 0u : lane == 5 ? use_rs : lane == 6 ? Msr != 0u : use_ss;
+    const uint32_t x = lane == 4 ? xrr : lane == 5 ? xrs : lane == 6 ? xsr : xss;
+    const double ld = (lane == 4 || lane == 6) ? ldi_r : ldi_s;
+    if (on) t = -gterm(a.xlx, x, ld);
+  } else if (lane < 12) {
+    const long long mass = lane == 8 ? mass4 : lane == 9 ? mass5 : lane == 10 ? mass6 : mass7;
+    const uint32_t d = lane == 8 ? dor - kO : lane == 9 ? dos + kO : lane == 10 ? dir - kI : dis + kI;
+    if (mass != 0) t = log2((double)d) * (double)mass;
+  } else if (lane == 12) {
+    t = -((dor ? (double)dor * ldo_r : 0.0) + (dos ? (double)dos * ldo_s : 0.0) +
+          (dir ? (double)dir * ldi_r : 0.0) + (dis ? (double)dis * ldi_s : 0.0));
   }
-  if (Mrs != 0u) {
-    q.a4 += g(Xrs, xrs, ldi_s) - g(XMrs, Mrs, ldi_s);
-    q.m4 += (long long)xrs - (long long)Mrs;
-  } else if (niR > 0u) {
-    q.a4 += g(Xrs, niR, ldi_s);
-    q.m4 += (long long)niR;
-  }
-  if (Msr != 0u) {
-    q.a5 += g(Xsr, xsr, ldi_r) - g(XMsr, Msr, ldi_r);
-    q.m5 += (long long)xsr - (long long)Msr;
-  }
-  if (Mss != 0u) {
-    q.a5 += g(Xss, xss, ldi_s) - g(XMss, Mss, ldi_s);
-    q.m5 += (long long)xss - (long long)Mss;
-  } else if (koS == 0u && niS > 0u) {
-    q.a5 += g(Xss, niS, ldi_s);
-    q.m5 += (long long)niS;
-  }
-  // old terms (calculate_dS_out, calculate_dS_in_nodal_r/_s)
-  double t1 = a.dSout[r] + a.dSout[s];
-  double t2 = a.sinfull[r] - f(XMrr, Mrr, ldo_r, ldi_r) - f(XMsr, Msr, ldo_s, ldi_r);
-  double t3 = a.sinfull[s] - f(XMrs, Mrs, ldo_r, ldi_s) - f(XMss, Mss, ldo_s, ldi_s);
-  // new rows r and s, out and in
-  long long mass4 = (long long)dor + q.m4;
-  long long mass5 = (long long)dos + q.m5;
-  long long mass6 = (long long)dir - (long long)Mrr - (long long)Msr + q.m6;
-  long long mass7 = (long long)dis - (long long)Mrs - (long long)Mss + q.m7;
-  double t4 = a.ambout[r] + q.a4;
-  if (mass4 != 0) t4 -= L4 * (double)mass4;
-  double t5 = a.ambout[s] + q.a5;
-  if (mass5 != 0) t5 -= L5 * (double)mass5;
-  double t6 = a.ambin[r] - g(XMrr, Mrr, ldo_r) - g(XMsr, Msr, ldo_s) + q.a6;
-  if (mass6 != 0) t6 -= L6 * (double)mass6;
-  double t7 = a.ambin[s] - g(XMrs, Mrs, ldo_r) - g(XMss, Mss, ldo_s) + q.a7;
-  if (mass7 != 0) t7 -= L7 * (double)mass7;
-  return t1 + t2 + t3 - t4 - t5 - t6 - t7;
+  q.acc += t;
 }
 
 // A thread group cooperating on one vertex: a warp (G = 32) or a CTA.
@@ -292,18 +243,6 @@ struct Group {
     return (long long)sum((double)x);  // |x| < 2^53: exact
   }
 };
-
-template <int G>
-__device__ __forceinline__ void reduce_acc(Acc& q, const Group<G>& grp) {
-  q.a4 = grp.sum(q.a4);
-  q.a5 = grp.sum(q.a5);
-  q.a6 = grp.sum(q.a6);
-  q.a7 = grp.sum(q.a7);
-  q.m4 = grp.sum_ll(q.m4);
-  q.m5 = grp.sum_ll(q.m5);
-  q.m6 = grp.sum_ll(q.m6);
-  q.m7 = grp.sum_ll(q.m7);
-}
 
 // Ascending bitonic sort of P (power of two) keys by the group.
 template <int G>
@@ -345,6 +284,25 @@ __device__ void stage_sorted(const int32_t* __restrict__ idx, const uint32_t* __
   group_sort<G>(key, P, grp);
 }
 
+// Group sums of the four direction weights v has to/from blocks r and s.
+struct RsWeights {
+  uint32_t koR, koS, niR, niS;
+};
+
+// Finishes a move's dS after every thread of the group has added its
+// entries to q: group totals of the count changes, then the corner and
+// degree terms on warp 0, then the group sum.
+template <bool DENSE, int G>
+__device__ double finish(const NodalArgs& a, const Rows<DENSE>& R, int v, int r, int s,
+                         const RsWeights& w, Acc q, const Group<G>& grp) {
+  q.m4 = (int)grp.sum_ll(q.m4);
+  q.m5 = (int)grp.sum_ll(q.m5);
+  q.m6 = (int)grp.sum_ll(q.m6);
+  q.m7 = (int)grp.sum_ll(q.m7);
+  if (G == 32 || threadIdx.x < 32) corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
+  return grp.sum(q.acc);
+}
+
 // dS from v's sorted neighbour-block lists ko[0..no) (out), ki[0..ni) (in).
 template <bool DENSE, int G>
 __device__ double delta_sorted(const NodalArgs& a, int v, int r, int s,
@@ -363,10 +321,8 @@ __device__ double delta_sorted(const NodalArgs& a, int v, int r, int s,
     niR += c == r ? kwt(ki[k]) : 0u;
     niS += c == s ? kwt(ki[k]) : 0u;
   }
-  koR = (uint32_t)grp.sum_ll(koR);
-  koS = (uint32_t)grp.sum_ll(koS);
-  niR = (uint32_t)grp.sum_ll(niR);
-  niS = (uint32_t)grp.sum_ll(niS);
+  RsWeights w{(uint32_t)grp.sum_ll(koR), (uint32_t)grp.sum_ll(koS), (uint32_t)grp.sum_ll(niR),
+              (uint32_t)grp.sum_ll(niS)};
   Acc q;
   for (int k = t; k < no; k += G) {
     const int32_t c = kblk(ko[k]);
@@ -374,7 +330,7 @@ __device__ double delta_sorted(const NodalArgs& a, int v, int r, int s,
     uint32_t kc = 0;
     if (leader)
       for (int j = k; j < no && kblk(ko[j]) == c; ++j) kc += kwt(ko[j]);
-    out_entry<DENSE>(a, R, r, s, niS, c, kwt(ko[k]), leader, kc, q);
+    entry<DENSE>(a, R, r, s, w.niS, false, c, kwt(ko[k]), leader, kc, q);
   }
   for (int k = t; k < ni; k += G) {
     const int32_t c = kblk(ki[k]);
@@ -382,45 +338,76 @@ __device__ double delta_sorted(const NodalArgs& a, int v, int r, int s,
     uint32_t kc = 0;
     if (leader)
       for (int j = k; j < ni && kblk(ki[j]) == c; ++j) kc += kwt(ki[j]);
-    in_entry<DENSE>(a, R, r, s, c, kwt(ki[k]), leader, kc, q);
+    entry<DENSE>(a, R, r, s, w.niS, true, c, kwt(ki[k]), leader, kc, q);
   }
-  reduce_acc(q, grp);
-  return finish_delta<DENSE>(a, R, v, r, s, koR, koS, niR, niS, q);
+  return finish<DENSE, G>(a, R, v, r, s, w, q, grp);
 }
 
-// dS when both lists fit in one warp: each lane holds one out- and one
-// in-entry; entries of the same block are grouped with __match_any_sync and
-// their weights summed with __reduce_add_sync.
+// dS when each direction's list fits in one warp: entries of the same block
+// are grouped with __match_any_sync on a direction-tagged key and their
+// weights summed with __reduce_add_sync.  When both lists fit together,
+// one pass covers both directions.
 template <bool DENSE>
 __device__ double delta_registers(const NodalArgs& a, int v, int r, int s, int32_t o0, int no,
                                   int32_t i0, int ni, int lane) {
   const Rows<DENSE> R(a, r, s);
-  const bool vo = lane < no, vi = lane < ni;
-  const int32_t co = vo ? __ldg(a.part + __ldg(a.oidx + o0 + lane)) : -1 - lane;
-  const uint32_t wo = vo ? __ldg(a.ow + o0 + lane) : 0u;
-  const int32_t ci = vi ? __ldg(a.part + __ldg(a.iidx + i0 + lane)) : -1 - lane;
-  const uint32_t wi = vi ? __ldg(a.iw + i0 + lane) : 0u;
-  const unsigned po = __match_any_sync(kFull, co);
-  const unsigned pi = __match_any_sync(kFull, ci);
-  const uint32_t kco = __reduce_add_sync(po, wo);
-  const uint32_t kci = __reduce_add_sync(pi, wi);
-  const uint32_t koR = __reduce_add_sync(kFull, co == r ? wo : 0u);
-  const uint32_t koS = __reduce_add_sync(kFull, co == s ? wo : 0u);
-  const uint32_t niR = __reduce_add_sync(kFull, ci == r ? wi : 0u);
-  const uint32_t niS = __reduce_add_sync(kFull, ci == s ? wi : 0u);
   Acc q;
-  if (vo) out_entry<DENSE>(a, R, r, s, niS, co, wo, lane == __ffs(po) - 1, kco, q);
-  if (vi) in_entry<DENSE>(a, R, r, s, ci, wi, lane == __ffs(pi) - 1, kci, q);
-  q.a4 = warp_sum(q.a4);
-  q.a5 = warp_sum(q.a5);
-  q.a6 = warp_sum(q.a6);
-  q.a7 = warp_sum(q.a7);
-  // per-lane count deltas are bounded by the vertex's degree: 32-bit sums
-  q.m4 = __reduce_add_sync(kFull, (int)q.m4);
-  q.m5 = __reduce_add_sync(kFull, (int)q.m5);
-  q.m6 = __reduce_add_sync(kFull, (int)q.m6);
-  q.m7 = __reduce_add_sync(kFull, (int)q.m7);
-  return finish_delta<DENSE>(a, R, v, r, s, koR, koS, niR, niS, q);
+  RsWeights w{0u, 0u, 0u, 0u};
+  const int passes = no + ni <= 32 ? 1 : 2;
+  // pass p, lane l: entry index e; combined pass: out-entries then in-entries
+  int32_t cs[2];
+  uint32_t ws[2];
+  bool ins[2], valid[2];
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    int k;
+    bool in;
+    if (passes == 1 && p == 1) {
+      valid[1] = false;
+      ins[1] = false;
+      cs[1] = -1;
+      ws[1] = 0u;
+      break;
+    }
+    if (passes == 1) {
+      in = lane >= no;
+      k = in ? lane - no : lane;
+      valid[p] = p == 0 && lane < no + ni;
+    } else {
+      in = p == 1;
+      k = lane;
+      valid[p] = lane < (in ? ni : no);
+    }
+    ins[p] = in;
+    cs[p] = -1;
+    ws[p] = 0u;
+    if (valid[p]) {
+      cs[p] = in ? __ldg(a.part + __ldg(a.iidx + i0 + k)) : __ldg(a.part + __ldg(a.oidx + o0 + k));
+      ws[p] = in ? __ldg(a.iw + i0 + k) : __ldg(a.ow + o0 + k);
+    }
+    const bool o = valid[p] && !in, i = valid[p] && in;
+    w.koR += __reduce_add_sync(kFull, o && cs[p] == r ? ws[p] : 0u);
+    w.koS += __reduce_add_sync(kFull, o && cs[p] == s ? ws[p] : 0u);
+    w.niR += __reduce_add_sync(kFull, i && cs[p] == r ? ws[p] : 0u);
+    w.niS += __reduce_add_sync(kFull, i && cs[p] == s ? ws[p] : 0u);
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    if (passes == 1 && p == 1) break;
+    // direction in the top bit, unique keys for idle lanes
+    const unsigned key = valid[p] ? ((unsigned)cs[p] | (ins[p] ? 0x80000000u : 0u))
+                                  : (0x7fffffe0u + (unsigned)lane);
+    const unsigned peers = __match_any_sync(kFull, key);
+    const uint32_t kc = __reduce_add_sync(peers, ws[p]);
+    if (valid[p])
+      entry<DENSE>(a, R, r, s, w.niS, ins[p], cs[p], ws[p], lane == __ffs(peers) - 1, kc, q);
+  }
+  q.m4 = __reduce_add_sync(kFull, q.m4);
+  q.m5 = __reduce_add_sync(kFull, q.m5);
+  q.m6 = __reduce_add_sync(kFull, q.m6);
+  q.m7 = __reduce_add_sync(kFull, q.m7);
+  corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
+  return warp_sum(q.acc);
 }
 
 // Lists too long for shared memory: per-block totals from a shared-memory
@@ -511,14 +498,12 @@ __device__ double delta_hashed(const NodalArgs& a, int v, int r, int s, HashTab 
         bool leader = h.first[slot] == k;
         uint32_t kc = h.sum[slot];
         uint32_t w = __ldg(wt + base + k);
-        if (dir == 0) out_entry<DENSE>(a, R, r, s, niS, c, w, leader, kc, q);
-        else in_entry<DENSE>(a, R, r, s, c, w, leader, kc, q);
+        entry<DENSE>(a, R, r, s, niS, dir == 1, c, w, leader, kc, q);
       }
       grp.sync();
     }
   }
-  reduce_acc(q, grp);
-  return finish_delta<DENSE>(a, R, v, r, s, koR, koS, niR, niS, q);
+  return finish<DENSE, G>(a, R, v, r, s, RsWeights{koR, koS, niR, niS}, q, grp);
 }
 
 // Neighbour of v whose running weight (out-entries, then in-entries) first
@@ -730,8 +715,8 @@ NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int3
   a.bop = m.optr; a.boc = m.ocol; a.bip = m.iptr; a.bic = m.icol;
   a.bon = m.ocnt; a.bin = m.icnt; a.d_out = m.d_out; a.d_in = m.d_in;
   a.Md = m.Md; a.MTd = m.MTd;
-  a.ld_out = m.ld_out; a.ld_in = m.ld_in; a.dSout = m.dSout; a.ambout = m.ambout;
-  a.ambin = m.ambin; a.sinfull = m.sinfull; a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
+  a.ld_out = m.ld_out; a.ld_in = m.ld_in;
+  a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
   a.B = B;
   a.heavy = aux.heavy;
   a.nheavy = aux.nheavy;
