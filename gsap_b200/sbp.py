@@ -101,6 +101,8 @@ _sig("sbp_merge_step", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32,
      C.c_uint64, C.c_uint32, _vp, _vp, C.POINTER(C.c_int32))
 _sig("sbp_mdl", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.POINTER(C.c_double),
      C.POINTER(C.c_double))
+_sig("sbp_mdl_device_static", C.c_int, C.c_int32, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp,
+     _vp, _vp, _vp)
 _sig("sbp_dcsbm_generate", C.c_int, C.POINTER(_DcsbmParams), C.POINTER(_vp))
 _sig("sbp_edges_size", C.c_int, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32))
 _sig("sbp_edges_copy", C.c_int, _vp, _vp, _vp, _vp, _vp)
@@ -118,6 +120,7 @@ EXPORTED = [
     "sbp_delta_mdl_nodal", "sbp_delta_mdl_merge", "sbp_merge_proposals", "sbp_nodal_batch",
     "sbp_merge_step", "sbp_nodal_sweeps", "sbp_mdl", "sbp_dcsbm_generate", "sbp_edges_size", "sbp_edges_copy",
     "sbp_edges_free", "sbp_csr_from_edges", "sbp_load_tsv", "sbp_evaluate",
+    "sbp_mdl_device_static",
 ]
 
 
@@ -366,6 +369,12 @@ def mdl(g: Graph, part, B):
     S, dS = C.c_double(), C.c_double()
     _check(_lib.sbp_mdl(C.byref(g.csr()), _p(part), B, C.byref(S), C.byref(dS)))
     return S.value, dS.value
+
+
+def mdl_device_static(N, E, B, out_ptr, out_col, out_cnt, d_out, d_in, S, data_S, stream=0):
+    """sbp_mdl_device_static on device pointers (integers); allocates nothing."""
+    _check(_lib.sbp_mdl_device_static(N, E, B, out_ptr, out_col, out_cnt, d_out, d_in, S, data_S,
+                                      stream))
 
 
 def evaluate(truth, given):

@@ -174,6 +174,21 @@ sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int3
 sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, double* S,
                    double* data_S);
 
+/* The MDL of a blockmodel already in device memory (out CSR with B+1 row
+ * pointers, block degrees), written to the device doubles *S and *data_S on
+ * `stream` (a cudaStream_t; NULL = default stream), without allocating
+ * anything: for callers that cannot call cudaMalloc where they need the
+ * objective (inside a CUDA graph capture, in serving loops that forbid
+ * allocation syncs, or under a host-owned memory pool).  Its scratch is a
+ * fixed ~1 MB device array of the library; B <= 65536.  The first call on a
+ * device looks that array up, so make it before any stream capture; calls
+ * that overlap on the GPU share the array and race.  This entry point has no
+ * counterpart in the reference. */
+sbp_status sbp_mdl_device_static(int32_t N, int32_t E, int32_t B, const int32_t* out_ptr,
+                                 const int32_t* out_col, const uint32_t* out_cnt,
+                                 const uint32_t* d_out, const uint32_t* d_in, double* S,
+                                 double* data_S, void* stream);
+
 /* ----------------------------------------------------------- host utilities */
 
 /* Seeded directed DCSBM generator standing in for the GraphChallenge static
