@@ -3,9 +3,19 @@ HH-style DCSBM graph (N=200,000, 71 planted blocks, p_in=0.5, Dirichlet
 alpha=1, out-degrees from a power law of exponent 2.5 on [5, 50]).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mode plain|batched|served]
 
 One step = one full partition (merges, nodal sweeps, golden-section search
 over B) of the graph.  Prints one JSON line on rank 0.
+
+--mode batched: 256 DCSBM graphs (N log-uniform on [1k, 50k], B =
+round(2.6 N^0.34), p_in and alpha drawn from {0.5, 0.8} x {1, 20}) through
+sbp_partition_batch, against the same 256 graphs partitioned one at a time
+with sbp_partition; graphs/s end to end, same labels by construction.
+--mode served: Poisson arrivals of requests of 1k/5k/20k/50k vertices
+(weights 0.4/0.3/0.2/0.1, random LL/LH/HL/HH) at swept rates, through the
+server (continuous batching) and through a one-at-a-time loop of
+sbp_partition; p50/p99 latency and throughput per rate.
 
   value    partitions/s over all ranks with the graph resident in HBM
            (sbp_partition_resident), CUDA-event time of the run's stream,
@@ -192,12 +202,16 @@ def run_ours(args, rank, world, local, dist):
     ms_max = dist.max(ms_dev)
     # end to end through the host-buffer C ABI call
     e2e_ms = 0.0
+    e2e_parts = {"c_total": 0.0, "h2d": 0.0, "device": 0.0}
     for i in range(args.steps):
         flush_l2(local)
         dist.barrier()
         t0 = time.perf_counter()
-        sbp.partition(g, seed=i, **opts)
+        r = sbp.partition(g, seed=i, **opts)
         e2e_ms += (time.perf_counter() - t0) * 1000.0
+        e2e_parts["c_total"] += r["ms_total"]
+        e2e_parts["h2d"] += r["ms_h2d"]
+        e2e_parts["device"] += r["ms_device"]
     e2e_max = dist.max(e2e_ms)
     rg.close()
     if rank != 0:
@@ -228,7 +242,9 @@ def run_ours(args, rank, world, local, dist):
                    "parallelism": f"replicas x{world}",
                    "l2": "graph working set < L2; 256 MB written between timed steps"},
         "e2e": {"value": world * K / (e2e_max / 1000.0), "unit": UNIT,
-                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(g.N * 4)},
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(g.N * 4),
+                "ms_per_step": e2e_max / K,
+                "breakdown_ms_per_step": {k: v / K for k, v in e2e_parts.items()}},
         "roofline": {"bound": "hbm", "kernel": "nodal dS kernels (warp + heavy-vertex CTA)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
@@ -245,6 +261,181 @@ def run_ours(args, rank, world, local, dist):
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(g, args.cpu_seconds)
     return line
+
+
+def batched_graphs(sbp, count, seed):
+    """The batched workload: graph i has N log-uniform on [1k, 50k],
+    B = round(2.6 N^0.34), p_in in {0.5, 0.8}, alpha in {1, 20}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        N = int(round(float(np.exp(rng.uniform(np.log(1000), np.log(50000))))))
+        B = int(round(2.6 * N ** 0.34))
+        p_in = float(rng.choice([0.5, 0.8]))
+        alpha = float(rng.choice([1.0, 20.0]))
+        out.append(sbp.dcsbm(N, B, alpha, p_in, seed=seed * 100000 + i))
+    return out
+
+
+def quality(sbp, g, lab, S):
+    rec, prec, _ = sbp.evaluate(g.true_partitions, lab)
+    return S, rec, prec
+
+
+def run_batched(args, rank, world, local, dist):
+    from gsap_b200 import sbp
+    count = args.batch_count
+    gs = batched_graphs(sbp, count, 7 + rank)
+    seeds = list(range(count))
+    opts = dict(device=local)
+    # warm-up: a small batch (kernels, pools)
+    for _ in range(max(1, args.warmup)):
+        sbp.partition_batch(gs[:8], seeds=seeds[:8], **opts)
+    dist.barrier()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        labs, reps, br = sbp.partition_batch(gs, seeds=seeds, **opts)
+        wall = (time.perf_counter() - t0) * 1000.0
+    wall_max = dist.max(wall)
+    dev_max = dist.max(br["ms_device"])
+    # the plain form, one graph at a time, same graphs and seeds
+    t0 = time.perf_counter()
+    seq_S, same = [], 0
+    for i, g in enumerate(gs):
+        rep = sbp.partition(g, seed=seeds[i], **opts)
+        seq_S.append(rep["S"])
+        same += int(np.array_equal(g.partitions, labs[i]) and rep["S"] == reps[i]["S"])
+    seq = (time.perf_counter() - t0) * 1000.0
+    seq_max = dist.max(seq)
+    if rank != 0:
+        return None
+    q = [quality(sbp, g, labs[i], reps[i]["S"]) for i, g in enumerate(gs)]
+    Ns = [g.N for g in gs]
+    h2d = sum(sum(a.nbytes for a in (g.out_ptr, g.out_idx, g.out_w, g.in_ptr, g.in_idx,
+                                     g.in_w, g.deg_out, g.deg_in)) for g in gs)
+    return {
+        "metric": "batched SBP graphs/s (256 DCSBM graphs, N log-uniform on [1k,50k])",
+        "value": world * count / (dev_max / 1000.0), "unit": "graphs/s", "n_gpus": world,
+        "steps": 1, "warmup": max(1, args.warmup), "ms_per_step": dev_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "batched-256", "graphs": count, "N_min": min(Ns),
+                   "N_max": max(Ns), "N_total": int(sum(Ns)),
+                   "E_total": int(sum(g.E for g in gs)), "parallelism": f"replicas x{world}"},
+        "e2e": {"value": world * count / (wall_max / 1000.0), "unit": "graphs/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(4 * sum(Ns))},
+        "sequential_plain": {"value": world * count / (seq_max / 1000.0), "unit": "graphs/s",
+                             "note": "the same graphs and seeds through sbp_partition, one at a "
+                                     "time (host buffers, end to end)"},
+        "speedup_vs_sequential_e2e": seq_max / wall_max,
+        "identical_results": f"{same}/{count}",
+        "quality": {"mean_S": float(np.mean([x[0] for x in q])),
+                    "mean_recall": float(np.mean([x[1] for x in q])),
+                    "mean_precision": float(np.mean([x[2] for x in q]))},
+        "batch": br, "gpu_launches": int(br["kernel_launches"]), "clocks": clk.summary(),
+    }
+
+
+def served_pool(sbp, seed):
+    """Graphs the request generator samples from: per size, a few seeded
+    graphs of each variant."""
+    rng = np.random.default_rng(seed)
+    pool = {}
+    for N in (1000, 5000, 20000, 50000):
+        B = int(round(2.6 * N ** 0.34))
+        pool[N] = [sbp.dcsbm_variant(v, N, B, seed=int(rng.integers(1 << 30)))
+                   for v in ("LL", "LH", "HL", "HH")]
+    return pool
+
+
+def arrivals(rate, count, seed):
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, count))
+    sizes = rng.choice([1000, 5000, 20000, 50000], size=count, p=[0.4, 0.3, 0.2, 0.1])
+    which = rng.integers(0, 4, count)
+    return t, sizes, which
+
+
+def serve_with_server(sbp, pool, t, sizes, which, local):
+    import threading as th
+    lat = [None] * len(t)
+    with sbp.Server(device=local) as srv:
+        ids = [None] * len(t)
+        t0 = time.perf_counter()
+        done_flag = th.Event()
+
+        def collect():
+            for i in range(len(t)):
+                while ids[i] is None:
+                    time.sleep(0.0005)
+                lab, rep, tm = srv.poll(ids[i], timeout_ms=-1)
+                lat[i] = tm["ms_latency"]
+            done_flag.set()
+
+        c = th.Thread(target=collect)
+        c.start()
+        for i in range(len(t)):
+            now = time.perf_counter() - t0
+            if t[i] > now:
+                time.sleep(t[i] - now)
+            ids[i] = srv.submit(pool[int(sizes[i])][int(which[i])], seed=i)
+        c.join()
+        span = time.perf_counter() - t0
+        st = srv.stats()
+    return np.array(lat), span, st
+
+
+def serve_one_at_a_time(sbp, pool, t, sizes, which, local):
+    """FIFO queue served by sbp_partition, one request at a time."""
+    lat = []
+    t0 = time.perf_counter()
+    for i in range(len(t)):
+        now = time.perf_counter() - t0
+        if t[i] > now:
+            time.sleep(t[i] - now)
+        sbp.partition(pool[int(sizes[i])][int(which[i])], seed=i, device=local)
+        lat.append((time.perf_counter() - t0 - t[i]) * 1000.0)
+    return np.array(lat), time.perf_counter() - t0
+
+
+def run_served(args, rank, world, local, dist):
+    from gsap_b200 import sbp
+    pool = served_pool(sbp, 11 + rank)
+    for N in pool:  # warm-up
+        sbp.partition(pool[N][0], seed=0, device=local)
+    rows = []
+    with ClockSampler(local) as clk:
+        for rate in args.rates:
+            count = int(min(args.served_max, max(30, rate * args.served_seconds)))
+            t, sizes, which = arrivals(rate, count, 100 + int(rate))
+            lat_s, span_s, st = serve_with_server(sbp, pool, t, sizes, which, local)
+            lat_p, span_p = serve_one_at_a_time(sbp, pool, t, sizes, which, local)
+            sel20 = sizes == 20000
+            rows.append({
+                "rate": rate, "requests": count,
+                "server": {"p50_ms": float(np.percentile(lat_s, 50)),
+                           "p99_ms": float(np.percentile(lat_s, 99)),
+                           "p99_20k_ms": float(np.percentile(lat_s[sel20], 99))
+                           if sel20.any() else None,
+                           "throughput": count / span_s, "max_active": st["max_active_seen"]},
+                "one_at_a_time": {"p50_ms": float(np.percentile(lat_p, 50)),
+                                  "p99_ms": float(np.percentile(lat_p, 99)),
+                                  "p99_20k_ms": float(np.percentile(lat_p[sel20], 99))
+                                  if sel20.any() else None,
+                                  "throughput": count / span_p}})
+    if rank != 0:
+        return None
+    top = rows[-1]
+    return {
+        "metric": "served SBP p99 latency (ms) and throughput, Poisson arrivals",
+        "value": top["server"]["p99_ms"], "unit": "ms", "n_gpus": world, "steps": len(rows),
+        "warmup": 1, "ms_per_step": None, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "served", "rates": args.rates,
+                   "sizes": "1k/5k/20k/50k at 0.4/0.3/0.2/0.1, LL/LH/HL/HH uniform",
+                   "parallelism": f"replicas x{world}"},
+        "rates": rows, "clocks": clk.summary(),
+    }
 
 
 def run_reference(args, rank, world, local):
@@ -307,6 +498,11 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=None)
     ap.add_argument("--ref-warmup", type=int, default=None)
     ap.add_argument("--ref-timeout", type=float, default=900.0)
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--rates", type=float, nargs="+", default=[5.0, 20.0, 50.0, 100.0, 200.0])
+    ap.add_argument("--served-seconds", type=float, default=6.0)
+    ap.add_argument("--served-max", type=int, default=400)
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -319,8 +515,9 @@ def main():
             print(json.dumps(line), flush=True)
         return
     dist = Dist(world, local)
+    runner = {"plain": run_ours, "batched": run_batched, "served": run_served}[args.mode]
     try:
-        line = run_ours(args, rank, world, local, dist)
+        line = runner(args, rank, world, local, dist)
     finally:
         dist.close()
     if line is not None:

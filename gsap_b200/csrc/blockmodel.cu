@@ -22,6 +22,7 @@
 // The result is exact integer work and identical to the oracle's builder.
 #include "common.cuh"
 #include "kernels.h"
+#include "multi.cuh"
 
 #include <algorithm>
 
@@ -65,63 +66,90 @@ __device__ __forceinline__ int cta_excl_scan(int x, int* sh, int* total) {
   return res;
 }
 
-__global__ void scan_tile_sums(const int32_t* __restrict__ in, int32_t n, int32_t* tile) {
-  __shared__ int sh[33];
-  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-  int s = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k)
-    if (base + k < n) s += in[base + k];
-  int tot;
-  cta_excl_scan(s, sh, &tot);
-  if (threadIdx.x == 0) tile[blockIdx.x] = tot;
-}
+// Scan of one array in three steps when it spans more than one CTA's tiles:
+// per-tile sums, a one-CTA scan of those sums, then each tile applies its
+// offset.  Short arrays take the one-CTA scan directly.
+struct ScanArgs {
+  const int32_t* in;
+  int32_t* out;
+  int32_t* tile;  // tile sums (tile body), offsets (apply body)
+  int32_t n, pad;
+};
 
-// Exclusive scan of `n` values in place, one CTA, tile by tile with a carry.
-__global__ void scan_single(const int32_t* __restrict__ in, int32_t* out, int32_t n) {
-  __shared__ int sh[33];
-  int carry = 0;
-  for (int t0 = 0; t0 < n; t0 += kScanTile) {
-    int base = t0 + threadIdx.x * kScanItems;
+struct ScanTileBody {
+  using Args = ScanArgs;
+  static constexpr int kThreads = kScanThreads, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int) {
+    __shared__ int sh[33];
+    int base = vb * kScanTile + threadIdx.x * kScanItems;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+      if (base + k < a.n) s += a.in[base + k];
+    int tot;
+    cta_excl_scan(s, sh, &tot);
+    if (threadIdx.x == 0) a.tile[vb] = tot;
+  }
+};
+
+// Exclusive scan of `n` values (in place allowed), one CTA, tile by tile with
+// a carry; out[n] = total.
+struct ScanSingleBody {
+  using Args = ScanArgs;
+  static constexpr int kThreads = kScanThreads, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int, int) {
+    __shared__ int sh[33];
+    int carry = 0;
+    for (int t0 = 0; t0 < a.n; t0 += kScanTile) {
+      int base = t0 + threadIdx.x * kScanItems;
+      int v[kScanItems];
+      int s = 0;
+#pragma unroll
+      for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < a.n ? a.in[base + k] : 0;
+        s += v[k];
+      }
+      int tot;
+      int pre = cta_excl_scan(s, sh, &tot) + carry;
+#pragma unroll
+      for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < a.n) a.out[base + k] = pre;
+        pre += v[k];
+      }
+      carry += tot;
+    }
+    if (threadIdx.x == 0) a.out[a.n] = carry;
+  }
+};
+
+struct ScanApplyBody {
+  using Args = ScanArgs;
+  static constexpr int kThreads = kScanThreads, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    __shared__ int sh[33];
+    int base = vb * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
     int s = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-      v[k] = base + k < n ? in[base + k] : 0;
+      v[k] = base + k < a.n ? a.in[base + k] : 0;
       s += v[k];
     }
     int tot;
-    int pre = cta_excl_scan(s, sh, &tot) + carry;
+    int pre = cta_excl_scan(s, sh, &tot) + a.tile[vb];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-      if (base + k < n) out[base + k] = pre;
+      if (base + k < a.n) a.out[base + k] = pre;
       pre += v[k];
     }
-    carry += tot;
+    if (vb == vg - 1 && threadIdx.x == blockDim.x - 1) a.out[a.n] = pre;
   }
-  if (threadIdx.x == 0) out[n] = carry;
-}
+};
 
-__global__ void scan_apply(const int32_t* __restrict__ in, int32_t* out, int32_t n,
-                           const int32_t* __restrict__ tile_off) {
-  __shared__ int sh[33];
-  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-  int v[kScanItems];
-  int s = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    v[k] = base + k < n ? in[base + k] : 0;
-    s += v[k];
-  }
-  int tot;
-  int pre = cta_excl_scan(s, sh, &tot) + tile_off[blockIdx.x];
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < n) out[base + k] = pre;
-    pre += v[k];
-  }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) out[n] = pre;
-}
+constexpr int kScanSingleMax = 8 * kScanTile;
 
 // ------------------------------------------------------------ rebuild ------
 struct RbSide {
@@ -149,18 +177,26 @@ struct RbSide {
 struct RbArgs {
   RbSide s[2];
   const int32_t* part;
-  int32_t N, E, B;
+  int32_t N, E, B, pad;
 };
 
+// The rebuild bodies work on both directions: virtual block vb serves
+// direction vb & 1 with the direction's own virtual block vb >> 1.
+
 // Per vertex: its entries form one run inside its block's segment.
-__global__ void rb_count(RbArgs a) {
-  const RbSide& d = a.s[blockIdx.y];
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= a.N) return;
+struct RbCountBody {
+  using Args = RbArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int) {
+  const RbSide& d = a.s[vb & 1];
+  int v = (vb >> 1) * blockDim.x + threadIdx.x;
+  const bool live = v < a.N;
+  const unsigned active = __ballot_sync(kFull, live);
+  if (!live) return;
   int b = a.part[v];
   int len = d.gptr[v + 1] - d.gptr[v];
   // warp-aggregated: lanes with the same block reserve one range together
-  unsigned active = __activemask();
   unsigned peers = __match_any_sync(active, b);
   int lane = threadIdx.x & 31;
   int leader = __ffs(peers) - 1;
@@ -175,19 +211,25 @@ __global__ void rb_count(RbArgs a) {
   if (lane == leader) base = atomicAdd(d.cnt + b, tot);
   base = __shfl_sync(peers, base, leader);
   d.vofs[v] = base + pre;
-}
+  }
+};
 
 // Per graph entry: (block of the neighbour, weight) into the owner's run.
-__global__ void rb_scatter(RbArgs a) {
-  const RbSide& d = a.s[blockIdx.y];
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.E) return;
-  int v = __ldg(d.gsrc + j);
-  int b = __ldg(a.part + v);
-  int pos = __ldg(d.seg + b) + __ldg(d.vofs + v) + (j - __ldg(d.gptr + v));
-  d.tcol[pos] = __ldg(a.part + __ldg(d.gidx + j));
-  d.tw[pos] = __ldg(d.gw + j);
-}
+struct RbScatterBody {
+  using Args = RbArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int) {
+    const RbSide& d = a.s[vb & 1];
+    int j = (vb >> 1) * blockDim.x + threadIdx.x;
+    if (j >= a.E) return;
+    int v = __ldg(d.gsrc + j);
+    int b = __ldg(a.part + v);
+    int pos = __ldg(d.seg + b) + __ldg(d.vofs + v) + (j - __ldg(d.gptr + v));
+    d.tcol[pos] = __ldg(a.part + __ldg(d.gidx + j));
+    d.tw[pos] = __ldg(d.gw + j);
+  }
+};
 
 constexpr int kWarpCap = 256;  // longest segment sorted by one warp
 constexpr int kRowsWarps = 8;
@@ -212,12 +254,18 @@ __device__ __forceinline__ void warp_bitonic(unsigned long long* key, int P, int
 }
 
 // Short segments: one warp each.  Long ones are listed for rb_rows_big.
-__global__ void __launch_bounds__(kRowsWarps * 32) rb_rows_small(RbArgs a) {
+struct RbRowsSmallBody {
+  using Args = RbArgs;
+  static constexpr int kThreads = kRowsWarps * 32, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
   __shared__ unsigned long long sk[kRowsWarps][kWarpCap];
-  const RbSide& d = a.s[blockIdx.y];
+  const RbSide& d = a.s[vb & 1];
+  vb >>= 1;
+  vg >>= 1;
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned long long* key = sk[wid];
-  for (int b = blockIdx.x * kRowsWarps + wid; b < a.B; b += gridDim.x * kRowsWarps) {
+  for (int b = vb * kRowsWarps + wid; b < a.B; b += vg * kRowsWarps) {
     int base = d.seg[b];
     int n = d.seg[b + 1] - base;
     if (n > kWarpCap) {
@@ -254,21 +302,28 @@ __global__ void __launch_bounds__(kRowsWarps * 32) rb_rows_small(RbArgs a) {
     if (lane == 0) d.uniq[b] = running;
     __syncwarp();
   }
-}
+  }
+};
 
 constexpr int kBigThreads = 512;
 constexpr int kHistCap = 16384;  // columns counted in shared memory at once
 constexpr int kSortCap = 8192;   // longest segment sorted in shared memory
 constexpr size_t kBigSmem = 65536;
 
-__global__ void __launch_bounds__(kBigThreads) rb_rows_big(RbArgs a) {
+struct RbRowsBigBody {
+  using Args = RbArgs;
+  static constexpr int kThreads = kBigThreads, kMinBlocks = 1;
+  static constexpr size_t kSmem = kBigSmem;
+  static __device__ void run(const Args& a, int vb, int vg) {
   extern __shared__ unsigned long long big_sm[];
   __shared__ int sh[33];
-  const RbSide& d = a.s[blockIdx.y];
+  const RbSide& d = a.s[vb & 1];
+  vb >>= 1;
+  vg >>= 1;
   uint32_t* hist = (uint32_t*)big_sm;
   int nbig = *d.big_count;
   int T = blockDim.x, tid = threadIdx.x;
-  for (int idx = blockIdx.x; idx < nbig; idx += gridDim.x) {
+  for (int idx = vb; idx < nbig; idx += vg) {
     int b = d.big[idx];
     int base = d.seg[b];
     int n = d.seg[b + 1] - base;
@@ -346,14 +401,21 @@ __global__ void __launch_bounds__(kBigThreads) rb_rows_big(RbArgs a) {
     if (tid == 0) d.uniq[b] = running;
     __syncthreads();
   }
-}
+  }
+};
 
 // Per row: unique entries into place, weighted degree and its log2.
-__global__ void rb_compact(RbArgs a) {
-  const RbSide& d = a.s[blockIdx.y];
+struct RbCompactBody {
+  using Args = RbArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+  const RbSide& d = a.s[vb & 1];
+  vb >>= 1;
+  vg >>= 1;
   int lane = threadIdx.x & 31;
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int nw = (gridDim.x * blockDim.x) >> 5;
+  int w = (vb * blockDim.x + threadIdx.x) >> 5;
+  int nw = (vg * blockDim.x) >> 5;
   for (int b = w; b < a.B; b += nw) {
     int src = d.seg[b], dst = d.bptr[b], u = d.uniq[b];
     unsigned long long s = 0;
@@ -370,7 +432,8 @@ __global__ void rb_compact(RbArgs a) {
       d.bld[b] = log2((double)deg);
     }
   }
-}
+  }
+};
 
 // ------------------------------------------------------------ block terms --
 struct BtArgs {
@@ -415,12 +478,16 @@ __device__ int warp_pick_row(const BtArgs& a, int b, uint64_t t, int lane) {
   return -1;
 }
 
-__global__ void block_terms_kernel(BtArgs a) {
+struct BlockTermsBody {
+  using Args = BtArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
   int lane = threadIdx.x & 31;
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int nw = (gridDim.x * blockDim.x) >> 5;
+  int w = (vb * blockDim.x + threadIdx.x) >> 5;
+  int nw = (vg * blockDim.x) >> 5;
   for (int b = w; b < a.B; b += nw) {
-   if (a.draws != 1) {
+    if (a.draws != 1) {
     double acc = 0.0;
     for (int i = a.optr[b] + lane; i < a.optr[b + 1]; i += 32) {
       uint32_t m = a.ocnt[i];
@@ -440,7 +507,7 @@ __global__ void block_terms_kernel(BtArgs a) {
       a.ambin[b] = ai;
       a.sinfull[b] = ai - (din ? (double)din * a.ld_in[b] : 0.0);
     }
-   }
+    }
     if (a.draws) {
       P4 x = draw(a.seed, kRngNodalBlock, a.seq, (uint32_t)b);
       uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
@@ -455,7 +522,8 @@ __global__ void block_terms_kernel(BtArgs a) {
       }
     }
   }
-}
+  }
+};
 
 
 // ------------------------------------------------------------ dense form --
@@ -464,57 +532,82 @@ __global__ void block_terms_kernel(BtArgs a) {
 // restore; after each nodal batch only the edges of the moved vertices are
 // applied, with integer atomics (exact, order-independent).
 
-__global__ void dense_edges_kernel(const int32_t* __restrict__ osrc,
-                                   const int32_t* __restrict__ oidx,
-                                   const uint32_t* __restrict__ ow,
-                                   const int32_t* __restrict__ part, int32_t E, int32_t B,
-                                   uint32_t* Md, uint32_t* MTd) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= E) return;
-  int r = __ldg(part + __ldg(osrc + j)), c = __ldg(part + __ldg(oidx + j));
-  uint32_t w = __ldg(ow + j);
-  atomicAdd(Md + (size_t)r * B + c, w);
-  atomicAdd(MTd + (size_t)c * B + r, w);
-}
+struct DenseArgs {
+  const int32_t *osrc, *optr, *oidx, *iptr, *iidx;
+  const uint32_t *ow, *iw, *kdo, *kdi;
+  const int32_t* part;
+  const int32_t* newlab;  // update: new labels of vertices lo..lo+count-1
+  uint32_t *Md, *MTd, *d_out, *d_in;
+  double *ld_out, *ld_in;
+  int32_t N, E, B, lo, count, pad;
+};
 
-__global__ void dense_degrees_kernel(const int32_t* __restrict__ part,
-                                     const uint32_t* __restrict__ kdo,
-                                     const uint32_t* __restrict__ kdi, int32_t N,
-                                     uint32_t* d_out, uint32_t* d_in) {
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= N) return;
-  int b = part[v];
-  atomicAdd(d_out + b, kdo[v]);
-  atomicAdd(d_in + b, kdi[v]);
-}
+// Build step 1: every edge adds its weight to M[r][c] (and the transpose).
+struct DenseEdgesBody {
+  using Args = DenseArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int) {
+    int j = vb * blockDim.x + threadIdx.x;
+    if (j >= a.E) return;
+    int r = __ldg(a.part + __ldg(a.osrc + j)), c = __ldg(a.part + __ldg(a.oidx + j));
+    uint32_t w = __ldg(a.ow + j);
+    atomicAdd(a.Md + (size_t)r * a.B + c, w);
+    atomicAdd(a.MTd + (size_t)c * a.B + r, w);
+  }
+};
 
-__global__ void dense_logs_kernel(const uint32_t* __restrict__ d_out,
-                                  const uint32_t* __restrict__ d_in, int32_t B, double* ld_out,
-                                  double* ld_in) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
-  ld_out[b] = log2((double)d_out[b]);
-  ld_in[b] = log2((double)d_in[b]);
-}
+// Build step 2: block degrees from vertex degrees.
+struct DenseDegreesBody {
+  using Args = DenseArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int) {
+    int v = vb * blockDim.x + threadIdx.x;
+    if (v >= a.N) return;
+    int b = a.part[v];
+    atomicAdd(a.d_out + b, a.kdo[v]);
+    atomicAdd(a.d_in + b, a.kdi[v]);
+  }
+};
+
+// Build step 3: log2 of the block degrees.
+struct DenseLogsBody {
+  using Args = DenseArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int) {
+    int b = vb * blockDim.x + threadIdx.x;
+    if (b >= a.B) return;
+    a.ld_out[b] = log2((double)a.d_out[b]);
+    a.ld_in[b] = log2((double)a.d_in[b]);
+  }
+};
 
 // One warp per batch vertex that moves: its out-edges move from
 // (r, old block of w) to (s, new block of w); its in-edges from unmoved
 // sources move from (b(u), r) to (b(u), s).  Edges between two moved vertices
 // are handled once, from the source's out-edges.
-__global__ void dense_update_kernel(const int32_t* __restrict__ optr,
-                                    const int32_t* __restrict__ oidx,
-                                    const uint32_t* __restrict__ ow,
-                                    const int32_t* __restrict__ iptr,
-                                    const int32_t* __restrict__ iidx,
-                                    const uint32_t* __restrict__ iw,
-                                    const uint32_t* __restrict__ kdo,
-                                    const uint32_t* __restrict__ kdi,
-                                    const int32_t* __restrict__ part, int32_t lo, int32_t count,
-                                    const int32_t* __restrict__ newlab, int32_t B, uint32_t* Md,
-                                    uint32_t* MTd, uint32_t* d_out, uint32_t* d_in) {
+struct DenseUpdateBody {
+  using Args = DenseArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+  const int32_t* __restrict__ optr = a.optr;
+  const int32_t* __restrict__ oidx = a.oidx;
+  const uint32_t* __restrict__ ow = a.ow;
+  const int32_t* __restrict__ iptr = a.iptr;
+  const int32_t* __restrict__ iidx = a.iidx;
+  const uint32_t* __restrict__ iw = a.iw;
+  const uint32_t* __restrict__ kdo = a.kdo;
+  const uint32_t* __restrict__ kdi = a.kdi;
+  const int32_t* __restrict__ part = a.part;
+  const int32_t* __restrict__ newlab = a.newlab;
+  const int32_t lo = a.lo, count = a.count, B = a.B;
+  uint32_t *Md = a.Md, *MTd = a.MTd, *d_out = a.d_out, *d_in = a.d_in;
   const int lane = threadIdx.x & 31;
-  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int w0 = (vb * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (vg * blockDim.x) >> 5;
   for (int i = w0; i < count; i += nw) {
     const int v = lo + i;
     const int r = part[v], s = newlab[i];
@@ -546,7 +639,8 @@ __global__ void dense_update_kernel(const int32_t* __restrict__ optr,
       atomicAdd(MTd + (size_t)s * B + bu, wt);
     }
   }
-}
+  }
+};
 
 // First column k of dense out-row ++ in-row of block b whose running count
 // exceeds t (zero columns never advance the count, so this is the same
@@ -587,15 +681,19 @@ struct BtDenseArgs {
   uint32_t seq;
 };
 
-__global__ void block_terms_dense_kernel(BtDenseArgs a) {
+struct BlockTermsDenseBody {
+  using Args = BtDenseArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
   int lane = threadIdx.x & 31;
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int nw = (gridDim.x * blockDim.x) >> 5;
+  int w = (vb * blockDim.x + threadIdx.x) >> 5;
+  int nw = (vg * blockDim.x) >> 5;
   const int B = a.B;
   for (int b = w; b < B; b += nw) {
     const uint32_t* orow = a.Md + (size_t)b * B;
     const uint32_t* irow = a.MTd + (size_t)b * B;
-   if (a.draws != 1) {
+    if (a.draws != 1) {
     double ao = 0.0, ai = 0.0;
     for (int c = lane; c < B; c += 32) {
       uint32_t mo = orow[c], mi = irow[c];
@@ -611,7 +709,7 @@ __global__ void block_terms_dense_kernel(BtDenseArgs a) {
       a.ambin[b] = ai;
       a.sinfull[b] = ai - (din ? (double)din * a.ld_in[b] : 0.0);
     }
-   }
+    }
     if (a.draws) {
       P4 x = draw(a.seed, kRngNodalBlock, a.seq, (uint32_t)b);
       uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
@@ -626,25 +724,78 @@ __global__ void block_terms_dense_kernel(BtDenseArgs a) {
       }
     }
   }
-}
+  }
+};
 
 __global__ void fill_xlx_kernel(double* tab) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x < kXlxTable) tab[x] = xlog2x(x);
 }
 
-__global__ void mdl_sum_kernel(const double* __restrict__ dSout, int32_t B, double* out) {
-  __shared__ double sh[1024];
-  double s = 0.0;
-  for (int b = threadIdx.x; b < B; b += blockDim.x) s += dSout[b];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+struct MdlArgs {
+  const double* dSout;
+  double* out;
+  int32_t B, pad;
+};
+
+// data_S = sum of dSout over the blocks, one CTA per job, fixed order.
+struct MdlSumBody {
+  using Args = MdlArgs;
+  static constexpr int kThreads = 512, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int, int) {
+    __shared__ double sh[kThreads];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < a.B; b += kThreads) s += a.dSout[b];
+    sh[threadIdx.x] = s;
     __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) *a.out = sh[0];
   }
-  if (threadIdx.x == 0) *out = sh[0];
-}
+};
+
+// Small utility bodies of the multi-job engine.
+struct WordsArgs {
+  uint32_t* dst;
+  const uint32_t* src;  // copy source (copy body)
+  long long n;          // 32-bit words
+};
+
+struct ZeroBody {
+  using Args = WordsArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    for (long long i = (long long)vb * kThreads + threadIdx.x; i < a.n;
+         i += (long long)vg * kThreads)
+      a.dst[i] = 0u;
+  }
+};
+
+struct CopyBody {
+  using Args = WordsArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    for (long long i = (long long)vb * kThreads + threadIdx.x; i < a.n;
+         i += (long long)vg * kThreads)
+      a.dst[i] = a.src[i];
+  }
+};
+
+struct IotaBody {
+  using Args = WordsArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    for (long long i = (long long)vb * kThreads + threadIdx.x; i < a.n;
+         i += (long long)vg * kThreads)
+      a.dst[i] = (uint32_t)i;
+  }
+};
 
 int grid_for(long long items, int per_block, int cap) {
   long long g = (items + per_block - 1) / per_block;
@@ -653,31 +804,8 @@ int grid_for(long long items, int per_block, int cap) {
   return (int)g;
 }
 
-}  // namespace
-
-cudaError_t init_kernel_attributes() {
-  return cudaFuncSetAttribute(rb_rows_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)kBigSmem);
-}
-
-void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, cudaStream_t st) {
-  if (n <= 8 * kScanTile) {
-    ++g_launches;
-    scan_single<<<1, kScanThreads, 0, st>>>(in, out, n);
-    return;
-  }
-  int tiles = (n + kScanTile - 1) / kScanTile;
-  ++g_launches;
-  scan_tile_sums<<<tiles, kScanThreads, 0, st>>>(in, n, tile);
-  ++g_launches;
-  scan_single<<<1, kScanThreads, 0, st>>>(tile, tile + tiles, tiles);
-  ++g_launches;
-  scan_apply<<<tiles, kScanThreads, 0, st>>>(in, out, n, tile + tiles);
-}
-
-void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
-                        RebuildScratch& rs, cudaStream_t st) {
-  RbArgs a;
+RbArgs rb_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, RebuildScratch& rs) {
+  RbArgs a{};
   a.part = part;
   a.N = g.N;
   a.E = g.E;
@@ -704,30 +832,24 @@ void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM
     s.bcnt = dir == 0 ? m.ocnt : m.icnt;
     s.bdeg = dir == 0 ? m.d_out : m.d_in;
     s.bld = dir == 0 ? m.ld_out : m.ld_in;
-    cudaMemsetAsync(r.cnt, 0, sizeof(int32_t) * (size_t)B, st);
   }
-  cudaMemsetAsync(rs.big_count, 0, sizeof(int32_t) * 2, st);
-  ++g_launches;
-  rb_count<<<dim3((g.N + 255) / 256, 2), 256, 0, st>>>(a);
-  for (int dir = 0; dir < 2; ++dir)
-    scan_exclusive(rs.d[dir].cnt, rs.d[dir].seg, B, rs.tile + dir * (rs.tile_cap / 2), st);
-  if (g.E > 0) {
-    ++g_launches;
-    rb_scatter<<<dim3((g.E + 255) / 256, 2), 256, 0, st>>>(a);
-  }
-  ++g_launches;
-  rb_rows_small<<<dim3(grid_for(B, kRowsWarps, 4096), 2), kRowsWarps * 32, 0, st>>>(a);
-  ++g_launches;
-  rb_rows_big<<<dim3(2 * 148, 2), kBigThreads, kBigSmem, st>>>(a);
-  for (int dir = 0; dir < 2; ++dir)
-    scan_exclusive(rs.d[dir].uniq, dir == 0 ? m.optr : m.iptr, B,
-                   rs.tile + dir * (rs.tile_cap / 2), st);
-  ++g_launches;
-  rb_compact<<<dim3(grid_for((long long)B * 32, 256, 4096), 2), 256, 0, st>>>(a);
+  return a;
 }
 
-void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cudaStream_t st) {
-  BtArgs a;
+// Virtual grids: functions of one job's sizes only.
+int32_t vg_count(const RbArgs& a) { return 2 * ceil_div(a.N, 256); }
+int32_t vg_scatter(const RbArgs& a) { return a.E > 0 ? 2 * ceil_div(a.E, 256) : 0; }
+int32_t vg_rows_small(const RbArgs& a) { return 2 * grid_for(a.B, kRowsWarps, 4096); }
+int32_t vg_rows_big(const RbArgs& a) {
+  return 2 * std::max(1, std::min(2 * 148, ceil_div(std::max(a.E, 1), 2048)));
+}
+int32_t vg_compact(const RbArgs& a) { return 2 * grid_for((long long)a.B * 32, 256, 4096); }
+int32_t vg_words(long long n) {
+  return n <= 0 ? 0 : (int32_t)std::min<long long>(4096, (n + 2047) / 2048);
+}
+
+BtArgs bt_args(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq) {
+  BtArgs a{};
   a.xlx = m.xlx;
   a.optr = m.optr; a.ocol = m.ocol; a.iptr = m.iptr; a.icol = m.icol;
   a.ocnt = m.ocnt; a.icnt = m.icnt; a.d_out = m.d_out; a.d_in = m.d_in;
@@ -735,8 +857,131 @@ void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cu
   a.dSout = m.dSout; a.ambout = m.ambout; a.ambin = m.ambin; a.sinfull = m.sinfull;
   a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
   a.B = B; a.draws = draws; a.seed = seed; a.seq = seq;
-  ++g_launches;
-  block_terms_kernel<<<grid_for((long long)B * 32, 256, 8192), 256, 0, st>>>(a);
+  return a;
+}
+
+BtDenseArgs bt_dense_args(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq) {
+  BtDenseArgs a{};
+  a.xlx = m.xlx;
+  a.Md = m.Md; a.MTd = m.MTd; a.d_out = m.d_out; a.d_in = m.d_in;
+  a.ld_out = m.ld_out; a.ld_in = m.ld_in;
+  a.dSout = m.dSout; a.ambout = m.ambout; a.ambin = m.ambin; a.sinfull = m.sinfull;
+  a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
+  a.B = B; a.draws = draws; a.seed = seed; a.seq = seq;
+  return a;
+}
+
+DenseArgs dense_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m) {
+  DenseArgs a{};
+  a.osrc = g.osrc; a.optr = g.optr; a.oidx = g.oidx; a.iptr = g.iptr; a.iidx = g.iidx;
+  a.ow = g.ow; a.iw = g.iw; a.kdo = g.kdo; a.kdi = g.kdi;
+  a.part = part;
+  a.Md = m.Md; a.MTd = m.MTd; a.d_out = m.d_out; a.d_in = m.d_in;
+  a.ld_out = m.ld_out; a.ld_in = m.ld_in;
+  a.N = g.N; a.E = g.E; a.B = B;
+  return a;
+}
+
+int32_t vg_block_terms(int32_t B) { return grid_for((long long)B * 32, 256, 8192); }
+int32_t vg_dense_update(int32_t count) { return grid_for((long long)count * 32, 256, 148 * 16); }
+
+const MultiKernel kmScanTile = multi_kernel_desc<ScanTileBody>("scan_tile");
+const MultiKernel kmScanSingle = multi_kernel_desc<ScanSingleBody>("scan_single");
+const MultiKernel kmScanApply = multi_kernel_desc<ScanApplyBody>("scan_apply");
+const MultiKernel kmRbCount = multi_kernel_desc<RbCountBody>("rb_count");
+const MultiKernel kmRbScatter = multi_kernel_desc<RbScatterBody>("rb_scatter");
+const MultiKernel kmRbRowsSmall = multi_kernel_desc<RbRowsSmallBody>("rb_rows_small");
+const MultiKernel kmRbRowsBig = multi_kernel_desc<RbRowsBigBody>("rb_rows_big");
+const MultiKernel kmRbCompact = multi_kernel_desc<RbCompactBody>("rb_compact");
+const MultiKernel kmBlockTerms = multi_kernel_desc<BlockTermsBody>("block_terms");
+const MultiKernel kmBlockTermsDense = multi_kernel_desc<BlockTermsDenseBody>("block_terms_dense");
+const MultiKernel kmDenseEdges = multi_kernel_desc<DenseEdgesBody>("dense_edges");
+const MultiKernel kmDenseDegrees = multi_kernel_desc<DenseDegreesBody>("dense_degrees");
+const MultiKernel kmDenseLogs = multi_kernel_desc<DenseLogsBody>("dense_logs");
+const MultiKernel kmDenseUpdate = multi_kernel_desc<DenseUpdateBody>("dense_update");
+const MultiKernel kmMdlSum = multi_kernel_desc<MdlSumBody>("mdl_sum");
+const MultiKernel kmZero = multi_kernel_desc<ZeroBody>("zero");
+const MultiKernel kmCopy = multi_kernel_desc<CopyBody>("copy");
+const MultiKernel kmIota = multi_kernel_desc<IotaBody>("iota");
+
+// One job's scan records: short arrays in one CTA, longer ones in three steps.
+void add_scan(Slot* sl, const int32_t* in, int32_t* out, int32_t n, int32_t* tile) {
+  ScanArgs a{};
+  if (n <= kScanSingleMax) {
+    a.in = in;
+    a.out = out;
+    a.n = n;
+    slot_push(slot_bind(sl[1], kmScanSingle), a, 1);
+    return;
+  }
+  const int32_t tiles = ceil_div(n, kScanTile);
+  a.in = in;
+  a.out = out;
+  a.tile = tile;
+  a.n = n;
+  slot_push(slot_bind(sl[0], kmScanTile), a, tiles);
+  ScanArgs b{};
+  b.in = tile;
+  b.out = tile + tiles;
+  b.n = tiles;
+  slot_push(slot_bind(sl[1], kmScanSingle), b, 1);
+  a.tile = tile + tiles;
+  slot_push(slot_bind(sl[2], kmScanApply), a, tiles);
+}
+
+}  // namespace
+
+cudaError_t init_kernel_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(single_kernel<RbRowsBigBody>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBigSmem);
+  cudaError_t e2 = cudaFuncSetAttribute(multi_kernel<RbRowsBigBody>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kBigSmem);
+  return e != cudaSuccess ? e : e2;
+}
+
+void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, cudaStream_t st) {
+  ScanArgs a{};
+  a.in = in;
+  a.out = out;
+  a.n = n;
+  if (n <= kScanSingleMax) {
+    launch_single<ScanSingleBody>(a, 1, st);
+    return;
+  }
+  int tiles = ceil_div(n, kScanTile);
+  a.tile = tile;
+  launch_single<ScanTileBody>(a, tiles, st);
+  ScanArgs b{};
+  b.in = tile;
+  b.out = tile + tiles;
+  b.n = tiles;
+  launch_single<ScanSingleBody>(b, 1, st);
+  a.tile = tile + tiles;
+  launch_single<ScanApplyBody>(a, tiles, st);
+}
+
+void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
+                        RebuildScratch& rs, cudaStream_t st) {
+  RbArgs a = rb_args(g, part, B, m, rs);
+  for (int dir = 0; dir < 2; ++dir)
+    cudaMemsetAsync(rs.d[dir].cnt, 0, sizeof(int32_t) * (size_t)B, st);
+  cudaMemsetAsync(rs.big_count, 0, sizeof(int32_t) * 2, st);
+  launch_single<RbCountBody>(a, vg_count(a), st);
+  for (int dir = 0; dir < 2; ++dir)
+    scan_exclusive(rs.d[dir].cnt, rs.d[dir].seg, B, rs.tile + dir * (rs.tile_cap / 2), st);
+  launch_single<RbScatterBody>(a, vg_scatter(a), st);
+  launch_single<RbRowsSmallBody>(a, vg_rows_small(a), st);
+  launch_single<RbRowsBigBody>(a, vg_rows_big(a), st);
+  for (int dir = 0; dir < 2; ++dir)
+    scan_exclusive(rs.d[dir].uniq, dir == 0 ? m.optr : m.iptr, B,
+                   rs.tile + dir * (rs.tile_cap / 2), st);
+  launch_single<RbCompactBody>(a, vg_compact(a), st);
+}
+
+void block_terms(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq, cudaStream_t st) {
+  launch_single<BlockTermsBody>(bt_args(m, B, draws, seed, seq), vg_block_terms(B), st);
 }
 
 void fill_xlx_table(double* tab, cudaStream_t st) {
@@ -750,43 +995,117 @@ void dense_build(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, cu
   cudaMemsetAsync(m.MTd, 0, bb * sizeof(uint32_t), st);
   cudaMemsetAsync(m.d_out, 0, (size_t)B * sizeof(uint32_t), st);
   cudaMemsetAsync(m.d_in, 0, (size_t)B * sizeof(uint32_t), st);
-  if (g.E > 0) {
-    ++g_launches;
-    dense_edges_kernel<<<(g.E + 255) / 256, 256, 0, st>>>(g.osrc, g.oidx, g.ow, part, g.E, B,
-                                                          m.Md, m.MTd);
-  }
-  ++g_launches;
-  dense_degrees_kernel<<<(g.N + 255) / 256, 256, 0, st>>>(part, g.kdo, g.kdi, g.N, m.d_out,
-                                                          m.d_in);
-  ++g_launches;
-  dense_logs_kernel<<<(B + 255) / 256, 256, 0, st>>>(m.d_out, m.d_in, B, m.ld_out, m.ld_in);
+  DenseArgs a = dense_args(g, part, B, m);
+  if (g.E > 0) launch_single<DenseEdgesBody>(a, ceil_div(g.E, 256), st);
+  launch_single<DenseDegreesBody>(a, ceil_div(g.N, 256), st);
+  launch_single<DenseLogsBody>(a, ceil_div(B, 256), st);
 }
 
 void dense_update(const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
                   const int32_t* newlab, int32_t B, DevBM& m, cudaStream_t st) {
   if (count <= 0) return;
-  ++g_launches;
-  dense_update_kernel<<<grid_for((long long)count * 32, 256, 148 * 16), 256, 0, st>>>(
-      g.optr, g.oidx, g.ow, g.iptr, g.iidx, g.iw, g.kdo, g.kdi, part, lo, count, newlab, B, m.Md,
-      m.MTd, m.d_out, m.d_in);
+  DenseArgs a = dense_args(g, part, B, m);
+  a.lo = lo;
+  a.count = count;
+  a.newlab = newlab;
+  launch_single<DenseUpdateBody>(a, vg_dense_update(count), st);
 }
 
 void block_terms_dense(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq,
                        cudaStream_t st) {
-  BtDenseArgs a;
-  a.xlx = m.xlx;
-  a.Md = m.Md; a.MTd = m.MTd; a.d_out = m.d_out; a.d_in = m.d_in;
-  a.ld_out = m.ld_out; a.ld_in = m.ld_in;
-  a.dSout = m.dSout; a.ambout = m.ambout; a.ambin = m.ambin; a.sinfull = m.sinfull;
-  a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
-  a.B = B; a.draws = draws; a.seed = seed; a.seq = seq;
-  ++g_launches;
-  block_terms_dense_kernel<<<grid_for((long long)B * 32, 256, 8192), 256, 0, st>>>(a);
+  launch_single<BlockTermsDenseBody>(bt_dense_args(m, B, draws, seed, seq), vg_block_terms(B),
+                                     st);
 }
 
 void mdl_data_sum(const DevBM& m, int32_t B, double* out, cudaStream_t st) {
-  ++g_launches;
-  mdl_sum_kernel<<<1, 1024, 0, st>>>(m.dSout, B, out);
+  MdlArgs a{m.dSout, out, B, 0};
+  launch_single<MdlSumBody>(a, 1, st);
+}
+
+// ------------------------------------------------------ multi-job records --
+void RebuildSlots::clear() {
+  for (Slot* x : all()) x->clear();
+}
+
+std::vector<Slot*> RebuildSlots::all() {
+  return {&zero,     &count,     &scan1[0],   &scan1[1], &scan1[2], &scatter,
+          &rows_small, &rows_big, &scan2[0], &scan2[1], &scan2[2], &compact};
+}
+
+void add_rebuild(RebuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
+                 RebuildScratch& rs) {
+  RbArgs a = rb_args(g, part, B, m, rs);
+  for (int dir = 0; dir < 2; ++dir) add_zero(s.zero, rs.d[dir].cnt, (size_t)B);
+  add_zero(s.zero, rs.big_count, 2);
+  slot_push(slot_bind(s.count, kmRbCount), a, vg_count(a));
+  for (int dir = 0; dir < 2; ++dir)
+    add_scan(s.scan1, rs.d[dir].cnt, rs.d[dir].seg, B, rs.tile + dir * (rs.tile_cap / 2));
+  slot_push(slot_bind(s.scatter, kmRbScatter), a, vg_scatter(a));
+  slot_push(slot_bind(s.rows_small, kmRbRowsSmall), a, vg_rows_small(a));
+  slot_push(slot_bind(s.rows_big, kmRbRowsBig), a, vg_rows_big(a));
+  for (int dir = 0; dir < 2; ++dir)
+    add_scan(s.scan2, rs.d[dir].uniq, dir == 0 ? m.optr : m.iptr, B,
+             rs.tile + dir * (rs.tile_cap / 2));
+  slot_push(slot_bind(s.compact, kmRbCompact), a, vg_compact(a));
+}
+
+void DenseBuildSlots::clear() {
+  for (Slot* x : all()) x->clear();
+}
+
+std::vector<Slot*> DenseBuildSlots::all() { return {&zero, &edges, &degrees, &logs}; }
+
+void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B,
+                     DevBM& m) {
+  const size_t bb = (size_t)B * B;
+  add_zero(s.zero, m.Md, bb);
+  add_zero(s.zero, m.MTd, bb);
+  add_zero(s.zero, m.d_out, (size_t)B);
+  add_zero(s.zero, m.d_in, (size_t)B);
+  DenseArgs a = dense_args(g, part, B, m);
+  slot_push(slot_bind(s.edges, kmDenseEdges), a, g.E > 0 ? ceil_div(g.E, 256) : 0);
+  slot_push(slot_bind(s.degrees, kmDenseDegrees), a, ceil_div(g.N, 256));
+  slot_push(slot_bind(s.logs, kmDenseLogs), a, ceil_div(B, 256));
+}
+
+void add_dense_update(Slot& s, const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
+                      const int32_t* newlab, int32_t B, DevBM& m) {
+  if (count <= 0) return;
+  DenseArgs a = dense_args(g, part, B, m);
+  a.lo = lo;
+  a.count = count;
+  a.newlab = newlab;
+  slot_push(slot_bind(s, kmDenseUpdate), a, vg_dense_update(count));
+}
+
+void add_block_terms(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq) {
+  slot_push(slot_bind(s, kmBlockTerms), bt_args(m, B, draws, seed, seq), vg_block_terms(B));
+}
+
+void add_block_terms_dense(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed,
+                           uint32_t seq) {
+  slot_push(slot_bind(s, kmBlockTermsDense), bt_dense_args(m, B, draws, seed, seq),
+            vg_block_terms(B));
+}
+
+void add_mdl_sum(Slot& s, const DevBM& m, int32_t B, double* out) {
+  MdlArgs a{m.dSout, out, B, 0};
+  slot_push(slot_bind(s, kmMdlSum), a, 1);
+}
+
+void add_zero(Slot& s, void* p, size_t words) {
+  WordsArgs a{(uint32_t*)p, nullptr, (long long)words};
+  slot_push(slot_bind(s, kmZero), a, vg_words((long long)words));
+}
+
+void add_copy(Slot& s, void* dst, const void* src, size_t words) {
+  WordsArgs a{(uint32_t*)dst, (const uint32_t*)src, (long long)words};
+  slot_push(slot_bind(s, kmCopy), a, vg_words((long long)words));
+}
+
+void add_iota(Slot& s, int32_t* p, int32_t n) {
+  WordsArgs a{(uint32_t*)p, nullptr, (long long)n};
+  slot_push(slot_bind(s, kmIota), a, vg_words(n));
 }
 
 }  // namespace sbp

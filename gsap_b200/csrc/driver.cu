@@ -18,6 +18,7 @@
 //     (partition.hpp:41-56).
 #include "../../include/sbp.h"
 #include "common.cuh"
+#include "job.h"
 #include "kernels.h"
 
 #include <algorithm>
@@ -36,22 +37,16 @@ namespace sbp {
 
 static thread_local std::string g_last_error;
 
-static sbp_status fail(sbp_status st, const std::string& msg) {
+sbp_status fail(sbp_status st, const std::string& msg) {
   g_last_error = msg;
   return st;
 }
 
 sbp_status host_fail(sbp_status st, const char* msg) { return fail(st, msg); }
 
-#define SBP_CUDA(call)                                                                  \
-  do {                                                                                  \
-    cudaError_t e__ = (call);                                                           \
-    if (e__ != cudaSuccess)                                                             \
-      return fail(SBP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
-  } while (0)
 
 // ------------------------------------------------------------ validation --
-static sbp_status validate_graph(const sbp_graph_csr* g) {
+sbp_status validate_graph(const sbp_graph_csr* g) {
   if (!g) return fail(SBP_ERR_INVALID, "graph is NULL");
   if (g->N < 1 || g->E < 0) return fail(SBP_ERR_INVALID, "need N >= 1 and E >= 0");
   if (!g->out_ptr || !g->in_ptr || !g->deg_out || !g->deg_in)
@@ -81,7 +76,7 @@ static sbp_status validate_graph(const sbp_graph_csr* g) {
   return SBP_OK;
 }
 
-static sbp_status validate_part(const int32_t* part, int32_t N, int32_t B) {
+sbp_status validate_part(const int32_t* part, int32_t N, int32_t B) {
   if (!part) return fail(SBP_ERR_INVALID, "labels are NULL");
   if (B < 1 || B > N) return fail(SBP_ERR_INVALID, "need 1 <= B <= N");
   for (int32_t v = 0; v < N; ++v)
@@ -90,87 +85,10 @@ static sbp_status validate_part(const int32_t* part, int32_t N, int32_t B) {
 }
 
 // ----------------------------------------------------------------- arena --
-struct Arena {
-  char* base = nullptr;
-  size_t cap = 0, off = 0;
-  template <typename T>
-  T* take(size_t n) {
-    size_t bytes = ((n * sizeof(T)) + 255) & ~size_t(255);
-    if (off + bytes > cap) return nullptr;
-    T* p = (T*)(base + off);
-    off += bytes;
-    return p;
-  }
-};
+static int32_t scan_tiles_cap(int32_t N) { return 2 * (2 * ((N + 1) / 2048 + 2) + 2); }
 
-// Everything one partition job keeps in HBM.
-struct Job {
-  int device = 0;
-  cudaStream_t st = nullptr;
-  int32_t N = 0, E = 0, np = 10, max_itr = 100;
-  void* mem = nullptr;
-  size_t mem_bytes = 0;
-  DevGraph g;
-  DevBM m;
-  RebuildScratch rs;
-  int32_t *part = nullptr, *newlab = nullptr, *props = nullptr, *best = nullptr, *map = nullptr;
-  int32_t* snap[3] = {nullptr, nullptr, nullptr};
-  double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
-  int32_t* heavy = nullptr;     // batch indices of the CTA-per-vertex kernel
-  int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
-  CommitScratch cs;
-  int32_t dense_cap = 0;        // largest B the dense arrays can hold
-  int32_t dense_eff = 0;        // largest B kept in dense form in this run
-  cudaStream_t side = nullptr;  // heavy vertices run here, next to the warp kernel
-  cudaEvent_t fork = nullptr, join = nullptr;
-  double* dsum = nullptr;       // per nodal iteration: sum of recorded dS
-  double* dataS = nullptr;      // per nodal iteration: MDL data term
-  long long* acc = nullptr;     // per nodal iteration: applied moves
-  // pinned host mirrors
-  int32_t* h_best = nullptr;
-  double* h_best_dS = nullptr;
-  int32_t* h_map = nullptr;
-  double* h_scal = nullptr;     // dsum, dataS of one iteration
-  long long* h_acc = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  std::vector<cudaEvent_t> bev;  // per-batch timing events of one sweep
-  std::vector<int32_t> h_optr, h_iptr;  // host copies of the graph's row pointers
-  int32_t* h_misc = nullptr;            // pinned: nnz, error count
-
-  ~Job() { release(); }
-
-  void release() {
-    if (mem) {
-      int cur = 0;
-      cudaGetDevice(&cur);
-      cudaSetDevice(device);
-      if (st) cudaStreamSynchronize(st);
-      cudaFree(mem);
-      for (auto& e : ev)
-        if (e) cudaEventDestroy(e), e = nullptr;
-      for (auto& e : bev) cudaEventDestroy(e);
-      bev.clear();
-      if (fork) cudaEventDestroy(fork);
-      if (join) cudaEventDestroy(join);
-      fork = join = nullptr;
-      if (side) cudaStreamDestroy(side);
-      side = nullptr;
-      if (st) cudaStreamDestroy(st);
-      cudaFreeHost(h_best);
-      cudaFreeHost(h_best_dS);
-      cudaFreeHost(h_map);
-      cudaFreeHost(h_scal);
-      cudaFreeHost(h_acc);
-      cudaFreeHost(h_misc);
-      cudaSetDevice(cur);
-      mem = nullptr;
-      st = nullptr;
-    }
-  }
-};
-
-static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t tiles,
-                        int32_t dense_cap) {
+size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t dense_cap) {
+  const int32_t tiles = scan_tiles_cap(N);
   size_t n1 = (size_t)N + 1, e = (size_t)E > 0 ? (size_t)E : 1;
   size_t b = 0;
   auto add = [&](size_t elems, size_t sz) { b += ((elems * sz) + 255) & ~size_t(255); };
@@ -198,13 +116,68 @@ static size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32
   add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
   add((size_t)N, 4); add(2, 4);
   add((size_t)dense_cap * dense_cap, 4); add((size_t)dense_cap * dense_cap, 4);
-  add(kXlxTable, 8); add(kCommitCtas, 8); add(kCommitCtas, 8); add(1, 4);
+  add(kCommitCtas, 8); add(kCommitCtas, 8); add(1, 4);
   return b + 4096;
 }
 
-static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np,
-                             int32_t max_itr, int32_t dense_max) {
+void Job::release() {
+  if (!mem && !st) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(device);
+  if (lean) {
+    if (mem) {
+      if (pool_stream) cudaFreeAsync(mem, pool_stream);
+      else cudaFree(mem);
+    }
+    mem = nullptr;
+    st = nullptr;
+    cudaSetDevice(cur);
+    return;
+  }
+  if (st) cudaStreamSynchronize(st);
+  if (mem) cudaFree(mem);
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+  fork = join = nullptr;
+  if (side) cudaStreamDestroy(side);
+  side = nullptr;
+  if (st) cudaStreamDestroy(st);
+  cudaFreeHost(h_best);
+  cudaFreeHost(h_best_dS);
+  cudaFreeHost(h_map);
+  h_best = nullptr;
+  h_best_dS = nullptr;
+  h_map = nullptr;
+  cudaSetDevice(cur);
+  mem = nullptr;
+  st = nullptr;
+}
+
+sbp_status device_xlx_table(int device, const double** out) {
+  static std::mutex mu;
+  static double* tab[64] = {};
+  if (device < 0 || device >= 64) return fail(SBP_ERR_INVALID, "device ordinal too large");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!tab[device]) {
+    double* t = nullptr;
+    SBP_CUDA(cudaMalloc(&t, sizeof(double) * kXlxTable));
+    cudaStream_t st;
+    SBP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    fill_xlx_table(t, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
+    tab[device] = t;
+  }
+  *out = tab[device];
+  return SBP_OK;
+}
+
+sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int32_t max_itr,
+                      int32_t dense_max, bool lean, cudaStream_t engine_stream) {
   J.device = device;
+  J.lean = lean;
   J.dense_cap = std::max(0, std::min(N, dense_max));
   J.dense_eff = J.dense_cap;
   J.N = N;
@@ -218,24 +191,27 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
       init_kernel_attributes();
       init_nodal_attributes();
     });
-  int32_t tiles = 2 * (2 * ((N + 1) / 2048 + 2) + 2);
-  J.mem_bytes = job_bytes(N, E, np, max_itr, tiles, J.dense_cap);
-  if (cudaMalloc(&J.mem, J.mem_bytes) != cudaSuccess) {
+  const double* xlx = nullptr;
+  sbp_status xs = device_xlx_table(device, &xlx);
+  if (xs != SBP_OK) return xs;
+  int32_t tiles = scan_tiles_cap(N);
+  J.mem_bytes = job_bytes(N, E, np, max_itr, J.dense_cap);
+  cudaError_t ae = lean ? cudaMallocAsync(&J.mem, J.mem_bytes, engine_stream)
+                        : cudaMalloc(&J.mem, J.mem_bytes);
+  if (ae != cudaSuccess) {
     cudaGetLastError();
     J.mem = nullptr;
     return fail(SBP_ERR_NOMEM, "device arena of " + std::to_string(J.mem_bytes) + " bytes");
   }
+  if (lean) {
+    J.pool_stream = engine_stream;
+    J.st = engine_stream;
+  } else {
   SBP_CUDA(cudaStreamCreateWithFlags(&J.st, cudaStreamNonBlocking));
   SBP_CUDA(cudaStreamCreateWithFlags(&J.side, cudaStreamNonBlocking));
   SBP_CUDA(cudaEventCreateWithFlags(&J.fork, cudaEventDisableTiming));
   SBP_CUDA(cudaEventCreateWithFlags(&J.join, cudaEventDisableTiming));
-  for (auto& e : J.ev) SBP_CUDA(cudaEventCreate(&e));
-  SBP_CUDA(cudaMallocHost(&J.h_best, sizeof(int32_t) * (size_t)N));
-  SBP_CUDA(cudaMallocHost(&J.h_best_dS, sizeof(double) * (size_t)N));
-  SBP_CUDA(cudaMallocHost(&J.h_map, sizeof(int32_t) * ((size_t)N + 1)));
-  SBP_CUDA(cudaMallocHost(&J.h_scal, sizeof(double) * 4));
-  SBP_CUDA(cudaMallocHost(&J.h_acc, sizeof(long long) * 2));
-  SBP_CUDA(cudaMallocHost(&J.h_misc, sizeof(int32_t) * 4));
+  }
   Arena A{(char*)J.mem, J.mem_bytes, 0};
   size_t n1 = (size_t)N + 1, e = (size_t)E > 0 ? (size_t)E : 1;
   DevGraph& g = J.g;
@@ -281,14 +257,13 @@ static sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t n
     m.Md = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
     m.MTd = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
   }
-  m.xlx = A.take<double>(kXlxTable);
+  m.xlx = const_cast<double*>(xlx);
   J.cs.part_sum = A.take<double>(kCommitCtas);
   J.cs.part_cnt = A.take<long long>(kCommitCtas);
   J.cs.ticket = A.take<unsigned>(1);
   if (!J.cs.ticket || (J.dense_cap > 0 && !m.MTd)) return fail(SBP_ERR_INTERNAL, "arena sizing");
   SBP_CUDA(cudaMemsetAsync(J.err, 0, 8, J.st));
   SBP_CUDA(cudaMemsetAsync(J.cs.ticket, 0, 4, J.st));
-  fill_xlx_table(m.xlx, J.st);
   return SBP_OK;
 }
 
@@ -298,12 +273,8 @@ __global__ void fill_src_kernel(const int32_t* __restrict__ ptr, int32_t N, int3
   for (int32_t j = ptr[v]; j < ptr[v + 1]; ++j) src[j] = v;
 }
 
-__global__ void iota_kernel(int32_t* p, int32_t N) {
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < N) p[v] = v;
-}
 
-static sbp_status job_upload(Job& J, const sbp_graph_csr* h) {
+sbp_status job_upload(Job& J, const sbp_graph_csr* h) {
   DevGraph& g = J.g;
   size_t n1 = (size_t)J.N + 1, E = (size_t)J.E;
   cudaStream_t st = J.st;
@@ -327,7 +298,7 @@ static sbp_status job_upload(Job& J, const sbp_graph_csr* h) {
   return SBP_OK;
 }
 
-static int resolve_device(int32_t d) {
+int resolve_device(int32_t d) {
   if (d >= 0) return d;
   int cur = 0;
   cudaGetDevice(&cur);
@@ -342,7 +313,7 @@ static int resolve_device(int32_t d) {
 // that label is itself.  Union-find gives the same labels as the reference's
 // relabel-all loop.  Surviving labels are renumbered in ascending order
 // (std::set, :58-68).  Returns the new block count.
-static int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
+int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
                                  const double* best_dS, int32_t* map_out) {
   std::vector<std::pair<uint64_t, int32_t>> key(B);
   for (int32_t b = 0; b < B; ++b) {
@@ -388,20 +359,12 @@ static int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* b
   return next;
 }
 
-static double model_S(int32_t B, int32_t N, int32_t E) {
+double model_S(int32_t B, int32_t N, int32_t E) {
   // partition.hpp:696-699 (Q6)
   double b = (double)B;
   double x = b * b / (double)E;
   return (double)E * (1.0 + x) * std::log(1.0 + x) - x * std::log(x) + (double)N * std::log(b);
 }
-
-struct Timer {
-  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
-  double ms() const {
-    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
-        .count();
-  }
-};
 
 static bool is_dense(const Job& J, int32_t B) { return B <= J.dense_eff; }
 
@@ -418,7 +381,7 @@ static void block_terms_any(Job& J, int32_t B, int draws, uint64_t seed, uint32_
   else block_terms(J.m, B, draws, seed, seq, st);
 }
 
-static bool heavy_vertex(const Job& J, int32_t v) {
+bool heavy_vertex(const Job& J, int32_t v) {
   const int32_t t = nodal_heavy_threshold();
   return J.h_optr[v + 1] - J.h_optr[v] > t || J.h_iptr[v + 1] - J.h_iptr[v] > t;
 }
@@ -437,6 +400,11 @@ static NodalAux aux_for(Job& J, const int32_t* heavy, int32_t n) {
 static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t seed, uint32_t seq,
                              bool keep_dS) {
   cudaStream_t st = J.st;
+  if (!J.h_best) {
+    SBP_CUDA(cudaMallocHost(&J.h_best, sizeof(int32_t) * (size_t)J.N));
+    SBP_CUDA(cudaMallocHost(&J.h_best_dS, sizeof(double) * (size_t)J.N));
+    SBP_CUDA(cudaMallocHost(&J.h_map, sizeof(int32_t) * ((size_t)J.N + 1)));
+  }
   // the merge kernels read the CSR form, stale after dense nodal sweeps
   if (is_dense(J, B)) rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
   block_terms(J.m, B, 0, seed, 0, st);
@@ -452,228 +420,8 @@ static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t se
   return SBP_OK;
 }
 
-struct Bracket {
-  int32_t B = 0;
-  int32_t B_to_merge = 0;
-  double S = std::numeric_limits<double>::infinity();
-  int slot = -1;  // snapshot buffer holding its labels
-};
-
-static sbp_status run_partition(Job& J, const sbp_options& o, int32_t* labels_out,
-                                sbp_report* rep) {
-  Timer total;
-  sbp_report R;
-  std::memset(&R, 0, sizeof(R));
-  cudaStream_t st = J.st;
-  const int32_t N = J.N, E = J.E;
-  const long long launches0 = g_launches;
-  SBP_CUDA(cudaEventRecord(J.ev[3], st));
-  ++g_launches;
-  iota_kernel<<<(N + 255) / 256, 256, 0, st>>>(J.part, N);
-  J.dense_eff = std::min(J.dense_cap, std::max(0, o.dense_max));
-  int32_t B = N;
-  int32_t B_to_merge = (int32_t)((float)B * o.reduction_rate);
-  build_model(J, B, st);
-  uint32_t seq = 0;
-  Bracket large, med, small;
-  // three snapshot buffers of labels; each bracket point owns one
-  bool optimal = false;
-  double S = 0.0;
-  int32_t BS = N / o.num_batches;
-  std::vector<double> itr_dS(o.max_nodal_itr);
-  float ms = 0.f;
-  // algorithmic bytes of one nodal batch's kernels: per vertex 28 bytes,
-  // per adjacency entry (either direction) 12, plus the blockmodel rows
-  // (16 per nonzero) and 8 per block
-  std::vector<double> batch_entries(o.num_batches, 0.0);
-  // heavy vertices of each batch (static: they depend on degrees only)
-  std::vector<int32_t> heavy_all, heavy_off(o.num_batches + 1, 0);
-  for (int32_t b = 0; b < o.num_batches; ++b) {
-    int32_t lo = b * BS, hi = (b + 1) * BS;
-    batch_entries[b] = (double)(J.h_optr[hi] - J.h_optr[lo]) + (double)(J.h_iptr[hi] - J.h_iptr[lo]);
-    for (int32_t v = lo; v < hi; ++v)
-      if (heavy_vertex(J, v)) heavy_all.push_back(v - lo);
-    heavy_off[b + 1] = (int32_t)heavy_all.size();
-  }
-  if (!heavy_all.empty())
-    SBP_CUDA(cudaMemcpyAsync(J.heavy, heavy_all.data(), 4 * heavy_all.size(),
-                             cudaMemcpyHostToDevice, st));
-  double nnz_now = (double)E;
-  while ((int)J.bev.size() < 4 * o.num_batches + 1) {
-    cudaEvent_t e;
-    SBP_CUDA(cudaEventCreate(&e));
-    J.bev.push_back(e);
-  }
-  while (!optimal) {
-    if (++R.outer_steps > o.max_outer) {
-      R.status = SBP_ERR_INTERNAL;
-      break;
-    }
-    // merge phase (partition.hpp:900-904)
-    SBP_CUDA(cudaEventRecord(J.ev[0], st));
-    R.bytes_merge += 320.0 * nnz_now + 8.0 * N;
-    sbp_status s = merge_step(J, B, B_to_merge, o.seed, seq++, false);
-    if (s != SBP_OK) return s;
-    SBP_CUDA(cudaEventRecord(J.ev[1], st));
-    build_model(J, B, st);
-    SBP_CUDA(cudaEventRecord(J.ev[2], st));
-    const bool dense = is_dense(J, B);
-    if (dense) nnz_now = std::min((double)E, (double)B * B);
-    // nodal phase (partition.hpp:906-935)
-    std::fill(itr_dS.begin(), itr_dS.end(), 0.0);
-    SBP_CUDA(cudaMemsetAsync(J.dsum, 0, sizeof(double) * o.max_nodal_itr, st));
-    SBP_CUDA(cudaMemsetAsync(J.acc, 0, sizeof(long long) * o.max_nodal_itr, st));
-    SBP_CUDA(cudaEventSynchronize(J.ev[2]));
-    SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[0], J.ev[1]));
-    R.ms_merge += ms;
-    SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[1], J.ev[2]));
-    R.ms_rebuild += ms;
-    for (int32_t itr = 0; itr < o.max_nodal_itr; ++itr) {
-      // events: bev[0] sweep start; batch b: bev[4b+1] after the per-block
-      // terms, bev[4b+2] after the nodal kernels, bev[4b+3] after the commit,
-      // bev[4b+4] after the rebuild; read at the sweep's one synchronisation
-      SBP_CUDA(cudaEventRecord(J.bev[0], st));
-      for (int32_t b = 0; b < o.num_batches; ++b) {
-        block_terms_any(J, B, 1, o.seed, seq, st);
-        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 1], st));
-        NodalAux aux = aux_for(J, J.heavy + heavy_off[b], heavy_off[b + 1] - heavy_off[b]);
-        nodal_batch_sample(J.g, J.part, J.m, B, dense, o.seed, seq, b * BS, BS, J.newlab, J.rec,
-                           nullptr, aux, st);
-        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 2], st));
-        if (dense) {
-          // the moved vertices' edges, applied to the dense form before the
-          // labels change (it reads old and new labels)
-          dense_update(J.g, J.part, b * BS, BS, J.newlab, B, J.m, st);
-          nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, &J.m, B,
-                       J.cs, st);
-        } else {
-          nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + itr, J.acc + itr, nullptr,
-                       0, J.cs, st);
-        }
-        ++seq;
-        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 3], st));
-        if (!dense) rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
-        SBP_CUDA(cudaEventRecord(J.bev[4 * b + 4], st));
-        R.nodal_proposals += BS;
-        R.nodal_launches += 1;
-        R.bytes_nodal += 28.0 * BS + 12.0 * batch_entries[b] + 16.0 * nnz_now + 8.0 * B;
-        R.bytes_rebuild += dense ? 12.0 * batch_entries[b] + 8.0 * (double)B * B
-                                 : 4.0 * N + 24.0 * E + 16.0 * nnz_now + 8.0 * B;
-      }
-      block_terms_any(J, B, 0, o.seed, 0, st);
-      mdl_data_sum(J.m, B, J.dataS + itr, st);
-      SBP_CUDA(cudaMemcpyAsync(J.h_scal, J.dsum + itr, 8, cudaMemcpyDeviceToHost, st));
-      SBP_CUDA(cudaMemcpyAsync(J.h_scal + 1, J.dataS + itr, 8, cudaMemcpyDeviceToHost, st));
-      SBP_CUDA(cudaMemcpyAsync(J.h_acc, J.acc + itr, 8, cudaMemcpyDeviceToHost, st));
-      SBP_CUDA(cudaMemcpyAsync(J.h_misc, J.err, 4, cudaMemcpyDeviceToHost, st));
-      SBP_CUDA(cudaMemcpyAsync(J.h_misc + 1, J.m.optr + B, 4, cudaMemcpyDeviceToHost, st));
-      SBP_CUDA(cudaStreamSynchronize(st));
-      SBP_CUDA(cudaGetLastError());
-      if (J.h_misc[0] != 0)
-        return fail(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
-      if (!dense) nnz_now = (double)J.h_misc[1];
-      for (int32_t b = 0; b < o.num_batches; ++b) {
-        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[4 * b], J.bev[4 * b + 3]));
-        R.ms_nodal += ms;
-        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[4 * b + 1], J.bev[4 * b + 2]));
-        R.ms_nodal_kernel += ms;
-        SBP_CUDA(cudaEventElapsedTime(&ms, J.bev[4 * b + 3], J.bev[4 * b + 4]));
-        R.ms_rebuild += ms;
-      }
-      ++R.nodal_itrs;
-      itr_dS[itr] = J.h_scal[0];
-      R.accepted_moves += J.h_acc[0];
-      S = model_S(B, N, E) - J.h_scal[1];
-      if (itr >= o.window - 1) {
-        bool isf = std::isfinite(large.S) && std::isfinite(med.S) && std::isfinite(small.S);
-        double mean = 0.0;
-        for (int32_t i = itr - o.window + 1; i < itr; ++i) mean += itr_dS[i];
-        mean /= (double)(o.window - 1);
-        if (!isf) {
-          if (-mean < (double)o.threshold1 * S) break;
-        } else {
-          if (-mean < (double)o.threshold2 * S) break;
-        }
-      }
-    }
-    if (o.verbose)
-      std::fprintf(stderr, "[sbp] step %d B=%d S=%.6f itrs=%d\n", R.outer_steps, B, S,
-                   R.nodal_itrs);
-    // golden section (prepare_for_partition_next, partition.hpp:80-322)
-    Bracket P;
-    P.B = B;
-    P.B_to_merge = B_to_merge;
-    P.S = S;
-    auto take_slot = [&](Bracket& x) {
-      // the slot of whichever bracket point is being replaced is reused
-      bool used[3] = {false, false, false};
-      for (Bracket* q : {&large, &med, &small})
-        if (q != &x && q->slot >= 0) used[q->slot] = true;
-      for (int i = 0; i < 3; ++i)
-        if (!used[i]) return i;
-      return -1;
-    };
-    if (P.S <= med.S) {
-      if (med.B > P.B) large = med;
-      else small = med;
-      med = P;
-      med.slot = take_slot(med);
-      SBP_CUDA(cudaMemcpyAsync(J.snap[med.slot], J.part, 4 * (size_t)N, cudaMemcpyDeviceToDevice,
-                               st));
-    } else {
-      Bracket& tgt = med.B > P.B ? small : large;
-      tgt = P;
-      tgt.slot = take_slot(tgt);
-      SBP_CUDA(cudaMemcpyAsync(J.snap[tgt.slot], J.part, 4 * (size_t)N, cudaMemcpyDeviceToDevice,
-                               st));
-    }
-    const Bracket* restore = nullptr;
-    if (std::isinf(small.S)) {
-      restore = &med;
-      B_to_merge = (int32_t)((float)med.B * o.reduction_rate);
-      if (B_to_merge == 0) optimal = true;
-    } else if (large.B - small.B == 2) {
-      optimal = true;
-      restore = &med;
-    } else if ((large.B - med.B) >= (med.B - small.B)) {
-      int32_t next_B = med.B + (int32_t)std::round((large.B - med.B) * 0.618);
-      restore = &large;
-      B_to_merge = large.B - next_B;
-    } else {
-      int32_t next_B = small.B + (int32_t)std::round((med.B - small.B) * 0.618);
-      restore = &med;
-      B_to_merge = med.B - next_B;
-    }
-    if (restore->slot < 0) return fail(SBP_ERR_INTERNAL, "bracket point without a snapshot");
-    SBP_CUDA(cudaMemcpyAsync(J.part, J.snap[restore->slot], 4 * (size_t)N,
-                             cudaMemcpyDeviceToDevice, st));
-    B = restore->B;
-    S = restore->S;
-    SBP_CUDA(cudaEventRecord(J.ev[0], st));
-    build_model(J, B, st);
-    SBP_CUDA(cudaEventRecord(J.ev[1], st));
-    SBP_CUDA(cudaEventSynchronize(J.ev[1]));
-    SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[0], J.ev[1]));
-    R.ms_rebuild += ms;
-  }
-  if (labels_out) {
-    SBP_CUDA(cudaMemcpyAsync(labels_out, J.part, 4 * (size_t)N, cudaMemcpyDeviceToHost, st));
-  }
-  SBP_CUDA(cudaEventRecord(J.ev[2], st));
-  SBP_CUDA(cudaStreamSynchronize(st));
-  SBP_CUDA(cudaGetLastError());
-  SBP_CUDA(cudaEventElapsedTime(&ms, J.ev[3], J.ev[2]));
-  R.ms_device = ms;
-  R.kernel_launches = g_launches - launches0;
-  R.B = B;
-  R.S = S;
-  R.ms_total = total.ms();
-  if (rep) *rep = R;
-  return R.status == 0 ? SBP_OK : (sbp_status)R.status;
-}
-
 // A job with the graph uploaded, for the one-shot entry points.
-static int32_t env_dense_max() {
+int32_t env_dense_max() {
   const char* e = std::getenv("SBP_DENSE_MAX");
   return e ? std::atoi(e) : 4096;
 }
@@ -702,6 +450,17 @@ static sbp_status prepare(Job& J, const sbp_graph_csr* g, const int32_t* part, i
   SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, J.st));
   rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
   if (is_dense(J, B)) dense_build(J.g, J.part, B, J.m, J.st);
+  return SBP_OK;
+}
+
+sbp_status check_options(const sbp_options* o) {
+  if (!o) return fail(SBP_ERR_INVALID, "options are NULL");
+  if (o->num_proposals < 1 || o->num_proposals > 32)
+    return fail(SBP_ERR_INVALID, "num_proposals must be in [1, 32]");
+  if (o->num_batches < 1 || o->max_nodal_itr < 1 || o->window < 2 || o->max_outer < 1)
+    return fail(SBP_ERR_INVALID, "bad loop options");
+  if (!(o->reduction_rate > 0.f && o->reduction_rate < 1.f))
+    return fail(SBP_ERR_INVALID, "reduction_rate must be in (0, 1)");
   return SBP_OK;
 }
 
@@ -752,17 +511,6 @@ const char* sbp_status_string(sbp_status s) {
 
 const char* sbp_last_error(void) { return g_last_error.c_str(); }
 
-static sbp_status check_options(const sbp_options* o) {
-  if (!o) return fail(SBP_ERR_INVALID, "options are NULL");
-  if (o->num_proposals < 1 || o->num_proposals > 32)
-    return fail(SBP_ERR_INVALID, "num_proposals must be in [1, 32]");
-  if (o->num_batches < 1 || o->max_nodal_itr < 1 || o->window < 2 || o->max_outer < 1)
-    return fail(SBP_ERR_INVALID, "bad loop options");
-  if (!(o->reduction_rate > 0.f && o->reduction_rate < 1.f))
-    return fail(SBP_ERR_INVALID, "reduction_rate must be in (0, 1)");
-  return SBP_OK;
-}
-
 sbp_status sbp_graph_upload(const sbp_graph_csr* g, int32_t device, sbp_graph_dev** out) {
   if (!out) return fail(SBP_ERR_INVALID, "out is NULL");
   *out = nullptr;
@@ -801,12 +549,11 @@ sbp_status sbp_partition_resident(sbp_graph_dev* gd, const sbp_options* o, int32
     int32_t np = std::max(o->num_proposals, J.np), mi = std::max(o->max_nodal_itr, J.max_itr);
     int32_t dm = std::max(want_dense, J.dense_cap);
     J.release();
-    J.bev.clear();
     s = job_for(J, &gd->shape, dev, np, mi, dm);
     if (s != SBP_OK) return s;
   }
   SBP_CUDA(cudaSetDevice(J.device));
-  return run_partition(J, *o, labels_out, report);
+  return run_solo(J, *o, labels_out, report);
 }
 
 sbp_status sbp_partition(const sbp_graph_csr* g, const sbp_options* o, int32_t* labels_out,
@@ -819,7 +566,7 @@ sbp_status sbp_partition(const sbp_graph_csr* g, const sbp_options* o, int32_t* 
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaStreamSynchronize(J.st));
   double up = t.ms();
-  s = run_partition(J, *o, labels_out, report);
+  s = run_solo(J, *o, labels_out, report);
   if (report) {
     report->ms_h2d = up;
     report->ms_total += up;
@@ -971,45 +718,11 @@ sbp_status sbp_nodal_sweeps(const sbp_graph_csr* g, int32_t* part, int32_t B, ui
   if (s != SBP_OK) return s;
   s = job_upload(J, g);
   if (s != SBP_OK) return s;
-  cudaStream_t st = J.st;
-  SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, st));
-  build_model(J, B, st);
-  const bool dense = is_dense(J, B);
-  const int32_t BS = J.N / num_batches;
-  std::vector<int32_t> heavy_all, heavy_off(num_batches + 1, 0);
-  for (int32_t b = 0; b < num_batches; ++b) {
-    for (int32_t v = b * BS; v < (b + 1) * BS; ++v)
-      if (heavy_vertex(J, v)) heavy_all.push_back(v - b * BS);
-    heavy_off[b + 1] = (int32_t)heavy_all.size();
-  }
-  if (!heavy_all.empty())
-    SBP_CUDA(cudaMemcpyAsync(J.heavy, heavy_all.data(), 4 * heavy_all.size(),
-                             cudaMemcpyHostToDevice, st));
-  SBP_CUDA(cudaMemsetAsync(J.dsum, 0, 8 * (size_t)nb, st));
-  SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8 * (size_t)nb, st));
-  uint32_t seq = seq0;
-  for (int32_t k = 0; k < nb; ++k) {
-    const int32_t b = k % num_batches;
-    block_terms_any(J, B, 1, seed, seq, st);
-    NodalAux aux = aux_for(J, J.heavy + heavy_off[b], heavy_off[b + 1] - heavy_off[b]);
-    nodal_batch_sample(J.g, J.part, J.m, B, dense, seed, seq, b * BS, BS, J.newlab, J.rec, nullptr,
-                       aux, st);
-    if (dense) {
-      dense_update(J.g, J.part, b * BS, BS, J.newlab, B, J.m, st);
-      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, &J.m, B, J.cs, st);
-    } else {
-      nodal_commit(J.part, b * BS, BS, J.newlab, J.rec, J.dsum + k, J.acc + k, nullptr, 0, J.cs, st);
-      rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
-    }
-    ++seq;
-  }
-  SBP_CUDA(cudaStreamSynchronize(st));
-  SBP_CUDA(cudaGetLastError());
-  int32_t err_h = 0;
-  SBP_CUDA(cudaMemcpy(&err_h, J.err, 4, cudaMemcpyDeviceToHost));
-  if (err_h) return fail(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
+  SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, J.st));
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  s = run_sweeps(J, B, seed, seq0, num_batches, sweeps, sums);
+  if (s != SBP_OK) return s;
   SBP_CUDA(cudaMemcpy(part, J.part, 4 * (size_t)J.N, cudaMemcpyDeviceToHost));
-  SBP_CUDA(cudaMemcpy(sums, J.dsum, 8 * (size_t)nb, cudaMemcpyDeviceToHost));
   return SBP_OK;
 }
 

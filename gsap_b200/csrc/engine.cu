@@ -1,0 +1,907 @@
+// The multi-job engine: GSAP's partition() loop (partition.hpp:852-954) for
+// many jobs at once.
+//
+// Each job is a Run: the loop's host state (block count, golden-section
+// bracket, stop test, RNG sequence) as a state machine that is advanced one
+// step per engine tick.  A step is either one merge step or one nodal sweep
+// (num_batches batches plus the MDL), preceded by the device work the last
+// host decision left pending (golden-section snapshot and restore copies,
+// the relabel after merges, the blockmodel build).
+//
+// A tick gathers the device work of every active Run and issues it as
+// multi-job launches: one launch per kernel body covers all jobs that need
+// it (multi.cuh), so a tick costs about the same number of launches for one
+// job as for hundreds.  Argument records, merge maps and heavy-vertex lists
+// go up in two host-to-device copies per tick, every result the host needs
+// (merge choices, sweep sums, MDL terms, final labels) comes back in one
+// device-to-host copy, and the host synchronises once per tick.
+//
+// sbp_partition is a batch of one.  sbp_partition_batch and the server
+// (server.cpp) admit jobs against an HBM budget as earlier jobs finish.
+#include "../../include/sbp.h"
+#include "common.cuh"
+#include "engine.h"
+#include "job.h"
+#include "kernels.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+
+namespace sbp {
+
+// ------------------------------------------------------------------- Run --
+void Run::setup_batches() {
+  const int nb = o.num_batches;
+  BS = J->N / nb;
+  batch_entries.assign(nb, 0.0);
+  heavy_all.clear();
+  heavy_off.assign(nb + 1, 0);
+  for (int32_t b = 0; b < nb; ++b) {
+    int32_t lo = b * BS, hi = (b + 1) * BS;
+    batch_entries[b] = (double)(J->h_optr[hi] - J->h_optr[lo]) +
+                       (double)(J->h_iptr[hi] - J->h_iptr[lo]);
+    for (int32_t v = lo; v < hi; ++v)
+      if (heavy_vertex(*J, v)) heavy_all.push_back(v - lo);
+    heavy_off[b + 1] = (int32_t)heavy_all.size();
+  }
+}
+
+void Run::start_partition() {
+  const int32_t N = J->N;
+  J->dense_eff = std::min(J->dense_cap, std::max(0, o.dense_max));
+  B = N;
+  B_to_merge = (int32_t)((float)B * o.reduction_rate);
+  itr_dS.assign(o.max_nodal_itr, 0.0);
+  nnz_now = (double)J->E;
+  setup_batches();
+  stage = kMerge;
+  init = true;
+  upload_heavy = !heavy_all.empty();
+}
+
+void Run::start_sweeps(int32_t B0, uint32_t seq0, int32_t sweeps) {
+  sweeps_only = true;
+  sweeps_total = sweeps;
+  J->dense_eff = J->dense_cap;
+  B = B0;
+  seq = seq0;
+  nnz_now = (double)J->E;
+  setup_batches();
+  stage = kSweep;
+  init = false;
+  build = true;
+  zero_itr = true;
+  upload_heavy = !heavy_all.empty();
+}
+
+bool Run::dense() const { return B <= J->dense_eff; }
+
+// The stop test and golden-section bookkeeping after a sweep
+// (partition.hpp:920-934, prepare_for_partition_next :80-322).
+void Run::after_sweep(double dsum, double dataS, long long acc) {
+  ++R.nodal_itrs;
+  itr_dS[itr] = dsum;
+  R.accepted_moves += acc;
+  S = model_S(B, J->N, J->E) - dataS;
+  bool stop = false;
+  if (itr >= o.window - 1) {
+    bool isf = std::isfinite(large.S) && std::isfinite(med.S) && std::isfinite(small.S);
+    double mean = 0.0;
+    for (int32_t i = itr - o.window + 1; i < itr; ++i) mean += itr_dS[i];
+    mean /= (double)(o.window - 1);
+    stop = !isf ? (-mean < (double)o.threshold1 * S) : (-mean < (double)o.threshold2 * S);
+  }
+  if (!stop && itr + 1 < o.max_nodal_itr) {
+    ++itr;
+    return;
+  }
+  if (o.verbose)
+    std::fprintf(stderr, "[sbp] step %d B=%d S=%.6f itrs=%d\n", R.outer_steps, B, S,
+                 R.nodal_itrs);
+  Bracket P;
+  P.B = B;
+  P.B_to_merge = B_to_merge;
+  P.S = S;
+  auto take_slot = [&](Bracket& x) {
+    // the slot of whichever bracket point is being replaced is reused
+    bool used[3] = {false, false, false};
+    for (Bracket* q : {&large, &med, &small})
+      if (q != &x && q->slot >= 0) used[q->slot] = true;
+    for (int i = 0; i < 3; ++i)
+      if (!used[i]) return i;
+    return -1;
+  };
+  if (P.S <= med.S) {
+    if (med.B > P.B) large = med;
+    else small = med;
+    med = P;
+    med.slot = take_slot(med);
+    snap_slot = med.slot;
+  } else {
+    Bracket& tgt = med.B > P.B ? small : large;
+    tgt = P;
+    tgt.slot = take_slot(tgt);
+    snap_slot = tgt.slot;
+  }
+  const Bracket* restore = nullptr;
+  bool optimal = false;
+  if (std::isinf(small.S)) {
+    restore = &med;
+    B_to_merge = (int32_t)((float)med.B * o.reduction_rate);
+    if (B_to_merge == 0) optimal = true;
+  } else if (large.B - small.B == 2) {
+    optimal = true;
+    restore = &med;
+  } else if ((large.B - med.B) >= (med.B - small.B)) {
+    int32_t next_B = med.B + (int32_t)std::round((large.B - med.B) * 0.618);
+    restore = &large;
+    B_to_merge = large.B - next_B;
+  } else {
+    int32_t next_B = small.B + (int32_t)std::round((med.B - small.B) * 0.618);
+    restore = &med;
+    B_to_merge = med.B - next_B;
+  }
+  if (snap_slot < 0 || restore->slot < 0) {
+    set_error(SBP_ERR_INTERNAL, "bracket point without a snapshot");
+    return;
+  }
+  restore_slot = restore->slot;
+  B = restore->B;
+  S = restore->S;
+  csr_fresh = false;
+  stage = optimal ? kFinish : kMerge;
+}
+
+void Run::set_error(sbp_status st, const std::string& msg) {
+  if (status == SBP_OK) {
+    status = st;
+    error = msg;
+  }
+  stage = kDone;
+}
+
+// ---------------------------------------------------------------- Engine --
+Engine::~Engine() {
+  if (!st) return;
+  cudaSetDevice(device);
+  cudaStreamSynchronize(st);
+  runs.clear();  // runs belong to the caller
+  cudaFree(up_dev);
+  cudaFree(desc_dev);
+  cudaFree(rd_dev);
+  cudaFreeHost(up_host);
+  cudaFreeHost(desc_host);
+  cudaFreeHost(rd_host);
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  if (ev_first) cudaEventDestroy(ev_first);
+  if (fork) cudaEventDestroy(fork);
+  if (join) cudaEventDestroy(join);
+  if (side) cudaStreamDestroy(side);
+  cudaStreamDestroy(st);
+}
+
+sbp_status Engine::init(int dev) {
+  device = dev;
+  SBP_CUDA(cudaSetDevice(device));
+  SBP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  SBP_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  SBP_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  SBP_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  return SBP_OK;
+}
+
+// Grows a pinned host + device buffer pair to at least `need` bytes (only
+// between ticks, when nothing in flight uses them).
+static sbp_status grow(size_t need, size_t& cap, void*& host, void*& dev) {
+  if (need <= cap) return SBP_OK;
+  size_t n = std::max(need, cap * 2);
+  n = std::max<size_t>(n, 1 << 16);
+  cudaFreeHost(host);
+  cudaFree(dev);
+  host = nullptr;
+  dev = nullptr;
+  cap = 0;
+  SBP_CUDA(cudaMallocHost(&host, n));
+  SBP_CUDA(cudaMalloc(&dev, n));
+  cap = n;
+  return SBP_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+void Engine::ensure_slots(int nb) {
+  if ((int)sw.size() >= nb) return;
+  sw.resize(nb);
+}
+
+void Engine::clear_slots() {
+  for (Slot* s : {&s_iota, &s_heavy, &s_snap, &s_restore, &s_relabel, &s_zero, &m_bt, &m_props,
+                  &m_delta, &e_bt_csr, &e_bt_dense, &e_mdl, &s_gather})
+    s->clear();
+  pre_dense.clear();
+  pre_rebuild.clear();
+  for (auto& b : sw) {
+    for (Slot* s : {&b.bt_csr, &b.bt_dense, &b.heavy_csr, &b.heavy_dense, &b.nodal_csr,
+                    &b.nodal_dense, &b.dupd, &b.commit})
+      s->clear();
+    b.rebuild.clear();
+  }
+}
+
+// Device work of one run for this tick, as records in the slots.
+void Engine::add_run_work(Run& r) {
+  Job& J = *r.J;
+  const int32_t N = J.N;
+  if (r.init) add_iota(s_iota, J.part, N);
+  if (r.upload_heavy)
+    add_copy(s_heavy, J.heavy, up_dev_ptr(r.up_heavy), r.heavy_all.size());
+  if (r.snap_slot >= 0) add_copy(s_snap, J.snap[r.snap_slot], J.part, (size_t)N);
+  if (r.restore_slot >= 0) add_copy(s_restore, J.part, J.snap[r.restore_slot], (size_t)N);
+  if (r.relabel) add_relabel(s_relabel, J.part, N, (const int32_t*)up_dev_ptr(r.up_map));
+  if (r.zero_itr) {
+    const size_t n = r.sweeps_only ? (size_t)r.sweeps_total * r.o.num_batches
+                                   : (size_t)r.o.max_nodal_itr;
+    add_zero(s_zero, J.dsum, 2 * n);
+    add_zero(s_zero, J.acc, 2 * n);
+  }
+  const bool dense = r.dense();
+  if (r.stage == Run::kMerge) {
+    // the merge kernels read the CSR form
+    if (!r.csr_fresh) add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs);
+    add_block_terms(m_bt, J.m, r.B, 0, r.o.seed, 0);
+    add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props);
+    add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS);
+    add_copy(s_gather, rd_dev_ptr(r.rd_off), J.best, (size_t)r.B);
+    add_copy(s_gather, rd_dev_ptr(r.rd_off + align256(4 * (size_t)r.B)), J.best_dS,
+             2 * (size_t)r.B);
+    return;
+  }
+  if (r.stage == Run::kSweep) {
+    if (r.build) {
+      if (dense) add_dense_build(pre_dense, J.g, J.part, r.B, J.m);
+      else add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs);
+    }
+    const int nb = r.o.num_batches;
+    for (int32_t b = 0; b < nb; ++b) {
+      SweepSlots& s = sw[b];
+      const uint32_t seq = r.seq + (uint32_t)b;
+      const int32_t k = r.sweeps_only ? r.itr * nb + b : r.itr;
+      const int32_t lo = b * r.BS;
+      if (dense) add_block_terms_dense(s.bt_dense, J.m, r.B, 1, r.o.seed, seq);
+      else add_block_terms(s.bt_csr, J.m, r.B, 1, r.o.seed, seq);
+      add_nodal(dense ? s.nodal_dense : s.nodal_csr, dense ? s.heavy_dense : s.heavy_csr, dense,
+                J.g, J.part, J.m, r.B, r.o.seed, seq, lo, r.BS, J.newlab, J.rec, nullptr,
+                J.heavy + r.heavy_off[b], r.heavy_off[b + 1] - r.heavy_off[b], J.err);
+      if (dense) {
+        // the moved vertices' edges, applied to the dense form before the
+        // labels change (it reads old and new labels)
+        add_dense_update(s.dupd, J.g, J.part, lo, r.BS, J.newlab, r.B, J.m);
+        add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, J.dsum + k, J.acc + k, &J.m,
+                   r.B, J.cs);
+      } else {
+        add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, J.dsum + k, J.acc + k, nullptr,
+                   0, J.cs);
+        add_rebuild(s.rebuild, J.g, J.part, r.B, J.m, J.rs);
+      }
+    }
+    if (!r.sweeps_only) {
+      if (dense) add_block_terms_dense(e_bt_dense, J.m, r.B, 0, r.o.seed, 0);
+      else add_block_terms(e_bt_csr, J.m, r.B, 0, r.o.seed, 0);
+      add_mdl_sum(e_mdl, J.m, r.B, J.dataS + r.itr);
+      // dsum[itr], dataS[itr], acc[itr], err, nnz: 8 words
+      add_copy(s_gather, rd_dev_ptr(r.rd_off), J.dsum + r.itr, 2);
+      add_copy(s_gather, rd_dev_ptr(r.rd_off + 8), J.dataS + r.itr, 2);
+      add_copy(s_gather, rd_dev_ptr(r.rd_off + 16), J.acc + r.itr, 2);
+    }
+    add_copy(s_gather, rd_dev_ptr(r.rd_off + 24), J.err, 1);
+    add_copy(s_gather, rd_dev_ptr(r.rd_off + 28), J.m.optr + r.B, 1);
+    return;
+  }
+  if (r.stage == Run::kFinish) {
+    add_copy(s_gather, rd_dev_ptr(r.rd_off), J.part, (size_t)N);
+    if (r.sweeps_only) {
+      const size_t n = (size_t)r.sweeps_total * r.o.num_batches;
+      add_copy(s_gather, rd_dev_ptr(r.rd_off + align256(4 * (size_t)N)), J.dsum, 2 * n);
+    }
+  }
+}
+
+// Readback bytes of one run this tick.
+static size_t rd_bytes(const Run& r) {
+  switch (r.stage) {
+    case Run::kMerge:
+      return align256(4 * (size_t)r.B) + align256(8 * (size_t)r.B);
+    case Run::kSweep:
+      return 256;
+    case Run::kFinish:
+      return align256(4 * (size_t)r.J->N) +
+             (r.sweeps_only ? align256(8 * (size_t)r.sweeps_total * r.o.num_batches) : 0);
+    default:
+      return 0;
+  }
+}
+
+sbp_status Engine::launch_slot(Slot& s, size_t off, cudaStream_t stream) {
+  if (s.empty()) return SBP_OK;
+  if (s.mismatch || !s.k) return fail(SBP_ERR_INTERNAL, "engine slot with mixed kernels");
+  if (s.njobs() == 1) {
+    s.k->launch_one(s.recs.data(), s.total(), stream);
+    return SBP_OK;
+  }
+  MultiSpan sp;
+  sp.args = (const char*)desc_dev + off;
+  sp.cta0 = (const int32_t*)((const char*)desc_dev + off + align256(s.recs.size()));
+  sp.njobs = s.njobs();
+  sp.total = s.total();
+  s.k->launch(sp, stream);
+  return SBP_OK;
+}
+
+sbp_status Engine::tick() {
+  SBP_CUDA(cudaSetDevice(device));
+  // runs that reach the outer-step limit stop at their next merge
+  for (Run* r : runs) {
+    if (r->stage != Run::kMerge) continue;
+    if (++r->R.outer_steps > r->o.max_outer) {
+      r->R.status = SBP_ERR_INTERNAL;
+      r->stage = Run::kFinish;
+    }
+  }
+  // pass 1: uploads (maps, heavy lists) and readbacks
+  size_t up = 0, rd = 0;
+  int nb_max = 0;
+  for (Run* r : runs) {
+    if (r->stage == Run::kDone) continue;
+    if (r->relabel) {
+      r->up_map = up;
+      up += align256(4 * r->map.size());
+    }
+    if (r->upload_heavy) {
+      r->up_heavy = up;
+      up += align256(4 * r->heavy_all.size());
+    }
+    r->rd_off = rd;
+    rd += rd_bytes(*r);
+    if (r->stage == Run::kSweep) nb_max = std::max(nb_max, r->o.num_batches);
+  }
+  sbp_status s = grow(up, up_cap, up_host, up_dev);
+  if (s != SBP_OK) return s;
+  s = grow(rd, rd_cap, rd_host, rd_dev);
+  if (s != SBP_OK) return s;
+  // pass 2: records
+  ensure_slots(nb_max);
+  clear_slots();
+  for (Run* r : runs) {
+    if (r->stage == Run::kDone) continue;
+    if (r->relabel)
+      std::memcpy((char*)up_host + r->up_map, r->map.data(), 4 * r->map.size());
+    if (r->upload_heavy)
+      std::memcpy((char*)up_host + r->up_heavy, r->heavy_all.data(), 4 * r->heavy_all.size());
+    add_run_work(*r);
+  }
+  // pass 3: pack the slots' records and offsets
+  std::vector<Slot*> order = {&s_iota, &s_heavy, &s_snap, &s_restore, &s_relabel, &s_zero};
+  for (Slot* x : pre_dense.all()) order.push_back(x);
+  for (Slot* x : pre_rebuild.all()) order.push_back(x);
+  for (Slot* x : {&m_bt, &m_props, &m_delta}) order.push_back(x);
+  for (int b = 0; b < nb_max; ++b) {
+    SweepSlots& w = sw[b];
+    for (Slot* x : {&w.bt_csr, &w.bt_dense, &w.heavy_csr, &w.heavy_dense, &w.nodal_csr,
+                    &w.nodal_dense, &w.dupd, &w.commit})
+      order.push_back(x);
+    for (Slot* x : w.rebuild.all()) order.push_back(x);
+  }
+  for (Slot* x : {&e_bt_csr, &e_bt_dense, &e_mdl, &s_gather}) order.push_back(x);
+  size_t desc = 0;
+  std::vector<size_t> off(order.size(), 0);
+  for (size_t i = 0; i < order.size(); ++i) {
+    if (order[i]->empty()) continue;
+    off[i] = desc;
+    desc += align256(order[i]->recs.size()) + align256(4 * order[i]->cta0.size());
+  }
+  s = grow(desc, desc_cap, desc_host, desc_dev);
+  if (s != SBP_OK) return s;
+  for (size_t i = 0; i < order.size(); ++i) {
+    Slot* x = order[i];
+    if (x->empty()) continue;
+    std::memcpy((char*)desc_host + off[i], x->recs.data(), x->recs.size());
+    std::memcpy((char*)desc_host + off[i] + align256(x->recs.size()), x->cta0.data(),
+                4 * x->cta0.size());
+  }
+  auto slot_off = [&](Slot* x) {
+    for (size_t i = 0; i < order.size(); ++i)
+      if (order[i] == x) return off[i];
+    return (size_t)0;
+  };
+  // pass 4: issue
+  const int n_ev = 4 + 5 * nb_max;
+  while ((int)ev.size() < n_ev) {
+    cudaEvent_t e;
+    SBP_CUDA(cudaEventCreate(&e));
+    ev.push_back(e);
+  }
+  if (!ev_first) {
+    SBP_CUDA(cudaEventCreate(&ev_first));
+    SBP_CUDA(cudaEventRecord(ev_first, st));
+  }
+  for (Run* r : runs)
+    if (r->stage != Run::kDone && !r->ev_begin) {
+      SBP_CUDA(cudaEventCreate(&r->ev_begin));
+      SBP_CUDA(cudaEventRecord(r->ev_begin, st));
+    }
+  SBP_CUDA(cudaEventRecord(ev[0], st));
+  if (up) SBP_CUDA(cudaMemcpyAsync(up_dev, up_host, up, cudaMemcpyHostToDevice, st));
+  if (desc) SBP_CUDA(cudaMemcpyAsync(desc_dev, desc_host, desc, cudaMemcpyHostToDevice, st));
+  size_t i = 0;
+  auto emit_until = [&](Slot* last) -> sbp_status {
+    for (; i < order.size(); ++i) {
+      sbp_status q = launch_slot(*order[i], off[i], st);
+      if (q != SBP_OK) return q;
+      if (order[i] == last) {
+        ++i;
+        break;
+      }
+    }
+    return SBP_OK;
+  };
+  s = emit_until(pre_rebuild.all().back());
+  if (s != SBP_OK) return s;
+  SBP_CUDA(cudaEventRecord(ev[1], st));
+  s = emit_until(&m_delta);
+  if (s != SBP_OK) return s;
+  SBP_CUDA(cudaEventRecord(ev[2], st));
+  for (int b = 0; b < nb_max; ++b) {
+    SweepSlots& w = sw[b];
+    cudaEvent_t* be = &ev[4 + 5 * b];
+    SBP_CUDA(cudaEventRecord(be[0], st));
+    s = emit_until(&w.bt_dense);
+    if (s != SBP_OK) return s;
+    SBP_CUDA(cudaEventRecord(be[1], st));
+    const bool heavy = !w.heavy_csr.empty() || !w.heavy_dense.empty();
+    if (heavy) {
+      // heavy vertices on the side stream, next to the warp kernels
+      SBP_CUDA(cudaEventRecord(fork, st));
+      SBP_CUDA(cudaStreamWaitEvent(side, fork, 0));
+      s = launch_slot(w.heavy_csr, slot_off(&w.heavy_csr), side);
+      if (s != SBP_OK) return s;
+      s = launch_slot(w.heavy_dense, slot_off(&w.heavy_dense), side);
+      if (s != SBP_OK) return s;
+      SBP_CUDA(cudaEventRecord(join, side));
+    }
+    i += 2;  // the heavy slots
+    s = emit_until(&w.nodal_dense);
+    if (s != SBP_OK) return s;
+    if (heavy) SBP_CUDA(cudaStreamWaitEvent(st, join, 0));
+    SBP_CUDA(cudaEventRecord(be[2], st));
+    s = emit_until(&w.commit);
+    if (s != SBP_OK) return s;
+    SBP_CUDA(cudaEventRecord(be[3], st));
+    s = emit_until(w.rebuild.all().back());
+    if (s != SBP_OK) return s;
+    SBP_CUDA(cudaEventRecord(be[4], st));
+  }
+  s = emit_until(&s_gather);
+  if (s != SBP_OK) return s;
+  if (rd) SBP_CUDA(cudaMemcpyAsync(rd_host, rd_dev, rd, cudaMemcpyDeviceToHost, st));
+  SBP_CUDA(cudaEventRecord(ev[3], st));
+  SBP_CUDA(cudaEventSynchronize(ev[3]));
+  SBP_CUDA(cudaGetLastError());
+  ++ticks;
+  // phase times of this tick (shared by the runs that took part)
+  float ms_pre = 0.f, ms_merge = 0.f;
+  SBP_CUDA(cudaEventElapsedTime(&ms_pre, ev[0], ev[1]));
+  SBP_CUDA(cudaEventElapsedTime(&ms_merge, ev[1], ev[2]));
+  std::vector<float> b_nodal(nb_max), b_kernel(nb_max), b_rebuild(nb_max);
+  for (int b = 0; b < nb_max; ++b) {
+    cudaEvent_t* be = &ev[4 + 5 * b];
+    SBP_CUDA(cudaEventElapsedTime(&b_nodal[b], be[0], be[3]));
+    SBP_CUDA(cudaEventElapsedTime(&b_kernel[b], be[1], be[2]));
+    SBP_CUDA(cudaEventElapsedTime(&b_rebuild[b], be[3], be[4]));
+  }
+  // host side of each run
+  for (Run* r : runs) {
+    if (r->stage == Run::kDone) continue;
+    r->R.ms_rebuild += ms_pre;
+    const char* rdp = (const char*)rd_host + r->rd_off;
+    r->init = false;
+    r->upload_heavy = false;
+    r->snap_slot = -1;
+    r->restore_slot = -1;
+    r->relabel = false;
+    r->zero_itr = false;
+    if (r->stage == Run::kMerge) {
+      Job& J = *r->J;
+      r->R.ms_merge += ms_merge;
+      r->R.bytes_merge += 320.0 * r->nnz_now + 8.0 * J.N;
+      const int32_t* best = (const int32_t*)rdp;
+      const double* best_dS = (const double*)(rdp + align256(4 * (size_t)r->B));
+      r->map.resize(r->B);
+      const int32_t nb = apply_merges_host(r->B, r->B_to_merge, best, best_dS, r->map.data());
+      ++r->seq;
+      r->B = nb;
+      r->csr_fresh = false;
+      r->relabel = true;
+      r->build = true;
+      r->zero_itr = true;
+      r->itr = 0;
+      r->stage = Run::kSweep;
+      if (r->dense()) r->nnz_now = std::min((double)J.E, (double)r->B * r->B);
+      continue;
+    }
+    if (r->stage == Run::kSweep) {
+      Job& J = *r->J;
+      const bool dense = r->dense();
+      r->build = false;
+      if (!dense) r->csr_fresh = true;
+      const int nb = r->o.num_batches;
+      for (int b = 0; b < nb; ++b) {
+        r->R.ms_nodal += b_nodal[b];
+        r->R.ms_nodal_kernel += b_kernel[b];
+        r->R.ms_rebuild += b_rebuild[b];
+        r->R.nodal_proposals += r->BS;
+        r->R.nodal_launches += 1;
+        r->R.bytes_nodal += 28.0 * r->BS + 12.0 * r->batch_entries[b] + 16.0 * r->nnz_now +
+                            8.0 * r->B;
+        r->R.bytes_rebuild += dense ? 12.0 * r->batch_entries[b] + 8.0 * (double)r->B * r->B
+                                    : 4.0 * J.N + 24.0 * J.E + 16.0 * r->nnz_now + 8.0 * r->B;
+      }
+      r->seq += (uint32_t)nb;
+      int32_t err = 0, nnz = 0;
+      std::memcpy(&err, rdp + 24, 4);
+      std::memcpy(&nnz, rdp + 28, 4);
+      if (err != 0) {
+        r->set_error(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
+        continue;
+      }
+      if (!dense) r->nnz_now = (double)nnz;
+      if (r->sweeps_only) {
+        if (++r->itr == r->sweeps_total) r->stage = Run::kFinish;
+        continue;
+      }
+      double dsum = 0.0, dataS = 0.0;
+      long long acc = 0;
+      std::memcpy(&dsum, rdp, 8);
+      std::memcpy(&dataS, rdp + 8, 8);
+      std::memcpy(&acc, rdp + 16, 8);
+      r->after_sweep(dsum, dataS, acc);
+      continue;
+    }
+    if (r->stage == Run::kFinish) {
+      if (r->labels_out) std::memcpy(r->labels_out, rdp, 4 * (size_t)r->J->N);
+      if (r->sweeps_only && r->sums_out)
+        std::memcpy(r->sums_out, rdp + align256(4 * (size_t)r->J->N),
+                    8 * (size_t)r->sweeps_total * r->o.num_batches);
+      float ms = 0.f;
+      SBP_CUDA(cudaEventElapsedTime(&ms, r->ev_begin, ev[3]));
+      r->R.ms_device = ms;
+      r->R.B = r->B;
+      r->R.S = r->S;
+      r->stage = Run::kDone;
+      r->finished = true;
+    }
+  }
+  return SBP_OK;
+}
+
+void Engine::reset() {
+  runs.clear();
+  ticks = 0;
+  if (ev_first) cudaEventDestroy(ev_first);
+  ev_first = nullptr;
+}
+
+double Engine::device_ms() {
+  if (!ev_first || ev.size() < 4) return 0.0;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ev_first, ev[3]) != cudaSuccess) return 0.0;
+  return ms;
+}
+
+Run::~Run() {
+  if (ev_begin) cudaEventDestroy(ev_begin);
+}
+
+void HostGraph::assign(const sbp_graph_csr& g) {
+  N = g.N;
+  E = g.E;
+  optr.assign(g.out_ptr, g.out_ptr + N + 1);
+  iptr.assign(g.in_ptr, g.in_ptr + N + 1);
+  oidx.assign(g.out_idx, g.out_idx + E);
+  iidx.assign(g.in_idx, g.in_idx + E);
+  ow.assign(g.out_w, g.out_w + E);
+  iw.assign(g.in_w, g.in_w + E);
+  kdo.assign(g.deg_out, g.deg_out + N);
+  kdi.assign(g.deg_in, g.deg_in + N);
+}
+
+sbp_graph_csr HostGraph::csr() const {
+  sbp_graph_csr g{};
+  g.N = N;
+  g.E = E;
+  g.out_ptr = optr.data();
+  g.out_idx = oidx.data();
+  g.out_w = ow.data();
+  g.in_ptr = iptr.data();
+  g.in_idx = iidx.data();
+  g.in_w = iw.data();
+  g.deg_out = kdo.data();
+  g.deg_in = kdi.data();
+  return g;
+}
+
+// ------------------------------------------------------------- Scheduler --
+sbp_status Scheduler::init(int device, uint64_t hbm_budget, int32_t max_active_jobs) {
+  sbp_status s = eng.init(device);
+  if (s != SBP_OK) return s;
+  // job arenas come from the stream-ordered pool; keep freed memory in it
+  cudaMemPool_t pool;
+  SBP_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t keep = ~0ull;
+  SBP_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  if (hbm_budget == 0) {
+    size_t free_b = 0, total_b = 0;
+    SBP_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    hbm_budget = (uint64_t)(0.9 * (double)free_b);
+  }
+  budget = hbm_budget;
+  max_active = max_active_jobs;
+  return SBP_OK;
+}
+
+static size_t run_bytes(const Run& r) {
+  const sbp_graph_csr& g = *r.graph;
+  return job_bytes(g.N, g.E, r.o.num_proposals, r.o.max_nodal_itr,
+                   std::max(0, std::min(g.N, r.o.dense_max)));
+}
+
+sbp_status Scheduler::admit(std::vector<Run*>& done) {
+  while (queued() > 0) {
+    Run* r = queue[queue_head];
+    if (max_active > 0 && (int32_t)eng.runs.size() >= max_active) break;
+    const double bytes = (double)run_bytes(*r);
+    if (bytes > (double)budget) {
+      ++queue_head;
+      r->set_error(SBP_ERR_BUDGET, "job arena exceeds the HBM budget");
+      done.push_back(r);
+      continue;
+    }
+    if (used + bytes > (double)budget) break;  // waits for running jobs, in order
+    ++queue_head;
+    r->owned.reset(new Job());
+    r->J = r->owned.get();
+    const sbp_graph_csr& g = *r->graph;
+    sbp_status s = job_create(*r->J, eng.device, g.N, g.E, r->o.num_proposals,
+                              r->o.max_nodal_itr, r->o.dense_max, true, eng.st);
+    if (s == SBP_OK) s = job_upload(*r->J, &g);
+    if (s != SBP_OK) {
+      r->set_error(s, sbp_last_error());
+      r->owned.reset();
+      r->J = nullptr;
+      done.push_back(r);
+      continue;
+    }
+    r->admit_bytes = bytes;
+    r->t_admit_ms = now_ms();
+    r->start_partition();
+    eng.runs.push_back(r);
+    used += bytes;
+    peak = std::max(peak, used);
+    max_active_seen = std::max(max_active_seen, (int32_t)eng.runs.size());
+  }
+  if (queue_head > 1024 && queue_head * 2 > queue.size()) {
+    queue.erase(queue.begin(), queue.begin() + (long)queue_head);
+    queue_head = 0;
+  }
+  return SBP_OK;
+}
+
+sbp_status Scheduler::step(std::vector<Run*>& done) {
+  sbp_status s = admit(done);
+  if (s != SBP_OK) return s;
+  if (eng.runs.empty()) return SBP_OK;
+  s = eng.tick();
+  if (s != SBP_OK) return s;
+  std::vector<Run*> keep;
+  keep.reserve(eng.runs.size());
+  for (Run* r : eng.runs) {
+    if (r->stage != Run::kDone) {
+      keep.push_back(r);
+      continue;
+    }
+    r->t_done_ms = now_ms();
+    used -= r->admit_bytes;
+    r->owned.reset();  // arena back to the pool, in stream order
+    r->J = nullptr;
+    done.push_back(r);
+  }
+  eng.runs.swap(keep);
+  return SBP_OK;
+}
+
+Scheduler::~Scheduler() {
+  // active jobs give their arenas back while the engine's stream exists
+  for (Run* r : eng.runs) {
+    r->owned.reset();
+    r->J = nullptr;
+  }
+  eng.runs.clear();
+}
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// Idle engines of one device, reused by single-job calls (streams, events
+// and staging buffers are made once).  They live until the process exits.
+class EnginePool {
+ public:
+  Engine* take(int device, sbp_status* st) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto& v = idle_[device];
+      if (!v.empty()) {
+        Engine* e = v.back();
+        v.pop_back();
+        *st = SBP_OK;
+        return e;
+      }
+    }
+    Engine* e = new Engine();
+    *st = e->init(device);
+    if (*st != SBP_OK) {
+      delete e;
+      return nullptr;
+    }
+    return e;
+  }
+  void give(Engine* e) {
+    e->reset();
+    std::lock_guard<std::mutex> lk(mu_);
+    idle_[e->device].push_back(e);
+  }
+
+ private:
+  std::mutex mu_;
+  std::map<int, std::vector<Engine*>> idle_;
+};
+
+static EnginePool& engine_pool() {
+  static EnginePool* p = new EnginePool();
+  return *p;
+}
+
+// Runs one job to the end on an engine of its own.
+static sbp_status run_one(Job& J, Run& r) {
+  sbp_status s = SBP_OK;
+  Engine* eng = engine_pool().take(J.device, &s);
+  if (!eng) return s;
+  // the job's uploads were issued on its own stream
+  cudaError_t e = cudaStreamSynchronize(J.st);
+  if (e != cudaSuccess) {
+    engine_pool().give(eng);
+    return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
+  }
+  const long long l0 = g_launches;
+  eng->runs.push_back(&r);
+  while (r.stage != Run::kDone) {
+    s = eng->tick();
+    if (s != SBP_OK) break;
+  }
+  eng->runs.clear();
+  // a failed tick leaves the engine's stream in an unknown state: drop it
+  if (s != SBP_OK) return s;
+  engine_pool().give(eng);
+  r.R.kernel_launches = g_launches - l0;
+  return SBP_OK;
+}
+
+sbp_status run_solo(Job& J, const sbp_options& o, int32_t* labels_out, sbp_report* rep) {
+  Timer t;
+  Run r;
+  r.J = &J;
+  r.o = o;
+  r.labels_out = labels_out;
+  r.start_partition();
+  sbp_status s = run_one(J, r);
+  if (s != SBP_OK) return s;
+  r.R.ms_total = t.ms();
+  if (r.status == SBP_OK && r.R.status != 0) r.status = (sbp_status)r.R.status;
+  r.R.status = r.status;
+  if (rep) *rep = r.R;
+  if (r.status != SBP_OK && !r.error.empty()) return fail(r.status, r.error);
+  return r.status;
+}
+
+sbp_status run_sweeps(Job& J, int32_t B, uint64_t seed, uint32_t seq0, int32_t num_batches,
+                      int32_t sweeps, double* sums) {
+  Run r;
+  r.J = &J;
+  sbp_default_options(&r.o);
+  r.o.seed = seed;
+  r.o.num_batches = num_batches;
+  r.sums_out = sums;
+  r.start_sweeps(B, seq0, sweeps);
+  sbp_status s = run_one(J, r);
+  if (s != SBP_OK) return s;
+  if (r.status != SBP_OK) return fail(r.status, r.error);
+  return SBP_OK;
+}
+
+}  // namespace sbp
+
+// ------------------------------------------------------------------ C ABI --
+using namespace sbp;
+
+extern "C" uint64_t sbp_job_bytes(int32_t N, int32_t E, const sbp_options* o) {
+  if (N < 1 || E < 0 || !o) return 0;
+  return job_bytes(N, E, o->num_proposals, o->max_nodal_itr, std::max(0, std::min(N, o->dense_max)));
+}
+
+extern "C" sbp_status sbp_partition_batch(const sbp_graph_csr* graphs, int32_t count,
+                                          const sbp_options* o, const uint64_t* seeds,
+                                          uint64_t hbm_budget, int32_t* const* labels_out,
+                                          sbp_report* reports, sbp_batch_report* batch) {
+  Timer t;
+  if (count < 0 || (count > 0 && (!graphs || !labels_out)))
+    return fail(SBP_ERR_INVALID, "bad batch arguments");
+  sbp_status s = check_options(o);
+  if (s != SBP_OK) return s;
+  for (int32_t i = 0; i < count; ++i) {
+    s = validate_graph(&graphs[i]);
+    if (s != SBP_OK) return fail(s, "graph " + std::to_string(i) + ": " + sbp_last_error());
+    if (!labels_out[i]) return fail(SBP_ERR_INVALID, "labels_out entry is NULL");
+  }
+  Scheduler sch;
+  s = sch.init(resolve_device(o->device), hbm_budget, 0);
+  if (s != SBP_OK) return s;
+  std::vector<std::unique_ptr<Run>> runs(count);
+  for (int32_t i = 0; i < count; ++i) {
+    runs[i].reset(new Run());
+    Run& r = *runs[i];
+    r.graph = &graphs[i];
+    r.o = *o;
+    if (seeds) r.o.seed = seeds[i];
+    r.labels_out = labels_out[i];
+    r.id = i;
+    sch.enqueue(&r);
+  }
+  const long long l0 = g_launches;
+  std::vector<Run*> done;
+  while (!sch.idle()) {
+    s = sch.step(done);
+    if (s != SBP_OK) return s;
+  }
+  sbp_status first = SBP_OK;
+  std::string first_msg;
+  for (int32_t i = 0; i < count; ++i) {
+    Run& r = *runs[i];
+    if (r.status == SBP_OK && r.R.status != 0) r.status = (sbp_status)r.R.status;
+    r.R.status = r.status;
+    r.R.ms_total = r.t_done_ms - r.t_admit_ms;
+    if (reports) reports[i] = r.R;
+    if (r.status != SBP_OK && first == SBP_OK) {
+      first = r.status;
+      first_msg = "graph " + std::to_string(i) + ": " + r.error;
+    }
+  }
+  if (batch) {
+    std::memset(batch, 0, sizeof(*batch));
+    batch->count = count;
+    batch->max_active = sch.max_active_seen;
+    batch->ticks = sch.eng.ticks;
+    batch->kernel_launches = g_launches - l0;
+    batch->ms_device = sch.eng.device_ms();
+    batch->peak_bytes = sch.peak;
+    batch->ms_total = t.ms();
+  }
+  if (first != SBP_OK) return fail(first, first_msg);
+  return SBP_OK;
+}

@@ -1,0 +1,152 @@
+// The multi-job engine (engine.cu): Run is one job's partition() state,
+// Engine advances a set of runs one tick at a time with multi-job launches.
+#pragma once
+
+#include "job.h"
+#include "kernels.h"
+
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace sbp {
+
+// Host clock in milliseconds (steady).
+double now_ms();
+
+// A graph held on the host by the engine (server requests are copied).
+struct HostGraph {
+  int32_t N = 0, E = 0;
+  std::vector<int32_t> optr, oidx, iptr, iidx;
+  std::vector<uint32_t> ow, iw, kdo, kdi;
+  void assign(const sbp_graph_csr& g);
+  sbp_graph_csr csr() const;
+};
+
+struct Run {
+  Job* J = nullptr;
+  const sbp_graph_csr* graph = nullptr;  // host graph uploaded at admission
+  HostGraph graph_copy;                  // server requests: the copied graph
+  sbp_graph_csr graph_view{};
+  std::unique_ptr<Job> owned;  // jobs the engine admitted itself
+  sbp_options o{};
+  int32_t* labels_out = nullptr;  // host labels, written when the run finishes
+  double* sums_out = nullptr;     // sweeps-only runs: per-batch dS sums
+  sbp_report R{};
+  sbp_status status = SBP_OK;
+  std::string error;
+  enum Stage { kMerge, kSweep, kFinish, kDone } stage = kMerge;
+  bool finished = false;
+  bool sweeps_only = false;
+  int32_t sweeps_total = 0;
+  // loop state (partition.hpp:852-954)
+  int32_t B = 0, B_to_merge = 0, BS = 0, itr = 0;
+  uint32_t seq = 0;
+  Bracket large, med, small;
+  double S = 0.0;
+  std::vector<double> itr_dS;
+  std::vector<int32_t> heavy_all, heavy_off;
+  std::vector<double> batch_entries;
+  double nnz_now = 0.0;
+  // device work left pending by the last host decision
+  bool init = false, upload_heavy = false, relabel = false, build = false, zero_itr = false;
+  bool csr_fresh = false;
+  int snap_slot = -1, restore_slot = -1;
+  std::vector<int32_t> map;  // merge map, uploaded for the relabel
+  // this tick's offsets in the upload and readback buffers
+  size_t up_map = 0, up_heavy = 0, rd_off = 0;
+  cudaEvent_t ev_begin = nullptr;
+  // scheduler / server bookkeeping
+  double admit_bytes = 0.0;
+  long long id = -1;
+  double t_submit_ms = 0.0, t_admit_ms = 0.0, t_done_ms = 0.0;
+  std::vector<int32_t> labels_store;
+
+  Run() = default;
+  Run(const Run&) = delete;
+  Run& operator=(const Run&) = delete;
+  ~Run();
+
+  void setup_batches();
+  void start_partition();
+  void start_sweeps(int32_t B0, uint32_t seq0, int32_t sweeps);
+  bool dense() const;
+  void after_sweep(double dsum, double dataS, long long acc);
+  void set_error(sbp_status st, const std::string& msg);
+};
+
+// The launches of one nodal batch position across runs.
+struct SweepSlots {
+  Slot bt_csr, bt_dense, heavy_csr, heavy_dense, nodal_csr, nodal_dense, dupd, commit;
+  RebuildSlots rebuild;
+};
+
+class Engine {
+ public:
+  int device = 0;
+  cudaStream_t st = nullptr, side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  std::vector<Run*> runs;
+  long long ticks = 0;
+  cudaEvent_t ev_first = nullptr;  // recorded at the first tick
+
+  Engine() = default;
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+  ~Engine();
+  sbp_status init(int dev);
+  // One step of every run that is not done; synchronises once.
+  sbp_status tick();
+  // CUDA-event time from the first tick to the end of the last one.
+  double device_ms();
+  // Forgets its runs and tick count (an idle engine, ready for reuse).
+  void reset();
+
+ private:
+  Slot s_iota, s_heavy, s_snap, s_restore, s_relabel, s_zero;
+  DenseBuildSlots pre_dense;
+  RebuildSlots pre_rebuild;
+  Slot m_bt, m_props, m_delta;
+  std::vector<SweepSlots> sw;
+  Slot e_bt_csr, e_bt_dense, e_mdl, s_gather;
+  std::vector<cudaEvent_t> ev;
+  void *up_host = nullptr, *up_dev = nullptr, *desc_host = nullptr, *desc_dev = nullptr;
+  void *rd_host = nullptr, *rd_dev = nullptr;
+  size_t up_cap = 0, desc_cap = 0, rd_cap = 0;
+
+  void* up_dev_ptr(size_t off) { return (char*)up_dev + off; }
+  void* rd_dev_ptr(size_t off) { return (char*)rd_dev + off; }
+  void ensure_slots(int nb);
+  void clear_slots();
+  void add_run_work(Run& r);
+  sbp_status launch_slot(Slot& s, size_t off, cudaStream_t stream);
+};
+
+// Admission against an HBM budget in front of an engine (batched calls and
+// the server): queued runs join the engine in order while their arenas fit.
+class Scheduler {
+ public:
+  Engine eng;
+  uint64_t budget = 0;
+  int32_t max_active = 0;
+  std::vector<Run*> queue;  // waiting, in arrival order (front = next)
+  size_t queue_head = 0;
+  double used = 0.0, peak = 0.0;
+  int32_t max_active_seen = 0;
+
+  Scheduler() = default;
+  Scheduler(const Scheduler&) = delete;
+  Scheduler& operator=(const Scheduler&) = delete;
+  ~Scheduler();
+  sbp_status init(int device, uint64_t hbm_budget, int32_t max_active_jobs);
+  void enqueue(Run* r) { queue.push_back(r); }
+  size_t queued() const { return queue.size() - queue_head; }
+  bool idle() const { return queued() == 0 && eng.runs.empty(); }
+  // Admits what fits, runs one tick, hands back the runs that ended.
+  sbp_status step(std::vector<Run*>& done);
+
+ private:
+  sbp_status admit(std::vector<Run*>& done);
+};
+
+}  // namespace sbp

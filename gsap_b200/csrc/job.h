@@ -1,0 +1,119 @@
+// One partition job's device state and the host helpers shared by the
+// one-shot entry points (driver.cu) and the multi-job engine (engine.cu).
+#pragma once
+
+#include "../../include/sbp.h"
+#include "kernels.h"
+
+#include <chrono>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace sbp {
+
+sbp_status fail(sbp_status st, const std::string& msg);
+
+#define SBP_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e__ = (call);                                                           \
+    if (e__ != cudaSuccess)                                                             \
+      return fail(SBP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, off = 0;
+  template <typename T>
+  T* take(size_t n) {
+    size_t bytes = ((n * sizeof(T)) + 255) & ~size_t(255);
+    if (off + bytes > cap) return nullptr;
+    T* p = (T*)(base + off);
+    off += bytes;
+    return p;
+  }
+};
+
+// Everything one partition job keeps in HBM.  A full job owns two streams
+// (the one-shot entry points launch on them); a lean job (admitted by the
+// engine) has only its arena, from the stream-ordered pool, and works on the
+// engine's stream.
+struct Job {
+  int device = 0;
+  bool lean = false;
+  cudaStream_t st = nullptr;
+  cudaStream_t pool_stream = nullptr;  // arena from the stream-ordered allocator
+  int32_t N = 0, E = 0, np = 10, max_itr = 100;
+  void* mem = nullptr;
+  size_t mem_bytes = 0;
+  DevGraph g;
+  DevBM m;
+  RebuildScratch rs;
+  int32_t *part = nullptr, *newlab = nullptr, *props = nullptr, *best = nullptr, *map = nullptr;
+  int32_t* snap[3] = {nullptr, nullptr, nullptr};
+  double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
+  int32_t* heavy = nullptr;     // batch indices of the CTA-per-vertex kernel
+  int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
+  CommitScratch cs;
+  int32_t dense_cap = 0;        // largest B the dense arrays can hold
+  int32_t dense_eff = 0;        // largest B kept in dense form in this run
+  cudaStream_t side = nullptr;  // heavy vertices run here, next to the warp kernel
+  cudaEvent_t fork = nullptr, join = nullptr;
+  double* dsum = nullptr;       // per nodal iteration (or batch): sum of recorded dS
+  double* dataS = nullptr;      // per nodal iteration: MDL data term
+  long long* acc = nullptr;     // per nodal iteration (or batch): applied moves
+  // pinned host mirrors (the one-shot merge step)
+  int32_t* h_best = nullptr;
+  double* h_best_dS = nullptr;
+  int32_t* h_map = nullptr;
+  std::vector<int32_t> h_optr, h_iptr;  // host copies of the graph's row pointers
+
+  Job() = default;
+  Job(const Job&) = delete;
+  Job& operator=(const Job&) = delete;
+  ~Job() { release(); }
+  void release();
+};
+
+sbp_status validate_graph(const sbp_graph_csr* g);
+sbp_status validate_part(const int32_t* part, int32_t N, int32_t B);
+int resolve_device(int32_t d);
+// Device arena bytes of a job (the engine's HBM admission test uses it).
+size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t dense_cap);
+sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int32_t max_itr,
+                      int32_t dense_max, bool lean = false, cudaStream_t engine_stream = nullptr);
+// Copies the graph to the job's arena (on J.st) and keeps host row pointers.
+sbp_status job_upload(Job& J, const sbp_graph_csr* h);
+// The process-wide x log2 x table of a device (filled once).
+sbp_status device_xlx_table(int device, const double** out);
+int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
+                          const double* best_dS, int32_t* map_out);
+double model_S(int32_t B, int32_t N, int32_t E);
+bool heavy_vertex(const Job& J, int32_t v);
+sbp_status check_options(const sbp_options* o);
+
+struct Timer {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+        .count();
+  }
+};
+
+struct Bracket {
+  int32_t B = 0;
+  int32_t B_to_merge = 0;
+  double S = std::numeric_limits<double>::infinity();
+  int slot = -1;  // snapshot buffer holding its labels
+};
+
+// partition() of one job through the engine (engine.cu); the job holds the
+// uploaded graph.
+sbp_status run_solo(Job& J, const sbp_options& o, int32_t* labels_out, sbp_report* rep);
+// sbp_nodal_sweeps through the engine: `sweeps` sweeps at a fixed B from the
+// job's current labels, per-batch dS sums into sums[].
+sbp_status run_sweeps(Job& J, int32_t B, uint64_t seed, uint32_t seq0, int32_t num_batches,
+                      int32_t sweeps, double* sums);
+
+}  // namespace sbp

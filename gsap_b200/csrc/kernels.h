@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstring>
+#include <vector>
+
 namespace sbp {
 
 // Kernels launched by this thread through the launchers below (the bench's
@@ -65,6 +68,88 @@ struct RebuildScratch {
   int32_t* tile = nullptr;       // scan tile sums (capacity >= 2 * tiles)
   int32_t tile_cap = 0;
 };
+
+// ------------------------------------------------------ multi-job launches --
+// One launch of a kernel body over many jobs: `args` holds njobs argument
+// records back to back, job j owns virtual blocks [cta0[j], cta0[j+1]).
+struct MultiSpan {
+  const void* args = nullptr;
+  const int32_t* cta0 = nullptr;
+  int32_t njobs = 0, total = 0;
+};
+
+struct MultiKernel {
+  size_t rec_bytes;
+  void (*launch)(const MultiSpan&, cudaStream_t);
+  void (*launch_one)(const void* rec, int32_t vctas, cudaStream_t);
+  const char* name;
+};
+
+// A multi-job launch being assembled on the host: records and offsets.
+struct Slot {
+  const MultiKernel* k = nullptr;
+  bool mismatch = false;  // records of two different kernels were added
+  std::vector<unsigned char> recs;
+  std::vector<int32_t> cta0 = std::vector<int32_t>(1, 0);
+  bool empty() const { return cta0.size() <= 1; }
+  int32_t njobs() const { return (int32_t)cta0.size() - 1; }
+  int32_t total() const { return cta0.back(); }
+  void clear() {
+    recs.clear();
+    cta0.assign(1, 0);
+  }
+};
+
+inline Slot& slot_bind(Slot& s, const MultiKernel& k) {
+  if (s.k && s.k != &k) s.mismatch = true;
+  s.k = &k;
+  return s;
+}
+
+// The launches of a blockmodel rebuild, in order.
+struct RebuildSlots {
+  Slot zero, count, scan1[3], scatter, rows_small, rows_big, scan2[3], compact;
+  void clear();
+  std::vector<Slot*> all();
+};
+
+// The launches of a dense-form build, in order.
+struct DenseBuildSlots {
+  Slot zero, edges, degrees, logs;
+  void clear();
+  std::vector<Slot*> all();
+};
+
+// Record builders: each adds one job's launch record(s) to the slot(s), with
+// a virtual grid that depends on that job's sizes only.
+void add_rebuild(RebuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
+                 RebuildScratch& rs);
+void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B,
+                     DevBM& m);
+void add_dense_update(Slot& s, const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
+                      const int32_t* newlab, int32_t B, DevBM& m);
+void add_block_terms(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq);
+void add_block_terms_dense(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed,
+                           uint32_t seq);
+void add_mdl_sum(Slot& s, const DevBM& m, int32_t B, double* out);
+void add_zero(Slot& s, void* p, size_t words);
+void add_copy(Slot& s, void* dst, const void* src, size_t words);
+void add_iota(Slot& s, int32_t* p, int32_t n);
+// Nodal batch of one job: the warp kernel's record goes to `warp`, the
+// CTA-per-vertex kernel's (heavy vertices) to `heavy`.  Use separate slots
+// for dense and CSR jobs.
+void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int32_t* part,
+               const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
+               int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
+               int32_t nheavy, int32_t* err);
+void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
+                const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
+                int32_t B, const CommitScratch& cs);
+void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
+                     int32_t* props);
+void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
+                     double* dS, int32_t* best, double* best_dS);
+void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map);
 
 // Opt-in shared-memory sizes; call once per device before the first launch.
 cudaError_t init_kernel_attributes();

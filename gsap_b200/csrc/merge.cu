@@ -13,6 +13,7 @@
 // find_best_warp, ties going to the lane further up.  FP64 throughout.
 #include "common.cuh"
 #include "kernels.h"
+#include "multi.cuh"
 
 #include <cfloat>
 
@@ -57,8 +58,15 @@ __device__ __forceinline__ int col_at(const MergeArgs& a, int b, int k) {
 }
 
 // choose_neighbors + propose_blocks (kernels.hpp:726-856) for one proposal.
-__global__ void merge_props_kernel(MergeArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+struct MergePropsBody {
+  using Args = MergeArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int);
+};
+
+__device__ void MergePropsBody::run(const MergeArgs& a, int vb, int) {
+  long long t = (long long)vb * kThreads + threadIdx.x;
   if (t >= (long long)a.B * a.np) return;
   int r = (int)(t / a.np);
   P4 x = draw(a.seed, kRngMerge, a.seq, (uint32_t)t);
@@ -160,9 +168,13 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) 
 
 constexpr int kMergeWarps = 8;
 
-__global__ void __launch_bounds__(kMergeWarps * 32) merge_delta_kernel(MergeArgs a) {
+struct MergeDeltaBody {
+  using Args = MergeArgs;
+  static constexpr int kThreads = kMergeWarps * 32, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int r = blockIdx.x * kMergeWarps + wid; r < a.B; r += gridDim.x * kMergeWarps) {
+  for (int r = vb * kMergeWarps + wid; r < a.B; r += vg * kMergeWarps) {
     double mine = DBL_MAX;
     int who = 0;
     for (int k = 0; k < a.np; ++k) {
@@ -188,12 +200,30 @@ __global__ void __launch_bounds__(kMergeWarps * 32) merge_delta_kernel(MergeArgs
       a.best_dS[r] = mine;
     }
   }
-}
+  }
+};
 
-__global__ void relabel_kernel(int32_t* part, int32_t N, const int32_t* __restrict__ map) {
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v < N) part[v] = map[part[v]];
-}
+struct RelabelArgs {
+  int32_t* part;
+  const int32_t* map;
+  int32_t N, pad;
+};
+
+struct RelabelBody {
+  using Args = RelabelArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int) {
+    int v = vb * kThreads + threadIdx.x;
+    if (v < a.N) a.part[v] = __ldg(a.map + a.part[v]);
+  }
+};
+
+int32_t vg_merge_delta(int32_t B) { return std::min(ceil_div(B, kMergeWarps), 148 * 32); }
+
+const MultiKernel kmMergeProps = multi_kernel_desc<MergePropsBody>("merge_props");
+const MultiKernel kmMergeDelta = multi_kernel_desc<MergeDeltaBody>("merge_delta");
+const MultiKernel kmRelabel = multi_kernel_desc<RelabelBody>("relabel");
 
 MergeArgs make_args(const DevBM& m, int32_t B, int32_t np) {
   MergeArgs a{};
@@ -216,10 +246,7 @@ void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint3
   a.seq = seq;
   a.props = props;
   long long n = (long long)B * np;
-  if (n > 0) {
-    ++g_launches;
-    merge_props_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(a);
-  }
+  if (n > 0) launch_single<MergePropsBody>(a, ceil_div(n, 256), st);
 }
 
 void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
@@ -229,19 +256,36 @@ void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, do
   a.dS = dS;
   a.best = best;
   a.best_dS = best_dS;
-  int g = (B + kMergeWarps - 1) / kMergeWarps;
-  if (g > 148 * 32) g = 148 * 32;
-  if (B > 0) {
-    ++g_launches;
-    merge_delta_kernel<<<g, kMergeWarps * 32, 0, st>>>(a);
-  }
+  if (B > 0) launch_single<MergeDeltaBody>(a, vg_merge_delta(B), st);
 }
 
 void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st) {
-  if (N > 0) {
-    ++g_launches;
-    relabel_kernel<<<(N + 255) / 256, 256, 0, st>>>(part, N, map);
-  }
+  RelabelArgs a{part, map, N, 0};
+  if (N > 0) launch_single<RelabelBody>(a, ceil_div(N, 256), st);
+}
+
+void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
+                     int32_t* props) {
+  MergeArgs a = make_args(m, B, np);
+  a.seed = seed;
+  a.seq = seq;
+  a.props = props;
+  slot_push(slot_bind(s, kmMergeProps), a, ceil_div((long long)B * np, 256));
+}
+
+void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
+                     double* dS, int32_t* best, double* best_dS) {
+  MergeArgs a = make_args(m, B, np);
+  a.props_in = props;
+  a.dS = dS;
+  a.best = best;
+  a.best_dS = best_dS;
+  slot_push(slot_bind(s, kmMergeDelta), a, B > 0 ? vg_merge_delta(B) : 0);
+}
+
+void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map) {
+  RelabelArgs a{part, map, N, 0};
+  slot_push(slot_bind(s, kmRelabel), a, ceil_div(N, 256));
 }
 
 }  // namespace sbp

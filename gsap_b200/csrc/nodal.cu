@@ -32,6 +32,7 @@
 // All entropy arithmetic is FP64.
 #include "common.cuh"
 #include "kernels.h"
+#include "multi.cuh"
 
 namespace sbp {
 
@@ -572,12 +573,16 @@ __device__ __forceinline__ bool is_heavy(int no, int ni) {
 }
 
 template <bool GIVEN, bool DENSE>
-__global__ void __launch_bounds__(kNodalWarps * 32, 3) nodal_kernel(NodalArgs a) {
+struct NodalBody {
+  using Args = NodalArgs;
+  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = 3;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
   __shared__ unsigned long long s_ko[kNodalWarps][kWarpList], s_ki[kNodalWarps][kWarpList];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int nw = gridDim.x * kNodalWarps;
+  const int nw = vg * kNodalWarps;
   Group<32> grp{nullptr};
-  for (int i = blockIdx.x * kNodalWarps + wid; i < a.count; i += nw) {
+  for (int i = vb * kNodalWarps + wid; i < a.count; i += nw) {
     const int vv = GIVEN ? a.verts[i] : a.lo + i;
     const int32_t o0 = a.optr[vv], no = a.optr[vv + 1] - o0;
     const int32_t i0 = a.iptr[vv], ni = a.iptr[vv + 1] - i0;
@@ -598,13 +603,18 @@ __global__ void __launch_bounds__(kNodalWarps * 32, 3) nodal_kernel(NodalArgs a)
     if (lane == 0) write_result(a, GIVEN, i, r, s, d);
     __syncwarp();
   }
-}
+  }
+};
 
 // Vertices with more than kWarpList entries in a direction: one CTA each,
 // lists sorted in shared memory up to kHeavyList entries, longer ones
 // through the hashed passes.
 template <bool GIVEN, bool DENSE>
-__global__ void __launch_bounds__(kHeavyThreads, 2) nodal_heavy_kernel(NodalArgs a) {
+struct NodalHeavyBody {
+  using Args = NodalArgs;
+  static constexpr int kThreads = kHeavyThreads, kMinBlocks = 2;
+  static constexpr size_t kSmem = kHeavySmem;
+  static __device__ void run(const Args& a, int vb, int vg) {
   extern __shared__ unsigned long long hsm[];
   __shared__ double red[kHeavyThreads / 32];
   __shared__ int flag, sh_v, sh_s;
@@ -612,7 +622,7 @@ __global__ void __launch_bounds__(kHeavyThreads, 2) nodal_heavy_kernel(NodalArgs
   unsigned long long* ko = hsm;
   unsigned long long* ki = hsm + kHeavyList;
   HashTab ht{(int32_t*)hsm, (uint32_t*)hsm + kHashSlots, (int32_t*)hsm + 2 * kHashSlots};
-  for (int h = blockIdx.x; h < a.nheavy; h += gridDim.x) {
+  for (int h = vb; h < a.nheavy; h += vg) {
     const int i = a.heavy[h];
     if (threadIdx.x < 32) {
       int v, s;
@@ -641,7 +651,8 @@ __global__ void __launch_bounds__(kHeavyThreads, 2) nodal_heavy_kernel(NodalArgs
     if (threadIdx.x == 0) write_result(a, GIVEN, i, r, s, d);
     __syncthreads();
   }
-}
+  }
+};
 
 // Applies the batch's labels and sums its recorded dS.  Each CTA sums a fixed
 // slice in a fixed order into its own partial; the last CTA to finish (a
@@ -650,59 +661,103 @@ __global__ void __launch_bounds__(kHeavyThreads, 2) nodal_heavy_kernel(NodalArgs
 // the block degrees that dense_update changed.
 constexpr int kCommitThreads = 512;
 
-__global__ void __launch_bounds__(kCommitThreads) commit_kernel(
-    int32_t* part, int32_t lo, int32_t count, const int32_t* __restrict__ newlab,
-    const double* __restrict__ rec, double* slot_sum, long long* slot_acc, int32_t B,
-    const uint32_t* __restrict__ d_out, const uint32_t* __restrict__ d_in, double* ld_out,
-    double* ld_in, double* part_sum, long long* part_cnt, unsigned* ticket) {
-  __shared__ double sh[kCommitThreads];
-  __shared__ long long shc[kCommitThreads];
-  __shared__ bool last;
-  const int tid = threadIdx.x;
-  double s = 0.0;
-  long long c = 0;
-  for (int i = blockIdx.x * kCommitThreads + tid; i < count; i += gridDim.x * kCommitThreads) {
-    int32_t nl = newlab[i];
-    if (part[lo + i] != nl) {
-      part[lo + i] = nl;
-      ++c;
+struct CommitArgs {
+  int32_t* part;
+  const int32_t* newlab;
+  const double* rec;
+  double* slot_sum;
+  long long* slot_acc;
+  const uint32_t *d_out, *d_in;  // dense mode: refresh ld_out / ld_in
+  double *ld_out, *ld_in;
+  double* part_sum;
+  long long* part_cnt;
+  unsigned* ticket;
+  int32_t lo, count, B, pad;
+};
+
+struct CommitBody {
+  using Args = CommitArgs;
+  static constexpr int kThreads = kCommitThreads, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    __shared__ double sh[kCommitThreads];
+    __shared__ long long shc[kCommitThreads];
+    __shared__ bool last;
+    const int tid = threadIdx.x;
+    double s = 0.0;
+    long long c = 0;
+    for (int i = vb * kCommitThreads + tid; i < a.count; i += vg * kCommitThreads) {
+      int32_t nl = a.newlab[i];
+      if (a.part[a.lo + i] != nl) {
+        a.part[a.lo + i] = nl;
+        ++c;
+      }
+      s += a.rec[i];
     }
-    s += rec[i];
-  }
-  if (ld_out)
-    for (int b = blockIdx.x * kCommitThreads + tid; b < B; b += gridDim.x * kCommitThreads) {
-      ld_out[b] = log2((double)d_out[b]);
-      ld_in[b] = log2((double)d_in[b]);
+    if (a.ld_out)
+      for (int b = vb * kCommitThreads + tid; b < a.B; b += vg * kCommitThreads) {
+        a.ld_out[b] = log2((double)a.d_out[b]);
+        a.ld_in[b] = log2((double)a.d_in[b]);
+      }
+    sh[tid] = s;
+    shc[tid] = c;
+    __syncthreads();
+    for (int o = kCommitThreads / 2; o > 0; o >>= 1) {
+      if (tid < o) {
+        sh[tid] += sh[tid + o];
+        shc[tid] += shc[tid + o];
+      }
+      __syncthreads();
     }
-  sh[tid] = s;
-  shc[tid] = c;
-  __syncthreads();
-  for (int o = kCommitThreads / 2; o > 0; o >>= 1) {
-    if (tid < o) {
-      sh[tid] += sh[tid + o];
-      shc[tid] += shc[tid + o];
+    if (tid == 0) {
+      a.part_sum[vb] = sh[0];
+      a.part_cnt[vb] = shc[0];
+      __threadfence();
+      last = atomicAdd(a.ticket, 1u) == (unsigned)vg - 1u;
     }
     __syncthreads();
-  }
-  if (tid == 0) {
-    part_sum[blockIdx.x] = sh[0];
-    part_cnt[blockIdx.x] = shc[0];
-    __threadfence();
-    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last && tid == 0) {
-    __threadfence();
-    double t = 0.0;
-    long long n = 0;
-    for (int k = 0; k < (int)gridDim.x; ++k) {
-      t += ((volatile double*)part_sum)[k];
-      n += ((volatile long long*)part_cnt)[k];
+    if (last && tid == 0) {
+      __threadfence();
+      double t = 0.0;
+      long long n = 0;
+      for (int k = 0; k < vg; ++k) {
+        t += ((volatile double*)a.part_sum)[k];
+        n += ((volatile long long*)a.part_cnt)[k];
+      }
+      *a.slot_sum += t;
+      *a.slot_acc += n;
+      *a.ticket = 0u;
     }
-    *slot_sum += t;
-    *slot_acc += n;
-    *ticket = 0u;
   }
+};
+
+// CTAs of one commit: a function of the batch size only.
+int32_t vg_commit(int32_t count) {
+  return std::max(1, std::min(kCommitCtas, ceil_div(count, kCommitThreads * 4)));
+}
+
+CommitArgs commit_args(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
+                       const double* rec, double* slot_sum, long long* slot_acc,
+                       const DevBM* dense_m, int32_t B, const CommitScratch& cs) {
+  CommitArgs a{};
+  a.part = part;
+  a.newlab = newlab;
+  a.rec = rec;
+  a.slot_sum = slot_sum;
+  a.slot_acc = slot_acc;
+  if (dense_m) {
+    a.d_out = dense_m->d_out;
+    a.d_in = dense_m->d_in;
+    a.ld_out = dense_m->ld_out;
+    a.ld_in = dense_m->ld_in;
+    a.B = B;
+  }
+  a.part_sum = cs.part_sum;
+  a.part_cnt = cs.part_cnt;
+  a.ticket = cs.ticket;
+  a.lo = lo;
+  a.count = count;
+  return a;
 }
 
 NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
@@ -735,15 +790,19 @@ void launch_pair(const NodalArgs& a, const NodalAux& aux, cudaStream_t st) {
     // heavy vertices on the side stream, next to the warp kernel
     cudaEventRecord(aux.fork, st);
     cudaStreamWaitEvent(aux.side, aux.fork, 0);
-    ++g_launches;
-    int grid = a.nheavy < 2 * 148 ? a.nheavy : 2 * 148;
-    nodal_heavy_kernel<GIVEN, DENSE><<<grid, kHeavyThreads, kHeavySmem, aux.side>>>(a);
+    launch_single<NodalHeavyBody<GIVEN, DENSE>>(a, std::min(a.nheavy, 2 * 148), aux.side);
     cudaEventRecord(aux.join, aux.side);
   }
-  ++g_launches;
-  nodal_kernel<GIVEN, DENSE><<<nodal_grid(a.count), kNodalWarps * 32, 0, st>>>(a);
+  launch_single<NodalBody<GIVEN, DENSE>>(a, nodal_grid(a.count), st);
   if (a.nheavy > 0) cudaStreamWaitEvent(st, aux.join, 0);
 }
+
+const MultiKernel kmNodal[2] = {multi_kernel_desc<NodalBody<false, false>>("nodal_csr"),
+                                multi_kernel_desc<NodalBody<false, true>>("nodal_dense")};
+const MultiKernel kmNodalHeavy[2] = {
+    multi_kernel_desc<NodalHeavyBody<false, false>>("nodal_heavy_csr"),
+    multi_kernel_desc<NodalHeavyBody<false, true>>("nodal_heavy_dense")};
+const MultiKernel kmCommit = multi_kernel_desc<CommitBody>("commit");
 
 }  // namespace
 
@@ -754,10 +813,12 @@ cudaError_t init_nodal_attributes() {
                                          (int)kHeavySmem);
     if (x != cudaSuccess) e = x;
   };
-  set((const void*)nodal_heavy_kernel<false, false>);
-  set((const void*)nodal_heavy_kernel<false, true>);
-  set((const void*)nodal_heavy_kernel<true, false>);
-  set((const void*)nodal_heavy_kernel<true, true>);
+  set((const void*)single_kernel<NodalHeavyBody<false, false>>);
+  set((const void*)single_kernel<NodalHeavyBody<false, true>>);
+  set((const void*)single_kernel<NodalHeavyBody<true, false>>);
+  set((const void*)single_kernel<NodalHeavyBody<true, true>>);
+  set((const void*)multi_kernel<NodalHeavyBody<false, false>>);
+  set((const void*)multi_kernel<NodalHeavyBody<false, true>>);
   return e;
 }
 
@@ -796,12 +857,38 @@ void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, i
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                   const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
                   int32_t B, const CommitScratch& cs, cudaStream_t st) {
-  ++g_launches;
-  commit_kernel<<<kCommitCtas, kCommitThreads, 0, st>>>(
-      part, lo, count, newlab, rec, slot_sum, slot_acc, dense_m ? B : 0,
-      dense_m ? dense_m->d_out : nullptr, dense_m ? dense_m->d_in : nullptr,
-      dense_m ? dense_m->ld_out : nullptr, dense_m ? dense_m->ld_in : nullptr, cs.part_sum,
-      cs.part_cnt, cs.ticket);
+  launch_single<CommitBody>(
+      commit_args(part, lo, count, newlab, rec, slot_sum, slot_acc, dense_m, B, cs),
+      vg_commit(count), st);
+}
+
+void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int32_t* part,
+               const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
+               int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
+               int32_t nheavy, int32_t* err) {
+  if (count <= 0) return;
+  NodalAux aux;
+  aux.heavy = heavy_list;
+  aux.nheavy = nheavy;
+  aux.err = err;
+  NodalArgs a = make_args(g, part, m, B, aux);
+  a.seed = seed;
+  a.seq = seq;
+  a.lo = lo;
+  a.count = count;
+  a.newlab = newlab;
+  a.rec = rec;
+  a.props_out = props;
+  slot_push(slot_bind(warp, kmNodal[dense ? 1 : 0]), a, ceil_div(count, kNodalWarps));
+  slot_push(slot_bind(heavy, kmNodalHeavy[dense ? 1 : 0]), a, nheavy);
+}
+
+void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
+                const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
+                int32_t B, const CommitScratch& cs) {
+  slot_push(slot_bind(s, kmCommit),
+            commit_args(part, lo, count, newlab, rec, slot_sum, slot_acc, dense_m, B, cs),
+            vg_commit(count));
 }
 
 }  // namespace sbp

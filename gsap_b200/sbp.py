@@ -64,6 +64,36 @@ class Report(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchReport(C.Structure):
+    _fields_ = [("count", C.c_int32), ("max_active", C.c_int32), ("ticks", C.c_int64),
+                ("kernel_launches", C.c_int64), ("ms_total", C.c_double),
+                ("ms_device", C.c_double), ("peak_bytes", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("partition", Options), ("hbm_budget", C.c_uint64), ("max_active", C.c_int32),
+                ("max_queued", C.c_int32)]
+
+
+class JobTimes(C.Structure):
+    _fields_ = [("ms_queue", C.c_double), ("ms_run", C.c_double), ("ms_latency", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("active", C.c_int32), ("queued", C.c_int32), ("max_active_seen", C.c_int32),
+                ("ticks", C.c_int64), ("bytes_active", C.c_double), ("peak_bytes", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class _DcsbmParams(C.Structure):
     _fields_ = [("N", C.c_int32), ("B", C.c_int32), ("alpha", C.c_double),
                 ("p_in", C.c_double), ("deg_min", C.c_int32), ("deg_max", C.c_int32),
@@ -103,6 +133,16 @@ _sig("sbp_mdl", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.POINTER(C.c_dou
      C.POINTER(C.c_double))
 _sig("sbp_mdl_device_static", C.c_int, C.c_int32, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp,
      _vp, _vp, _vp)
+_sig("sbp_partition_batch", C.c_int, _vp, C.c_int32, C.POINTER(Options), _vp, C.c_uint64, _vp,
+     _vp, C.POINTER(BatchReport))
+_sig("sbp_job_bytes", C.c_uint64, C.c_int32, C.c_int32, C.POINTER(Options))
+_sig("sbp_server_default_options", None, C.POINTER(ServerOptions))
+_sig("sbp_server_create", C.c_int, C.POINTER(ServerOptions), C.POINTER(_vp))
+_sig("sbp_server_submit", C.c_int, _vp, C.POINTER(_GraphCSR), C.c_uint64, C.POINTER(C.c_int64))
+_sig("sbp_server_poll", C.c_int, _vp, C.c_int64, C.c_int32, _vp, C.POINTER(Report),
+     C.POINTER(JobTimes))
+_sig("sbp_server_stats_get", C.c_int, _vp, C.POINTER(ServerStats))
+_sig("sbp_server_destroy", C.c_int, _vp)
 _sig("sbp_dcsbm_generate", C.c_int, C.POINTER(_DcsbmParams), C.POINTER(_vp))
 _sig("sbp_edges_size", C.c_int, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32))
 _sig("sbp_edges_copy", C.c_int, _vp, _vp, _vp, _vp, _vp)
@@ -120,7 +160,9 @@ EXPORTED = [
     "sbp_delta_mdl_nodal", "sbp_delta_mdl_merge", "sbp_merge_proposals", "sbp_nodal_batch",
     "sbp_merge_step", "sbp_nodal_sweeps", "sbp_mdl", "sbp_dcsbm_generate", "sbp_edges_size", "sbp_edges_copy",
     "sbp_edges_free", "sbp_csr_from_edges", "sbp_load_tsv", "sbp_evaluate",
-    "sbp_mdl_device_static",
+    "sbp_mdl_device_static", "sbp_job_bytes", "sbp_partition_batch", "sbp_server_default_options",
+    "sbp_server_create", "sbp_server_submit", "sbp_server_poll", "sbp_server_stats_get",
+    "sbp_server_destroy",
 ]
 
 
@@ -258,6 +300,85 @@ def partition(g: Graph, options: Optional[Options] = None, **kw):
     _check(st)
     g.partitions = lab
     return rep.as_dict()
+
+
+def job_bytes(N, E, options: Optional[Options] = None, **kw):
+    """Device arena bytes of one job (the batch / server admission unit)."""
+    o = options or default_options(**kw)
+    return int(_lib.sbp_job_bytes(N, E, C.byref(o)))
+
+
+def partition_batch(graphs, options: Optional[Options] = None, seeds=None, hbm_budget=0, **kw):
+    """sbp_partition_batch: partitions the graphs together; returns
+    (labels per graph, report per graph, batch report)."""
+    o = options or default_options(**kw)
+    n = len(graphs)
+    csrs = (_GraphCSR * max(n, 1))()
+    for i, g in enumerate(graphs):
+        csrs[i] = g.csr()
+    labs = [np.empty(g.N, np.int32) for g in graphs]
+    ptrs = (C.c_void_p * max(n, 1))(*[lab.ctypes.data for lab in labs])
+    reps = (Report * max(n, 1))()
+    seed_arr = None
+    if seeds is not None:
+        seed_arr = np.ascontiguousarray(seeds, dtype=np.uint64)
+        assert seed_arr.size == n
+    br = BatchReport()
+    st = _lib.sbp_partition_batch(C.cast(csrs, _vp), n, C.byref(o),
+                                  None if seed_arr is None else seed_arr.ctypes.data,
+                                  hbm_budget, C.cast(ptrs, _vp), C.cast(reps, _vp), C.byref(br))
+    _check(st)
+    return labs, [reps[i].as_dict() for i in range(n)], br.as_dict()
+
+
+class Server:
+    """sbp_server_*: a partition server with continuous batching on the device."""
+
+    def __init__(self, options: Optional[Options] = None, hbm_budget=0, max_active=0,
+                 max_queued=0, **kw):
+        so = ServerOptions()
+        _lib.sbp_server_default_options(C.byref(so))
+        so.partition = options or default_options(**kw)
+        so.hbm_budget = hbm_budget
+        so.max_active = max_active
+        so.max_queued = max_queued
+        self.h = _vp()
+        self._n = {}
+        _check(_lib.sbp_server_create(C.byref(so), C.byref(self.h)))
+
+    def submit(self, g: Graph, seed=0):
+        jid = C.c_int64()
+        _check(_lib.sbp_server_submit(self.h, C.byref(g.csr()), seed, C.byref(jid)))
+        self._n[jid.value] = g.N
+        return jid.value
+
+    def poll(self, jid, timeout_ms=-1):
+        """(labels, report, times) when done; None while running (BUSY)."""
+        lab = np.empty(self._n.get(jid, 0), np.int32)
+        rep = Report()
+        t = JobTimes()
+        st = _lib.sbp_server_poll(self.h, jid, timeout_ms, _p(lab), C.byref(rep), C.byref(t))
+        if st == 7:  # SBP_ERR_BUSY
+            return None
+        self._n.pop(jid, None)
+        _check(st)
+        return lab, rep.as_dict(), t.as_dict()
+
+    def stats(self):
+        s = ServerStats()
+        _check(_lib.sbp_server_stats_get(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def close(self):
+        if self.h:
+            _lib.sbp_server_destroy(self.h)
+            self.h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class ResidentGraph:

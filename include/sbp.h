@@ -117,6 +117,88 @@ sbp_status sbp_graph_release(sbp_graph_dev* g);
 sbp_status sbp_partition_resident(sbp_graph_dev* g, const sbp_options* o, int32_t* labels_out,
                                   sbp_report* report);
 
+/* ----------------------------------------------------------------- batched
+ * Partitions `count` independent graphs in one call (no GSAP counterpart:
+ * GSAP partitions one graph per process).  A multi-job engine advances every
+ * admitted job one step per tick (a merge step or a nodal sweep), with one
+ * kernel launch per kernel body for all jobs together.  Jobs are admitted in
+ * order while their device arenas fit `hbm_budget` bytes (0: 90% of the
+ * device's free memory); later jobs join as earlier ones finish.  Each
+ * graph's labels and MDL are the same bits as sbp_partition of that graph
+ * alone with the same options and seed.
+ *   labels_out[i]  N_i labels of graph i
+ *   seeds          per-graph seeds (NULL: o->seed for every graph)
+ *   reports        one report per graph (optional)
+ * Returns SBP_OK when every job succeeded, else the first failing job's
+ * status (the other jobs still complete). */
+typedef struct sbp_batch_report {
+  int32_t count;
+  int32_t max_active;       /* most jobs on the device at once */
+  int64_t ticks;            /* engine steps */
+  int64_t kernel_launches;  /* kernels launched by the call */
+  double ms_total;          /* wall time of the call */
+  double ms_device;         /* CUDA-event time from the first tick to the last */
+  double peak_bytes;        /* largest sum of admitted job arenas */
+} sbp_batch_report;
+
+/* Device arena bytes of one job of N vertices and E edges under options o
+ * (what the batch and server admission counts against the HBM budget). */
+uint64_t sbp_job_bytes(int32_t N, int32_t E, const sbp_options* o);
+
+sbp_status sbp_partition_batch(const sbp_graph_csr* graphs, int32_t count, const sbp_options* o,
+                               const uint64_t* seeds, uint64_t hbm_budget,
+                               int32_t* const* labels_out, sbp_report* reports,
+                               sbp_batch_report* batch);
+
+/* ------------------------------------------------------------------ served
+ * A partition server (no GSAP counterpart): a host thread runs the same
+ * engine continuously.  Requests are queued by sbp_server_submit (the graph
+ * is copied, the caller may free it on return) and admitted in arrival order
+ * as soon as the active jobs' device arenas leave room for them under the
+ * HBM budget; admitted jobs join the running engine at its next tick, so
+ * jobs that arrive while others run overlap on the device with them.  Each
+ * job keeps its graph, blockmodel, labels and RNG state resident until it
+ * finishes; its result is the same bits as sbp_partition alone. */
+typedef struct sbp_server sbp_server;
+
+typedef struct sbp_server_options {
+  sbp_options partition;    /* loop options of every job (seed per request) */
+  uint64_t hbm_budget;      /* bytes of job arenas at once (0: 90% of free memory) */
+  int32_t max_active;       /* jobs on the device at once (0: no limit) */
+  int32_t max_queued;       /* queued requests before submit says BUSY (0: no limit) */
+} sbp_server_options;
+
+typedef struct sbp_job_times {
+  double ms_queue;          /* submit -> admitted to the device */
+  double ms_run;            /* admitted -> result ready */
+  double ms_latency;        /* submit -> result ready */
+} sbp_job_times;
+
+typedef struct sbp_server_stats {
+  int64_t submitted, completed, failed;
+  int32_t active, queued, max_active_seen;
+  int64_t ticks;
+  double bytes_active;      /* device bytes of the active jobs' arenas */
+  double peak_bytes;
+} sbp_server_stats;
+
+void sbp_server_default_options(sbp_server_options* o);
+sbp_status sbp_server_create(const sbp_server_options* o, sbp_server** out);
+/* Queues a request; *id identifies it.  SBP_ERR_BUSY when the queue is full,
+ * SBP_ERR_BUDGET when the job alone exceeds the HBM budget. */
+sbp_status sbp_server_submit(sbp_server* s, const sbp_graph_csr* g, uint64_t seed, int64_t* id);
+/* Result of a request: SBP_ERR_BUSY while it is queued or running
+ * (timeout_ms = 0), or waits up to timeout_ms (< 0: no limit) for it.  On
+ * completion fills labels_out (N ints), rep and times (each optional),
+ * releases the request and returns the job's status; SBP_ERR_NOT_FOUND for
+ * an unknown or already collected id. */
+sbp_status sbp_server_poll(sbp_server* s, int64_t id, int32_t timeout_ms, int32_t* labels_out,
+                           sbp_report* rep, sbp_job_times* times);
+sbp_status sbp_server_stats_get(sbp_server* s, sbp_server_stats* out);
+/* Stops the server thread after the jobs on the device finish; queued
+ * requests are cancelled. */
+sbp_status sbp_server_destroy(sbp_server* s);
+
 /* ---------------------------------------------------- path pieces (parity)
  * Each runs one phase of the loop on the GPU from host inputs. */
 
