@@ -25,6 +25,9 @@
 #include "multi.cuh"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
 
 namespace sbp {
 
@@ -73,6 +76,7 @@ struct ScanArgs {
   const int32_t* in;
   int32_t* out;
   int32_t* tile;  // tile sums (tile body), offsets (apply body)
+  const int32_t* ctl;
   int32_t n, pad;
 };
 
@@ -81,6 +85,7 @@ struct ScanTileBody {
   static constexpr int kThreads = kScanThreads, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int) {
+    if (ctl_stopped(a.ctl)) return;
     __shared__ int sh[33];
     int base = vb * kScanTile + threadIdx.x * kScanItems;
     int s = 0;
@@ -100,6 +105,7 @@ struct ScanSingleBody {
   static constexpr int kThreads = kScanThreads, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int, int) {
+    if (ctl_stopped(a.ctl)) return;
     __shared__ int sh[33];
     int carry = 0;
     for (int t0 = 0; t0 < a.n; t0 += kScanTile) {
@@ -129,6 +135,7 @@ struct ScanApplyBody {
   static constexpr int kThreads = kScanThreads, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+    if (ctl_stopped(a.ctl)) return;
     __shared__ int sh[33];
     int base = vb * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
@@ -177,7 +184,9 @@ struct RbSide {
 struct RbArgs {
   RbSide s[2];
   const int32_t* part;
-  int32_t N, E, B, pad;
+  const int32_t* ctl;
+  int32_t N, E, B;
+  int32_t warp_cap;  // longest segment a warp reduces; longer ones go to a CTA
 };
 
 // The rebuild bodies work on both directions: virtual block vb serves
@@ -189,6 +198,7 @@ struct RbCountBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int) {
+  if (ctl_stopped(a.ctl)) return;
   const RbSide& d = a.s[vb & 1];
   int v = (vb >> 1) * blockDim.x + threadIdx.x;
   const bool live = v < a.N;
@@ -220,6 +230,7 @@ struct RbScatterBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int) {
+    if (ctl_stopped(a.ctl)) return;
     const RbSide& d = a.s[vb & 1];
     int j = (vb >> 1) * blockDim.x + threadIdx.x;
     if (j >= a.E) return;
@@ -259,6 +270,7 @@ struct RbRowsSmallBody {
   static constexpr int kThreads = kRowsWarps * 32, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
   __shared__ unsigned long long sk[kRowsWarps][kWarpCap];
   const RbSide& d = a.s[vb & 1];
   vb >>= 1;
@@ -268,12 +280,35 @@ struct RbRowsSmallBody {
   for (int b = vb * kRowsWarps + wid; b < a.B; b += vg * kRowsWarps) {
     int base = d.seg[b];
     int n = d.seg[b + 1] - base;
-    if (n > kWarpCap) {
+    if (n > a.warp_cap) {
       if (lane == 0) d.big[atomicAdd(d.big_count, 1)] = b;
       continue;
     }
     if (n == 0) {
       if (lane == 0) d.uniq[b] = 0;
+      continue;
+    }
+    if (n <= 32) {
+      // one entry per lane: lanes with equal columns group and sum in
+      // registers; each group's leader writes at its column's rank among
+      // the distinct columns (ascending order, as a sort would give)
+      const bool valid = lane < n;
+      const uint32_t c = valid ? (uint32_t)d.tcol[base + lane] : 0xffffffffu;
+      const uint32_t w = valid ? d.tw[base + lane] : 0u;
+      const unsigned peers = __match_any_sync(kFull, c);
+      const uint32_t sum = __reduce_add_sync(peers, w);
+      const bool leader = valid && __ffs(peers) - 1 == lane;
+      const unsigned leaders = __ballot_sync(kFull, leader);
+      int rank = 0;
+      for (unsigned m = leaders; m; m &= m - 1) {
+        const uint32_t cj = __shfl_sync(kFull, c, __ffs(m) - 1);
+        rank += cj < c ? 1 : 0;
+      }
+      if (leader) {
+        d.ucol[base + rank] = (int32_t)c;
+        d.uw[base + rank] = sum;
+      }
+      if (lane == 0) d.uniq[b] = __popc(leaders);
       continue;
     }
     int P = 32;
@@ -315,6 +350,7 @@ struct RbRowsBigBody {
   static constexpr int kThreads = kBigThreads, kMinBlocks = 1;
   static constexpr size_t kSmem = kBigSmem;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
   extern __shared__ unsigned long long big_sm[];
   __shared__ int sh[33];
   const RbSide& d = a.s[vb & 1];
@@ -410,6 +446,7 @@ struct RbCompactBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
   const RbSide& d = a.s[vb & 1];
   vb >>= 1;
   vg >>= 1;
@@ -444,11 +481,24 @@ struct BtArgs {
   double *dSout, *ambout, *ambin, *sinfull;
   int32_t* nbr_s;
   uint8_t* use_rand;
+  const int32_t* ctl;  // sweep control: gate, and seq += ctl[0] * seq_mul
   int32_t B;
   int draws;
   uint64_t seed;
-  uint32_t seq;
+  uint32_t seq, seq_mul;
 };
+
+// One cell's share of a row sum, x log2 x - x * ld, with one rounding order
+// (a fused multiply-add) wherever the per-block sums are formed, so the CSR
+// and the dense form give the same bits.
+__device__ __forceinline__ double cell_term(const double* tab, uint32_t m, double ld) {
+  return __fma_rn(-(double)m, ld, xlx(tab, m));
+}
+
+// Row sum minus its degree term; d == 0 leaves the sum (log2 0 = -inf).
+__device__ __forceinline__ double row_total(double s, uint32_t d, double ld) {
+  return d ? __dsub_rn(s, __dmul_rn((double)d, ld)) : s;
+}
 
 // First entry k of out-row ++ in-row of block b whose running count exceeds
 // t; the whole warp returns the column (or -1).
@@ -483,33 +533,31 @@ struct BlockTermsBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
+  const uint32_t seq = a.seq + ctl_itr(a.ctl) * a.seq_mul;
   int lane = threadIdx.x & 31;
   int w = (vb * blockDim.x + threadIdx.x) >> 5;
   int nw = (vg * blockDim.x) >> 5;
   for (int b = w; b < a.B; b += nw) {
     if (a.draws != 1) {
     double acc = 0.0;
-    for (int i = a.optr[b] + lane; i < a.optr[b + 1]; i += 32) {
-      uint32_t m = a.ocnt[i];
-      acc += xlx(a.xlx, m) - (double)m * a.ld_in[a.ocol[i]];
-    }
+    // the row's k-th nonzero is added by lane k % 32, in order of k
+    for (int i = a.optr[b] + lane; i < a.optr[b + 1]; i += 32)
+      acc += cell_term(a.xlx, a.ocnt[i], a.ld_in[a.ocol[i]]);
     double ao = warp_sum(acc);
     acc = 0.0;
-    for (int i = a.iptr[b] + lane; i < a.iptr[b + 1]; i += 32) {
-      uint32_t m = a.icnt[i];
-      acc += xlx(a.xlx, m) - (double)m * a.ld_out[a.icol[i]];
-    }
+    for (int i = a.iptr[b] + lane; i < a.iptr[b + 1]; i += 32)
+      acc += cell_term(a.xlx, a.icnt[i], a.ld_out[a.icol[i]]);
     double ai = warp_sum(acc);
     if (lane == 0) {
-      uint32_t dout = a.d_out[b], din = a.d_in[b];
       a.ambout[b] = ao;
-      a.dSout[b] = ao - (dout ? (double)dout * a.ld_out[b] : 0.0);
+      a.dSout[b] = row_total(ao, a.d_out[b], a.ld_out[b]);
       a.ambin[b] = ai;
-      a.sinfull[b] = ai - (din ? (double)din * a.ld_in[b] : 0.0);
+      a.sinfull[b] = row_total(ai, a.d_in[b], a.ld_in[b]);
     }
     }
     if (a.draws) {
-      P4 x = draw(a.seed, kRngNodalBlock, a.seq, (uint32_t)b);
+      P4 x = draw(a.seed, kRngNodalBlock, seq, (uint32_t)b);
       uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
       int nb = 0;
       if (deg > 0) {
@@ -539,6 +587,7 @@ struct DenseArgs {
   const int32_t* newlab;  // update: new labels of vertices lo..lo+count-1
   uint32_t *Md, *MTd, *d_out, *d_in;
   double *ld_out, *ld_in;
+  const int32_t* ctl;
   int32_t N, E, B, lo, count, pad;
 };
 
@@ -593,6 +642,7 @@ struct DenseUpdateBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
   const int32_t* __restrict__ optr = a.optr;
   const int32_t* __restrict__ oidx = a.oidx;
   const uint32_t* __restrict__ ow = a.ow;
@@ -668,6 +718,31 @@ __device__ int warp_pick_dense(const uint32_t* orow, const uint32_t* irow, int B
   return -1;
 }
 
+// Sum of cell_term over a dense row with the CSR loop's order: each chunk of
+// 32 columns hands its nonzeros, by their rank in the row, to lanes
+// (rank % 32) through a 32-slot shared buffer of the warp, so every lane adds
+// the same terms in the same order as over the row's CSR entries.
+__device__ __forceinline__ double dense_row_sum(const double* tab, const uint32_t* row,
+                                                const double* ld, int B, int lane,
+                                                double* buf) {
+  double acc = 0.0;
+  int k = 0;  // nonzeros before this chunk
+  const unsigned lt = (1u << lane) - 1u;
+  for (int c0 = 0; c0 < B; c0 += 32) {
+    const int c = c0 + lane;
+    const uint32_t m = c < B ? row[c] : 0u;
+    const unsigned nz = __ballot_sync(kFull, m != 0u);
+    if (nz == 0u) continue;
+    const int n = __popc(nz);
+    if (m) buf[(k + __popc(nz & lt)) & 31] = cell_term(tab, m, ld[c]);
+    __syncwarp();
+    if (((lane - k) & 31) < n) acc += buf[lane];
+    __syncwarp();
+    k += n;
+  }
+  return acc;
+}
+
 struct BtDenseArgs {
   const double* xlx;
   const uint32_t *Md, *MTd, *d_out, *d_in;
@@ -675,10 +750,11 @@ struct BtDenseArgs {
   double *dSout, *ambout, *ambin, *sinfull;
   int32_t* nbr_s;
   uint8_t* use_rand;
+  const int32_t* ctl;  // sweep control: gate, and seq += ctl[0] * seq_mul
   int32_t B;
   int draws;
   uint64_t seed;
-  uint32_t seq;
+  uint32_t seq, seq_mul;
 };
 
 struct BlockTermsDenseBody {
@@ -686,6 +762,9 @@ struct BlockTermsDenseBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
+  __shared__ double tbuf[kThreads / 32][32];
+  const uint32_t seq = a.seq + ctl_itr(a.ctl) * a.seq_mul;
   int lane = threadIdx.x & 31;
   int w = (vb * blockDim.x + threadIdx.x) >> 5;
   int nw = (vg * blockDim.x) >> 5;
@@ -694,24 +773,18 @@ struct BlockTermsDenseBody {
     const uint32_t* orow = a.Md + (size_t)b * B;
     const uint32_t* irow = a.MTd + (size_t)b * B;
     if (a.draws != 1) {
-    double ao = 0.0, ai = 0.0;
-    for (int c = lane; c < B; c += 32) {
-      uint32_t mo = orow[c], mi = irow[c];
-      if (mo) ao += xlx(a.xlx, mo) - (double)mo * a.ld_in[c];
-      if (mi) ai += xlx(a.xlx, mi) - (double)mi * a.ld_out[c];
-    }
-    ao = warp_sum(ao);
-    ai = warp_sum(ai);
+    double* buf = tbuf[threadIdx.x >> 5];
+    double ao = warp_sum(dense_row_sum(a.xlx, orow, a.ld_in, B, lane, buf));
+    double ai = warp_sum(dense_row_sum(a.xlx, irow, a.ld_out, B, lane, buf));
     if (lane == 0) {
-      uint32_t dout = a.d_out[b], din = a.d_in[b];
       a.ambout[b] = ao;
-      a.dSout[b] = ao - (dout ? (double)dout * a.ld_out[b] : 0.0);
+      a.dSout[b] = row_total(ao, a.d_out[b], a.ld_out[b]);
       a.ambin[b] = ai;
-      a.sinfull[b] = ai - (din ? (double)din * a.ld_in[b] : 0.0);
+      a.sinfull[b] = row_total(ai, a.d_in[b], a.ld_in[b]);
     }
     }
     if (a.draws) {
-      P4 x = draw(a.seed, kRngNodalBlock, a.seq, (uint32_t)b);
+      P4 x = draw(a.seed, kRngNodalBlock, seq, (uint32_t)b);
       uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
       int nb = 0;
       if (deg > 0) {
@@ -734,7 +807,8 @@ __global__ void fill_xlx_kernel(double* tab) {
 
 struct MdlArgs {
   const double* dSout;
-  double* out;
+  double* out;  // written at out[ctl[0]] under sweep control
+  const int32_t* ctl;
   int32_t B, pad;
 };
 
@@ -744,6 +818,7 @@ struct MdlSumBody {
   static constexpr int kThreads = 512, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int, int) {
+    if (ctl_stopped(a.ctl)) return;
     __shared__ double sh[kThreads];
     double s = 0.0;
     for (int b = threadIdx.x; b < a.B; b += kThreads) s += a.dSout[b];
@@ -753,7 +828,41 @@ struct MdlSumBody {
       if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
       __syncthreads();
     }
-    if (threadIdx.x == 0) *a.out = sh[0];
+    if (threadIdx.x == 0) a.out[ctl_itr(a.ctl)] = sh[0];
+  }
+};
+
+// The stop test of a queued sweep (partition.hpp:920-934), one thread per
+// job, after the sweep's MDL: ctl[0] = sweeps done so far including this
+// one; ctl[1] = 1 once the moving-average dS test or the sweep limit ends
+// the outer step.  The arithmetic is the host's, operation for operation.
+struct SweepCtlArgs {
+  int32_t* ctl;
+  const double* dsum;   // per sweep of the outer step
+  const double* dataS;  // per sweep of the outer step
+  double model_S;       // E(1+x)ln(1+x) - x ln x + N ln B of the step's B
+  double thr;           // threshold1 or threshold2 by the bracket's state
+  int32_t window;       // 0: no stop test (a fixed number of sweeps)
+  int32_t max_itr;
+};
+
+struct SweepCtlBody {
+  using Args = SweepCtlArgs;
+  static constexpr int kThreads = 32, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int, int) {
+    if (threadIdx.x != 0 || a.ctl[1] != 0) return;
+    const int itr = a.ctl[0];
+    bool stop = false;
+    if (a.window > 0 && itr >= a.window - 1) {
+      double mean = 0.0;
+      for (int i = itr - a.window + 1; i < itr; ++i) mean += a.dsum[i];
+      mean /= (double)(a.window - 1);
+      const double S = a.model_S - a.dataS[itr];
+      stop = -mean < a.thr * S;
+    }
+    a.ctl[0] = itr + 1;
+    if (stop || itr + 1 >= a.max_itr) a.ctl[1] = 1;
   }
 };
 
@@ -762,6 +871,7 @@ struct WordsArgs {
   uint32_t* dst;
   const uint32_t* src;  // copy source (copy body)
   long long n;          // 32-bit words
+  const int32_t* ctl;
 };
 
 struct ZeroBody {
@@ -769,6 +879,7 @@ struct ZeroBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+    if (ctl_stopped(a.ctl)) return;
     for (long long i = (long long)vb * kThreads + threadIdx.x; i < a.n;
          i += (long long)vg * kThreads)
       a.dst[i] = 0u;
@@ -780,6 +891,7 @@ struct CopyBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+    if (ctl_stopped(a.ctl)) return;
     for (long long i = (long long)vb * kThreads + threadIdx.x; i < a.n;
          i += (long long)vg * kThreads)
       a.dst[i] = a.src[i];
@@ -791,6 +903,7 @@ struct IotaBody {
   static constexpr int kThreads = 256, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+    if (ctl_stopped(a.ctl)) return;
     for (long long i = (long long)vb * kThreads + threadIdx.x; i < a.n;
          i += (long long)vg * kThreads)
       a.dst[i] = (uint32_t)i;
@@ -804,8 +917,10 @@ int grid_for(long long items, int per_block, int cap) {
   return (int)g;
 }
 
-RbArgs rb_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, RebuildScratch& rs) {
+RbArgs rb_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, RebuildScratch& rs,
+               const RebuildTune& t) {
   RbArgs a{};
+  a.warp_cap = std::max(32, std::min(kWarpCap, t.warp_cap));
   a.part = part;
   a.N = g.N;
   a.E = g.E;
@@ -840,8 +955,9 @@ RbArgs rb_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, Rebu
 int32_t vg_count(const RbArgs& a) { return 2 * ceil_div(a.N, 256); }
 int32_t vg_scatter(const RbArgs& a) { return a.E > 0 ? 2 * ceil_div(a.E, 256) : 0; }
 int32_t vg_rows_small(const RbArgs& a) { return 2 * grid_for(a.B, kRowsWarps, 4096); }
-int32_t vg_rows_big(const RbArgs& a) {
-  return 2 * std::max(1, std::min(2 * 148, ceil_div(std::max(a.E, 1), 2048)));
+int32_t vg_rows_big(const RbArgs& a, const RebuildTune& t) {
+  const int32_t per = ceil_div(std::max(a.E, 1), std::max(256, t.big_entries));
+  return 2 * std::max(1, std::min(t.big_ctas > 0 ? t.big_ctas : 2 * 148, per));
 }
 int32_t vg_compact(const RbArgs& a) { return 2 * grid_for((long long)a.B * 32, 256, 4096); }
 int32_t vg_words(long long n) {
@@ -900,13 +1016,16 @@ const MultiKernel kmDenseDegrees = multi_kernel_desc<DenseDegreesBody>("dense_de
 const MultiKernel kmDenseLogs = multi_kernel_desc<DenseLogsBody>("dense_logs");
 const MultiKernel kmDenseUpdate = multi_kernel_desc<DenseUpdateBody>("dense_update");
 const MultiKernel kmMdlSum = multi_kernel_desc<MdlSumBody>("mdl_sum");
+const MultiKernel kmSweepCtl = multi_kernel_desc<SweepCtlBody>("sweep_ctl");
 const MultiKernel kmZero = multi_kernel_desc<ZeroBody>("zero");
 const MultiKernel kmCopy = multi_kernel_desc<CopyBody>("copy");
 const MultiKernel kmIota = multi_kernel_desc<IotaBody>("iota");
 
 // One job's scan records: short arrays in one CTA, longer ones in three steps.
-void add_scan(Slot* sl, const int32_t* in, int32_t* out, int32_t n, int32_t* tile) {
+void add_scan(Slot* sl, const int32_t* in, int32_t* out, int32_t n, int32_t* tile,
+              const int32_t* ctl) {
   ScanArgs a{};
+  a.ctl = ctl;
   if (n <= kScanSingleMax) {
     a.in = in;
     a.out = out;
@@ -924,6 +1043,7 @@ void add_scan(Slot* sl, const int32_t* in, int32_t* out, int32_t n, int32_t* til
   b.in = tile;
   b.out = tile + tiles;
   b.n = tiles;
+  b.ctl = ctl;
   slot_push(slot_bind(sl[1], kmScanSingle), b, 1);
   a.tile = tile + tiles;
   slot_push(slot_bind(sl[2], kmScanApply), a, tiles);
@@ -963,8 +1083,8 @@ void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, c
 }
 
 void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
-                        RebuildScratch& rs, cudaStream_t st) {
-  RbArgs a = rb_args(g, part, B, m, rs);
+                        RebuildScratch& rs, cudaStream_t st, const RebuildTune& t) {
+  RbArgs a = rb_args(g, part, B, m, rs, t);
   for (int dir = 0; dir < 2; ++dir)
     cudaMemsetAsync(rs.d[dir].cnt, 0, sizeof(int32_t) * (size_t)B, st);
   cudaMemsetAsync(rs.big_count, 0, sizeof(int32_t) * 2, st);
@@ -973,7 +1093,7 @@ void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM
     scan_exclusive(rs.d[dir].cnt, rs.d[dir].seg, B, rs.tile + dir * (rs.tile_cap / 2), st);
   launch_single<RbScatterBody>(a, vg_scatter(a), st);
   launch_single<RbRowsSmallBody>(a, vg_rows_small(a), st);
-  launch_single<RbRowsBigBody>(a, vg_rows_big(a), st);
+  launch_single<RbRowsBigBody>(a, vg_rows_big(a, t), st);
   for (int dir = 0; dir < 2; ++dir)
     scan_exclusive(rs.d[dir].uniq, dir == 0 ? m.optr : m.iptr, B,
                    rs.tile + dir * (rs.tile_cap / 2), st);
@@ -1018,8 +1138,84 @@ void block_terms_dense(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t s
 }
 
 void mdl_data_sum(const DevBM& m, int32_t B, double* out, cudaStream_t st) {
-  MdlArgs a{m.dSout, out, B, 0};
+  MdlArgs a{m.dSout, out, nullptr, B, 0};
   launch_single<MdlSumBody>(a, 1, st);
+}
+
+// -------------------------------------------------------------- autotuner --
+// The rebuild's segment width (the longest segment one warp reduces; longer
+// ones go to a CTA) and the CTA grid for the long segments are picked by
+// timing rebuilds of a job's own blockmodel, once per device and size class
+// (log2 of B and of the mean segment length E/B).  Every candidate builds
+// the same matrix, so the choice changes only the time.
+namespace {
+struct TuneKey {
+  int device, lb, ls;
+  bool operator<(const TuneKey& o) const {
+    return device != o.device ? device < o.device : lb != o.lb ? lb < o.lb : ls < o.ls;
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, RebuildTune> g_tune;
+
+int ilog2(long long x) {
+  int l = 0;
+  while (x > 1) {
+    x >>= 1;
+    ++l;
+  }
+  return l;
+}
+
+TuneKey tune_key(int device, int32_t E, int32_t B) {
+  return TuneKey{device, ilog2(std::max(B, 1)), ilog2(std::max<long long>(1, (long long)E / std::max(B, 1)))};
+}
+}  // namespace
+
+bool rebuild_tuned(int device, int32_t E, int32_t B, RebuildTune* out) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(device, E, B));
+  if (it == g_tune.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+cudaError_t tune_rebuild(int device, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
+                         RebuildScratch& rs, cudaStream_t st, RebuildTune* out) {
+  std::vector<RebuildTune> cands;
+  for (int wc : {32, 64, 128, 256})
+    for (int be : {2048, 512}) cands.push_back(RebuildTune{wc, 0, be});
+  cudaEvent_t e0, e1;
+  cudaError_t err = cudaEventCreate(&e0);
+  if (err != cudaSuccess) return err;
+  err = cudaEventCreate(&e1);
+  if (err != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return err;
+  }
+  RebuildTune best = RebuildTune{};
+  float best_ms = 1e30f;
+  for (const RebuildTune& c : cands) {
+    rebuild_blockmodel(g, part, B, m, rs, st, c);  // warm
+    float ms = 0.f;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 2; ++r) rebuild_blockmodel(g, part, B, m, rs, st, c);
+    cudaEventRecord(e1, st);
+    err = cudaEventSynchronize(e1);
+    if (err != cudaSuccess) break;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return err;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[tune_key(device, g.E, B)] = best;
+  *out = best;
+  return cudaSuccess;
 }
 
 // ------------------------------------------------------ multi-job records --
@@ -1033,19 +1229,20 @@ std::vector<Slot*> RebuildSlots::all() {
 }
 
 void add_rebuild(RebuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
-                 RebuildScratch& rs) {
-  RbArgs a = rb_args(g, part, B, m, rs);
-  for (int dir = 0; dir < 2; ++dir) add_zero(s.zero, rs.d[dir].cnt, (size_t)B);
-  add_zero(s.zero, rs.big_count, 2);
+                 RebuildScratch& rs, const int32_t* ctl, const RebuildTune& t) {
+  RbArgs a = rb_args(g, part, B, m, rs, t);
+  a.ctl = ctl;
+  for (int dir = 0; dir < 2; ++dir) add_zero(s.zero, rs.d[dir].cnt, (size_t)B, ctl);
+  add_zero(s.zero, rs.big_count, 2, ctl);
   slot_push(slot_bind(s.count, kmRbCount), a, vg_count(a));
   for (int dir = 0; dir < 2; ++dir)
-    add_scan(s.scan1, rs.d[dir].cnt, rs.d[dir].seg, B, rs.tile + dir * (rs.tile_cap / 2));
+    add_scan(s.scan1, rs.d[dir].cnt, rs.d[dir].seg, B, rs.tile + dir * (rs.tile_cap / 2), ctl);
   slot_push(slot_bind(s.scatter, kmRbScatter), a, vg_scatter(a));
   slot_push(slot_bind(s.rows_small, kmRbRowsSmall), a, vg_rows_small(a));
-  slot_push(slot_bind(s.rows_big, kmRbRowsBig), a, vg_rows_big(a));
+  slot_push(slot_bind(s.rows_big, kmRbRowsBig), a, vg_rows_big(a, t));
   for (int dir = 0; dir < 2; ++dir)
     add_scan(s.scan2, rs.d[dir].uniq, dir == 0 ? m.optr : m.iptr, B,
-             rs.tile + dir * (rs.tile_cap / 2));
+             rs.tile + dir * (rs.tile_cap / 2), ctl);
   slot_push(slot_bind(s.compact, kmRbCompact), a, vg_compact(a));
 }
 
@@ -1069,42 +1266,55 @@ void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part,
 }
 
 void add_dense_update(Slot& s, const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
-                      const int32_t* newlab, int32_t B, DevBM& m) {
+                      const int32_t* newlab, int32_t B, DevBM& m, const int32_t* ctl) {
   if (count <= 0) return;
   DenseArgs a = dense_args(g, part, B, m);
+  a.ctl = ctl;
   a.lo = lo;
   a.count = count;
   a.newlab = newlab;
   slot_push(slot_bind(s, kmDenseUpdate), a, vg_dense_update(count));
 }
 
-void add_block_terms(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq) {
-  slot_push(slot_bind(s, kmBlockTerms), bt_args(m, B, draws, seed, seq), vg_block_terms(B));
+void add_block_terms(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq,
+                     const int32_t* ctl, uint32_t seq_mul) {
+  BtArgs a = bt_args(m, B, draws, seed, seq);
+  a.ctl = ctl;
+  a.seq_mul = seq_mul;
+  slot_push(slot_bind(s, kmBlockTerms), a, vg_block_terms(B));
 }
 
 void add_block_terms_dense(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed,
-                           uint32_t seq) {
-  slot_push(slot_bind(s, kmBlockTermsDense), bt_dense_args(m, B, draws, seed, seq),
-            vg_block_terms(B));
+                           uint32_t seq, const int32_t* ctl, uint32_t seq_mul) {
+  BtDenseArgs a = bt_dense_args(m, B, draws, seed, seq);
+  a.ctl = ctl;
+  a.seq_mul = seq_mul;
+  slot_push(slot_bind(s, kmBlockTermsDense), a, vg_block_terms(B));
 }
 
-void add_mdl_sum(Slot& s, const DevBM& m, int32_t B, double* out) {
-  MdlArgs a{m.dSout, out, B, 0};
+void add_mdl_sum(Slot& s, const DevBM& m, int32_t B, double* out, const int32_t* ctl) {
+  MdlArgs a{m.dSout, out, ctl, B, 0};
   slot_push(slot_bind(s, kmMdlSum), a, 1);
 }
 
-void add_zero(Slot& s, void* p, size_t words) {
-  WordsArgs a{(uint32_t*)p, nullptr, (long long)words};
+void add_sweep_ctl(Slot& s, int32_t* ctl, const double* dsum, const double* dataS,
+                   double model_S, double thr, int32_t window, int32_t max_itr) {
+  SweepCtlArgs a{ctl, dsum, dataS, model_S, thr, window, max_itr};
+  slot_push(slot_bind(s, kmSweepCtl), a, 1);
+}
+
+void add_zero(Slot& s, void* p, size_t words, const int32_t* ctl) {
+  WordsArgs a{(uint32_t*)p, nullptr, (long long)words, ctl};
   slot_push(slot_bind(s, kmZero), a, vg_words((long long)words));
 }
 
 void add_copy(Slot& s, void* dst, const void* src, size_t words) {
-  WordsArgs a{(uint32_t*)dst, (const uint32_t*)src, (long long)words};
+  WordsArgs a{(uint32_t*)dst, (const uint32_t*)src, (long long)words, nullptr};
   slot_push(slot_bind(s, kmCopy), a, vg_words((long long)words));
 }
 
 void add_iota(Slot& s, int32_t* p, int32_t n) {
-  WordsArgs a{(uint32_t*)p, nullptr, (long long)n};
+  WordsArgs a{(uint32_t*)p, nullptr, (long long)n, nullptr};
   slot_push(slot_bind(s, kmIota), a, vg_words(n));
 }
 

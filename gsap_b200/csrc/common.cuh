@@ -126,6 +126,16 @@ __device__ __forceinline__ double xlx(const double* __restrict__ tab, uint32_t w
   return w < kXlxTable ? __ldg(tab + w) : xlog2x_big(w);
 }
 
+// Sweep control of one job, in device memory: ctl[0] = sweeps completed in
+// the current outer step, ctl[1] = 1 once the stop test has ended them.
+// Kernels of a queued sweep read it: they skip all work once ctl[1] is set
+// and take their RNG sequence and result slot from ctl[0].  A null ctl
+// means an ungated launch.
+__device__ __forceinline__ bool ctl_stopped(const int32_t* ctl) { return ctl && ctl[1] != 0; }
+__device__ __forceinline__ uint32_t ctl_itr(const int32_t* ctl) {
+  return ctl ? (uint32_t)ctl[0] : 0u;
+}
+
 // Binary search of column c in the CSR row [lo, hi); its count, or 0.
 __device__ __forceinline__ uint32_t row_lookup(const int32_t* __restrict__ col,
                                                const uint32_t* __restrict__ cnt, int32_t lo,

@@ -114,7 +114,7 @@ size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t dens
   add((size_t)N * np, 8);
   add(N, 8);
   add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
-  add((size_t)N, 4); add(2, 4);
+  add((size_t)N, 4); add(2, 4); add(2, 4);
   add((size_t)dense_cap * dense_cap, 4); add((size_t)dense_cap * dense_cap, 4);
   add(kCommitCtas, 8); add(kCommitCtas, 8); add(1, 4);
   return b + 4096;
@@ -253,6 +253,7 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
   J.acc = (long long*)A.take<double>(max_itr);
   J.heavy = A.take<int32_t>((size_t)N);
   J.err = A.take<int32_t>(2);
+  J.ctl = A.take<int32_t>(2);
   if (J.dense_cap > 0) {
     m.Md = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
     m.MTd = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);

@@ -28,6 +28,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -215,14 +216,14 @@ static sbp_status grow(size_t need, size_t& cap, void*& host, void*& dev) {
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-void Engine::ensure_slots(int nb) {
-  if ((int)sw.size() >= nb) return;
-  sw.resize(nb);
+void Engine::ensure_slots(int K, int nb) {
+  if ((int)sw.size() < K * nb) sw.resize(K * nb);
+  if ((int)ends.size() < K) ends.resize(K);
 }
 
 void Engine::clear_slots() {
   for (Slot* s : {&s_iota, &s_heavy, &s_snap, &s_restore, &s_relabel, &s_zero, &m_bt, &m_props,
-                  &m_delta, &e_bt_csr, &e_bt_dense, &e_mdl, &s_gather})
+                  &m_delta, &s_gather})
     s->clear();
   pre_dense.clear();
   pre_rebuild.clear();
@@ -232,7 +233,44 @@ void Engine::clear_slots() {
       s->clear();
     b.rebuild.clear();
   }
+  for (auto& e : ends)
+    for (Slot* s : {&e.bt_csr, &e.bt_dense, &e.mdl, &e.ctl}) s->clear();
 }
+
+// Sweeps queued for a run this tick: the first `window` sweeps of an outer
+// step cannot end it, later ticks queue kSweepsAhead; queued sweeps after
+// the stop test fires do nothing.
+static int32_t sweeps_to_queue(const Run& r) {
+  static const int32_t ahead = [] {
+    const char* e = std::getenv("SBP_SWEEPS_AHEAD");
+    int v = e ? std::atoi(e) : 3;
+    return std::max(1, std::min(v, 16));
+  }();
+  if (r.sweeps_only) return std::min(ahead, r.sweeps_total - r.itr);
+  const int32_t left = r.o.max_nodal_itr - r.itr;
+  const int32_t k = r.itr == 0 ? std::max(ahead, r.o.window) : ahead;
+  return std::max(1, std::min(k, left));
+}
+
+// The rebuild launch shape for a job's size class: the autotuner's choice
+// when it has one, else the defaults.
+static RebuildTune tune_for(const Job& J, int32_t B) {
+  RebuildTune t;
+  rebuild_tuned(J.device, J.E, B, &t);
+  return t;
+}
+
+static bool tuning_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("SBP_TUNE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// Readback layout of a sweeping run: ctl pair, err, nnz, then dsum, dataS
+// and acc of the queued sweeps.
+static size_t sweep_rd_bytes(int32_t K) { return (16 + 24 * (size_t)K + 255) & ~size_t(255); }
 
 // Device work of one run for this tick, as records in the slots.
 void Engine::add_run_work(Run& r) {
@@ -249,11 +287,12 @@ void Engine::add_run_work(Run& r) {
                                    : (size_t)r.o.max_nodal_itr;
     add_zero(s_zero, J.dsum, 2 * n);
     add_zero(s_zero, J.acc, 2 * n);
+    add_zero(s_zero, J.ctl, 2);
   }
   const bool dense = r.dense();
   if (r.stage == Run::kMerge) {
     // the merge kernels read the CSR form
-    if (!r.csr_fresh) add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs);
+    if (!r.csr_fresh) add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
     add_block_terms(m_bt, J.m, r.B, 0, r.o.seed, 0);
     add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props);
     add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS);
@@ -265,42 +304,59 @@ void Engine::add_run_work(Run& r) {
   if (r.stage == Run::kSweep) {
     if (r.build) {
       if (dense) add_dense_build(pre_dense, J.g, J.part, r.B, J.m);
-      else add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs);
+      else add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
     }
     const int nb = r.o.num_batches;
-    for (int32_t b = 0; b < nb; ++b) {
-      SweepSlots& s = sw[b];
-      const uint32_t seq = r.seq + (uint32_t)b;
-      const int32_t k = r.sweeps_only ? r.itr * nb + b : r.itr;
-      const int32_t lo = b * r.BS;
-      if (dense) add_block_terms_dense(s.bt_dense, J.m, r.B, 1, r.o.seed, seq);
-      else add_block_terms(s.bt_csr, J.m, r.B, 1, r.o.seed, seq);
-      add_nodal(dense ? s.nodal_dense : s.nodal_csr, dense ? s.heavy_dense : s.heavy_csr, dense,
-                J.g, J.part, J.m, r.B, r.o.seed, seq, lo, r.BS, J.newlab, J.rec, nullptr,
-                J.heavy + r.heavy_off[b], r.heavy_off[b + 1] - r.heavy_off[b], J.err);
-      if (dense) {
-        // the moved vertices' edges, applied to the dense form before the
-        // labels change (it reads old and new labels)
-        add_dense_update(s.dupd, J.g, J.part, lo, r.BS, J.newlab, r.B, J.m);
-        add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, J.dsum + k, J.acc + k, &J.m,
-                   r.B, J.cs);
+    const RebuildTune tune = tune_for(J, r.B);
+    const int32_t* ctl = J.ctl;
+    const bool isf = std::isfinite(r.large.S) && std::isfinite(r.med.S) && std::isfinite(r.small.S);
+    const double thr = isf ? (double)r.o.threshold2 : (double)r.o.threshold1;
+    const double mS = model_S(r.B, J.N, J.E);
+    for (int32_t k = 0; k < r.sweep_k; ++k) {
+      for (int32_t b = 0; b < nb; ++b) {
+        SweepSlots& s = sw[k * nb + b];
+        const uint32_t seq = r.seq_sweep0 + (uint32_t)b;  // + ctl[0] * nb on the device
+        double* slot_sum = r.sweeps_only ? J.dsum + b : J.dsum;
+        long long* slot_acc = r.sweeps_only ? J.acc + b : J.acc;
+        const int32_t slot_mul = r.sweeps_only ? nb : 1;
+        const int32_t lo = b * r.BS;
+        if (dense) add_block_terms_dense(s.bt_dense, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
+        else add_block_terms(s.bt_csr, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
+        add_nodal(dense ? s.nodal_dense : s.nodal_csr, dense ? s.heavy_dense : s.heavy_csr,
+                  dense, J.g, J.part, J.m, r.B, r.o.seed, seq, lo, r.BS, J.newlab, J.rec,
+                  nullptr, J.heavy + r.heavy_off[b], r.heavy_off[b + 1] - r.heavy_off[b], J.err,
+                  ctl, nb);
+        if (dense) {
+          // the moved vertices' edges, applied to the dense form before the
+          // labels change (it reads old and new labels)
+          add_dense_update(s.dupd, J.g, J.part, lo, r.BS, J.newlab, r.B, J.m, ctl);
+          add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, slot_sum, slot_acc, &J.m,
+                     r.B, J.cs, ctl, slot_mul);
+        } else {
+          add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, slot_sum, slot_acc, nullptr,
+                     0, J.cs, ctl, slot_mul);
+          add_rebuild(s.rebuild, J.g, J.part, r.B, J.m, J.rs, ctl, tune);
+        }
+      }
+      SweepEndSlots& e = ends[k];
+      if (r.sweeps_only) {
+        add_sweep_ctl(e.ctl, J.ctl, J.dsum, J.dataS, 0.0, 0.0, 0, r.sweeps_total);
       } else {
-        add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, J.dsum + k, J.acc + k, nullptr,
-                   0, J.cs);
-        add_rebuild(s.rebuild, J.g, J.part, r.B, J.m, J.rs);
+        if (dense) add_block_terms_dense(e.bt_dense, J.m, r.B, 0, r.o.seed, 0, ctl, 0);
+        else add_block_terms(e.bt_csr, J.m, r.B, 0, r.o.seed, 0, ctl, 0);
+        add_mdl_sum(e.mdl, J.m, r.B, J.dataS, ctl);
+        add_sweep_ctl(e.ctl, J.ctl, J.dsum, J.dataS, mS, thr, r.o.window, r.o.max_nodal_itr);
       }
     }
+    add_copy(s_gather, rd_dev_ptr(r.rd_off), J.ctl, 2);
+    add_copy(s_gather, rd_dev_ptr(r.rd_off + 8), J.err, 1);
+    add_copy(s_gather, rd_dev_ptr(r.rd_off + 12), J.m.optr + r.B, 1);
     if (!r.sweeps_only) {
-      if (dense) add_block_terms_dense(e_bt_dense, J.m, r.B, 0, r.o.seed, 0);
-      else add_block_terms(e_bt_csr, J.m, r.B, 0, r.o.seed, 0);
-      add_mdl_sum(e_mdl, J.m, r.B, J.dataS + r.itr);
-      // dsum[itr], dataS[itr], acc[itr], err, nnz: 8 words
-      add_copy(s_gather, rd_dev_ptr(r.rd_off), J.dsum + r.itr, 2);
-      add_copy(s_gather, rd_dev_ptr(r.rd_off + 8), J.dataS + r.itr, 2);
-      add_copy(s_gather, rd_dev_ptr(r.rd_off + 16), J.acc + r.itr, 2);
+      const size_t K = (size_t)r.sweep_k;
+      add_copy(s_gather, rd_dev_ptr(r.rd_off + 16), J.dsum + r.itr, 2 * K);
+      add_copy(s_gather, rd_dev_ptr(r.rd_off + 16 + 8 * K), J.dataS + r.itr, 2 * K);
+      add_copy(s_gather, rd_dev_ptr(r.rd_off + 16 + 16 * K), J.acc + r.itr, 2 * K);
     }
-    add_copy(s_gather, rd_dev_ptr(r.rd_off + 24), J.err, 1);
-    add_copy(s_gather, rd_dev_ptr(r.rd_off + 28), J.m.optr + r.B, 1);
     return;
   }
   if (r.stage == Run::kFinish) {
@@ -318,7 +374,7 @@ static size_t rd_bytes(const Run& r) {
     case Run::kMerge:
       return align256(4 * (size_t)r.B) + align256(8 * (size_t)r.B);
     case Run::kSweep:
-      return 256;
+      return sweep_rd_bytes(r.sweep_k);
     case Run::kFinish:
       return align256(4 * (size_t)r.J->N) +
              (r.sweeps_only ? align256(8 * (size_t)r.sweeps_total * r.o.num_batches) : 0);
@@ -353,11 +409,18 @@ sbp_status Engine::tick() {
       r->stage = Run::kFinish;
     }
   }
-  // pass 1: uploads (maps, heavy lists) and readbacks
+  // pass 1: sweeps to queue, uploads (maps, heavy lists) and readbacks
   size_t up = 0, rd = 0;
-  int nb_max = 0;
+  int nb_max = 0, k_max = 0;
   for (Run* r : runs) {
     if (r->stage == Run::kDone) continue;
+    r->sweep_k = 0;
+    if (r->stage == Run::kSweep) {
+      r->sweep_k = sweeps_to_queue(*r);
+      if (r->itr == 0) r->seq_sweep0 = r->seq;
+      nb_max = std::max(nb_max, r->o.num_batches);
+      k_max = std::max(k_max, r->sweep_k);
+    }
     if (r->relabel) {
       r->up_map = up;
       up += align256(4 * r->map.size());
@@ -368,14 +431,13 @@ sbp_status Engine::tick() {
     }
     r->rd_off = rd;
     rd += rd_bytes(*r);
-    if (r->stage == Run::kSweep) nb_max = std::max(nb_max, r->o.num_batches);
   }
   sbp_status s = grow(up, up_cap, up_host, up_dev);
   if (s != SBP_OK) return s;
   s = grow(rd, rd_cap, rd_host, rd_dev);
   if (s != SBP_OK) return s;
   // pass 2: records
-  ensure_slots(nb_max);
+  ensure_slots(k_max, nb_max);
   clear_slots();
   for (Run* r : runs) {
     if (r->stage == Run::kDone) continue;
@@ -390,14 +452,18 @@ sbp_status Engine::tick() {
   for (Slot* x : pre_dense.all()) order.push_back(x);
   for (Slot* x : pre_rebuild.all()) order.push_back(x);
   for (Slot* x : {&m_bt, &m_props, &m_delta}) order.push_back(x);
-  for (int b = 0; b < nb_max; ++b) {
-    SweepSlots& w = sw[b];
-    for (Slot* x : {&w.bt_csr, &w.bt_dense, &w.heavy_csr, &w.heavy_dense, &w.nodal_csr,
-                    &w.nodal_dense, &w.dupd, &w.commit})
-      order.push_back(x);
-    for (Slot* x : w.rebuild.all()) order.push_back(x);
+  for (int k = 0; k < k_max; ++k) {
+    for (int b = 0; b < nb_max; ++b) {
+      SweepSlots& w = sw[k * nb_max + b];
+      for (Slot* x : {&w.bt_csr, &w.bt_dense, &w.heavy_csr, &w.heavy_dense, &w.nodal_csr,
+                      &w.nodal_dense, &w.dupd, &w.commit})
+        order.push_back(x);
+      for (Slot* x : w.rebuild.all()) order.push_back(x);
+    }
+    SweepEndSlots& e = ends[k];
+    for (Slot* x : {&e.bt_csr, &e.bt_dense, &e.mdl, &e.ctl}) order.push_back(x);
   }
-  for (Slot* x : {&e_bt_csr, &e_bt_dense, &e_mdl, &s_gather}) order.push_back(x);
+  order.push_back(&s_gather);
   size_t desc = 0;
   std::vector<size_t> off(order.size(), 0);
   for (size_t i = 0; i < order.size(); ++i) {
@@ -420,7 +486,8 @@ sbp_status Engine::tick() {
     return (size_t)0;
   };
   // pass 4: issue
-  const int n_ev = 4 + 5 * nb_max;
+  const int nbatch = k_max * nb_max;
+  const int n_ev = 4 + 5 * nbatch;
   while ((int)ev.size() < n_ev) {
     cudaEvent_t e;
     SBP_CUDA(cudaEventCreate(&e));
@@ -456,35 +523,39 @@ sbp_status Engine::tick() {
   s = emit_until(&m_delta);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaEventRecord(ev[2], st));
-  for (int b = 0; b < nb_max; ++b) {
-    SweepSlots& w = sw[b];
-    cudaEvent_t* be = &ev[4 + 5 * b];
-    SBP_CUDA(cudaEventRecord(be[0], st));
-    s = emit_until(&w.bt_dense);
-    if (s != SBP_OK) return s;
-    SBP_CUDA(cudaEventRecord(be[1], st));
-    const bool heavy = !w.heavy_csr.empty() || !w.heavy_dense.empty();
-    if (heavy) {
-      // heavy vertices on the side stream, next to the warp kernels
-      SBP_CUDA(cudaEventRecord(fork, st));
-      SBP_CUDA(cudaStreamWaitEvent(side, fork, 0));
-      s = launch_slot(w.heavy_csr, slot_off(&w.heavy_csr), side);
+  for (int k = 0; k < k_max; ++k) {
+    for (int b = 0; b < nb_max; ++b) {
+      SweepSlots& w = sw[k * nb_max + b];
+      cudaEvent_t* be = &ev[4 + 5 * (k * nb_max + b)];
+      SBP_CUDA(cudaEventRecord(be[0], st));
+      s = emit_until(&w.bt_dense);
       if (s != SBP_OK) return s;
-      s = launch_slot(w.heavy_dense, slot_off(&w.heavy_dense), side);
+      SBP_CUDA(cudaEventRecord(be[1], st));
+      const bool heavy = !w.heavy_csr.empty() || !w.heavy_dense.empty();
+      if (heavy) {
+        // heavy vertices on the side stream, next to the warp kernels
+        SBP_CUDA(cudaEventRecord(fork, st));
+        SBP_CUDA(cudaStreamWaitEvent(side, fork, 0));
+        s = launch_slot(w.heavy_csr, slot_off(&w.heavy_csr), side);
+        if (s != SBP_OK) return s;
+        s = launch_slot(w.heavy_dense, slot_off(&w.heavy_dense), side);
+        if (s != SBP_OK) return s;
+        SBP_CUDA(cudaEventRecord(join, side));
+      }
+      i += 2;  // the heavy slots
+      s = emit_until(&w.nodal_dense);
       if (s != SBP_OK) return s;
-      SBP_CUDA(cudaEventRecord(join, side));
+      if (heavy) SBP_CUDA(cudaStreamWaitEvent(st, join, 0));
+      SBP_CUDA(cudaEventRecord(be[2], st));
+      s = emit_until(&w.commit);
+      if (s != SBP_OK) return s;
+      SBP_CUDA(cudaEventRecord(be[3], st));
+      s = emit_until(w.rebuild.all().back());
+      if (s != SBP_OK) return s;
+      SBP_CUDA(cudaEventRecord(be[4], st));
     }
-    i += 2;  // the heavy slots
-    s = emit_until(&w.nodal_dense);
+    s = emit_until(&ends[k].ctl);
     if (s != SBP_OK) return s;
-    if (heavy) SBP_CUDA(cudaStreamWaitEvent(st, join, 0));
-    SBP_CUDA(cudaEventRecord(be[2], st));
-    s = emit_until(&w.commit);
-    if (s != SBP_OK) return s;
-    SBP_CUDA(cudaEventRecord(be[3], st));
-    s = emit_until(w.rebuild.all().back());
-    if (s != SBP_OK) return s;
-    SBP_CUDA(cudaEventRecord(be[4], st));
   }
   s = emit_until(&s_gather);
   if (s != SBP_OK) return s;
@@ -497,12 +568,16 @@ sbp_status Engine::tick() {
   float ms_pre = 0.f, ms_merge = 0.f;
   SBP_CUDA(cudaEventElapsedTime(&ms_pre, ev[0], ev[1]));
   SBP_CUDA(cudaEventElapsedTime(&ms_merge, ev[1], ev[2]));
-  std::vector<float> b_nodal(nb_max), b_kernel(nb_max), b_rebuild(nb_max);
-  for (int b = 0; b < nb_max; ++b) {
-    cudaEvent_t* be = &ev[4 + 5 * b];
-    SBP_CUDA(cudaEventElapsedTime(&b_nodal[b], be[0], be[3]));
-    SBP_CUDA(cudaEventElapsedTime(&b_kernel[b], be[1], be[2]));
-    SBP_CUDA(cudaEventElapsedTime(&b_rebuild[b], be[3], be[4]));
+  float t_nodal = 0.f, t_kernel = 0.f, t_rebuild = 0.f;
+  for (int q = 0; q < nbatch; ++q) {
+    cudaEvent_t* be = &ev[4 + 5 * q];
+    float a = 0.f, b = 0.f, c = 0.f;
+    SBP_CUDA(cudaEventElapsedTime(&a, be[0], be[3]));
+    SBP_CUDA(cudaEventElapsedTime(&b, be[1], be[2]));
+    SBP_CUDA(cudaEventElapsedTime(&c, be[3], be[4]));
+    t_nodal += a;
+    t_kernel += b;
+    t_rebuild += c;
   }
   // host side of each run
   for (Run* r : runs) {
@@ -537,39 +612,61 @@ sbp_status Engine::tick() {
     if (r->stage == Run::kSweep) {
       Job& J = *r->J;
       const bool dense = r->dense();
+      const int nb = r->o.num_batches;
       r->build = false;
       if (!dense) r->csr_fresh = true;
-      const int nb = r->o.num_batches;
-      for (int b = 0; b < nb; ++b) {
-        r->R.ms_nodal += b_nodal[b];
-        r->R.ms_nodal_kernel += b_kernel[b];
-        r->R.ms_rebuild += b_rebuild[b];
-        r->R.nodal_proposals += r->BS;
-        r->R.nodal_launches += 1;
-        r->R.bytes_nodal += 28.0 * r->BS + 12.0 * r->batch_entries[b] + 16.0 * r->nnz_now +
-                            8.0 * r->B;
-        r->R.bytes_rebuild += dense ? 12.0 * r->batch_entries[b] + 8.0 * (double)r->B * r->B
-                                    : 4.0 * J.N + 24.0 * J.E + 16.0 * r->nnz_now + 8.0 * r->B;
-      }
-      r->seq += (uint32_t)nb;
-      int32_t err = 0, nnz = 0;
-      std::memcpy(&err, rdp + 24, 4);
-      std::memcpy(&nnz, rdp + 28, 4);
+      r->R.ms_nodal += t_nodal;
+      r->R.ms_nodal_kernel += t_kernel;
+      r->R.ms_rebuild += t_rebuild;
+      int32_t ctl[2] = {0, 0}, err = 0, nnz = 0;
+      std::memcpy(ctl, rdp, 8);
+      std::memcpy(&err, rdp + 8, 4);
+      std::memcpy(&nnz, rdp + 12, 4);
+      const int32_t done = ctl[0] - r->itr;  // sweeps that ran this tick
       if (err != 0) {
         r->set_error(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
         continue;
       }
-      if (!dense) r->nnz_now = (double)nnz;
-      if (r->sweeps_only) {
-        if (++r->itr == r->sweeps_total) r->stage = Run::kFinish;
+      if (done < 1 || done > r->sweep_k) {
+        r->set_error(SBP_ERR_INTERNAL, "sweep control out of step");
         continue;
       }
-      double dsum = 0.0, dataS = 0.0;
-      long long acc = 0;
-      std::memcpy(&dsum, rdp, 8);
-      std::memcpy(&dataS, rdp + 8, 8);
-      std::memcpy(&acc, rdp + 16, 8);
-      r->after_sweep(dsum, dataS, acc);
+      for (int32_t q = 0; q < done; ++q)
+        for (int b = 0; b < nb; ++b) {
+          r->R.nodal_proposals += r->BS;
+          r->R.nodal_launches += 1;
+          r->R.bytes_nodal += 28.0 * r->BS + 12.0 * r->batch_entries[b] +
+                              16.0 * r->nnz_now + 8.0 * r->B;
+          r->R.bytes_rebuild += dense ? 12.0 * r->batch_entries[b] + 8.0 * (double)r->B * r->B
+                                      : 4.0 * J.N + 24.0 * J.E + 16.0 * r->nnz_now + 8.0 * r->B;
+        }
+      r->seq = r->seq_sweep0 + (uint32_t)ctl[0] * (uint32_t)nb;
+      if (!dense) r->nnz_now = (double)nnz;
+      // the labels are those of this B now: tune the rebuild for its class
+      RebuildTune known;
+      if (!dense && tuning_enabled() && !rebuild_tuned(J.device, J.E, r->B, &known)) {
+        cudaError_t te = tune_rebuild(J.device, J.g, J.part, r->B, J.m, J.rs, st, &known);
+        if (te != cudaSuccess) return fail(SBP_ERR_CUDA, cudaGetErrorString(te));
+      }
+      if (r->sweeps_only) {
+        r->itr = ctl[0];
+        if (ctl[1]) r->stage = Run::kFinish;
+        continue;
+      }
+      const size_t K = (size_t)r->sweep_k;
+      for (int32_t q = 0; q < done && r->stage == Run::kSweep; ++q) {
+        double dsum = 0.0, dataS = 0.0;
+        long long acc = 0;
+        std::memcpy(&dsum, rdp + 16 + 8 * q, 8);
+        std::memcpy(&dataS, rdp + 16 + 8 * K + 8 * q, 8);
+        std::memcpy(&acc, rdp + 16 + 16 * K + 8 * q, 8);
+        const bool last = q == done - 1;
+        r->after_sweep(dsum, dataS, acc);
+        // the device's stop test and the host's must agree
+        const bool host_stopped = r->stage != Run::kSweep;
+        if (host_stopped != (last && ctl[1] != 0) && r->status == SBP_OK)
+          r->set_error(SBP_ERR_INTERNAL, "device and host stop tests disagree");
+      }
       continue;
     }
     if (r->stage == Run::kFinish) {

@@ -42,6 +42,8 @@ struct Run {
   // loop state (partition.hpp:852-954)
   int32_t B = 0, B_to_merge = 0, BS = 0, itr = 0;
   uint32_t seq = 0;
+  uint32_t seq_sweep0 = 0;  // seq of the outer step's first sweep
+  int32_t sweep_k = 0;      // sweeps queued this tick
   Bracket large, med, small;
   double S = 0.0;
   std::vector<double> itr_dS;
@@ -81,6 +83,11 @@ struct SweepSlots {
   RebuildSlots rebuild;
 };
 
+// The launches that end one queued sweep: MDL terms, MDL sum, stop test.
+struct SweepEndSlots {
+  Slot bt_csr, bt_dense, mdl, ctl;
+};
+
 class Engine {
  public:
   int device = 0;
@@ -107,8 +114,9 @@ class Engine {
   DenseBuildSlots pre_dense;
   RebuildSlots pre_rebuild;
   Slot m_bt, m_props, m_delta;
-  std::vector<SweepSlots> sw;
-  Slot e_bt_csr, e_bt_dense, e_mdl, s_gather;
+  std::vector<SweepSlots> sw;     // [queued sweep][batch]
+  std::vector<SweepEndSlots> ends;  // [queued sweep]
+  Slot s_gather;
   std::vector<cudaEvent_t> ev;
   void *up_host = nullptr, *up_dev = nullptr, *desc_host = nullptr, *desc_dev = nullptr;
   void *rd_host = nullptr, *rd_dev = nullptr;
@@ -116,7 +124,7 @@ class Engine {
 
   void* up_dev_ptr(size_t off) { return (char*)up_dev + off; }
   void* rd_dev_ptr(size_t off) { return (char*)rd_dev + off; }
-  void ensure_slots(int nb);
+  void ensure_slots(int K, int nb);
   void clear_slots();
   void add_run_work(Run& r);
   sbp_status launch_slot(Slot& s, size_t off, cudaStream_t stream);

@@ -55,6 +55,7 @@ struct Job {
   double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
   int32_t* heavy = nullptr;     // batch indices of the CTA-per-vertex kernel
   int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
+  int32_t* ctl = nullptr;       // sweep control: sweeps done in the outer step, stop flag
   CommitScratch cs;
   int32_t dense_cap = 0;        // largest B the dense arrays can hold
   int32_t dense_eff = 0;        // largest B kept in dense form in this run

@@ -69,6 +69,16 @@ struct RebuildScratch {
   int32_t tile_cap = 0;
 };
 
+// Launch shape of a rebuild (the autotuner's choice; results never depend
+// on it): segments longer than warp_cap entries are reduced by a CTA,
+// big_ctas CTAs per direction (0: 296 at most) take one per big_entries graph
+// entries.
+struct RebuildTune {
+  int32_t warp_cap = 256;
+  int32_t big_ctas = 0;
+  int32_t big_entries = 2048;
+};
+
 // ------------------------------------------------------ multi-job launches --
 // One launch of a kernel body over many jobs: `args` holds njobs argument
 // records back to back, job j owns virtual blocks [cta0[j], cta0[j+1]).
@@ -121,18 +131,28 @@ struct DenseBuildSlots {
 };
 
 // Record builders: each adds one job's launch record(s) to the slot(s), with
-// a virtual grid that depends on that job's sizes only.
+// a virtual grid that depends on that job's sizes only.  `ctl` (optional)
+// is the job's sweep control (int32 pair in device memory: sweeps done in
+// the outer step, stop flag): a gated launch does nothing once the stop
+// flag is set, and takes its RNG sequence as seq + ctl[0] * seq_mul and its
+// result slot as slot + ctl[0] * slot_mul.
 void add_rebuild(RebuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
-                 RebuildScratch& rs);
+                 RebuildScratch& rs, const int32_t* ctl = nullptr,
+                 const RebuildTune& t = RebuildTune{});
 void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B,
                      DevBM& m);
 void add_dense_update(Slot& s, const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
-                      const int32_t* newlab, int32_t B, DevBM& m);
-void add_block_terms(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq);
+                      const int32_t* newlab, int32_t B, DevBM& m, const int32_t* ctl = nullptr);
+void add_block_terms(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq,
+                     const int32_t* ctl = nullptr, uint32_t seq_mul = 0);
 void add_block_terms_dense(Slot& s, DevBM& m, int32_t B, int draws, uint64_t seed,
-                           uint32_t seq);
-void add_mdl_sum(Slot& s, const DevBM& m, int32_t B, double* out);
-void add_zero(Slot& s, void* p, size_t words);
+                           uint32_t seq, const int32_t* ctl = nullptr, uint32_t seq_mul = 0);
+// data_S into out[ctl[0]] (out[0] without ctl).
+void add_mdl_sum(Slot& s, const DevBM& m, int32_t B, double* out, const int32_t* ctl = nullptr);
+// The stop test after a queued sweep (window 0: count sweeps to max_itr).
+void add_sweep_ctl(Slot& s, int32_t* ctl, const double* dsum, const double* dataS,
+                   double model_S, double thr, int32_t window, int32_t max_itr);
+void add_zero(Slot& s, void* p, size_t words, const int32_t* ctl = nullptr);
 void add_copy(Slot& s, void* dst, const void* src, size_t words);
 void add_iota(Slot& s, int32_t* p, int32_t n);
 // Nodal batch of one job: the warp kernel's record goes to `warp`, the
@@ -141,15 +161,23 @@ void add_iota(Slot& s, int32_t* p, int32_t n);
 void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int32_t* part,
                const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
                int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
-               int32_t nheavy, int32_t* err);
+               int32_t nheavy, int32_t* err, const int32_t* ctl = nullptr, uint32_t seq_mul = 0);
 void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                 const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
-                int32_t B, const CommitScratch& cs);
+                int32_t B, const CommitScratch& cs, const int32_t* ctl = nullptr,
+                int32_t slot_mul = 0);
 void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
                      int32_t* props);
 void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
                      double* dS, int32_t* best, double* best_dS);
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map);
+
+// Tuned shape for a device and a blockmodel size class, if known.
+bool rebuild_tuned(int device, int32_t E, int32_t B, RebuildTune* out);
+// Times the candidate shapes on this blockmodel (labels `part` must be in
+// [0, B)), caches and returns the fastest.  Synchronises the stream.
+cudaError_t tune_rebuild(int device, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
+                         RebuildScratch& rs, cudaStream_t st, RebuildTune* out);
 
 // Opt-in shared-memory sizes; call once per device before the first launch.
 cudaError_t init_kernel_attributes();
@@ -159,7 +187,8 @@ void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, c
 
 // calculate_new_csr (partition.hpp:707-849): rebuild M from the labels.
 void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
-                        RebuildScratch& rs, cudaStream_t st);
+                        RebuildScratch& rs, cudaStream_t st,
+                        const RebuildTune& t = RebuildTune{});
 
 // Per-block work: draws == 0 computes the per-block sums (dSout, ambout,
 // ambin, sinfull; the MDL and the merge phase read them), draws == 1 only

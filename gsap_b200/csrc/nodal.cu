@@ -73,6 +73,8 @@ struct NodalArgs {
   const int32_t* heavy;     // batch indices handled by the CTA kernel
   int32_t nheavy;
   int32_t* err;             // error counter (hash table overflow)
+  const int32_t* ctl;       // sweep control: gate, and seq += ctl[0] * seq_mul
+  uint32_t seq_mul;
 };
 
 // g(x, a) = x log2 x - x a, zero for x == 0
@@ -344,6 +346,43 @@ __device__ double delta_sorted(const NodalArgs& a, int v, int r, int s,
   return finish<DENSE, G>(a, R, v, r, s, w, q, grp);
 }
 
+// dS from the warp's entries, one per lane and pass (see delta_registers).
+template <bool DENSE>
+__device__ __forceinline__ double delta_from_entries(const NodalArgs& a, const Rows<DENSE>& R,
+                                                     int v, int r, int s, int passes,
+                                                     const int32_t* cs, const uint32_t* ws,
+                                                     const bool* ins, const bool* valid,
+                                                     int lane) {
+  Acc q;
+  RsWeights w{0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    if (passes == 1 && p == 1) break;
+    const bool o = valid[p] && !ins[p], i = valid[p] && ins[p];
+    w.koR += __reduce_add_sync(kFull, o && cs[p] == r ? ws[p] : 0u);
+    w.koS += __reduce_add_sync(kFull, o && cs[p] == s ? ws[p] : 0u);
+    w.niR += __reduce_add_sync(kFull, i && cs[p] == r ? ws[p] : 0u);
+    w.niS += __reduce_add_sync(kFull, i && cs[p] == s ? ws[p] : 0u);
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    if (passes == 1 && p == 1) break;
+    // direction in the top bit, unique keys for idle lanes
+    const unsigned key = valid[p] ? ((unsigned)cs[p] | (ins[p] ? 0x80000000u : 0u))
+                                  : (0x7fffffe0u + (unsigned)lane);
+    const unsigned peers = __match_any_sync(kFull, key);
+    const uint32_t kc = __reduce_add_sync(peers, ws[p]);
+    if (valid[p])
+      entry<DENSE>(a, R, r, s, w.niS, ins[p], cs[p], ws[p], lane == __ffs(peers) - 1, kc, q);
+  }
+  q.m4 = __reduce_add_sync(kFull, q.m4);
+  q.m5 = __reduce_add_sync(kFull, q.m5);
+  q.m6 = __reduce_add_sync(kFull, q.m6);
+  q.m7 = __reduce_add_sync(kFull, q.m7);
+  corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
+  return warp_sum(q.acc);
+}
+
 // dS when each direction's list fits in one warp: entries of the same block
 // are grouped with __match_any_sync on a direction-tagged key and their
 // weights summed with __reduce_add_sync.  When both lists fit together,
@@ -352,8 +391,6 @@ template <bool DENSE>
 __device__ double delta_registers(const NodalArgs& a, int v, int r, int s, int32_t o0, int no,
                                   int32_t i0, int ni, int lane) {
   const Rows<DENSE> R(a, r, s);
-  Acc q;
-  RsWeights w{0u, 0u, 0u, 0u};
   const int passes = no + ni <= 32 ? 1 : 2;
   // pass p, lane l: entry index e; combined pass: out-entries then in-entries
   int32_t cs[2];
@@ -386,30 +423,10 @@ __device__ double delta_registers(const NodalArgs& a, int v, int r, int s, int32
       cs[p] = in ? __ldg(a.part + __ldg(a.iidx + i0 + k)) : __ldg(a.part + __ldg(a.oidx + o0 + k));
       ws[p] = in ? __ldg(a.iw + i0 + k) : __ldg(a.ow + o0 + k);
     }
-    const bool o = valid[p] && !in, i = valid[p] && in;
-    w.koR += __reduce_add_sync(kFull, o && cs[p] == r ? ws[p] : 0u);
-    w.koS += __reduce_add_sync(kFull, o && cs[p] == s ? ws[p] : 0u);
-    w.niR += __reduce_add_sync(kFull, i && cs[p] == r ? ws[p] : 0u);
-    w.niS += __reduce_add_sync(kFull, i && cs[p] == s ? ws[p] : 0u);
   }
-#pragma unroll
-  for (int p = 0; p < 2; ++p) {
-    if (passes == 1 && p == 1) break;
-    // direction in the top bit, unique keys for idle lanes
-    const unsigned key = valid[p] ? ((unsigned)cs[p] | (ins[p] ? 0x80000000u : 0u))
-                                  : (0x7fffffe0u + (unsigned)lane);
-    const unsigned peers = __match_any_sync(kFull, key);
-    const uint32_t kc = __reduce_add_sync(peers, ws[p]);
-    if (valid[p])
-      entry<DENSE>(a, R, r, s, w.niS, ins[p], cs[p], ws[p], lane == __ffs(peers) - 1, kc, q);
-  }
-  q.m4 = __reduce_add_sync(kFull, q.m4);
-  q.m5 = __reduce_add_sync(kFull, q.m5);
-  q.m6 = __reduce_add_sync(kFull, q.m6);
-  q.m7 = __reduce_add_sync(kFull, q.m7);
-  corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
-  return warp_sum(q.acc);
+  return delta_from_entries<DENSE>(a, R, v, r, s, passes, cs, ws, ins, valid, lane);
 }
+
 
 // Lists too long for shared memory: per-block totals from a shared-memory
 // hash table, built in passes that each take the blocks of one hash class,
@@ -544,7 +561,7 @@ __device__ __forceinline__ void item(const NodalArgs& a, int i, int lane, int& v
     return;
   }
   v = a.lo + i;
-  P4 x = draw(a.seed, kRngNodalVertex, a.seq, (uint32_t)v);
+  P4 x = draw(a.seed, kRngNodalVertex, a.seq + ctl_itr(a.ctl) * a.seq_mul, (uint32_t)v);
   int rnd = (int)(x.v[0] % (uint32_t)a.B);
   uint64_t deg = (uint64_t)a.kdo[v] + a.kdi[v];
   if (deg == 0) {
@@ -578,6 +595,7 @@ struct NodalBody {
   static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = 3;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
   __shared__ unsigned long long s_ko[kNodalWarps][kWarpList], s_ki[kNodalWarps][kWarpList];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = vg * kNodalWarps;
@@ -587,6 +605,49 @@ struct NodalBody {
     const int32_t o0 = a.optr[vv], no = a.optr[vv + 1] - o0;
     const int32_t i0 = a.iptr[vv], ni = a.iptr[vv + 1] - i0;
     if (is_heavy(no, ni)) continue;  // the CTA kernel's
+    if (!GIVEN && no + ni <= 32) {
+      // one entry per lane, loaded once: the proposal's neighbour pick (out-
+      // then in-entries, pick_neighbour's order) and the dS both read it
+      const int v = vv;
+      const P4 x = draw(a.seed, kRngNodalVertex, a.seq + ctl_itr(a.ctl) * a.seq_mul, (uint32_t)v);
+      const int rnd = (int)(x.v[0] % (uint32_t)a.B);
+      const bool in = lane >= no;
+      const bool valid = lane < no + ni;
+      const int k = in ? lane - no : lane;
+      int32_t c = -1;
+      uint32_t w = 0u;
+      if (valid) {
+        const int32_t u = in ? __ldg(a.iidx + i0 + k) : __ldg(a.oidx + o0 + k);
+        w = in ? __ldg(a.iw + i0 + k) : __ldg(a.ow + o0 + k);
+        c = __ldg(a.part + u);
+      }
+      const int r = a.part[v];
+      const uint64_t deg = (uint64_t)a.kdo[v] + a.kdi[v];
+      int s = rnd;
+      if (deg != 0) {
+        const uint64_t t = scale_draw(x.v[1], deg);
+        uint64_t incl = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint64_t y = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += y;
+        }
+        const unsigned hit = __ballot_sync(kFull, valid && incl > t);
+        const int cu = hit ? __shfl_sync(kFull, c, __ffs(hit) - 1) : a.part[0];
+        s = a.use_rand[cu] ? rnd : a.nbr_s[cu];
+      }
+      double d = 0.0;
+      if (r != s) {
+        const Rows<DENSE> R(a, r, s);
+        const int32_t cs[2] = {c, -1};
+        const uint32_t ws[2] = {w, 0u};
+        const bool ins[2] = {in, false}, valids[2] = {valid, false};
+        d = delta_from_entries<DENSE>(a, R, v, r, s, 1, cs, ws, ins, valids, lane);
+      }
+      if (lane == 0) write_result(a, false, i, r, s, d);
+      __syncwarp();
+      continue;
+    }
     int v, s;
     item<GIVEN>(a, i, lane, v, s);
     const int r = a.part[v];
@@ -615,6 +676,7 @@ struct NodalHeavyBody {
   static constexpr int kThreads = kHeavyThreads, kMinBlocks = 2;
   static constexpr size_t kSmem = kHeavySmem;
   static __device__ void run(const Args& a, int vb, int vg) {
+  if (ctl_stopped(a.ctl)) return;
   extern __shared__ unsigned long long hsm[];
   __shared__ double red[kHeavyThreads / 32];
   __shared__ int flag, sh_v, sh_s;
@@ -672,7 +734,8 @@ struct CommitArgs {
   double* part_sum;
   long long* part_cnt;
   unsigned* ticket;
-  int32_t lo, count, B, pad;
+  const int32_t* ctl;  // sweep control: gate, and slots advance ctl[0] * slot_mul
+  int32_t lo, count, B, slot_mul;
 };
 
 struct CommitBody {
@@ -680,6 +743,7 @@ struct CommitBody {
   static constexpr int kThreads = kCommitThreads, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+    if (ctl_stopped(a.ctl)) return;
     __shared__ double sh[kCommitThreads];
     __shared__ long long shc[kCommitThreads];
     __shared__ bool last;
@@ -724,8 +788,9 @@ struct CommitBody {
         t += ((volatile double*)a.part_sum)[k];
         n += ((volatile long long*)a.part_cnt)[k];
       }
-      *a.slot_sum += t;
-      *a.slot_acc += n;
+      const int k = (int)ctl_itr(a.ctl) * a.slot_mul;
+      a.slot_sum[k] += t;
+      a.slot_acc[k] += n;
       *a.ticket = 0u;
     }
   }
@@ -865,7 +930,7 @@ void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newla
 void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int32_t* part,
                const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
                int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
-               int32_t nheavy, int32_t* err) {
+               int32_t nheavy, int32_t* err, const int32_t* ctl, uint32_t seq_mul) {
   if (count <= 0) return;
   NodalAux aux;
   aux.heavy = heavy_list;
@@ -879,16 +944,19 @@ void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int
   a.newlab = newlab;
   a.rec = rec;
   a.props_out = props;
+  a.ctl = ctl;
+  a.seq_mul = seq_mul;
   slot_push(slot_bind(warp, kmNodal[dense ? 1 : 0]), a, ceil_div(count, kNodalWarps));
   slot_push(slot_bind(heavy, kmNodalHeavy[dense ? 1 : 0]), a, nheavy);
 }
 
 void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                 const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
-                int32_t B, const CommitScratch& cs) {
-  slot_push(slot_bind(s, kmCommit),
-            commit_args(part, lo, count, newlab, rec, slot_sum, slot_acc, dense_m, B, cs),
-            vg_commit(count));
+                int32_t B, const CommitScratch& cs, const int32_t* ctl, int32_t slot_mul) {
+  CommitArgs a = commit_args(part, lo, count, newlab, rec, slot_sum, slot_acc, dense_m, B, cs);
+  a.ctl = ctl;
+  a.slot_mul = slot_mul;
+  slot_push(slot_bind(s, kmCommit), a, vg_commit(count));
 }
 
 }  // namespace sbp

@@ -29,6 +29,8 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--dense-max", type=int, default=None,
+                    help="largest B kept in the dense blockmodel form")
     a = ap.parse_args(argv)
     if a.synthetic:
         g = sbp.dcsbm_variant(a.synthetic, a.N, a.B, seed=a.graph_seed)
@@ -40,7 +42,8 @@ def main(argv=None):
         ap.error("give --synthetic, --tsv or --dataset")
     for i in range(a.repeat):
         t0 = time.perf_counter()
-        rep = sbp.partition(g, seed=a.seed + i, device=a.device, verbose=int(a.verbose))
+        kw = {} if a.dense_max is None else {"dense_max": a.dense_max}
+        rep = sbp.partition(g, seed=a.seed + i, device=a.device, verbose=int(a.verbose), **kw)
         rep["wall_ms"] = (time.perf_counter() - t0) * 1000.0
         rep["N"], rep["E"] = g.N, g.E
         if g.true_partitions is not None and g.true_partitions.min() >= 0:

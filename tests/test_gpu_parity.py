@@ -212,3 +212,30 @@ def test_nodal_sweeps_match_oracle(sbp, orc, case, mode, dmax):
         want.append(tot)
     assert np.array_equal(lab, q)
     assert close(sums, np.array(want)).all()
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_nodal_sweeps_same_bits_in_both_forms(sbp, case):
+    # the dense and the CSR form of M give the same labels and the same dS
+    # sums, bit for bit
+    _, g, p, B = case
+    runs = [sbp.nodal_sweeps(g, p, B, seed=3, seq0=7, num_batches=4, sweeps=2, dense_max=d)
+            for d in (0, g.N)]
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+
+
+@pytest.mark.parametrize("variant,N,B,seed", [("LL", 2000, 16, 0), ("HH", 5000, 24, 1),
+                                              ("LH", 3000, 20, 2), ("HL", 6000, 28, 3)])
+def test_partition_same_bits_in_both_forms(sbp, variant, N, B, seed):
+    # every per-block sum is added in the same order in both forms, so the
+    # form chosen at each B never changes a partition
+    g = graphs.dcsbm(variant, N, B, seed)
+    out = []
+    for dmax in (0, 1024, N):
+        rep = sbp.partition(g, seed=seed, dense_max=dmax)
+        out.append((g.partitions.copy(), rep))
+    for lab, rep in out[1:]:
+        assert np.array_equal(lab, out[0][0])
+        assert rep["S"] == out[0][1]["S"] and rep["B"] == out[0][1]["B"]
+        assert rep["nodal_itrs"] == out[0][1]["nodal_itrs"]
