@@ -802,7 +802,10 @@ struct BlockTermsDenseBody {
 
 __global__ void fill_xlx_kernel(double* tab) {
   uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x < kXlxTable) tab[x] = xlog2x(x);
+  if (x < kXlxTable) {
+    tab[x] = xlog2x(x);
+    tab[kXlxTable + x] = log2((double)x);
+  }
 }
 
 struct MdlArgs {

@@ -116,14 +116,18 @@ __device__ __forceinline__ double xlog2x(uint32_t w) {
   return w == 0u ? 0.0 : (double)w * log2((double)w);
 }
 
-// x*log2(x) of small counts from a table (tab[x] holds exactly
-// xlog2x(x), filled on the device), larger ones computed.
+// x*log2(x) and log2(x) of small counts from a table (tab[x] holds exactly
+// xlog2x(x), tab[kXlxTable + x] exactly log2(x), both filled on the device
+// with the same functions), larger ones computed.
 constexpr uint32_t kXlxTable = 1u << 16;
 static __device__ __forceinline__ double xlog2x_big(uint32_t w) {
   return (double)w * log2((double)w);
 }
 __device__ __forceinline__ double xlx(const double* __restrict__ tab, uint32_t w) {
   return w < kXlxTable ? __ldg(tab + w) : xlog2x_big(w);
+}
+__device__ __forceinline__ double l2x(const double* __restrict__ tab, uint32_t w) {
+  return w < kXlxTable ? __ldg(tab + kXlxTable + w) : log2((double)w);
 }
 
 // Sweep control of one job, in device memory: ctl[0] = sweeps completed in

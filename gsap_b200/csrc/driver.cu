@@ -161,7 +161,7 @@ sbp_status device_xlx_table(int device, const double** out) {
   std::lock_guard<std::mutex> lk(mu);
   if (!tab[device]) {
     double* t = nullptr;
-    SBP_CUDA(cudaMalloc(&t, sizeof(double) * kXlxTable));
+    SBP_CUDA(cudaMalloc(&t, sizeof(double) * 2 * kXlxTable));
     cudaStream_t st;
     SBP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     fill_xlx_table(t, st);

@@ -38,7 +38,8 @@ struct DevBM {
   // dense form for small B: Md[r*B + c] = M[r][c], MTd[c*B + r] = M[r][c]
   uint32_t* Md = nullptr;
   uint32_t* MTd = nullptr;
-  // xlx[x] = x log2 x for x < kXlxTable (filled by fill_xlx_table)
+  // xlx[x] = x log2 x and xlx[kXlxTable + x] = log2 x for x < kXlxTable
+  // (filled by fill_xlx_table)
   double* xlx = nullptr;
 };
 

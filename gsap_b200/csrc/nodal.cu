@@ -99,6 +99,9 @@ struct Rows<false> {
   __device__ __forceinline__ uint32_t out_s(int c) const { return row_lookup(oc, on, sO0, sO1, c); }
   __device__ __forceinline__ uint32_t in_r(int c) const { return row_lookup(ic, inn, rI0, rI1, c); }
   __device__ __forceinline__ uint32_t in_s(int c) const { return row_lookup(ic, inn, sI0, sI1, c); }
+  __device__ __forceinline__ uint32_t out_at(bool row_s, int c) const {
+    return row_lookup(oc, on, row_s ? sO0 : rO0, row_s ? sO1 : rO1, c);
+  }
 };
 
 template <>
@@ -111,6 +114,9 @@ struct Rows<true> {
   __device__ __forceinline__ uint32_t out_s(int c) const { return __ldg(ors + c); }
   __device__ __forceinline__ uint32_t in_r(int c) const { return __ldg(irr + c); }
   __device__ __forceinline__ uint32_t in_s(int c) const { return __ldg(irs + c); }
+  __device__ __forceinline__ uint32_t out_at(bool row_s, int c) const {
+    return __ldg((row_s ? ors : orr) + c);
+  }
 };
 
 // Per-thread partial of a move's dS.  GSAP's seven terms (kernels.hpp:143-182,
@@ -175,11 +181,8 @@ __device__ __forceinline__ void corner_terms(const NodalArgs& a, const Rows<DENS
                                              int r, int s, uint32_t koR, uint32_t koS,
                                              uint32_t niR, uint32_t niS, Acc& q) {
   const int lane = threadIdx.x & 31;
-  uint32_t mm = 0u;
-  if (lane == 0) mm = R.out_r(r);
-  else if (lane == 1) mm = R.out_r(s);
-  else if (lane == 2) mm = R.out_s(r);
-  else if (lane == 3) mm = R.out_s(s);
+  // lane 0: M[r][r], 1: M[r][s], 2: M[s][r], 3: M[s][s]
+  const uint32_t mm = lane < 4 ? R.out_at((lane & 2) != 0, (lane & 1) ? s : r) : 0u;
   const uint32_t Mrr = __shfl_sync(kFull, mm, 0), Mrs = __shfl_sync(kFull, mm, 1);
   const uint32_t Msr = __shfl_sync(kFull, mm, 2), Mss = __shfl_sync(kFull, mm, 3);
   const uint32_t xrr = Mrr - koR - niR;
@@ -200,25 +203,29 @@ __device__ __forceinline__ void corner_terms(const NodalArgs& a, const Rows<DENS
   const long long mass7 = (long long)dis - (long long)Mrs - (long long)Mss + q.m7;
   const double ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
   const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s];
-  double t = 0.0;
+  // Straight-line, no lane branches: every lane evaluates the cell form and
+  // the row form of its operands and keeps the one its lane range owns.
   // lanes 0-3: old corner cells, + M log2 M; lanes 4-7: new corner cells,
-  // - g(x); lanes 8-11: + L mass of the four new rows; lane 12: old degrees
-  if (lane < 4) {
-    const uint32_t M = lane == 0 ? Mrr : lane == 1 ? Mrs : lane == 2 ? Msr : Mss;
-    if (M != 0u) t = xlx(a.xlx, M);
-  } else if (lane < 8) {
-    const bool on = lane == 4 ? Mrr != 0u : lane == 5 ? use_rs : lane == 6 ? Msr != 0u : use_ss;
-    const uint32_t x = lane == 4 ? xrr : lane == 5 ? xrs : lane == 6 ? xsr : xss;
-    const double ld = (lane == 4 || lane == 6) ? ldi_r : ldi_s;
-    if (on) t = -gterm(a.xlx, x, ld);
-  } else if (lane < 12) {
-    const long long mass = lane == 8 ? mass4 : lane == 9 ? mass5 : lane == 10 ? mass6 : mass7;
-    const uint32_t d = lane == 8 ? dor - kO : lane == 9 ? dos + kO : lane == 10 ? dir - kI : dis + kI;
-    if (mass != 0) t = log2((double)d) * (double)mass;
-  } else if (lane == 12) {
-    t = -((dor ? (double)dor * ldo_r : 0.0) + (dos ? (double)dos * ldo_s : 0.0) +
-          (dir ? (double)dir * ldi_r : 0.0) + (dis ? (double)dis * ldi_s : 0.0));
-  }
+  // - g(x); lanes 8-11: + L mass of the four new rows; lane 12: the old row
+  // degrees.
+  const int j = lane & 3;
+  const uint32_t Mold = j == 0 ? Mrr : j == 1 ? Mrs : j == 2 ? Msr : Mss;
+  const uint32_t xnew = j == 0 ? xrr : j == 1 ? xrs : j == 2 ? xsr : xss;
+  const bool on = j == 0 ? Mrr != 0u : j == 1 ? use_rs : j == 2 ? Msr != 0u : use_ss;
+  const double ld = (j & 1) ? ldi_s : ldi_r;
+  const bool old_cell = lane < 4;
+  const uint32_t X = old_cell ? Mold : xnew;
+  const bool cell_on = old_cell ? Mold != 0u : on;
+  const double cell = old_cell ? xlx(a.xlx, X) : -gterm(a.xlx, X, ld);
+  const long long mass = j == 0 ? mass4 : j == 1 ? mass5 : j == 2 ? mass6 : mass7;
+  const uint32_t d = j == 0 ? dor - kO : j == 1 ? dos + kO : j == 2 ? dir - kI : dis + kI;
+  const double row = mass != 0 ? l2x(a.xlx, d) * (double)mass : 0.0;
+  const double deg = -((dor ? (double)dor * ldo_r : 0.0) + (dos ? (double)dos * ldo_s : 0.0) +
+                       (dir ? (double)dir * ldi_r : 0.0) + (dis ? (double)dis * ldi_s : 0.0));
+  double t = 0.0;
+  if (lane < 8) t = cell_on ? cell : 0.0;
+  else if (lane < 12) t = row;
+  else if (lane == 12) t = deg;
   q.acc += t;
 }
 
@@ -592,7 +599,7 @@ __device__ __forceinline__ bool is_heavy(int no, int ni) {
 template <bool GIVEN, bool DENSE>
 struct NodalBody {
   using Args = NodalArgs;
-  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = 3;
+  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = DENSE ? 4 : 3;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
   if (ctl_stopped(a.ctl)) return;
