@@ -356,10 +356,10 @@ def arrivals(rate, count, seed):
     return t, sizes, which
 
 
-def serve_with_server(sbp, pool, t, sizes, which, local):
+def serve_with_server(sbp, pool, t, sizes, which, local, lanes=0):
     import threading as th
     lat = [None] * len(t)
-    with sbp.Server(device=local) as srv:
+    with sbp.Server(device=local, lanes=lanes) as srv:
         ids = [None] * len(t)
         t0 = time.perf_counter()
         done_flag = th.Event()
@@ -408,7 +408,7 @@ def run_served(args, rank, world, local, dist):
         for rate in args.rates:
             count = int(min(args.served_max, max(30, rate * args.served_seconds)))
             t, sizes, which = arrivals(rate, count, 100 + int(rate))
-            lat_s, span_s, st = serve_with_server(sbp, pool, t, sizes, which, local)
+            lat_s, span_s, st = serve_with_server(sbp, pool, t, sizes, which, local, args.lanes)
             lat_p, span_p = serve_one_at_a_time(sbp, pool, t, sizes, which, local)
             sel20 = sizes == 20000
             rows.append({
@@ -503,6 +503,7 @@ def main():
     ap.add_argument("--rates", type=float, nargs="+", default=[5.0, 20.0, 50.0, 100.0, 200.0])
     ap.add_argument("--served-seconds", type=float, default=6.0)
     ap.add_argument("--served-max", type=int, default=400)
+    ap.add_argument("--lanes", type=int, default=0, help="server lanes (0: the default)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":

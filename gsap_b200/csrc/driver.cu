@@ -135,8 +135,8 @@ void Job::release() {
     cudaSetDevice(cur);
     return;
   }
+  if (mem) cudaFreeAsync(mem, st);
   if (st) cudaStreamSynchronize(st);
-  if (mem) cudaFree(mem);
   if (fork) cudaEventDestroy(fork);
   if (join) cudaEventDestroy(join);
   fork = join = nullptr;
@@ -187,31 +187,36 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
   SBP_CUDA(cudaSetDevice(device));
   static std::once_flag once[64];
   if (device >= 0 && device < 64)
-    std::call_once(once[device], [] {
+    std::call_once(once[device], [device] {
       init_kernel_attributes();
       init_nodal_attributes();
+      // arenas come from the stream-ordered pool; freed ones stay in it, so
+      // repeated calls reuse device memory without allocating from the driver
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
     });
   const double* xlx = nullptr;
   sbp_status xs = device_xlx_table(device, &xlx);
   if (xs != SBP_OK) return xs;
   int32_t tiles = scan_tiles_cap(N);
   J.mem_bytes = job_bytes(N, E, np, max_itr, J.dense_cap);
-  cudaError_t ae = lean ? cudaMallocAsync(&J.mem, J.mem_bytes, engine_stream)
-                        : cudaMalloc(&J.mem, J.mem_bytes);
-  if (ae != cudaSuccess) {
+  if (lean) {
+    J.st = engine_stream;
+  } else {
+    SBP_CUDA(cudaStreamCreateWithFlags(&J.st, cudaStreamNonBlocking));
+    SBP_CUDA(cudaStreamCreateWithFlags(&J.side, cudaStreamNonBlocking));
+    SBP_CUDA(cudaEventCreateWithFlags(&J.fork, cudaEventDisableTiming));
+    SBP_CUDA(cudaEventCreateWithFlags(&J.join, cudaEventDisableTiming));
+  }
+  if (cudaMallocAsync(&J.mem, J.mem_bytes, J.st) != cudaSuccess) {
     cudaGetLastError();
     J.mem = nullptr;
     return fail(SBP_ERR_NOMEM, "device arena of " + std::to_string(J.mem_bytes) + " bytes");
   }
-  if (lean) {
-    J.pool_stream = engine_stream;
-    J.st = engine_stream;
-  } else {
-  SBP_CUDA(cudaStreamCreateWithFlags(&J.st, cudaStreamNonBlocking));
-  SBP_CUDA(cudaStreamCreateWithFlags(&J.side, cudaStreamNonBlocking));
-  SBP_CUDA(cudaEventCreateWithFlags(&J.fork, cudaEventDisableTiming));
-  SBP_CUDA(cudaEventCreateWithFlags(&J.join, cudaEventDisableTiming));
-  }
+  J.pool_stream = J.st;
   Arena A{(char*)J.mem, J.mem_bytes, 0};
   size_t n1 = (size_t)N + 1, e = (size_t)E > 0 ? (size_t)E : 1;
   DevGraph& g = J.g;
@@ -316,6 +321,9 @@ int resolve_device(int32_t d) {
 // (std::set, :58-68).  Returns the new block count.
 int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
                                  const double* best_dS, int32_t* map_out) {
+  // the targets come from the device: never index with one out of range
+  for (int32_t b = 0; b < B; ++b)
+    if (best[b] < 0 || best[b] >= B) return -1;
   std::vector<std::pair<uint64_t, int32_t>> key(B);
   for (int32_t b = 0; b < B; ++b) {
     double x = best_dS[b];
@@ -415,6 +423,7 @@ static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t se
   SBP_CUDA(cudaMemcpyAsync(J.h_best_dS, J.best_dS, 8 * (size_t)B, cudaMemcpyDeviceToHost, st));
   SBP_CUDA(cudaStreamSynchronize(st));
   int32_t nb = apply_merges_host(B, B_to_merge, J.h_best, J.h_best_dS, J.h_map);
+  if (nb < 0) return fail(SBP_ERR_INTERNAL, "merge target out of range");
   SBP_CUDA(cudaMemcpyAsync(J.map, J.h_map, 4 * (size_t)B, cudaMemcpyHostToDevice, st));
   relabel(J.part, J.N, J.map, st);
   B = nb;
@@ -438,6 +447,16 @@ static sbp_status job_for(Job& J, const sbp_graph_csr* g, int device, int32_t np
 
 // Validates the graph and the labels, then creates the job, uploads both
 // and builds the blockmodel of the labels.
+// Rebuild shape of the one-shot entry points: the defaults, or the one in
+// SBP_REBUILD_WARP_CAP / SBP_REBUILD_BIG_ENTRIES (tests check every shape
+// the autotuner may pick).
+static RebuildTune env_rebuild_shape() {
+  RebuildTune t;
+  if (const char* e = std::getenv("SBP_REBUILD_WARP_CAP")) t.warp_cap = std::atoi(e);
+  if (const char* e = std::getenv("SBP_REBUILD_BIG_ENTRIES")) t.big_entries = std::atoi(e);
+  return t;
+}
+
 static sbp_status prepare(Job& J, const sbp_graph_csr* g, const int32_t* part, int32_t B,
                           int32_t np, int32_t max_itr) {
   sbp_status s = validate_graph(g);
@@ -449,7 +468,7 @@ static sbp_status prepare(Job& J, const sbp_graph_csr* g, const int32_t* part, i
   s = job_upload(J, g);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaMemcpyAsync(J.part, part, 4 * (size_t)J.N, cudaMemcpyHostToDevice, J.st));
-  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st);
+  rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, J.st, env_rebuild_shape());
   if (is_dense(J, B)) dense_build(J.g, J.part, B, J.m, J.st);
   return SBP_OK;
 }

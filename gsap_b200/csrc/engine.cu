@@ -17,7 +17,7 @@
 // device-to-host copy, and the host synchronises once per tick.
 //
 // sbp_partition is a batch of one.  sbp_partition_batch and the server
-// (server.cpp) admit jobs against an HBM budget as earlier jobs finish.
+// (server.cu) admit jobs against an HBM budget as earlier jobs finish.
 #include "../../include/sbp.h"
 #include "common.cuh"
 #include "engine.h"
@@ -314,7 +314,7 @@ void Engine::add_run_work(Run& r) {
     const double mS = model_S(r.B, J.N, J.E);
     for (int32_t k = 0; k < r.sweep_k; ++k) {
       for (int32_t b = 0; b < nb; ++b) {
-        SweepSlots& s = sw[k * nb + b];
+        SweepSlots& s = sw[k * nb_slots_ + b];
         const uint32_t seq = r.seq_sweep0 + (uint32_t)b;  // + ctl[0] * nb on the device
         double* slot_sum = r.sweeps_only ? J.dsum + b : J.dsum;
         long long* slot_acc = r.sweeps_only ? J.acc + b : J.acc;
@@ -399,7 +399,18 @@ sbp_status Engine::launch_slot(Slot& s, size_t off, cudaStream_t stream) {
   return SBP_OK;
 }
 
+// Engines in different host threads (the server's lanes) hand their CUDA
+// calls to the driver one thread at a time; only the wait for a tick's end
+// runs outside this lock, so the lanes' device work still overlaps.
+// Concurrent launches from the lane threads corrupted kernel arguments in
+// the driver on this platform.
+std::mutex& cuda_submit_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+
 sbp_status Engine::tick() {
+  std::unique_lock<std::mutex> submit(cuda_submit_mutex());
   SBP_CUDA(cudaSetDevice(device));
   // runs that reach the outer-step limit stop at their next merge
   for (Run* r : runs) {
@@ -438,6 +449,7 @@ sbp_status Engine::tick() {
   if (s != SBP_OK) return s;
   // pass 2: records
   ensure_slots(k_max, nb_max);
+  nb_slots_ = nb_max;
   clear_slots();
   for (Run* r : runs) {
     if (r->stage == Run::kDone) continue;
@@ -561,7 +573,10 @@ sbp_status Engine::tick() {
   if (s != SBP_OK) return s;
   if (rd) SBP_CUDA(cudaMemcpyAsync(rd_host, rd_dev, rd, cudaMemcpyDeviceToHost, st));
   SBP_CUDA(cudaEventRecord(ev[3], st));
-  SBP_CUDA(cudaEventSynchronize(ev[3]));
+  submit.unlock();
+  const cudaError_t waited = cudaEventSynchronize(ev[3]);
+  submit.lock();
+  SBP_CUDA(waited);
   SBP_CUDA(cudaGetLastError());
   ++ticks;
   // phase times of this tick (shared by the runs that took part)
@@ -598,6 +613,11 @@ sbp_status Engine::tick() {
       const double* best_dS = (const double*)(rdp + align256(4 * (size_t)r->B));
       r->map.resize(r->B);
       const int32_t nb = apply_merges_host(r->B, r->B_to_merge, best, best_dS, r->map.data());
+      if (nb < 0) {
+        r->set_error(SBP_ERR_INTERNAL, "merge target out of range (B=" + std::to_string(r->B) +
+                                           ", N=" + std::to_string(J.N) + ")");
+        continue;
+      }
       ++r->seq;
       r->B = nb;
       r->csr_fresh = false;
@@ -733,9 +753,15 @@ sbp_graph_csr HostGraph::csr() const {
 }
 
 // ------------------------------------------------------------- Scheduler --
-sbp_status Scheduler::init(int device, uint64_t hbm_budget, int32_t max_active_jobs) {
+sbp_status Scheduler::init(int device, uint64_t hbm_budget, int32_t max_active_jobs,
+                           std::shared_ptr<HbmBudget> shared) {
   sbp_status s = eng.init(device);
   if (s != SBP_OK) return s;
+  max_active = max_active_jobs;
+  if (shared) {
+    hbm = shared;
+    return SBP_OK;
+  }
   // job arenas come from the stream-ordered pool; keep freed memory in it
   cudaMemPool_t pool;
   SBP_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
@@ -746,8 +772,8 @@ sbp_status Scheduler::init(int device, uint64_t hbm_budget, int32_t max_active_j
     SBP_CUDA(cudaMemGetInfo(&free_b, &total_b));
     hbm_budget = (uint64_t)(0.9 * (double)free_b);
   }
-  budget = hbm_budget;
-  max_active = max_active_jobs;
+  hbm = std::make_shared<HbmBudget>();
+  hbm->cap = (double)hbm_budget;
   return SBP_OK;
 }
 
@@ -758,17 +784,18 @@ static size_t run_bytes(const Run& r) {
 }
 
 sbp_status Scheduler::admit(std::vector<Run*>& done) {
+  std::lock_guard<std::mutex> submit(cuda_submit_mutex());
   while (queued() > 0) {
     Run* r = queue[queue_head];
     if (max_active > 0 && (int32_t)eng.runs.size() >= max_active) break;
     const double bytes = (double)run_bytes(*r);
-    if (bytes > (double)budget) {
+    if (bytes > hbm->cap) {
       ++queue_head;
       r->set_error(SBP_ERR_BUDGET, "job arena exceeds the HBM budget");
       done.push_back(r);
       continue;
     }
-    if (used + bytes > (double)budget) break;  // waits for running jobs, in order
+    if (!hbm->take(bytes)) break;  // waits for running jobs, in order
     ++queue_head;
     r->owned.reset(new Job());
     r->J = r->owned.get();
@@ -777,6 +804,7 @@ sbp_status Scheduler::admit(std::vector<Run*>& done) {
                               r->o.max_nodal_itr, r->o.dense_max, true, eng.st);
     if (s == SBP_OK) s = job_upload(*r->J, &g);
     if (s != SBP_OK) {
+      hbm->give(bytes);
       r->set_error(s, sbp_last_error());
       r->owned.reset();
       r->J = nullptr;
@@ -787,8 +815,6 @@ sbp_status Scheduler::admit(std::vector<Run*>& done) {
     r->t_admit_ms = now_ms();
     r->start_partition();
     eng.runs.push_back(r);
-    used += bytes;
-    peak = std::max(peak, used);
     max_active_seen = std::max(max_active_seen, (int32_t)eng.runs.size());
   }
   if (queue_head > 1024 && queue_head * 2 > queue.size()) {
@@ -804,6 +830,7 @@ sbp_status Scheduler::step(std::vector<Run*>& done) {
   if (eng.runs.empty()) return SBP_OK;
   s = eng.tick();
   if (s != SBP_OK) return s;
+  std::lock_guard<std::mutex> submit(cuda_submit_mutex());
   std::vector<Run*> keep;
   keep.reserve(eng.runs.size());
   for (Run* r : eng.runs) {
@@ -812,7 +839,7 @@ sbp_status Scheduler::step(std::vector<Run*>& done) {
       continue;
     }
     r->t_done_ms = now_ms();
-    used -= r->admit_bytes;
+    hbm->give(r->admit_bytes);
     r->owned.reset();  // arena back to the pool, in stream order
     r->J = nullptr;
     done.push_back(r);
@@ -824,6 +851,7 @@ sbp_status Scheduler::step(std::vector<Run*>& done) {
 Scheduler::~Scheduler() {
   // active jobs give their arenas back while the engine's stream exists
   for (Run* r : eng.runs) {
+    if (hbm) hbm->give(r->admit_bytes);
     r->owned.reset();
     r->J = nullptr;
   }
@@ -996,7 +1024,7 @@ extern "C" sbp_status sbp_partition_batch(const sbp_graph_csr* graphs, int32_t c
     batch->ticks = sch.eng.ticks;
     batch->kernel_launches = g_launches - l0;
     batch->ms_device = sch.eng.device_ms();
-    batch->peak_bytes = sch.peak;
+    batch->peak_bytes = sch.hbm->peak;
     batch->ms_total = t.ms();
   }
   if (first != SBP_OK) return fail(first, first_msg);

@@ -5,7 +5,9 @@
 #include "job.h"
 #include "kernels.h"
 
+#include <algorithm>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -13,6 +15,9 @@ namespace sbp {
 
 // Host clock in milliseconds (steady).
 double now_ms();
+
+// Serialises the CUDA calls of engines that run in different host threads.
+std::mutex& cuda_submit_mutex();
 
 // A graph held on the host by the engine (server requests are copied).
 struct HostGraph {
@@ -121,6 +126,7 @@ class Engine {
   void *up_host = nullptr, *up_dev = nullptr, *desc_host = nullptr, *desc_dev = nullptr;
   void *rd_host = nullptr, *rd_dev = nullptr;
   size_t up_cap = 0, desc_cap = 0, rd_cap = 0;
+  int nb_slots_ = 0;  // batch positions per queued sweep in this tick's slots
 
   void* up_dev_ptr(size_t off) { return (char*)up_dev + off; }
   void* rd_dev_ptr(size_t off) { return (char*)rd_dev + off; }
@@ -130,23 +136,43 @@ class Engine {
   sbp_status launch_slot(Slot& s, size_t off, cudaStream_t stream);
 };
 
+// Device bytes of admitted job arenas against a cap; shared by the
+// schedulers of one server.
+struct HbmBudget {
+  std::mutex mu;
+  double cap = 0.0, used = 0.0, peak = 0.0;
+  bool take(double bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    if (used + bytes > cap) return false;
+    used += bytes;
+    peak = std::max(peak, used);
+    return true;
+  }
+  void give(double bytes) {
+    std::lock_guard<std::mutex> lk(mu);
+    used -= bytes;
+  }
+};
+
 // Admission against an HBM budget in front of an engine (batched calls and
 // the server): queued runs join the engine in order while their arenas fit.
 class Scheduler {
  public:
   Engine eng;
-  uint64_t budget = 0;
+  std::shared_ptr<HbmBudget> hbm;
   int32_t max_active = 0;
   std::vector<Run*> queue;  // waiting, in arrival order (front = next)
   size_t queue_head = 0;
-  double used = 0.0, peak = 0.0;
   int32_t max_active_seen = 0;
 
   Scheduler() = default;
   Scheduler(const Scheduler&) = delete;
   Scheduler& operator=(const Scheduler&) = delete;
   ~Scheduler();
-  sbp_status init(int device, uint64_t hbm_budget, int32_t max_active_jobs);
+  // hbm_budget 0: 90% of the device's free memory.  `shared` (optional)
+  // is a budget other schedulers also draw on; it is then used as is.
+  sbp_status init(int device, uint64_t hbm_budget, int32_t max_active_jobs,
+                  std::shared_ptr<HbmBudget> shared = nullptr);
   void enqueue(Run* r) { queue.push_back(r); }
   size_t queued() const { return queue.size() - queue_head; }
   bool idle() const { return queued() == 0 && eng.runs.empty(); }

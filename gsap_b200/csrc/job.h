@@ -88,6 +88,7 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
 sbp_status job_upload(Job& J, const sbp_graph_csr* h);
 // The process-wide x log2 x table of a device (filled once).
 sbp_status device_xlx_table(int device, const double** out);
+// Returns the new block count, or -1 when a target lies outside [0, B).
 int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
                           const double* best_dS, int32_t* map_out);
 double model_S(int32_t B, int32_t N, int32_t E);

@@ -1,13 +1,17 @@
-// The partition server: a host thread that keeps a Scheduler (engine.cu)
+// The partition server: host threads that keep Schedulers (engine.cu)
 // running while requests arrive.
 //
 // Continuous batching: a request is admitted as soon as the HBM budget and
-// the active-job limit allow and joins the engine at its next tick, next to
-// the jobs already on the device; a finished job leaves at the end of its
-// tick and its arena goes back to the stream-ordered pool.  Each tick is one
-// step (a merge step or a nodal sweep) of every active job, issued as
-// multi-job launches, so requests that arrive while others run share the
-// device with them instead of waiting for them.
+// the active-job limit allow and joins its lane's engine at the next tick,
+// next to the jobs already on the device; a finished job leaves at the end
+// of its tick and its arena goes back to the stream-ordered pool.  Each tick
+// is one step (a merge step or queued nodal sweeps) of every active job of
+// the lane, issued as multi-job launches.
+//
+// Lanes: a tick lasts as long as its largest job's step, so requests are
+// split by graph size into lanes, each with its own engine, stream and host
+// thread, all drawing on one HBM budget.  The GPU runs the lanes' launches
+// side by side, and a small request's steps do not wait for a large one's.
 #include "../../include/sbp.h"
 #include "engine.h"
 #include "job.h"
@@ -19,21 +23,38 @@
 #include <thread>
 #include <unordered_map>
 
-struct sbp_server {
+namespace {
+
+struct Lane {
   sbp::Scheduler sch;
+  std::thread th;
+  std::deque<sbp::Run*> inbox;  // submitted to this lane, not yet queued
+  int32_t active = 0, queued = 0, max_active_seen = 0;
+  int64_t ticks = 0;
+};
+
+}  // namespace
+
+struct sbp_server {
   sbp_server_options opt{};
   int device = 0;
-  std::thread th;
+  int32_t split = 10000;
+  std::shared_ptr<sbp::HbmBudget> hbm;
+  std::vector<std::unique_ptr<Lane>> lanes;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<sbp::Run*> inbox;                                  // submitted, not yet queued
   std::unordered_map<int64_t, std::unique_ptr<sbp::Run>> live;  // every uncollected request
   int64_t next_id = 0;
   bool stop = false;
   sbp_status thread_status = SBP_OK;
   std::string thread_error;
-  sbp_server_stats stats{};
-  void loop();
+  int64_t completed = 0, failed = 0, submitted = 0;
+  void loop(Lane& L);
+  int32_t queued_total() const {
+    int32_t q = 0;
+    for (const auto& l : lanes) q += l->queued + (int32_t)l->inbox.size();
+    return q;
+  }
 };
 
 namespace {
@@ -47,64 +68,64 @@ void finish_run(sbp::Run& r) {
 
 }  // namespace
 
-void sbp_server::loop() {
+void sbp_server::loop(Lane& L) {
   cudaSetDevice(device);
+  sbp::Scheduler& sch = L.sch;
   std::vector<sbp::Run*> done;
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(mu);
-      cv_work.wait(lk, [&] { return stop || !inbox.empty() || !sch.idle(); });
+      cv_work.wait(lk, [&] { return stop || !L.inbox.empty() || !sch.idle(); });
       if (stop) {
         // cancel what has not reached the device
-        for (sbp::Run* r : inbox) r->set_error(SBP_ERR_CANCELLED, "server stopped");
-        for (size_t i = sch.queue_head; i < sch.queue.size(); ++i)
-          sch.queue[i]->set_error(SBP_ERR_CANCELLED, "server stopped");
-        for (sbp::Run* r : inbox) {
-          r->t_done_ms = sbp::now_ms();
+        const double t = sbp::now_ms();
+        for (sbp::Run* r : L.inbox) {
+          r->set_error(SBP_ERR_CANCELLED, "server stopped");
+          r->t_done_ms = t;
           finish_run(*r);
         }
         for (size_t i = sch.queue_head; i < sch.queue.size(); ++i) {
-          sch.queue[i]->t_done_ms = sbp::now_ms();
+          sch.queue[i]->set_error(SBP_ERR_CANCELLED, "server stopped");
+          sch.queue[i]->t_done_ms = t;
           finish_run(*sch.queue[i]);
         }
-        inbox.clear();
+        L.inbox.clear();
         sch.queue_head = sch.queue.size();
         cv_done.notify_all();
         if (sch.eng.runs.empty()) break;
       }
-      while (!inbox.empty()) {
-        sch.enqueue(inbox.front());
-        inbox.pop_front();
+      while (!L.inbox.empty()) {
+        sch.enqueue(L.inbox.front());
+        L.inbox.pop_front();
       }
     }
     done.clear();
     sbp_status s = sch.step(done);
     std::lock_guard<std::mutex> lk(mu);
     if (s != SBP_OK) {
-      // an engine failure ends every job on the device
+      // an engine failure ends every job of the lane that is on the device
       thread_status = s;
       thread_error = sbp_last_error();
+      std::lock_guard<std::mutex> submit(sbp::cuda_submit_mutex());
       for (sbp::Run* r : sch.eng.runs) {
         r->set_error(s, thread_error);
+        sch.hbm->give(r->admit_bytes);
         r->owned.reset();
         r->J = nullptr;
         r->t_done_ms = sbp::now_ms();
         done.push_back(r);
       }
       sch.eng.runs.clear();
-      sch.used = 0.0;
     }
     for (sbp::Run* r : done) {
       finish_run(*r);
-      ++stats.completed;
-      if (r->status != SBP_OK) ++stats.failed;
+      ++completed;
+      if (r->status != SBP_OK) ++failed;
     }
-    stats.active = (int32_t)sch.eng.runs.size();
-    stats.queued = (int32_t)(sch.queued() + inbox.size());
-    stats.max_active_seen = sch.max_active_seen;
-    stats.ticks = sch.eng.ticks;
-    stats.bytes_active = sch.used;
-    stats.peak_bytes = sch.peak;
+    L.active = (int32_t)sch.eng.runs.size();
+    L.queued = (int32_t)sch.queued();
+    L.max_active_seen = sch.max_active_seen;
+    L.ticks = sch.eng.ticks;
     if (!done.empty()) cv_done.notify_all();
   }
 }
@@ -117,6 +138,8 @@ void sbp_server_default_options(sbp_server_options* o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
   sbp_default_options(&o->partition);
+  o->lanes = 2;
+  o->lane_split = 10000;
 }
 
 sbp_status sbp_server_create(const sbp_server_options* o, sbp_server** out) {
@@ -124,13 +147,23 @@ sbp_status sbp_server_create(const sbp_server_options* o, sbp_server** out) {
   *out = nullptr;
   sbp_status s = check_options(&o->partition);
   if (s != SBP_OK) return s;
+  if (o->lanes < 0 || o->lanes > 8) return fail(SBP_ERR_INVALID, "lanes must be in [0, 8]");
   std::unique_ptr<sbp_server> h(new (std::nothrow) sbp_server());
   if (!h) return fail(SBP_ERR_NOMEM, "host allocation");
   h->opt = *o;
   h->device = resolve_device(o->partition.device);
-  s = h->sch.init(h->device, o->hbm_budget, o->max_active);
-  if (s != SBP_OK) return s;
-  h->th = std::thread([p = h.get()] { p->loop(); });
+  h->split = o->lane_split > 0 ? o->lane_split : 10000;
+  const int nl = o->lanes > 0 ? o->lanes : 2;
+  for (int i = 0; i < nl; ++i) {
+    h->lanes.emplace_back(new Lane());
+    s = h->lanes.back()->sch.init(h->device, o->hbm_budget, o->max_active, h->hbm);
+    if (s != SBP_OK) return s;
+    if (!h->hbm) h->hbm = h->lanes.back()->sch.hbm;
+  }
+  for (auto& l : h->lanes) {
+    Lane* lp = l.get();
+    l->th = std::thread([p = h.get(), lp] { p->loop(*lp); });
+  }
   *out = h.release();
   return SBP_OK;
 }
@@ -143,8 +176,7 @@ sbp_status sbp_server_submit(sbp_server* srv, const sbp_graph_csr* g, uint64_t s
   const sbp_options& po = srv->opt.partition;
   const double bytes = (double)job_bytes(g->N, g->E, po.num_proposals, po.max_nodal_itr,
                                          std::max(0, std::min(g->N, po.dense_max)));
-  if (bytes > (double)srv->sch.budget)
-    return fail(SBP_ERR_BUDGET, "job arena exceeds the HBM budget");
+  if (bytes > srv->hbm->cap) return fail(SBP_ERR_BUDGET, "job arena exceeds the HBM budget");
   std::unique_ptr<Run> r(new Run());
   r->graph_copy.assign(*g);
   r->graph_view = r->graph_copy.csr();
@@ -154,17 +186,19 @@ sbp_status sbp_server_submit(sbp_server* srv, const sbp_graph_csr* g, uint64_t s
   r->labels_store.assign((size_t)g->N, 0);
   r->labels_out = r->labels_store.data();
   r->t_submit_ms = now_ms();
+  // lane 0 takes the smallest graphs, each further lane sizes up to 4x more
+  size_t lane = 0;
+  for (int64_t lim = srv->split; lane + 1 < srv->lanes.size() && g->N > lim; lim *= 4) ++lane;
   std::lock_guard<std::mutex> lk(srv->mu);
   if (srv->stop) return fail(SBP_ERR_CANCELLED, "server stopped");
-  if (srv->opt.max_queued > 0 &&
-      (int64_t)(srv->inbox.size() + srv->stats.queued) >= srv->opt.max_queued)
+  if (srv->opt.max_queued > 0 && srv->queued_total() >= srv->opt.max_queued)
     return fail(SBP_ERR_BUSY, "request queue is full");
   r->id = srv->next_id++;
   *id = r->id;
-  srv->inbox.push_back(r.get());
+  srv->lanes[lane]->inbox.push_back(r.get());
   srv->live[r->id] = std::move(r);
-  ++srv->stats.submitted;
-  srv->cv_work.notify_one();
+  ++srv->submitted;
+  srv->cv_work.notify_all();
   return SBP_OK;
 }
 
@@ -174,6 +208,8 @@ sbp_status sbp_server_poll(sbp_server* srv, int64_t id, int32_t timeout_ms, int3
   std::unique_lock<std::mutex> lk(srv->mu);
   auto it = srv->live.find(id);
   if (it == srv->live.end()) return fail(SBP_ERR_NOT_FOUND, "unknown request id");
+  // the Run stays put while the map may rehash (submits during the wait
+  // below): keep the pointer, never the iterator
   Run* r = it->second.get();
   if (!r->finished) {
     if (timeout_ms == 0) return fail(SBP_ERR_BUSY, "request still running");
@@ -192,7 +228,7 @@ sbp_status sbp_server_poll(sbp_server* srv, int64_t id, int32_t timeout_ms, int3
   }
   const sbp_status st = r->status;
   const std::string msg = r->error;
-  srv->live.erase(it);
+  srv->live.erase(id);
   if (st != SBP_OK) return fail(st, msg);
   return SBP_OK;
 }
@@ -200,7 +236,21 @@ sbp_status sbp_server_poll(sbp_server* srv, int64_t id, int32_t timeout_ms, int3
 sbp_status sbp_server_stats_get(sbp_server* srv, sbp_server_stats* out) {
   if (!srv || !out) return fail(SBP_ERR_INVALID, "bad arguments");
   std::lock_guard<std::mutex> lk(srv->mu);
-  *out = srv->stats;
+  std::memset(out, 0, sizeof(*out));
+  out->submitted = srv->submitted;
+  out->completed = srv->completed;
+  out->failed = srv->failed;
+  for (const auto& l : srv->lanes) {
+    out->active += l->active;
+    out->queued += l->queued + (int32_t)l->inbox.size();
+    out->max_active_seen += l->max_active_seen;
+    out->ticks += l->ticks;
+  }
+  {
+    std::lock_guard<std::mutex> lb(srv->hbm->mu);
+    out->bytes_active = srv->hbm->used;
+    out->peak_bytes = srv->hbm->peak;
+  }
   if (srv->thread_status != SBP_OK) return fail(srv->thread_status, srv->thread_error);
   return SBP_OK;
 }
@@ -212,7 +262,8 @@ sbp_status sbp_server_destroy(sbp_server* srv) {
     srv->stop = true;
   }
   srv->cv_work.notify_all();
-  if (srv->th.joinable()) srv->th.join();
+  for (auto& l : srv->lanes)
+    if (l->th.joinable()) l->th.join();
   delete srv;
   return SBP_OK;
 }

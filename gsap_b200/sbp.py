@@ -75,7 +75,7 @@ class BatchReport(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("partition", Options), ("hbm_budget", C.c_uint64), ("max_active", C.c_int32),
-                ("max_queued", C.c_int32)]
+                ("max_queued", C.c_int32), ("lanes", C.c_int32), ("lane_split", C.c_int32)]
 
 
 class JobTimes(C.Structure):
@@ -335,13 +335,15 @@ class Server:
     """sbp_server_*: a partition server with continuous batching on the device."""
 
     def __init__(self, options: Optional[Options] = None, hbm_budget=0, max_active=0,
-                 max_queued=0, **kw):
+                 max_queued=0, lanes=0, lane_split=0, **kw):
         so = ServerOptions()
         _lib.sbp_server_default_options(C.byref(so))
         so.partition = options or default_options(**kw)
         so.hbm_budget = hbm_budget
         so.max_active = max_active
         so.max_queued = max_queued
+        so.lanes = lanes
+        so.lane_split = lane_split
         self.h = _vp()
         self._n = {}
         _check(_lib.sbp_server_create(C.byref(so), C.byref(self.h)))

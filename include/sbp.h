@@ -156,16 +156,21 @@ sbp_status sbp_partition_batch(const sbp_graph_csr* graphs, int32_t count, const
  * is copied, the caller may free it on return) and admitted in arrival order
  * as soon as the active jobs' device arenas leave room for them under the
  * HBM budget; admitted jobs join the running engine at its next tick, so
- * jobs that arrive while others run overlap on the device with them.  Each
- * job keeps its graph, blockmodel, labels and RNG state resident until it
- * finishes; its result is the same bits as sbp_partition alone. */
+ * jobs that arrive while others run overlap on the device with them.  Small
+ * and large graphs run in separate lanes (engines with their own stream and
+ * host thread, one shared budget), so a small job's steps do not wait for a
+ * large job's.  Each job keeps its graph, blockmodel, labels and RNG state
+ * resident until it finishes; its result is the same bits as sbp_partition
+ * alone. */
 typedef struct sbp_server sbp_server;
 
 typedef struct sbp_server_options {
   sbp_options partition;    /* loop options of every job (seed per request) */
   uint64_t hbm_budget;      /* bytes of job arenas at once (0: 90% of free memory) */
-  int32_t max_active;       /* jobs on the device at once (0: no limit) */
+  int32_t max_active;       /* jobs on the device at once, per lane (0: no limit) */
   int32_t max_queued;       /* queued requests before submit says BUSY (0: no limit) */
+  int32_t lanes;            /* engines by graph size, each on its own stream (0: 2) */
+  int32_t lane_split;       /* graphs of N <= lane_split go to the small lane (0: 10000) */
 } sbp_server_options;
 
 typedef struct sbp_job_times {

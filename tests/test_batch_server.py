@@ -89,9 +89,48 @@ def test_server_mix_equals_solo(sbp, solo):
         assert times["ms_queue"] >= 0.0
 
 
+def test_server_lanes_equal_solo(sbp, solo):
+    # a low split spreads the requests over three lanes (engines on their
+    # own streams and threads); every result is still the job alone
+    gs, seeds, ref = solo
+    with sbp.Server(lanes=3, lane_split=1500) as srv:
+        ids = [srv.submit(g, s) for g, s in zip(gs, seeds)]
+        res = [srv.poll(j, timeout_ms=-1) for j in ids]
+        st = srv.stats()
+    assert st["completed"] == len(gs) and st["failed"] == 0
+    for i, (lab, rep, _) in enumerate(res):
+        _same(lab, rep, *ref[i])
+
+
+def test_server_submit_while_polling(sbp, solo):
+    # a poll that waits while new requests arrive (the request table grows
+    # under it) still returns the right job
+    import threading
+    import time
+    gs, seeds, ref = solo
+    with sbp.Server() as srv:
+        ids = [None] * 40
+        out = [None] * 40
+
+        def collect():
+            for i in range(40):
+                while ids[i] is None:
+                    time.sleep(0.0002)
+                out[i] = srv.poll(ids[i], timeout_ms=-1)
+
+        th = threading.Thread(target=collect)
+        th.start()
+        for i in range(40):
+            k = i % len(gs)
+            ids[i] = srv.submit(gs[k], seeds[k])
+        th.join()
+    for i in range(40):
+        _same(out[i][0], out[i][1], *ref[i % len(gs)])
+
+
 def test_server_one_at_a_time(sbp, solo):
     gs, seeds, ref = solo
-    with sbp.Server(max_active=1) as srv:
+    with sbp.Server(max_active=1, lanes=1) as srv:
         ids = [srv.submit(g, s) for g, s in zip(gs, seeds)]
         res = [srv.poll(j, timeout_ms=-1) for j in ids]
         assert srv.stats()["max_active_seen"] == 1

@@ -60,6 +60,30 @@ def test_blockmodel_long_rows(sbp, orc):
             assert np.array_equal(a[k], b[k]), k
 
 
+@pytest.fixture(scope="module")
+def big_graph(sbp):
+    return sbp.dcsbm_variant("HH", 50000, 96, seed=5)
+
+
+@pytest.mark.parametrize("warp_cap", [32, 64, 128, 256])
+@pytest.mark.parametrize("big_entries", [512, 2048])
+def test_blockmodel_every_rebuild_shape(sbp, orc, big_graph, warp_cap, big_entries,
+                                        monkeypatch):
+    # the autotuner picks among these launch shapes by timing; each must
+    # build the same blockmodel, at the block counts the loop passes through
+    monkeypatch.setenv("SBP_REBUILD_WARP_CAP", str(warp_cap))
+    monkeypatch.setenv("SBP_REBUILD_BIG_ENTRIES", str(big_entries))
+    g = big_graph
+    rng = np.random.default_rng(warp_cap + big_entries)
+    for B in (32500, 21000, 13700, 8900, 5800, 96):
+        p = rng.integers(0, B, g.N).astype(np.int32)
+        p[:B] = np.arange(B, dtype=np.int32)
+        a = sbp.build_blockmodel(g, p, B)
+        b = orc.build_blockmodel(g, p, B)
+        for k in ("optr", "ocol", "ocnt", "iptr", "icol", "icnt", "d_out", "d_in"):
+            assert np.array_equal(a[k], b[k]), (B, k)
+
+
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_nodal_delta(sbp, orc, case):
     _, g, p, B = case
