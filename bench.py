@@ -188,6 +188,8 @@ def run_ours(args, rank, world, local, dist):
     g = make_graph(sbp)
     rg = sbp.ResidentGraph(g, device=local)
     opts = dict(device=local)
+    if args.graphs is not None:
+        opts["use_graphs"] = args.graphs
     for i in range(args.warmup):
         rg.partition(seed=1000 + i, **opts)
     reports, labels = [], None
@@ -254,6 +256,8 @@ def run_ours(args, rank, world, local, dist):
         "gpu_launches": int(tot["kernel_launches"]),
         "phases_ms_per_step": {k: tot[k] / K for k in ("ms_merge", "ms_nodal", "ms_rebuild",
                                                         "ms_nodal_kernel")},
+        "cuda_graphs": {"captures": int(sum(r.get("graph_captures", 0) for r in reports)),
+                        "replays": int(sum(r.get("graph_replays", 0) for r in reports))},
         "nodal_moves_per_s": tot["nodal_proposals"] / (tot["ms_nodal"] / 1000.0),
         "quality": {"B": rep["B"], "S": rep["S"], "recall": rec, "precision": prec, "nmi": nmi},
         "clocks": clk.summary(),
@@ -504,6 +508,8 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=6.0)
     ap.add_argument("--served-max", type=int, default=400)
     ap.add_argument("--lanes", type=int, default=0, help="server lanes (0: the default)")
+    ap.add_argument("--graphs", type=int, default=None,
+                    help="capture sweep ticks as CUDA graphs (default: the library's)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":

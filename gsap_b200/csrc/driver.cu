@@ -508,7 +508,7 @@ void sbp_default_options(sbp_options* o) {
   o->window = 3;
   o->max_outer = 1000;
   o->device = -1;
-  o->use_graphs = 0;
+  o->use_graphs = 1;
   o->verbose = 0;
   o->dense_max = 4096;
 }

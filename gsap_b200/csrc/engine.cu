@@ -179,6 +179,7 @@ Engine::~Engine() {
   cudaFreeHost(up_host);
   cudaFreeHost(desc_host);
   cudaFreeHost(rd_host);
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
   for (cudaEvent_t e : ev) cudaEventDestroy(e);
   if (ev_first) cudaEventDestroy(ev_first);
   if (fork) cudaEventDestroy(fork);
@@ -420,6 +421,10 @@ sbp_status Engine::tick() {
       r->stage = Run::kFinish;
     }
   }
+  // graphs only when every active run asks for them
+  use_graphs = true;
+  for (Run* r : runs)
+    if (r->stage != Run::kDone && !r->o.use_graphs) use_graphs = false;
   // pass 1: sweeps to queue, uploads (maps, heavy lists) and readbacks
   size_t up = 0, rd = 0;
   int nb_max = 0, k_max = 0;
@@ -535,39 +540,121 @@ sbp_status Engine::tick() {
   s = emit_until(&m_delta);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaEventRecord(ev[2], st));
-  for (int k = 0; k < k_max; ++k) {
-    for (int b = 0; b < nb_max; ++b) {
-      SweepSlots& w = sw[k * nb_max + b];
-      cudaEvent_t* be = &ev[4 + 5 * (k * nb_max + b)];
-      SBP_CUDA(cudaEventRecord(be[0], st));
-      s = emit_until(&w.bt_dense);
-      if (s != SBP_OK) return s;
-      SBP_CUDA(cudaEventRecord(be[1], st));
-      const bool heavy = !w.heavy_csr.empty() || !w.heavy_dense.empty();
-      if (heavy) {
-        // heavy vertices on the side stream, next to the warp kernels
-        SBP_CUDA(cudaEventRecord(fork, st));
-        SBP_CUDA(cudaStreamWaitEvent(side, fork, 0));
-        s = launch_slot(w.heavy_csr, slot_off(&w.heavy_csr), side);
-        if (s != SBP_OK) return s;
-        s = launch_slot(w.heavy_dense, slot_off(&w.heavy_dense), side);
-        if (s != SBP_OK) return s;
-        SBP_CUDA(cudaEventRecord(join, side));
+  // the queued sweeps; timing events are external records so that they
+  // also time a replayed graph
+  const size_t sweep_first = i;
+  bool capturing = false;
+  auto record = [&](cudaEvent_t e) {
+    return capturing ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal)
+                     : cudaEventRecord(e, st);
+  };
+  auto issue_sweeps = [&]() -> sbp_status {
+    for (int k = 0; k < k_max; ++k) {
+      for (int b = 0; b < nb_max; ++b) {
+        SweepSlots& w = sw[k * nb_max + b];
+        cudaEvent_t* be = &ev[4 + 5 * (k * nb_max + b)];
+        SBP_CUDA(record(be[0]));
+        sbp_status q = emit_until(&w.bt_dense);
+        if (q != SBP_OK) return q;
+        SBP_CUDA(record(be[1]));
+        const bool heavy = !w.heavy_csr.empty() || !w.heavy_dense.empty();
+        if (heavy) {
+          // heavy vertices on the side stream, next to the warp kernels
+          SBP_CUDA(cudaEventRecord(fork, st));
+          SBP_CUDA(cudaStreamWaitEvent(side, fork, 0));
+          q = launch_slot(w.heavy_csr, slot_off(&w.heavy_csr), side);
+          if (q != SBP_OK) return q;
+          q = launch_slot(w.heavy_dense, slot_off(&w.heavy_dense), side);
+          if (q != SBP_OK) return q;
+          SBP_CUDA(cudaEventRecord(join, side));
+        }
+        i += 2;  // the heavy slots
+        q = emit_until(&w.nodal_dense);
+        if (q != SBP_OK) return q;
+        if (heavy) SBP_CUDA(cudaStreamWaitEvent(st, join, 0));
+        SBP_CUDA(record(be[2]));
+        q = emit_until(&w.commit);
+        if (q != SBP_OK) return q;
+        SBP_CUDA(record(be[3]));
+        q = emit_until(w.rebuild.all().back());
+        if (q != SBP_OK) return q;
+        SBP_CUDA(record(be[4]));
       }
-      i += 2;  // the heavy slots
-      s = emit_until(&w.nodal_dense);
-      if (s != SBP_OK) return s;
-      if (heavy) SBP_CUDA(cudaStreamWaitEvent(st, join, 0));
-      SBP_CUDA(cudaEventRecord(be[2], st));
-      s = emit_until(&w.commit);
-      if (s != SBP_OK) return s;
-      SBP_CUDA(cudaEventRecord(be[3], st));
-      s = emit_until(w.rebuild.all().back());
-      if (s != SBP_OK) return s;
-      SBP_CUDA(cudaEventRecord(be[4], st));
+      sbp_status q = emit_until(&ends[k].ctl);
+      if (q != SBP_OK) return q;
     }
-    s = emit_until(&ends[k].ctl);
+    return SBP_OK;
+  };
+  // A tick of queued sweeps only (no pending build, copy or merge) is one
+  // CUDA graph: its launches and arguments repeat tick after tick within an
+  // outer step (RNG sequence and result slots come from the device-side
+  // sweep control), so it is captured once and replayed; a changed step
+  // (new B) updates the executable graph in place.
+  bool graphable = use_graphs && k_max > 0;
+  for (size_t q = 0; q < sweep_first && graphable; ++q)
+    if (!order[q]->empty()) graphable = false;
+  if (!graphable) {
+    s = issue_sweeps();
     if (s != SBP_OK) return s;
+  } else {
+    uint64_t key = 1469598103934665603ull;  // FNV-1a over the sweeps' launches
+    auto mix = [&](const void* p, size_t n) {
+      const unsigned char* c = (const unsigned char*)p;
+      for (size_t x = 0; x < n; ++x) key = (key ^ c[x]) * 1099511628211ull;
+    };
+    mix(&k_max, sizeof(k_max));
+    mix(&nb_max, sizeof(nb_max));
+    for (size_t q = sweep_first; q < order.size(); ++q) {
+      const Slot* x = order[q];
+      if (x == &s_gather || x->empty()) continue;
+      mix(&q, sizeof(q));
+      mix(&x->k, sizeof(x->k));
+      mix(x->recs.data(), x->recs.size());
+      mix(x->cta0.data(), 4 * x->cta0.size());
+      mix(&off[q], sizeof(off[q]));
+    }
+    mix(&desc_dev, sizeof(desc_dev));
+    if (graph_exec && key == graph_key) {
+      // replay: skip the slots the graph holds
+      i = sweep_first;
+      while (i < order.size() && order[i] != &s_gather) ++i;
+      ++graph_replays;
+      g_launches += graph_kernels;
+    } else {
+      SBP_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const long long l0 = g_launches;
+      capturing = true;
+      sbp_status q = issue_sweeps();
+      capturing = false;
+      graph_kernels = g_launches - l0;
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      if (q != SBP_OK) {
+        if (g) cudaGraphDestroy(g);
+        return q;
+      }
+      if (ce != cudaSuccess) return fail(SBP_ERR_CUDA, cudaGetErrorString(ce));
+      if (graph_exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(graph_exec, g, &info) != cudaSuccess) {
+          cudaGetLastError();
+          cudaGraphExecDestroy(graph_exec);
+          graph_exec = nullptr;
+        }
+      }
+      if (!graph_exec) {
+        const cudaError_t ie = cudaGraphInstantiate(&graph_exec, g, 0);
+        if (ie != cudaSuccess) {
+          cudaGraphDestroy(g);
+          graph_exec = nullptr;
+          return fail(SBP_ERR_CUDA, cudaGetErrorString(ie));
+        }
+      }
+      cudaGraphDestroy(g);
+      graph_key = key;
+      ++graph_captures;
+    }
+    SBP_CUDA(cudaGraphLaunch(graph_exec, st));
   }
   s = emit_until(&s_gather);
   if (s != SBP_OK) return s;
@@ -915,6 +1002,7 @@ static sbp_status run_one(Job& J, Run& r) {
     return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
   }
   const long long l0 = g_launches;
+  const long long c0 = eng->graph_captures, p0 = eng->graph_replays;
   eng->runs.push_back(&r);
   while (r.stage != Run::kDone) {
     s = eng->tick();
@@ -923,6 +1011,8 @@ static sbp_status run_one(Job& J, Run& r) {
   eng->runs.clear();
   // a failed tick leaves the engine's stream in an unknown state: drop it
   if (s != SBP_OK) return s;
+  r.R.graph_captures = eng->graph_captures - c0;
+  r.R.graph_replays = eng->graph_replays - p0;
   engine_pool().give(eng);
   r.R.kernel_launches = g_launches - l0;
   return SBP_OK;

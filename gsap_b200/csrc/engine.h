@@ -101,6 +101,8 @@ class Engine {
   std::vector<Run*> runs;
   long long ticks = 0;
   cudaEvent_t ev_first = nullptr;  // recorded at the first tick
+  bool use_graphs = false;         // ticks of queued sweeps as CUDA graphs
+  long long graph_captures = 0, graph_replays = 0;
 
   Engine() = default;
   Engine(const Engine&) = delete;
@@ -126,6 +128,9 @@ class Engine {
   void *up_host = nullptr, *up_dev = nullptr, *desc_host = nullptr, *desc_dev = nullptr;
   void *rd_host = nullptr, *rd_dev = nullptr;
   size_t up_cap = 0, desc_cap = 0, rd_cap = 0;
+  cudaGraphExec_t graph_exec = nullptr;  // the last captured sweep tick
+  uint64_t graph_key = 0;
+  long long graph_kernels = 0;            // kernel launches the graph holds
   int nb_slots_ = 0;  // batch positions per queued sweep in this tick's slots
 
   void* up_dev_ptr(size_t off) { return (char*)up_dev + off; }

@@ -58,7 +58,8 @@ class Report(C.Structure):
                 ("bytes_nodal", C.c_double), ("bytes_rebuild", C.c_double),
                 ("bytes_merge", C.c_double), ("status", C.c_int32),
                 ("ms_device", C.c_double), ("ms_nodal_kernel", C.c_double),
-                ("nodal_launches", C.c_int64), ("kernel_launches", C.c_int64)]
+                ("nodal_launches", C.c_int64), ("kernel_launches", C.c_int64),
+                ("graph_captures", C.c_int64), ("graph_replays", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

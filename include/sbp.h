@@ -68,7 +68,7 @@ typedef struct sbp_options {
   int32_t window;          /* moving-average window, 3 (:861) */
   int32_t max_outer;       /* cap on merge/golden-section steps (no reference counterpart) */
   int32_t device;          /* CUDA device ordinal, -1 = current device */
-  int32_t use_graphs;      /* capture each nodal sweep in a CUDA graph */
+  int32_t use_graphs;      /* ticks of queued nodal sweeps as CUDA graphs (default 1) */
   int32_t verbose;         /* 1: one line per outer step on stderr */
   int32_t dense_max;       /* keep M as dense B x B matrices while B <= dense_max
                               (default 4096; 0 = always CSR) */
@@ -96,6 +96,8 @@ typedef struct sbp_report {
   double ms_nodal_kernel;   /* CUDA-event time of the nodal dS kernels alone */
   int64_t nodal_launches;   /* nodal batches run (one warp-kernel launch each) */
   int64_t kernel_launches;  /* kernels this library launched during the run */
+  int64_t graph_captures;   /* sweep ticks captured as CUDA graphs (use_graphs) */
+  int64_t graph_replays;    /* sweep ticks replayed from a captured graph */
 } sbp_report;
 
 void sbp_default_options(sbp_options* o);

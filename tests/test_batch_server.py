@@ -149,3 +149,18 @@ def test_server_errors(sbp, solo):
         assert srv.poll(j, timeout_ms=-1) is not None
         with pytest.raises(sbp.SbpError, match="unknown request"):
             srv.poll(j, timeout_ms=0)
+
+
+def test_graph_replay_same_bits(sbp, solo):
+    # ticks of queued sweeps captured as CUDA graphs and replayed (the
+    # default) give the same partition as direct launches, alone and in a
+    # batch
+    gs, seeds, ref = solo
+    for i in (0, 2, 4):
+        assert ref[i][1]["graph_captures"] > 0 and ref[i][1]["graph_replays"] > 0
+        rep = sbp.partition(gs[i], seed=seeds[i], use_graphs=0)
+        assert rep["graph_captures"] == 0 and rep["graph_replays"] == 0
+        _same(gs[i].partitions, rep, *ref[i])
+    labs, reps, _ = sbp.partition_batch(gs, seeds=seeds, use_graphs=0)
+    for i in range(len(gs)):
+        _same(labs[i], reps[i], *ref[i])
