@@ -38,7 +38,8 @@ class Options(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("num_proposals", C.c_int32),
                 ("reduction_rate", C.c_float), ("max_nodal_itr", C.c_int32),
                 ("num_batches", C.c_int32), ("threshold1", C.c_float),
-                ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32)]
+                ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32),
+                ("exact", C.c_int32), ("mh", C.c_int32), ("beta", C.c_double)]
 
 
 class Report(C.Structure):
@@ -61,6 +62,10 @@ _sig("orc_build_blockmodel", C.c_int64, _GP, _vp, C.c_int32, _vp, _vp, _vp, _vp,
 _sig("orc_nodal_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
 _sig("orc_merge_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
 _sig("orc_mdl", C.c_double, _GP, _vp, C.c_int32, C.POINTER(C.c_double))
+_sig("orc_nodal_delta_mode", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, C.c_int32, _vp, _vp)
+_sig("orc_merge_delta_mode", None, _GP, _vp, C.c_int32, C.c_int32, _vp, C.c_int32, _vp, _vp, _vp)
+_sig("orc_nodal_batch_mode", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_uint32, C.c_int32,
+     C.c_int32, C.c_int32, C.c_int32, C.c_double, _vp, _vp)
 _sig("orc_merge_proposals", None, _GP, _vp, C.c_int32, C.c_int32, C.c_uint64, C.c_uint32, _vp)
 _sig("orc_nodal_batch", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_uint32, C.c_int32,
      C.c_int32, _vp, _vp)
@@ -117,6 +122,39 @@ def nodal_delta(g, part, B, verts, props):
     return dS[:verts.size], q3[:verts.size].astype(bool)
 
 
+def nodal_delta_exact(g, part, B, verts, props):
+    """Exact-mode dS of the moves and their log Hastings ratios."""
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    verts = np.ascontiguousarray(verts, dtype=np.int32)
+    props = np.ascontiguousarray(props, dtype=np.int32)
+    dS = np.zeros(max(verts.size, 1))
+    lh = np.zeros(max(verts.size, 1))
+    _lib.orc_nodal_delta_mode(C.byref(_g(g)), _p(part), B, verts.size, _p(verts), _p(props), 1,
+                              _p(dS), _p(lh))
+    return dS[:verts.size], lh[:verts.size]
+
+
+def merge_delta_exact(g, part, B, props, np_=10):
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    props = np.ascontiguousarray(props, dtype=np.int32)
+    dS = np.zeros(B * np_)
+    best = np.zeros(B, np.int32)
+    bds = np.zeros(B)
+    _lib.orc_merge_delta_mode(C.byref(_g(g)), _p(part), B, np_, _p(props), 1, _p(dS), _p(best),
+                              _p(bds))
+    return dS, best, bds
+
+
+def nodal_batch_mode(g, part, B, seed, seq, lo, hi, exact=1, mh=1, beta=3.0):
+    part = np.array(part, dtype=np.int32, copy=True)
+    n = max(hi - lo, 1)
+    dS = np.zeros(n)
+    props = np.zeros(n, np.int32)
+    tot = _lib.orc_nodal_batch_mode(C.byref(_g(g)), _p(part), B, seed, seq, lo, hi, exact, mh,
+                                    beta, _p(dS), _p(props))
+    return part, dS[:hi - lo], props[:hi - lo], tot
+
+
 def merge_delta(g, part, B, props, np_=10):
     part = np.ascontiguousarray(part, dtype=np.int32)
     props = np.ascontiguousarray(props, dtype=np.int32)
@@ -169,7 +207,8 @@ def apply_merges(part, B, B_to_merge, best, best_dS):
 
 def default_options(**kw):
     o = Options(seed=0, num_proposals=10, reduction_rate=0.35, max_nodal_itr=100, num_batches=4,
-                threshold1=5e-4, threshold2=1e-4, window=3, max_outer=1000)
+                threshold1=5e-4, threshold2=1e-4, window=3, max_outer=1000, exact=0, mh=0,
+                beta=3.0)
     for k, v in kw.items():
         setattr(o, k, v)
     return o

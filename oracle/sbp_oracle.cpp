@@ -33,6 +33,7 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <numeric>
 #include <set>
 #include <vector>
@@ -205,6 +206,161 @@ double dS_in_block_excl(const BM& m, int32_t r, int32_t x, int32_t y) {
     }
   }
   return dS;
+}
+
+// ---------------------------------------------------------- exact-MDL mode --
+// GSAP's dS terms above approximate the change of the MDL (merged columns
+// kept apart, Q1; old column degrees, Q2; one term per list entry).  The
+// exact mode computes the change of the same data term,
+//   data_S = sum_cells M log2 M - sum_b d_out[b] log2 d_out[b]
+//            - sum_b d_in[b] log2 d_in[b]
+// (each row of sum M log2(M / (d_out d_in)) split by its row and column
+// sums), over the cells a move or a merge changes; dS = -(change of data_S),
+// as in S = model - data_S.  The Metropolis-Hastings acceptance uses the
+// Hastings ratio of the proposal distribution GSAP samples from
+// (choose_neighbored_node_block, kernels.hpp:877-1032): a neighbour u of v
+// in proportion to edge weight, then, with t = b(u), block s with
+// probability (M[t][s] + M[s][t] + 1) / (d[t] + B), d = d_out + d_in; this
+// is the standard SBP sampler (Peixoto, Phys. Rev. E 89, 012804, 2014).
+struct Mode {
+  int exact = 0;     // 0: GSAP's dS terms; 1: the exact change of the MDL
+  int mh = 0;        // 0: accept iff dS < 0 (GSAP); 1: Metropolis-Hastings
+  double beta = 3.0;  // inverse temperature of the MH acceptance (dS in bits)
+};
+
+inline double xl2(double x) { return x > 0.0 ? x * L2(x) : 0.0; }
+
+uint32_t cell_at(const BM& m, int32_t r, int32_t c) {
+  auto b = m.ocol.begin() + m.optr[r], e = m.ocol.begin() + m.optr[r + 1];
+  auto it = std::lower_bound(b, e, c);
+  return (it != e && *it == c) ? m.ocnt[it - m.ocol.begin()] : 0u;
+}
+
+// v's edge weight to (out) and from (in) each neighbour block, its
+// self-loop weight apart.
+struct MoveLists {
+  std::map<int32_t, int64_t> kout, kin, ktot;  // ktot: both directions, self loops twice
+  int64_t self = 0;
+};
+
+MoveLists move_lists(const Graph& g, const int32_t* part, int32_t v) {
+  MoveLists L;
+  for (int32_t j = g.out_ptr[v]; j < g.out_ptr[v + 1]; ++j) {
+    int32_t u = g.out_idx[j];
+    L.ktot[part[u]] += g.out_w[j];
+    if (u == v) L.self += g.out_w[j];
+    else L.kout[part[u]] += g.out_w[j];
+  }
+  for (int32_t j = g.in_ptr[v]; j < g.in_ptr[v + 1]; ++j) {
+    int32_t u = g.in_idx[j];
+    L.ktot[part[u]] += g.in_w[j];
+    if (u != v) L.kin[part[u]] += g.in_w[j];
+  }
+  return L;
+}
+
+// Cell changes of moving v from r to s.
+std::map<std::pair<int32_t, int32_t>, int64_t> move_cells(const MoveLists& L, int32_t r, int32_t s) {
+  std::map<std::pair<int32_t, int32_t>, int64_t> dl;
+  for (const auto& kv : L.kout) {
+    dl[{r, kv.first}] -= kv.second;
+    dl[{s, kv.first}] += kv.second;
+  }
+  for (const auto& kv : L.kin) {
+    dl[{kv.first, r}] -= kv.second;
+    dl[{kv.first, s}] += kv.second;
+  }
+  if (L.self) {
+    dl[{r, r}] -= L.self;
+    dl[{s, s}] += L.self;
+  }
+  return dl;
+}
+
+double nodal_delta_exact(const Graph& g, const BM& m, const int32_t* part, int32_t v, int32_t s) {
+  const int32_t r = part[v];
+  if (r == s) return 0.0;
+  MoveLists L = move_lists(g, part, v);
+  double cells = 0.0;
+  for (const auto& kv : move_cells(L, r, s)) {
+    if (kv.second == 0) continue;
+    const double x = cell_at(m, kv.first.first, kv.first.second);
+    cells += xl2(x + (double)kv.second) - xl2(x);
+  }
+  const double kO = g.deg_out[v], kI = g.deg_in[v];
+  const double dor = m.d_out[r], dos = m.d_out[s], dir = m.d_in[r], dis = m.d_in[s];
+  const double degs = xl2(dor - kO) - xl2(dor) + xl2(dos + kO) - xl2(dos) + xl2(dir - kI) -
+                      xl2(dir) + xl2(dis + kI) - xl2(dis);
+  return -(cells - degs);
+}
+
+// log(p(s -> r) / p(r -> s)) of the move, p as in the comment above.
+double hastings_log(const Graph& g, const BM& m, const int32_t* part, int32_t v, int32_t s) {
+  const int32_t r = part[v];
+  const double kv = (double)g.deg_out[v] + g.deg_in[v];
+  if (r == s || kv == 0.0) return 0.0;
+  MoveLists L = move_lists(g, part, v);
+  auto dl = move_cells(L, r, s);
+  auto newcell = [&](int32_t a, int32_t b) {
+    auto it = dl.find({a, b});
+    return (double)cell_at(m, a, b) + (it == dl.end() ? 0.0 : (double)it->second);
+  };
+  const double Bd = (double)m.B;
+  auto dtot = [&](int32_t t) { return (double)m.d_out[t] + m.d_in[t]; };
+  double fwd = 0.0, bwd = 0.0;
+  // after the move the self-loop entries point at s
+  std::map<int32_t, int64_t> kafter = L.ktot;
+  if (L.self) {
+    kafter[r] -= 2 * L.self;
+    kafter[s] += 2 * L.self;
+  }
+  for (const auto& kv2 : L.ktot) {
+    const int32_t t = kv2.first;
+    fwd += (double)kv2.second * ((double)cell_at(m, t, s) + cell_at(m, s, t) + 1.0) /
+           (dtot(t) + Bd);
+  }
+  for (const auto& kv2 : kafter) {
+    const int32_t t = kv2.first;
+    if (kv2.second == 0) continue;
+    double dt = dtot(t);
+    if (t == r) dt -= kv;
+    if (t == s) dt += kv;
+    bwd += (double)kv2.second * (newcell(t, r) + newcell(r, t) + 1.0) / (dt + Bd);
+  }
+  return std::log(bwd) - std::log(fwd);
+}
+
+// Acceptance of a move with dS (bits) and log Hastings ratio, uniform x.
+inline bool mh_accept(double dS, double logH, uint32_t x, double beta) {
+  const double a = -beta * dS * 0.6931471805599453 + logH;
+  if (a >= 0.0) return true;
+  return std::log((double)x * 2.3283064365386963e-10) < a;
+}
+
+// Exact merge dS of block r into s: rows r, s and columns r, s fold into
+// row and column s; only cells present in both rows (both columns) and the
+// four corner cells change the sum of M log2 M.
+double merge_delta_exact(const BM& m, int32_t r, int32_t s) {
+  if (r == s) return 0.0;
+  double cells = 0.0;
+  for (int32_t i = m.optr[r]; i < m.optr[r + 1]; ++i) {
+    const int32_t c = m.ocol[i];
+    if (c == r || c == s) continue;
+    const double a = m.ocnt[i], b = cell_at(m, s, c);
+    if (b != 0.0) cells += xl2(a + b) - xl2(a) - xl2(b);
+  }
+  for (int32_t i = m.iptr[r]; i < m.iptr[r + 1]; ++i) {
+    const int32_t t = m.icol[i];
+    if (t == r || t == s) continue;
+    const double a = m.icnt[i], b = cell_at(m, t, s);
+    if (b != 0.0) cells += xl2(a + b) - xl2(a) - xl2(b);
+  }
+  const double Mrr = cell_at(m, r, r), Mrs = cell_at(m, r, s), Msr = cell_at(m, s, r),
+               Mss = cell_at(m, s, s);
+  cells += xl2(Mrr + Mrs + Msr + Mss) - xl2(Mrr) - xl2(Mrs) - xl2(Msr) - xl2(Mss);
+  const double dor = m.d_out[r], dos = m.d_out[s], dir = m.d_in[r], dis = m.d_in[s];
+  const double degs = xl2(dor + dos) - xl2(dor) - xl2(dos) + xl2(dir + dis) - xl2(dir) - xl2(dis);
+  return -(cells - degs);
 }
 
 // A vertex's neighbour blocks with weights, sorted by block: what
@@ -463,7 +619,7 @@ double merge_new_in(const BM& m, int32_t r, int32_t s) {
 // proposals, reduced over 32 lanes by halving offsets; on equal values the
 // lane further up wins.  Lanes past num_proposals hold (largest finite, 0).
 void merge_deltas(const BM& m, const int32_t* props, int np, double* dS, int32_t* best,
-                  double* best_dS) {
+                  double* best_dS, const Mode& md = Mode()) {
   int32_t B = m.B;
   std::vector<double> dso(B);
   for (int32_t b = 0; b < B; ++b) dso[b] = dS_out_block(m, b);
@@ -476,10 +632,14 @@ void merge_deltas(const BM& m, const int32_t* props, int np, double* dS, int32_t
     int32_t r = t / np, s = props[t], k = t % np;
     int32_t sid = s * np + k;
     double d = 0.0;
-    d += dso[r] + dso[s];
-    d += dsin[t] + dsin[sid];
-    d += merge_new_out(m, r, s);
-    d += merge_new_in(m, r, s);
+    if (md.exact) {
+      d = merge_delta_exact(m, r, s);
+    } else {
+      d += dso[r] + dso[s];
+      d += dsin[t] + dsin[sid];
+      d += merge_new_out(m, r, s);
+      d += merge_new_in(m, r, s);
+    }
     dS[t] = d;
   }
   for (int32_t r = 0; r < B; ++r) {
@@ -617,7 +777,8 @@ int32_t nodal_proposal(const Graph& g, const int32_t* part, int32_t B, int32_t v
 // (dS < 0, kernels.hpp:634-640) are applied together.  Returns the sum of
 // accepted dS.
 double nodal_batch(const Graph& g, std::vector<int32_t>& part, const BM& m, uint64_t seed,
-                   uint32_t seq, int32_t lo, int32_t hi, double* dS_out_arr, int32_t* props_out) {
+                   uint32_t seq, int32_t lo, int32_t hi, double* dS_out_arr, int32_t* props_out,
+                   const Mode& md = Mode()) {
   int32_t B = m.B;
   std::vector<int32_t> nbr_s;
   std::vector<uint8_t> use_rand;
@@ -629,9 +790,15 @@ double nodal_batch(const Graph& g, std::vector<int32_t>& part, const BM& m, uint
   for (int32_t v = lo; v < hi; ++v) {
     int32_t s = nodal_proposal(g, part.data(), B, v, seed, seq, nbr_s, use_rand);
     bool q3 = false;
-    double d = nodal_delta(g, m, dso.data(), part.data(), v, s, &q3);
+    double d = md.exact ? nodal_delta_exact(g, m, part.data(), v, s)
+                        : nodal_delta(g, m, dso.data(), part.data(), v, s, &q3);
+    bool acc = d < 0.0;
+    if (md.mh && s != part[v]) {
+      P4 x = draw(seed, RNG_NODAL_VERTEX, seq, (uint32_t)v);
+      acc = mh_accept(d, hastings_log(g, m, part.data(), v, s), x.v[2], md.beta);
+    }
     double rec = 0.0;
-    if (d < 0.0) { newpart[v] = s; rec = d; }
+    if (acc && s != part[v]) { newpart[v] = s; rec = d; }
     total += rec;
     if (dS_out_arr) dS_out_arr[v - lo] = rec;
     if (props_out) props_out[v - lo] = s;
@@ -687,6 +854,7 @@ struct Options {
   float threshold2;
   int32_t window;
   int32_t max_outer;
+  Mode mode;
 };
 
 struct Report {
@@ -743,7 +911,8 @@ int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep
     for (int32_t t = 0; t < B * o.num_proposals; ++t)
       props[t] = merge_proposal(m, t / o.num_proposals, o.seed, seq, (uint32_t)t);
     ++seq;
-    merge_deltas(m, props.data(), o.num_proposals, mdS.data(), best.data(), best_dS.data());
+    merge_deltas(m, props.data(), o.num_proposals, mdS.data(), best.data(), best_dS.data(),
+                 o.mode);
     B = apply_merges(part, B, B_to_merge, best.data(), best_dS.data());
     R.ms_merge += ms_since(t0);
     t0 = Clock::now();
@@ -754,7 +923,8 @@ int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep
     for (int32_t itr = 0; itr < o.max_nodal_itr; ++itr) {
       for (int32_t b = 0; b < o.num_batches; ++b) {
         t0 = Clock::now();
-        itr_dS[itr] += nodal_batch(g, part, m, o.seed, seq, b * BS, (b + 1) * BS, nullptr, nullptr);
+        itr_dS[itr] += nodal_batch(g, part, m, o.seed, seq, b * BS, (b + 1) * BS, nullptr, nullptr,
+                                   o.mode);
         ++seq;
         R.nodal_proposals += BS;
         R.ms_nodal += ms_since(t0);
@@ -888,6 +1058,49 @@ void orc_nodal_delta(const orc_graph* xg, const int32_t* part, int32_t B, int32_
   }
 }
 
+// Exact-mode dS (exact = 1) or GSAP's (0) of moving verts[i] to props[i],
+// and log Hastings ratios of those moves.
+void orc_nodal_delta_mode(const orc_graph* xg, const int32_t* part, int32_t B, int32_t nv,
+                          const int32_t* verts, const int32_t* props, int32_t exact,
+                          double* dS, double* logH) {
+  Graph g = to_graph(xg);
+  BM m = build_bm(g, part, B);
+  std::vector<double> dso(B);
+  for (int32_t b = 0; b < B; ++b) dso[b] = dS_out_block(m, b);
+  for (int32_t i = 0; i < nv; ++i) {
+    bool q3 = false;
+    if (dS)
+      dS[i] = exact ? nodal_delta_exact(g, m, part, verts[i], props[i])
+                    : nodal_delta(g, m, dso.data(), part, verts[i], props[i], &q3);
+    if (logH) logH[i] = hastings_log(g, m, part, verts[i], props[i]);
+  }
+}
+
+void orc_merge_delta_mode(const orc_graph* xg, const int32_t* part, int32_t B, int32_t np,
+                          const int32_t* props, int32_t exact, double* dS, int32_t* best,
+                          double* best_dS) {
+  Graph g = to_graph(xg);
+  BM m = build_bm(g, part, B);
+  Mode md;
+  md.exact = exact;
+  merge_deltas(m, props, np, dS, best, best_dS, md);
+}
+
+double orc_nodal_batch_mode(const orc_graph* xg, int32_t* part, int32_t B, uint64_t seed,
+                            uint32_t seq, int32_t lo, int32_t hi, int32_t exact, int32_t mh,
+                            double beta, double* dS, int32_t* props) {
+  Graph g = to_graph(xg);
+  std::vector<int32_t> p(part, part + g.N);
+  BM m = build_bm(g, p.data(), B);
+  Mode md;
+  md.exact = exact;
+  md.mh = mh;
+  md.beta = beta;
+  double tot = nodal_batch(g, p, m, seed, seq, lo, hi, dS, props, md);
+  std::copy(p.begin(), p.end(), part);
+  return tot;
+}
+
 // Merge dS of all B*np proposals, best proposal and its dS per block.
 void orc_merge_delta(const orc_graph* xg, const int32_t* part, int32_t B, int32_t np,
                      const int32_t* props, double* dS, int32_t* best, double* best_dS) {
@@ -960,6 +1173,9 @@ typedef struct orc_options {
   float threshold2;
   int32_t window;
   int32_t max_outer;
+  int32_t exact;
+  int32_t mh;
+  double beta;
 } orc_options;
 
 typedef struct orc_report {
@@ -976,7 +1192,10 @@ typedef struct orc_report {
 int orc_partition(const orc_graph* xg, const orc_options* xo, int32_t* labels, orc_report* rep) {
   Graph g = to_graph(xg);
   Options o{xo->seed, xo->num_proposals, xo->reduction_rate, xo->max_nodal_itr, xo->num_batches,
-            xo->threshold1, xo->threshold2, xo->window, xo->max_outer};
+            xo->threshold1, xo->threshold2, xo->window, xo->max_outer, Mode()};
+  o.mode.exact = xo->exact;
+  o.mode.mh = xo->mh;
+  o.mode.beta = xo->beta;
   Report R{};
   int st = run_partition(g, o, labels, &R);
   if (rep) {
