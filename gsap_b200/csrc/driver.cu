@@ -481,6 +481,10 @@ sbp_status check_options(const sbp_options* o) {
     return fail(SBP_ERR_INVALID, "bad loop options");
   if (!(o->reduction_rate > 0.f && o->reduction_rate < 1.f))
     return fail(SBP_ERR_INVALID, "reduction_rate must be in (0, 1)");
+  if ((o->exact != 0 && o->exact != 1) || (o->mh != 0 && o->mh != 1))
+    return fail(SBP_ERR_INVALID, "exact and mh must be 0 or 1");
+  if (o->mh && !(o->beta >= 0.0 && o->beta < 1e300))
+    return fail(SBP_ERR_INVALID, "beta must be finite and >= 0");
   return SBP_OK;
 }
 
@@ -511,6 +515,9 @@ void sbp_default_options(sbp_options* o) {
   o->use_graphs = 1;
   o->verbose = 0;
   o->dense_max = 4096;
+  o->exact = 0;
+  o->mh = 0;
+  o->beta = 3.0;
 }
 
 const char* sbp_status_string(sbp_status s) {
@@ -622,7 +629,14 @@ sbp_status sbp_build_blockmodel(const sbp_graph_csr* g, const int32_t* part, int
 
 sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t nv,
                                const int32_t* verts, const int32_t* props, double* dS) {
+  return sbp_delta_mdl_nodal_mode(g, part, B, nv, verts, props, 0, dS, nullptr);
+}
+
+sbp_status sbp_delta_mdl_nodal_mode(const sbp_graph_csr* g, const int32_t* part, int32_t B,
+                                    int32_t nv, const int32_t* verts, const int32_t* props,
+                                    int32_t exact, double* dS, double* logH) {
   if (!g) return fail(SBP_ERR_INVALID, "graph is NULL");
+  if (exact != 0 && exact != 1) return fail(SBP_ERR_INVALID, "exact must be 0 or 1");
   if (nv < 0 || (nv > 0 && (!verts || !props || !dS)))
     return fail(SBP_ERR_INVALID, "bad vertex/proposal arrays");
   for (int32_t i = 0; i < nv; ++i) {
@@ -633,11 +647,15 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
   sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
   int32_t *dv = nullptr, *dp = nullptr;
-  double* dd = nullptr;
+  double *dd = nullptr, *dl = nullptr;
   size_t n = (size_t)(nv > 0 ? nv : 1);
   SBP_CUDA(cudaMalloc(&dv, 4 * n));
   SBP_CUDA(cudaMalloc(&dp, 4 * n));
   SBP_CUDA(cudaMalloc(&dd, 8 * n));
+  if (logH) SBP_CUDA(cudaMalloc(&dl, 8 * n));
+  ScoreMode md;
+  md.exact = exact;
+  md.mh = logH ? 1 : 0;
   cudaMemcpyAsync(dv, verts, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
   cudaMemcpyAsync(dp, props, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
   std::vector<int32_t> hv;
@@ -647,16 +665,18 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
     cudaMemcpyAsync(J.heavy, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice, J.st);
   block_terms_any(J, B, 0, 0, 0, J.st);
   nodal_delta_given(J.g, J.part, J.m, B, is_dense(J, B), nv, dv, dp, dd,
-                    aux_for(J, J.heavy, (int32_t)hv.size()), J.st);
+                    aux_for(J, J.heavy, (int32_t)hv.size()), J.st, md, dl);
   cudaStreamSynchronize(J.st);
   int32_t err_h = 0;
   cudaMemcpy(&err_h, J.err, 4, cudaMemcpyDeviceToHost);
   cudaMemcpyAsync(dS, dd, 8 * (size_t)nv, cudaMemcpyDeviceToHost, J.st);
+  if (logH) cudaMemcpyAsync(logH, dl, 8 * (size_t)nv, cudaMemcpyDeviceToHost, J.st);
   cudaError_t e = cudaStreamSynchronize(J.st);
   if (e == cudaSuccess) e = cudaGetLastError();
   cudaFree(dv);
   cudaFree(dp);
   cudaFree(dd);
+  if (dl) cudaFree(dl);
   if (e != cudaSuccess) return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
   if (err_h) return fail(SBP_ERR_INTERNAL, "neighbour-block table overflow in the nodal kernel");
   return SBP_OK;
@@ -664,7 +684,14 @@ sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int3
 
 sbp_status sbp_delta_mdl_merge(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
                                const int32_t* props, double* dS, int32_t* best, double* best_dS) {
+  return sbp_delta_mdl_merge_mode(g, part, B, np, props, 0, dS, best, best_dS);
+}
+
+sbp_status sbp_delta_mdl_merge_mode(const sbp_graph_csr* g, const int32_t* part, int32_t B,
+                                    int32_t np, const int32_t* props, int32_t exact, double* dS,
+                                    int32_t* best, double* best_dS) {
   if (np < 1 || np > 32 || !props || B < 1) return fail(SBP_ERR_INVALID, "bad proposals");
+  if (exact != 0 && exact != 1) return fail(SBP_ERR_INVALID, "exact must be 0 or 1");
   for (int64_t t = 0; t < (int64_t)B * np; ++t)
     if (props[t] < 0 || props[t] >= B) return fail(SBP_ERR_INVALID, "proposal out of [0, B)");
   Job J;
@@ -673,7 +700,7 @@ sbp_status sbp_delta_mdl_merge(const sbp_graph_csr* g, const int32_t* part, int3
   size_t nt = (size_t)B * np;
   SBP_CUDA(cudaMemcpyAsync(J.props, props, 4 * nt, cudaMemcpyHostToDevice, J.st));
   block_terms(J.m, B, 0, 0, 0, J.st);
-  merge_delta(J.m, B, np, J.props, J.mdS, J.best, J.best_dS, J.st);
+  merge_delta(J.m, B, np, J.props, J.mdS, J.best, J.best_dS, J.st, exact);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());
   if (dS) SBP_CUDA(cudaMemcpy(dS, J.mdS, 8 * nt, cudaMemcpyDeviceToHost));
@@ -698,7 +725,19 @@ sbp_status sbp_merge_proposals(const sbp_graph_csr* g, const int32_t* part, int3
 sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
                            uint32_t seq, int32_t lo, int32_t hi, double* dS_rec, int32_t* props,
                            double* sum) {
+  return sbp_nodal_batch_mode(g, part, B, seed, seq, lo, hi, 0, 0, 3.0, dS_rec, props, sum);
+}
+
+sbp_status sbp_nodal_batch_mode(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
+                                uint32_t seq, int32_t lo, int32_t hi, int32_t exact, int32_t mh,
+                                double beta, double* dS_rec, int32_t* props, double* sum) {
   if (!g || lo < 0 || hi < lo || hi > g->N) return fail(SBP_ERR_INVALID, "bad batch range");
+  if ((exact != 0 && exact != 1) || (mh != 0 && mh != 1) || !(beta >= 0.0 && beta < 1e300))
+    return fail(SBP_ERR_INVALID, "bad scoring mode");
+  ScoreMode md;
+  md.exact = exact;
+  md.mh = mh;
+  md.beta = beta;
   Job J;
   sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
@@ -713,7 +752,7 @@ sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uin
   SBP_CUDA(cudaMemsetAsync(J.dsum, 0, 8, J.st));
   SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8, J.st));
   nodal_batch_sample(J.g, J.part, J.m, B, dense, seed, seq, lo, cnt, J.newlab, J.rec, J.props,
-                     aux_for(J, J.heavy, (int32_t)hv.size()), J.st);
+                     aux_for(J, J.heavy, (int32_t)hv.size()), J.st, md);
   nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, nullptr, 0, J.cs, J.st);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());

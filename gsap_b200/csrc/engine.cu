@@ -229,9 +229,9 @@ void Engine::clear_slots() {
   pre_dense.clear();
   pre_rebuild.clear();
   for (auto& b : sw) {
-    for (Slot* s : {&b.bt_csr, &b.bt_dense, &b.heavy_csr, &b.heavy_dense, &b.nodal_csr,
-                    &b.nodal_dense, &b.dupd, &b.commit})
-      s->clear();
+    for (Slot* s : {&b.bt_csr, &b.bt_dense, &b.dupd, &b.commit}) s->clear();
+    for (Slot& s : b.heavy) s.clear();
+    for (Slot& s : b.nodal) s.clear();
     b.rebuild.clear();
   }
   for (auto& e : ends)
@@ -296,7 +296,7 @@ void Engine::add_run_work(Run& r) {
     if (!r.csr_fresh) add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
     add_block_terms(m_bt, J.m, r.B, 0, r.o.seed, 0);
     add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props);
-    add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS);
+    add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS, r.o.exact);
     add_copy(s_gather, rd_dev_ptr(r.rd_off), J.best, (size_t)r.B);
     add_copy(s_gather, rd_dev_ptr(r.rd_off + align256(4 * (size_t)r.B)), J.best_dS,
              2 * (size_t)r.B);
@@ -313,6 +313,7 @@ void Engine::add_run_work(Run& r) {
     const bool isf = std::isfinite(r.large.S) && std::isfinite(r.med.S) && std::isfinite(r.small.S);
     const double thr = isf ? (double)r.o.threshold2 : (double)r.o.threshold1;
     const double mS = model_S(r.B, J.N, J.E);
+    const ScoreMode md = score_mode(r.o);
     for (int32_t k = 0; k < r.sweep_k; ++k) {
       for (int32_t b = 0; b < nb; ++b) {
         SweepSlots& s = sw[k * nb_slots_ + b];
@@ -323,8 +324,9 @@ void Engine::add_run_work(Run& r) {
         const int32_t lo = b * r.BS;
         if (dense) add_block_terms_dense(s.bt_dense, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
         else add_block_terms(s.bt_csr, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
-        add_nodal(dense ? s.nodal_dense : s.nodal_csr, dense ? s.heavy_dense : s.heavy_csr,
-                  dense, J.g, J.part, J.m, r.B, r.o.seed, seq, lo, r.BS, J.newlab, J.rec,
+        const int ms = md.slot(dense);
+        add_nodal(s.nodal[ms], s.heavy[ms], dense, md, J.g, J.part, J.m, r.B, r.o.seed, seq, lo,
+                  r.BS, J.newlab, J.rec,
                   nullptr, J.heavy + r.heavy_off[b], r.heavy_off[b + 1] - r.heavy_off[b], J.err,
                   ctl, nb);
         if (dense) {
@@ -401,10 +403,9 @@ sbp_status Engine::launch_slot(Slot& s, size_t off, cudaStream_t stream) {
 }
 
 // Engines in different host threads (the server's lanes) hand their CUDA
-// calls to the driver one thread at a time; only the wait for a tick's end
-// runs outside this lock, so the lanes' device work still overlaps.
-// Concurrent launches from the lane threads corrupted kernel arguments in
-// the driver on this platform.
+// calls to the driver one thread at a time, so a tick's launches (and a
+// graph capture) stay contiguous; only the wait for a tick's end runs
+// outside this lock, so the lanes' device work still overlaps.
 std::mutex& cuda_submit_mutex() {
   static std::mutex mu;
   return mu;
@@ -472,9 +473,12 @@ sbp_status Engine::tick() {
   for (int k = 0; k < k_max; ++k) {
     for (int b = 0; b < nb_max; ++b) {
       SweepSlots& w = sw[k * nb_max + b];
-      for (Slot* x : {&w.bt_csr, &w.bt_dense, &w.heavy_csr, &w.heavy_dense, &w.nodal_csr,
-                      &w.nodal_dense, &w.dupd, &w.commit})
-        order.push_back(x);
+      order.push_back(&w.bt_csr);
+      order.push_back(&w.bt_dense);
+      for (Slot& x : w.heavy) order.push_back(&x);
+      for (Slot& x : w.nodal) order.push_back(&x);
+      order.push_back(&w.dupd);
+      order.push_back(&w.commit);
       for (Slot* x : w.rebuild.all()) order.push_back(x);
     }
     SweepEndSlots& e = ends[k];
@@ -557,19 +561,20 @@ sbp_status Engine::tick() {
         sbp_status q = emit_until(&w.bt_dense);
         if (q != SBP_OK) return q;
         SBP_CUDA(record(be[1]));
-        const bool heavy = !w.heavy_csr.empty() || !w.heavy_dense.empty();
+        bool heavy = false;
+        for (const Slot& x : w.heavy) heavy = heavy || !x.empty();
         if (heavy) {
           // heavy vertices on the side stream, next to the warp kernels
           SBP_CUDA(cudaEventRecord(fork, st));
           SBP_CUDA(cudaStreamWaitEvent(side, fork, 0));
-          q = launch_slot(w.heavy_csr, slot_off(&w.heavy_csr), side);
-          if (q != SBP_OK) return q;
-          q = launch_slot(w.heavy_dense, slot_off(&w.heavy_dense), side);
-          if (q != SBP_OK) return q;
+          for (Slot& x : w.heavy) {
+            q = launch_slot(x, slot_off(&x), side);
+            if (q != SBP_OK) return q;
+          }
           SBP_CUDA(cudaEventRecord(join, side));
         }
-        i += 2;  // the heavy slots
-        q = emit_until(&w.nodal_dense);
+        i += 4;  // the heavy slots
+        q = emit_until(&w.nodal[3]);
         if (q != SBP_OK) return q;
         if (heavy) SBP_CUDA(cudaStreamWaitEvent(st, join, 0));
         SBP_CUDA(record(be[2]));
@@ -787,7 +792,8 @@ sbp_status Engine::tick() {
       r->R.B = r->B;
       r->R.S = r->S;
       r->stage = Run::kDone;
-      r->finished = true;
+      // a server request is published (Run::finished) by its lane, under
+      // the server's lock, once the engine no longer touches it
     }
   }
   return SBP_OK;
@@ -807,9 +813,12 @@ double Engine::device_ms() {
   return ms;
 }
 
-Run::~Run() {
+void Run::release_events() {
   if (ev_begin) cudaEventDestroy(ev_begin);
+  ev_begin = nullptr;
 }
+
+Run::~Run() { release_events(); }
 
 void HostGraph::assign(const sbp_graph_csr& g) {
   N = g.N;
@@ -929,6 +938,7 @@ sbp_status Scheduler::step(std::vector<Run*>& done) {
     hbm->give(r->admit_bytes);
     r->owned.reset();  // arena back to the pool, in stream order
     r->J = nullptr;
+    r->release_events();
     done.push_back(r);
   }
   eng.runs.swap(keep);

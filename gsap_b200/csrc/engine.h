@@ -41,7 +41,7 @@ struct Run {
   sbp_status status = SBP_OK;
   std::string error;
   enum Stage { kMerge, kSweep, kFinish, kDone } stage = kMerge;
-  bool finished = false;
+  bool finished = false;  // server requests: set by the lane under the server's lock
   bool sweeps_only = false;
   int32_t sweeps_total = 0;
   // loop state (partition.hpp:852-954)
@@ -72,6 +72,9 @@ struct Run {
   Run() = default;
   Run(const Run&) = delete;
   Run& operator=(const Run&) = delete;
+  // CUDA events of the run; call on the thread that drives the engine (a
+  // server request is destroyed by whichever thread collects it)
+  void release_events();
   ~Run();
 
   void setup_batches();
@@ -84,7 +87,8 @@ struct Run {
 
 // The launches of one nodal batch position across runs.
 struct SweepSlots {
-  Slot bt_csr, bt_dense, heavy_csr, heavy_dense, nodal_csr, nodal_dense, dupd, commit;
+  // heavy / nodal indexed by ScoreMode::slot(dense)
+  Slot bt_csr, bt_dense, heavy[4], nodal[4], dupd, commit;
   RebuildSlots rebuild;
 };
 

@@ -92,6 +92,14 @@ sbp_status device_xlx_table(int device, const double** out);
 int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
                           const double* best_dS, int32_t* map_out);
 double model_S(int32_t B, int32_t N, int32_t E);
+
+inline ScoreMode score_mode(const sbp_options& o) {
+  ScoreMode m;
+  m.exact = o.exact;
+  m.mh = o.mh;
+  m.beta = o.beta;
+  return m;
+}
 bool heavy_vertex(const Job& J, int32_t v);
 sbp_status check_options(const sbp_options* o);
 

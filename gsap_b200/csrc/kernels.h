@@ -80,6 +80,19 @@ struct RebuildTune {
   int32_t big_entries = 2048;
 };
 
+// How a nodal move is scored and accepted.  exact = 0: GSAP's dS terms
+// (kernels.hpp:494-643, 1153-1726, quirks kept); 1: the exact change of the
+// MDL.  mh = 0: accept iff dS < 0 (kernels.hpp:634-640); 1: Metropolis-
+// Hastings with inverse temperature beta (dS in bits) and the Hastings
+// ratio of GSAP's proposal.  Anything but (0, 0) runs the general-mode
+// kernels; the merge phase reads only `exact`.
+struct ScoreMode {
+  int32_t exact = 0, mh = 0;
+  double beta = 3.0;
+  bool general() const { return exact != 0 || mh != 0; }
+  int slot(bool dense) const { return (dense ? 1 : 0) + (general() ? 2 : 0); }
+};
+
 // ------------------------------------------------------ multi-job launches --
 // One launch of a kernel body over many jobs: `args` holds njobs argument
 // records back to back, job j owns virtual blocks [cta0[j], cta0[j+1]).
@@ -158,8 +171,10 @@ void add_copy(Slot& s, void* dst, const void* src, size_t words);
 void add_iota(Slot& s, int32_t* p, int32_t n);
 // Nodal batch of one job: the warp kernel's record goes to `warp`, the
 // CTA-per-vertex kernel's (heavy vertices) to `heavy`.  Use separate slots
-// for dense and CSR jobs.
-void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int32_t* part,
+// per md.slot(dense): dense and CSR jobs, GSAP-mode and general-mode jobs
+// run different kernels.
+void add_nodal(Slot& warp, Slot& heavy, bool dense, const ScoreMode& md, const DevGraph& g,
+               const int32_t* part,
                const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
                int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
                int32_t nheavy, int32_t* err, const int32_t* ctl = nullptr, uint32_t seq_mul = 0);
@@ -170,7 +185,7 @@ void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t
 void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
                      int32_t* props);
 void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
-                     double* dS, int32_t* best, double* best_dS);
+                     double* dS, int32_t* best, double* best_dS, int32_t exact = 0);
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map);
 
 // Tuned shape for a device and a blockmodel size class, if known.
@@ -233,11 +248,13 @@ struct NodalAux {
 void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                         bool dense, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
                         int32_t* newlab, double* rec, int32_t* props, const NodalAux& aux,
-                        cudaStream_t st);
-// dS of given (vertex, proposal) pairs, no accept.
+                        cudaStream_t st, const ScoreMode& md = ScoreMode());
+// dS of given (vertex, proposal) pairs, no accept; with md.mh, logH[i] (if
+// given) receives the log Hastings ratio of move i.
 void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                        bool dense, int32_t nv, const int32_t* verts, const int32_t* props,
-                       double* dS, const NodalAux& aux, cudaStream_t st);
+                       double* dS, const NodalAux& aux, cudaStream_t st,
+                       const ScoreMode& md = ScoreMode(), double* logH = nullptr);
 // Apply a batch: part[lo+i] = newlab[i]; slot_sum[0] += sum(rec) in a fixed
 // order, slot_acc[0] += number of moves.  With dense_m, also recomputes the
 // log2 of its block degrees.
@@ -250,7 +267,7 @@ void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newla
 void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
                      int32_t* props, cudaStream_t st);
 void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
-                 int32_t* best, double* best_dS, cudaStream_t st);
+                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact = 0);
 // part[v] = map[part[v]] (update_partitions, kernels.hpp:1728-1740).
 void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st);
 

@@ -34,6 +34,7 @@ struct MergeArgs {
   double* dS;
   int32_t* best;
   double* best_dS;
+  int32_t exact;  // 1: exact merge dS (merge_one_exact)
 };
 
 // First index k of out-row ++ in-row of block b with running count > t.
@@ -166,6 +167,48 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) 
   return a.dSout[r] + a.dSout[s] + in_r + in_s + new_out + new_in;
 }
 
+// Exact change of the MDL when block r merges into s: rows r and s add up
+// into row s, columns r and s into column s.  Of the sum of M log2 M only
+// the cells present in both rows (both columns) and the four corner cells,
+// which become one, change; of the degree terms the two rows' and the two
+// columns'.  dS = -(change of data_S), B fixed.  Warp-cooperative: the
+// shorter row is walked, the longer one searched.
+__device__ double merge_one_exact(const MergeArgs& a, int r, int s, int lane) {
+  if (r == s) return 0.0;
+  double acc = 0.0;  // - (change of the off-corner cells)
+  int x = r, y = s;
+  if (a.optr[s + 1] - a.optr[s] < a.optr[r + 1] - a.optr[r]) { x = s; y = r; }
+  int y0 = a.optr[y], y1 = a.optr[y + 1];
+  for (int i = a.optr[x] + lane; i < a.optr[x + 1]; i += 32) {
+    const int c = a.ocol[i];
+    if (c == r || c == s) continue;
+    const uint32_t b = row_lookup(a.ocol, a.ocnt, y0, y1, c);
+    if (b) acc -= xlx(a.xlx, a.ocnt[i] + b) - xlx(a.xlx, a.ocnt[i]) - xlx(a.xlx, b);
+  }
+  x = r; y = s;
+  if (a.iptr[s + 1] - a.iptr[s] < a.iptr[r + 1] - a.iptr[r]) { x = s; y = r; }
+  y0 = a.iptr[y]; y1 = a.iptr[y + 1];
+  for (int i = a.iptr[x] + lane; i < a.iptr[x + 1]; i += 32) {
+    const int c = a.icol[i];
+    if (c == r || c == s) continue;
+    const uint32_t b = row_lookup(a.icol, a.icnt, y0, y1, c);
+    if (b) acc -= xlx(a.xlx, a.icnt[i] + b) - xlx(a.xlx, a.icnt[i]) - xlx(a.xlx, b);
+  }
+  if (lane == 0) {
+    const uint32_t Mrr = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], r);
+    const uint32_t Mrs = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], s);
+    const uint32_t Msr = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], r);
+    const uint32_t Mss = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], s);
+    const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
+    const double corner = xlx(a.xlx, Mrr + Mrs + Msr + Mss) - xlx(a.xlx, Mrr) -
+                          xlx(a.xlx, Mrs) - xlx(a.xlx, Msr) - xlx(a.xlx, Mss);
+    const double degs = xlx(a.xlx, dor + dos) - xlx(a.xlx, dor) - xlx(a.xlx, dos) +
+                        xlx(a.xlx, dir + dis) - xlx(a.xlx, dir) - xlx(a.xlx, dis);
+    acc += degs - corner;
+  }
+  return warp_sum(acc);
+}
+
 constexpr int kMergeWarps = 8;
 
 struct MergeDeltaBody {
@@ -180,7 +223,7 @@ struct MergeDeltaBody {
     for (int k = 0; k < a.np; ++k) {
       int s = a.props_in[(long long)r * a.np + k];
       int s2 = a.props_in[(long long)s * a.np + k];
-      double d = merge_one(a, r, s, s2, lane);
+      double d = a.exact ? merge_one_exact(a, r, s, lane) : merge_one(a, r, s, s2, lane);
       if (lane == k) {
         mine = d;
         who = s;
@@ -250,8 +293,9 @@ void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint3
 }
 
 void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
-                 int32_t* best, double* best_dS, cudaStream_t st) {
+                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact) {
   MergeArgs a = make_args(m, B, np);
+  a.exact = exact;
   a.props_in = props;
   a.dS = dS;
   a.best = best;
@@ -274,8 +318,9 @@ void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t se
 }
 
 void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
-                     double* dS, int32_t* best, double* best_dS) {
+                     double* dS, int32_t* best, double* best_dS, int32_t exact) {
   MergeArgs a = make_args(m, B, np);
+  a.exact = exact;
   a.props_in = props;
   a.dS = dS;
   a.best = best;

@@ -75,6 +75,10 @@ struct NodalArgs {
   int32_t* err;             // error counter (hash table overflow)
   const int32_t* ctl;       // sweep control: gate, and seq += ctl[0] * seq_mul
   uint32_t seq_mul;
+  // general-mode kernels only (ScoreMode)
+  int32_t exact, mh;
+  double beta;
+  double* logH_raw;         // given mode: log Hastings ratio of each move
 };
 
 // g(x, a) = x log2 x - x a, zero for x == 0
@@ -560,15 +564,19 @@ __device__ int32_t pick_neighbour(const NodalArgs& a, int v, uint64_t t, int lan
 }
 
 // Vertex and proposal of batch item i (computed by one warp).
+// u2 = the vertex's third draw (the Metropolis-Hastings uniform).
 template <bool GIVEN>
-__device__ __forceinline__ void item(const NodalArgs& a, int i, int lane, int& v, int& s) {
+__device__ __forceinline__ void item(const NodalArgs& a, int i, int lane, int& v, int& s,
+                                     uint32_t& u2) {
   if (GIVEN) {
     v = a.verts[i];
     s = a.props_in[i];
+    u2 = 0u;
     return;
   }
   v = a.lo + i;
   P4 x = draw(a.seed, kRngNodalVertex, a.seq + ctl_itr(a.ctl) * a.seq_mul, (uint32_t)v);
+  u2 = x.v[2];
   int rnd = (int)(x.v[0] % (uint32_t)a.B);
   uint64_t deg = (uint64_t)a.kdo[v] + a.kdi[v];
   if (deg == 0) {
@@ -596,10 +604,372 @@ __device__ __forceinline__ bool is_heavy(int no, int ni) {
   return no > kWarpList || ni > kWarpList;
 }
 
-template <bool GIVEN, bool DENSE>
+// ------------------------------------------------------------ general mode --
+// Kernels instantiated with GEN = true score a move by the exact change of
+// the MDL (exact = 1) or by GSAP's terms (exact = 0), and accept it by
+// Metropolis-Hastings (mh = 1) or iff dS < 0.
+//
+// Exact dS.  S = model - data_S with
+//   data_S = sum_cells M log2 M - sum_rows d_out log2 d_out - sum_cols d_in log2 d_in
+// and the model term fixed while B is.  Moving v from r to s, with kout[c]
+// and kin[c] v's weight to and from block c (self loops of weight `self`
+// apart), moves kout[c] from cell (r,c) to (s,c) and kin[c] from (c,r) to
+// (c,s) for every c other than r and s, changes the four corner cells as in
+// corner_exact, and moves v's out- and in-degree between the rows and
+// columns r and s; dS = -(change of data_S).  Only those cells and four
+// degrees enter, each as x log2 x.
+//
+// Hastings ratio of GSAP's proposal (kernels.hpp:877-1032): v picks an
+// incident edge with probability proportional to its weight, the edge's
+// other end lies in block t, and s is proposed with probability
+// (M_ts + M_st + 1) / (d_t + B), d_t = d_out[t] + d_in[t], so
+//   p(r -> s) = sum_t k_t (M_ts + M_st + 1) / (d_t + B) / k_v
+// with k_t v's weight to and from t (a self loop counts in both directions)
+// and k_v the sum of the k_t.  The reverse move reads the blockmodel after
+// the move, in which the self loops sit in block s.  A move is accepted when
+//   u < 2^(-beta dS) p(s -> r) / p(r -> s)
+// with u the vertex's third draw scaled to [0, 1).
+
+struct Hast {
+  double f = 0.0, b = 0.0;  // forward and reverse proposal weights (k_v times p)
+};
+
+// Exact dS of the off-corner cells of one neighbour block c (direction
+// `in`, v's total weight kc to or from c, counted once per block).
+template <bool DENSE>
+__device__ __forceinline__ void entry_exact(const NodalArgs& a, const Rows<DENSE>& R, int r, int s,
+                                            bool in, int32_t c, bool leader, uint32_t kc,
+                                            Acc& q) {
+  if (!leader || c == r || c == s) return;
+  const uint32_t Mo = in ? R.in_r(c) : R.out_r(c);
+  const uint32_t Mt = in ? R.in_s(c) : R.out_s(c);
+  q.acc += xlx(a.xlx, Mo) - xlx(a.xlx, Mo - kc) + xlx(a.xlx, Mt) - xlx(a.xlx, Mt + kc);
+}
+
+// Corner cells and the four degrees of the exact dS, on lanes 0..15 of the
+// calling warp: lanes 0-3 the old cells (r,r), (r,s), (s,r), (s,s), lanes
+// 4-7 the same cells after the move, lanes 8-11 the new degrees d_out[r],
+// d_out[s], d_in[r], d_in[s], lanes 12-15 the old ones.  koR..niS include
+// the self loops (their other end is in r).
+template <bool DENSE>
+__device__ __forceinline__ void corner_exact(const NodalArgs& a, const Rows<DENSE>& R, int v,
+                                             int r, int s, const RsWeights& w, uint32_t self,
+                                             Acc& q) {
+  const int lane = threadIdx.x & 31;
+  if (lane >= 16) return;
+  const int j = lane & 3;
+  double t;
+  if (lane < 8) {
+    const uint32_t M = R.out_at((j & 2) != 0, (j & 1) ? s : r);
+    // unsigned wrap-around in the middle is fine: the results are >= 0
+    const uint32_t x = j == 0   ? M - w.koR - w.niR + self
+                       : j == 1 ? M - w.koS + (w.niR - self)
+                       : j == 2 ? M + (w.koR - self) - w.niS
+                                : M + w.koS + w.niS + self;
+    t = lane < 4 ? xlx(a.xlx, M) : -xlx(a.xlx, x);
+  } else {
+    const uint32_t kO = a.kdo[v], kI = a.kdi[v];
+    const uint32_t d0 = j == 0 ? a.d_out[r] : j == 1 ? a.d_out[s] : j == 2 ? a.d_in[r] : a.d_in[s];
+    const uint32_t d1 = j == 0 ? d0 - kO : j == 1 ? d0 + kO : j == 2 ? d0 - kI : d0 + kI;
+    t = lane < 12 ? xlx(a.xlx, d1) : -xlx(a.xlx, d0);
+  }
+  q.acc += t;
+}
+
+// Proposal weights of a neighbour block t other than r and s, kt = v's
+// weight to and from t.
+template <bool DENSE>
+__device__ __forceinline__ void hast_block(const NodalArgs& a, const Rows<DENSE>& R, int32_t t,
+                                           uint32_t kt, Hast& h) {
+  const double D = (double)a.d_out[t] + (double)a.d_in[t] + (double)a.B;
+  const double k = (double)kt;
+  h.f += k * ((double)R.in_s(t) + (double)R.out_s(t) + 1.0) / D;
+  h.b += k * ((double)R.in_r(t) + (double)R.out_r(t) - k + 1.0) / D;
+}
+
+// Proposal weights of blocks r and s (one thread of the group).
+template <bool DENSE>
+__device__ __forceinline__ void hast_rs(const NodalArgs& a, const Rows<DENSE>& R, int v, int r,
+                                        int s, const RsWeights& w, uint32_t self, Hast& h) {
+  const uint32_t Mrr = R.out_at(false, r), Mrs = R.out_at(false, s);
+  const uint32_t Msr = R.out_at(true, r), Mss = R.out_at(true, s);
+  const uint32_t xrr = Mrr - w.koR - w.niR + self;
+  const uint32_t xrs = Mrs - w.koS + (w.niR - self);
+  const uint32_t xsr = Msr + (w.koR - self) - w.niS;
+  const double kv = (double)a.kdo[v] + (double)a.kdi[v], Bd = (double)a.B;
+  const double Dr = (double)a.d_out[r] + (double)a.d_in[r];
+  const double Ds = (double)a.d_out[s] + (double)a.d_in[s];
+  const double kr = (double)w.koR + (double)w.niR, ks = (double)w.koS + (double)w.niS;
+  const double sl = 2.0 * (double)self;
+  h.f += kr * ((double)Mrs + (double)Msr + 1.0) / (Dr + Bd);
+  h.f += ks * ((double)Mss + (double)Mss + 1.0) / (Ds + Bd);
+  h.b += (kr - sl) * ((double)xrr + (double)xrr + 1.0) / (Dr - kv + Bd);
+  h.b += (ks + sl) * ((double)xsr + (double)xrs + 1.0) / (Ds + kv + Bd);
+}
+
+// v's self-loop weight (group sum over its out-list).
+template <int G>
+__device__ uint32_t self_weight(const NodalArgs& a, int v, const Group<G>& grp) {
+  const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
+  uint32_t t = 0u;
+  for (int k = grp.rank(); k < no; k += G)
+    if (__ldg(a.oidx + o0 + k) == v) t += __ldg(a.ow + o0 + k);
+  return (uint32_t)grp.sum_ll(t);
+}
+
+// Group totals, then the corner terms (exact or GSAP's) on warp 0, then the
+// sums of dS and of the proposal weights.
+template <bool DENSE, int G>
+__device__ double finish_gen(const NodalArgs& a, const Rows<DENSE>& R, int v, int r, int s,
+                             const RsWeights& w, uint32_t self, Acc q, Hast h,
+                             const Group<G>& grp, double& logH) {
+  if (a.exact) {
+    if (G == 32 || threadIdx.x < 32) corner_exact<DENSE>(a, R, v, r, s, w, self, q);
+  } else {
+    q.m4 = (int)grp.sum_ll(q.m4);
+    q.m5 = (int)grp.sum_ll(q.m5);
+    q.m6 = (int)grp.sum_ll(q.m6);
+    q.m7 = (int)grp.sum_ll(q.m7);
+    if (G == 32 || threadIdx.x < 32)
+      corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
+  }
+  logH = 0.0;
+  if (a.mh) {
+    const double f = grp.sum(h.f), b = grp.sum(h.b);
+    if ((uint64_t)a.kdo[v] + a.kdi[v] != 0u) logH = log(b) - log(f);
+  }
+  return grp.sum(q.acc);
+}
+
+// Both lists fit one warp together: lane l holds entry l (out-entries,
+// then in-entries).
+template <bool DENSE>
+__device__ double delta_registers_gen(const NodalArgs& a, int v, int r, int s, int32_t o0, int no,
+                                      int32_t i0, int ni, int lane, double& logH) {
+  const Rows<DENSE> R(a, r, s);
+  const bool in = lane >= no, valid = lane < no + ni;
+  const int k = in ? lane - no : lane;
+  int32_t c = -1;
+  uint32_t w = 0u, selfp = 0u;
+  if (valid) {
+    const int32_t u = in ? __ldg(a.iidx + i0 + k) : __ldg(a.oidx + o0 + k);
+    w = in ? __ldg(a.iw + i0 + k) : __ldg(a.ow + o0 + k);
+    c = __ldg(a.part + u);
+    if (!in && u == v) selfp = w;
+  }
+  RsWeights rw;
+  rw.koR = __reduce_add_sync(kFull, valid && !in && c == r ? w : 0u);
+  rw.koS = __reduce_add_sync(kFull, valid && !in && c == s ? w : 0u);
+  rw.niR = __reduce_add_sync(kFull, valid && in && c == r ? w : 0u);
+  rw.niS = __reduce_add_sync(kFull, valid && in && c == s ? w : 0u);
+  const uint32_t self = __reduce_add_sync(kFull, selfp);
+  Acc q;
+  const unsigned key = valid ? ((unsigned)c | (in ? 0x80000000u : 0u)) : (0x7fffffe0u + (unsigned)lane);
+  const unsigned peers = __match_any_sync(kFull, key);
+  const uint32_t kc = __reduce_add_sync(peers, w);
+  const bool leader = lane == __ffs(peers) - 1;
+  if (valid) {
+    if (a.exact) entry_exact<DENSE>(a, R, r, s, in, c, leader, kc, q);
+    else entry<DENSE>(a, R, r, s, rw.niS, in, c, w, leader, kc, q);
+  }
+  Hast h;
+  if (a.mh) {
+    // per block over both directions
+    const unsigned pa = __match_any_sync(kFull, valid ? (unsigned)c : 0x7fffffe0u + (unsigned)lane);
+    const uint32_t kt = __reduce_add_sync(pa, w);
+    if (valid && lane == __ffs(pa) - 1 && c != r && c != s) hast_block<DENSE>(a, R, c, kt, h);
+    if (lane == 0) hast_rs<DENSE>(a, R, v, r, s, rw, self, h);
+  }
+  return finish_gen<DENSE, 32>(a, R, v, r, s, rw, self, q, h, Group<32>{nullptr}, logH);
+}
+
+// Weight of block c's run in a sorted list; false when c is absent.
+__device__ __forceinline__ bool run_weight(const unsigned long long* key, int n, int32_t c,
+                                           uint32_t& w) {
+  const unsigned long long k0 = (unsigned long long)(uint32_t)c << 32;
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (key[mid] < k0) lo = mid + 1;
+    else hi = mid;
+  }
+  w = 0u;
+  const bool found = lo < n && kblk(key[lo]) == c;
+  for (; lo < n && kblk(key[lo]) == c; ++lo) w += kwt(key[lo]);
+  return found;
+}
+
+template <bool DENSE, int G>
+__device__ double delta_sorted_gen(const NodalArgs& a, int v, int r, int s,
+                                   const unsigned long long* ko, int no,
+                                   const unsigned long long* ki, int ni, const Group<G>& grp,
+                                   double& logH) {
+  const int t = grp.rank();
+  const Rows<DENSE> R(a, r, s);
+  uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
+  for (int k = t; k < no; k += G) {
+    int32_t c = kblk(ko[k]);
+    koR += c == r ? kwt(ko[k]) : 0u;
+    koS += c == s ? kwt(ko[k]) : 0u;
+  }
+  for (int k = t; k < ni; k += G) {
+    int32_t c = kblk(ki[k]);
+    niR += c == r ? kwt(ki[k]) : 0u;
+    niS += c == s ? kwt(ki[k]) : 0u;
+  }
+  const RsWeights w{(uint32_t)grp.sum_ll(koR), (uint32_t)grp.sum_ll(koS),
+                    (uint32_t)grp.sum_ll(niR), (uint32_t)grp.sum_ll(niS)};
+  const uint32_t self = self_weight<G>(a, v, grp);
+  Acc q;
+  Hast h;
+  for (int k = t; k < no; k += G) {
+    const int32_t c = kblk(ko[k]);
+    const bool leader = k == 0 || kblk(ko[k - 1]) != c;
+    uint32_t kc = 0;
+    if (leader)
+      for (int j = k; j < no && kblk(ko[j]) == c; ++j) kc += kwt(ko[j]);
+    if (a.exact) entry_exact<DENSE>(a, R, r, s, false, c, leader, kc, q);
+    else entry<DENSE>(a, R, r, s, w.niS, false, c, kwt(ko[k]), leader, kc, q);
+    if (a.mh && leader && c != r && c != s) {
+      uint32_t kin;
+      run_weight(ki, ni, c, kin);
+      hast_block<DENSE>(a, R, c, kc + kin, h);
+    }
+  }
+  for (int k = t; k < ni; k += G) {
+    const int32_t c = kblk(ki[k]);
+    const bool leader = k == 0 || kblk(ki[k - 1]) != c;
+    uint32_t kc = 0;
+    if (leader)
+      for (int j = k; j < ni && kblk(ki[j]) == c; ++j) kc += kwt(ki[j]);
+    if (a.exact) entry_exact<DENSE>(a, R, r, s, true, c, leader, kc, q);
+    else entry<DENSE>(a, R, r, s, w.niS, true, c, kwt(ki[k]), leader, kc, q);
+    uint32_t kout;
+    // blocks on both lists were counted with the out-list
+    if (a.mh && leader && c != r && c != s && !run_weight(ko, no, c, kout))
+      hast_block<DENSE>(a, R, c, kc, h);
+  }
+  if (a.mh && t == 0) hast_rs<DENSE>(a, R, v, r, s, w, self, h);
+  return finish_gen<DENSE, G>(a, R, v, r, s, w, self, q, h, grp, logH);
+}
+
+template <bool DENSE, int G>
+__device__ double delta_hashed_gen(const NodalArgs& a, int v, int r, int s, HashTab h, int* flag,
+                                   const Group<G>& grp, double& logH) {
+  const int t = grp.rank();
+  const Rows<DENSE> R(a, r, s);
+  const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
+  const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
+  logH = 0.0;
+  uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
+  for (int k = t; k < no; k += G) {
+    int32_t c = __ldg(a.part + __ldg(a.oidx + o0 + k));
+    uint32_t w = __ldg(a.ow + o0 + k);
+    koR += c == r ? w : 0u;
+    koS += c == s ? w : 0u;
+  }
+  for (int k = t; k < ni; k += G) {
+    int32_t c = __ldg(a.part + __ldg(a.iidx + i0 + k));
+    uint32_t w = __ldg(a.iw + i0 + k);
+    niR += c == r ? w : 0u;
+    niS += c == s ? w : 0u;
+  }
+  const RsWeights rw{(uint32_t)grp.sum_ll(koR), (uint32_t)grp.sum_ll(koS),
+                     (uint32_t)grp.sum_ll(niR), (uint32_t)grp.sum_ll(niS)};
+  const uint32_t self = self_weight<G>(a, v, grp);
+  Acc q;
+  Hast hs;
+  // dS: per direction, one hash class of blocks per pass
+  for (int dir = 0; dir < 2; ++dir) {
+    const int32_t base = dir == 0 ? o0 : i0, n = dir == 0 ? no : ni;
+    const int32_t* idx = dir == 0 ? a.oidx : a.iidx;
+    const uint32_t* wt = dir == 0 ? a.ow : a.iw;
+    const uint32_t P = (uint32_t)((n + kHashSlots / 4 - 1) / (kHashSlots / 4));
+    for (uint32_t pass = 0; pass < P; ++pass) {
+      for (int i = t; i < kHashSlots; i += G) {
+        h.key[i] = -1;
+        h.sum[i] = 0u;
+        h.first[i] = 0x7fffffff;
+      }
+      if (t == 0) *flag = 0;
+      grp.sync();
+      for (int k = t; k < n; k += G) {
+        int32_t c = __ldg(a.part + __ldg(idx + base + k));
+        if (hclass(c, P) == pass && !hash_add(h, c, __ldg(wt + base + k), k)) *flag = 1;
+      }
+      grp.sync();
+      if (*flag) return __longlong_as_double(0x7ff8000000000000ll);  // table overflow
+      for (int k = t; k < n; k += G) {
+        int32_t c = __ldg(a.part + __ldg(idx + base + k));
+        if (hclass(c, P) != pass) continue;
+        const int slot = hash_find(h, c);
+        const bool leader = h.first[slot] == k;
+        const uint32_t kc = h.sum[slot];
+        if (a.exact) entry_exact<DENSE>(a, R, r, s, dir == 1, c, leader, kc, q);
+        else entry<DENSE>(a, R, r, s, rw.niS, dir == 1, c, __ldg(wt + base + k), leader, kc, q);
+      }
+      grp.sync();
+    }
+  }
+  if (a.mh) {
+    // proposal weights: per block over both directions, one hash class per pass
+    const int n = no + ni;
+    const uint32_t P = (uint32_t)((n + kHashSlots / 4 - 1) / (kHashSlots / 4));
+    for (uint32_t pass = 0; pass < P; ++pass) {
+      for (int i = t; i < kHashSlots; i += G) {
+        h.key[i] = -1;
+        h.sum[i] = 0u;
+        h.first[i] = 0x7fffffff;
+      }
+      if (t == 0) *flag = 0;
+      grp.sync();
+      for (int k = t; k < n; k += G) {
+        const bool in = k >= no;
+        const int j = in ? k - no : k;
+        const int32_t c = __ldg(a.part + __ldg((in ? a.iidx + i0 : a.oidx + o0) + j));
+        if (c == r || c == s || hclass(c, P) != pass) continue;
+        if (!hash_add(h, c, __ldg((in ? a.iw + i0 : a.ow + o0) + j), k)) *flag = 1;
+      }
+      grp.sync();
+      if (*flag) return __longlong_as_double(0x7ff8000000000000ll);
+      for (int i = t; i < kHashSlots; i += G)
+        if (h.key[i] != -1) hast_block<DENSE>(a, R, h.key[i], h.sum[i], hs);
+      grp.sync();
+    }
+    if (t == 0) hast_rs<DENSE>(a, R, v, r, s, rw, self, hs);
+  }
+  return finish_gen<DENSE, G>(a, R, v, r, s, rw, self, q, hs, grp, logH);
+}
+
+constexpr double kLn2 = 0.6931471805599453;
+
+// Accept test of a general-mode move (r != s).
+__device__ __forceinline__ bool accept_move(const NodalArgs& a, double d, double logH,
+                                            uint32_t u) {
+  if (!a.mh) return d < 0.0;
+  // -beta * dS * ln 2 + logH, rounded step by step (no contraction)
+  const double x = __dadd_rn(__dmul_rn(__dmul_rn(-a.beta, d), kLn2), logH);
+  if (x >= 0.0) return true;
+  return log((double)u * 2.3283064365386963e-10) < x;
+}
+
+__device__ __forceinline__ void write_result_gen(const NodalArgs& a, bool given, int i, int r,
+                                                 int s, double d, double logH, uint32_t u) {
+  if (given) {
+    a.dS_raw[i] = d;
+    if (a.logH_raw) a.logH_raw[i] = logH;
+    return;
+  }
+  const bool acc = r != s && accept_move(a, d, logH, u);
+  a.newlab[i] = acc ? s : r;
+  a.rec[i] = acc ? d : 0.0;
+  if (a.props_out) a.props_out[i] = s;
+}
+
+template <bool GIVEN, bool DENSE, bool GEN>
 struct NodalBody {
   using Args = NodalArgs;
-  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = DENSE ? 4 : 3;
+  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = GEN ? 2 : DENSE ? 4 : 3;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
   if (ctl_stopped(a.ctl)) return;
@@ -612,6 +982,25 @@ struct NodalBody {
     const int32_t o0 = a.optr[vv], no = a.optr[vv + 1] - o0;
     const int32_t i0 = a.iptr[vv], ni = a.iptr[vv + 1] - i0;
     if (is_heavy(no, ni)) continue;  // the CTA kernel's
+    if constexpr (GEN) {
+      int v, s;
+      uint32_t u2;
+      item<GIVEN>(a, i, lane, v, s, u2);
+      const int r = a.part[v];
+      double d = 0.0, lh = 0.0;
+      if (r != s) {
+        if (no + ni <= 32) {
+          d = delta_registers_gen<DENSE>(a, v, r, s, o0, no, i0, ni, lane, lh);
+        } else {
+          stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, s_ko[wid], grp);
+          stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, s_ki[wid], grp);
+          d = delta_sorted_gen<DENSE, 32>(a, v, r, s, s_ko[wid], no, s_ki[wid], ni, grp, lh);
+        }
+      }
+      if (lane == 0) write_result_gen(a, GIVEN, i, r, s, d, lh, u2);
+      __syncwarp();
+      continue;
+    }
     if (!GIVEN && no + ni <= 32) {
       // one entry per lane, loaded once: the proposal's neighbour pick (out-
       // then in-entries, pick_neighbour's order) and the dS both read it
@@ -656,7 +1045,8 @@ struct NodalBody {
       continue;
     }
     int v, s;
-    item<GIVEN>(a, i, lane, v, s);
+    uint32_t u2;
+    item<GIVEN>(a, i, lane, v, s, u2);
     const int r = a.part[v];
     double d = 0.0;
     if (r != s) {
@@ -677,7 +1067,7 @@ struct NodalBody {
 // Vertices with more than kWarpList entries in a direction: one CTA each,
 // lists sorted in shared memory up to kHeavyList entries, longer ones
 // through the hashed passes.
-template <bool GIVEN, bool DENSE>
+template <bool GIVEN, bool DENSE, bool GEN>
 struct NodalHeavyBody {
   using Args = NodalArgs;
   static constexpr int kThreads = kHeavyThreads, kMinBlocks = 2;
@@ -687,6 +1077,7 @@ struct NodalHeavyBody {
   extern __shared__ unsigned long long hsm[];
   __shared__ double red[kHeavyThreads / 32];
   __shared__ int flag, sh_v, sh_s;
+  __shared__ uint32_t sh_u2;
   Group<kHeavyThreads> grp{red};
   unsigned long long* ko = hsm;
   unsigned long long* ki = hsm + kHeavyList;
@@ -695,10 +1086,12 @@ struct NodalHeavyBody {
     const int i = a.heavy[h];
     if (threadIdx.x < 32) {
       int v, s;
-      item<GIVEN>(a, i, threadIdx.x, v, s);
+      uint32_t u2;
+      item<GIVEN>(a, i, threadIdx.x, v, s, u2);
       if (threadIdx.x == 0) {
         sh_v = v;
         sh_s = s;
+        sh_u2 = u2;
       }
     }
     __syncthreads();
@@ -706,18 +1099,27 @@ struct NodalHeavyBody {
     const int r = a.part[v];
     const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
     const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
-    double d = 0.0;
+    double d = 0.0, lh = 0.0;
     if (r != s) {
       if (no <= kHeavyList && ni <= kHeavyList) {
         stage_sorted<kHeavyThreads>(a.oidx, a.ow, a.part, o0, no, ko, grp);
         stage_sorted<kHeavyThreads>(a.iidx, a.iw, a.part, i0, ni, ki, grp);
-        d = delta_sorted<DENSE, kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp);
+        if constexpr (GEN)
+          d = delta_sorted_gen<DENSE, kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp, lh);
+        else
+          d = delta_sorted<DENSE, kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp);
       } else {
-        d = delta_hashed<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp);
+        if constexpr (GEN)
+          d = delta_hashed_gen<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp, lh);
+        else
+          d = delta_hashed<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp);
         if (threadIdx.x == 0 && d != d) atomicAdd(a.err, 1);
       }
     }
-    if (threadIdx.x == 0) write_result(a, GIVEN, i, r, s, d);
+    if (threadIdx.x == 0) {
+      if constexpr (GEN) write_result_gen(a, GIVEN, i, r, s, d, lh, sh_u2);
+      else write_result(a, GIVEN, i, r, s, d);
+    }
     __syncthreads();
   }
   }
@@ -856,24 +1258,42 @@ int nodal_grid(int count) {
   return g < 1 ? 1 : (g > 148 * 64 ? 148 * 64 : g);
 }
 
-template <bool GIVEN, bool DENSE>
+template <bool GIVEN, bool DENSE, bool GEN>
 void launch_pair(const NodalArgs& a, const NodalAux& aux, cudaStream_t st) {
   if (a.nheavy > 0) {
     // heavy vertices on the side stream, next to the warp kernel
     cudaEventRecord(aux.fork, st);
     cudaStreamWaitEvent(aux.side, aux.fork, 0);
-    launch_single<NodalHeavyBody<GIVEN, DENSE>>(a, std::min(a.nheavy, 2 * 148), aux.side);
+    launch_single<NodalHeavyBody<GIVEN, DENSE, GEN>>(a, std::min(a.nheavy, 2 * 148), aux.side);
     cudaEventRecord(aux.join, aux.side);
   }
-  launch_single<NodalBody<GIVEN, DENSE>>(a, nodal_grid(a.count), st);
+  launch_single<NodalBody<GIVEN, DENSE, GEN>>(a, nodal_grid(a.count), st);
   if (a.nheavy > 0) cudaStreamWaitEvent(st, aux.join, 0);
 }
 
-const MultiKernel kmNodal[2] = {multi_kernel_desc<NodalBody<false, false>>("nodal_csr"),
-                                multi_kernel_desc<NodalBody<false, true>>("nodal_dense")};
-const MultiKernel kmNodalHeavy[2] = {
-    multi_kernel_desc<NodalHeavyBody<false, false>>("nodal_heavy_csr"),
-    multi_kernel_desc<NodalHeavyBody<false, true>>("nodal_heavy_dense")};
+template <bool GIVEN, bool DENSE>
+void launch_mode(const NodalArgs& a, const NodalAux& aux, cudaStream_t st, bool gen) {
+  if (gen) launch_pair<GIVEN, DENSE, true>(a, aux, st);
+  else launch_pair<GIVEN, DENSE, false>(a, aux, st);
+}
+
+// indexed by ScoreMode::slot(dense)
+const MultiKernel kmNodal[4] = {
+    multi_kernel_desc<NodalBody<false, false, false>>("nodal_csr"),
+    multi_kernel_desc<NodalBody<false, true, false>>("nodal_dense"),
+    multi_kernel_desc<NodalBody<false, false, true>>("nodal_gen_csr"),
+    multi_kernel_desc<NodalBody<false, true, true>>("nodal_gen_dense")};
+const MultiKernel kmNodalHeavy[4] = {
+    multi_kernel_desc<NodalHeavyBody<false, false, false>>("nodal_heavy_csr"),
+    multi_kernel_desc<NodalHeavyBody<false, true, false>>("nodal_heavy_dense"),
+    multi_kernel_desc<NodalHeavyBody<false, false, true>>("nodal_heavy_gen_csr"),
+    multi_kernel_desc<NodalHeavyBody<false, true, true>>("nodal_heavy_gen_dense")};
+
+void set_mode(NodalArgs& a, const ScoreMode& md) {
+  a.exact = md.exact;
+  a.mh = md.mh;
+  a.beta = md.beta;
+}
 const MultiKernel kmCommit = multi_kernel_desc<CommitBody>("commit");
 
 }  // namespace
@@ -885,12 +1305,18 @@ cudaError_t init_nodal_attributes() {
                                          (int)kHeavySmem);
     if (x != cudaSuccess) e = x;
   };
-  set((const void*)single_kernel<NodalHeavyBody<false, false>>);
-  set((const void*)single_kernel<NodalHeavyBody<false, true>>);
-  set((const void*)single_kernel<NodalHeavyBody<true, false>>);
-  set((const void*)single_kernel<NodalHeavyBody<true, true>>);
-  set((const void*)multi_kernel<NodalHeavyBody<false, false>>);
-  set((const void*)multi_kernel<NodalHeavyBody<false, true>>);
+  set((const void*)single_kernel<NodalHeavyBody<false, false, false>>);
+  set((const void*)single_kernel<NodalHeavyBody<false, true, false>>);
+  set((const void*)single_kernel<NodalHeavyBody<true, false, false>>);
+  set((const void*)single_kernel<NodalHeavyBody<true, true, false>>);
+  set((const void*)multi_kernel<NodalHeavyBody<false, false, false>>);
+  set((const void*)multi_kernel<NodalHeavyBody<false, true, false>>);
+  set((const void*)single_kernel<NodalHeavyBody<false, false, true>>);
+  set((const void*)single_kernel<NodalHeavyBody<false, true, true>>);
+  set((const void*)single_kernel<NodalHeavyBody<true, false, true>>);
+  set((const void*)single_kernel<NodalHeavyBody<true, true, true>>);
+  set((const void*)multi_kernel<NodalHeavyBody<false, false, true>>);
+  set((const void*)multi_kernel<NodalHeavyBody<false, true, true>>);
   return e;
 }
 
@@ -899,8 +1325,9 @@ int nodal_heavy_threshold() { return kWarpList; }
 void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                         bool dense, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
                         int32_t* newlab, double* rec, int32_t* props, const NodalAux& aux,
-                        cudaStream_t st) {
+                        cudaStream_t st, const ScoreMode& md) {
   NodalArgs a = make_args(g, part, m, B, aux);
+  set_mode(a, md);
   a.seed = seed;
   a.seq = seq;
   a.lo = lo;
@@ -909,21 +1336,24 @@ void nodal_batch_sample(const DevGraph& g, const int32_t* part, const DevBM& m, 
   a.rec = rec;
   a.props_out = props;
   if (count <= 0) return;
-  if (dense) launch_pair<false, true>(a, aux, st);
-  else launch_pair<false, false>(a, aux, st);
+  if (dense) launch_mode<false, true>(a, aux, st, md.general());
+  else launch_mode<false, false>(a, aux, st, md.general());
 }
 
 void nodal_delta_given(const DevGraph& g, const int32_t* part, const DevBM& m, int32_t B,
                        bool dense, int32_t nv, const int32_t* verts, const int32_t* props,
-                       double* dS, const NodalAux& aux, cudaStream_t st) {
+                       double* dS, const NodalAux& aux, cudaStream_t st, const ScoreMode& md,
+                       double* logH) {
   NodalArgs a = make_args(g, part, m, B, aux);
+  set_mode(a, md);
   a.count = nv;
   a.verts = verts;
   a.props_in = props;
   a.dS_raw = dS;
+  a.logH_raw = logH;
   if (nv <= 0) return;
-  if (dense) launch_pair<true, true>(a, aux, st);
-  else launch_pair<true, false>(a, aux, st);
+  if (dense) launch_mode<true, true>(a, aux, st, md.general());
+  else launch_mode<true, false>(a, aux, st, md.general());
 }
 
 void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
@@ -934,7 +1364,8 @@ void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newla
       vg_commit(count), st);
 }
 
-void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int32_t* part,
+void add_nodal(Slot& warp, Slot& heavy, bool dense, const ScoreMode& md, const DevGraph& g,
+               const int32_t* part,
                const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
                int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
                int32_t nheavy, int32_t* err, const int32_t* ctl, uint32_t seq_mul) {
@@ -953,8 +1384,9 @@ void add_nodal(Slot& warp, Slot& heavy, bool dense, const DevGraph& g, const int
   a.props_out = props;
   a.ctl = ctl;
   a.seq_mul = seq_mul;
-  slot_push(slot_bind(warp, kmNodal[dense ? 1 : 0]), a, ceil_div(count, kNodalWarps));
-  slot_push(slot_bind(heavy, kmNodalHeavy[dense ? 1 : 0]), a, nheavy);
+  set_mode(a, md);
+  slot_push(slot_bind(warp, kmNodal[md.slot(dense)]), a, ceil_div(count, kNodalWarps));
+  slot_push(slot_bind(heavy, kmNodalHeavy[md.slot(dense)]), a, nheavy);
 }
 
 void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,

@@ -112,6 +112,7 @@ void sbp_server::loop(Lane& L) {
         sch.hbm->give(r->admit_bytes);
         r->owned.reset();
         r->J = nullptr;
+        r->release_events();
         r->t_done_ms = sbp::now_ms();
         done.push_back(r);
       }

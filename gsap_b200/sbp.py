@@ -40,13 +40,18 @@ class _GraphCSR(C.Structure):
 
 
 class Options(C.Structure):
-    """sbp_options; defaults are GSAP's hyper-parameters (partition.hpp:855-861)."""
+    """sbp_options; defaults are GSAP's hyper-parameters (partition.hpp:855-861).
+
+    exact = 1 scores moves and merges by the exact change of the MDL, mh = 1
+    accepts nodal moves by Metropolis-Hastings at inverse temperature beta
+    (per bit); the defaults (0, 0) reproduce GSAP."""
     _fields_ = [("seed", C.c_uint64), ("num_proposals", C.c_int32),
                 ("reduction_rate", C.c_float), ("max_nodal_itr", C.c_int32),
                 ("num_batches", C.c_int32), ("threshold1", C.c_float),
                 ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32),
                 ("device", C.c_int32), ("use_graphs", C.c_int32), ("verbose", C.c_int32),
-                ("dense_max", C.c_int32)]
+                ("dense_max", C.c_int32), ("exact", C.c_int32), ("mh", C.c_int32),
+                ("beta", C.c_double)]
 
 
 class Report(C.Structure):
@@ -122,6 +127,13 @@ _sig("sbp_delta_mdl_nodal", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_i
      _vp)
 _sig("sbp_delta_mdl_merge", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, _vp, _vp,
      _vp, _vp)
+_sig("sbp_delta_mdl_nodal_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, _vp,
+     _vp, C.c_int32, _vp, _vp)
+_sig("sbp_delta_mdl_merge_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, _vp,
+     C.c_int32, _vp, _vp, _vp)
+_sig("sbp_nodal_batch_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint64,
+     C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, _vp, _vp,
+     C.POINTER(C.c_double))
 _sig("sbp_merge_proposals", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, C.c_uint64,
      C.c_uint32, _vp)
 _sig("sbp_nodal_batch", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint64, C.c_uint32,
@@ -450,6 +462,32 @@ def delta_mdl_merge(g: Graph, part, B, props, np_=10):
     return dS, best, best_dS
 
 
+def delta_mdl_nodal_mode(g: Graph, part, B, verts, props, exact=1, hastings=True):
+    """dS of each move in a scoring mode (exact = 1: the exact change of the
+    MDL) and, with hastings, each move's log Hastings ratio."""
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    verts = np.ascontiguousarray(verts, dtype=np.int32)
+    props = np.ascontiguousarray(props, dtype=np.int32)
+    n = max(verts.size, 1)
+    dS = np.zeros(n, np.float64)
+    lh = np.zeros(n, np.float64) if hastings else None
+    _check(_lib.sbp_delta_mdl_nodal_mode(C.byref(g.csr()), _p(part), B, verts.size, _p(verts),
+                                         _p(props), exact, _p(dS),
+                                         _p(lh) if hastings else None))
+    return dS[:verts.size], (lh[:verts.size] if hastings else None)
+
+
+def delta_mdl_merge_mode(g: Graph, part, B, props, np_=10, exact=1):
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    props = np.ascontiguousarray(props, dtype=np.int32)
+    dS = np.zeros(B * np_, np.float64)
+    best = np.zeros(B, np.int32)
+    best_dS = np.zeros(B, np.float64)
+    _check(_lib.sbp_delta_mdl_merge_mode(C.byref(g.csr()), _p(part), B, np_, _p(props), exact,
+                                         _p(dS), _p(best), _p(best_dS)))
+    return dS, best, best_dS
+
+
 def merge_proposals(g: Graph, part, B, seed, seq, np_=10):
     part = np.ascontiguousarray(part, dtype=np.int32)
     props = np.zeros(B * np_, np.int32)
@@ -465,6 +503,17 @@ def nodal_batch(g: Graph, part, B, seed, seq, lo, hi):
     tot = C.c_double()
     _check(_lib.sbp_nodal_batch(C.byref(g.csr()), _p(part), B, seed, seq, lo, hi, _p(dS),
                                 _p(props), C.byref(tot)))
+    return part, dS[:hi - lo], props[:hi - lo], tot.value
+
+
+def nodal_batch_mode(g: Graph, part, B, seed, seq, lo, hi, exact=1, mh=1, beta=3.0):
+    part = np.array(part, dtype=np.int32, copy=True)
+    n = max(hi - lo, 1)
+    dS = np.zeros(n, np.float64)
+    props = np.zeros(n, np.int32)
+    tot = C.c_double()
+    _check(_lib.sbp_nodal_batch_mode(C.byref(g.csr()), _p(part), B, seed, seq, lo, hi, exact, mh,
+                                     beta, _p(dS), _p(props), C.byref(tot)))
     return part, dS[:hi - lo], props[:hi - lo], tot.value
 
 

@@ -72,6 +72,15 @@ typedef struct sbp_options {
   int32_t verbose;         /* 1: one line per outer step on stderr */
   int32_t dense_max;       /* keep M as dense B x B matrices while B <= dense_max
                               (default 4096; 0 = always CSR) */
+  /* Scoring mode (no reference counterpart; defaults reproduce GSAP):
+   * exact = 1 scores nodal moves and merges by the exact change of the MDL
+   * (merged columns folded, new column degrees, self loops moved with the
+   * vertex) instead of GSAP's dS terms; mh = 1 accepts nodal moves by
+   * Metropolis-Hastings, u < 2^(-beta dS) p(s->r)/p(r->s) with the Hastings
+   * ratio of GSAP's proposal, instead of dS < 0. */
+  int32_t exact;           /* 0 (default) or 1 */
+  int32_t mh;              /* 0 (default) or 1 */
+  double beta;             /* inverse temperature of the MH test, per bit (default 3) */
 } sbp_options;
 
 /* What one partition run did.  Timings are CUDA-event milliseconds on the
@@ -224,11 +233,26 @@ sbp_status sbp_build_blockmodel(const sbp_graph_csr* g, const int32_t* part, int
 sbp_status sbp_delta_mdl_nodal(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t nv,
                                const int32_t* verts, const int32_t* props, double* dS);
 
+/* sbp_delta_mdl_nodal in a scoring mode: exact = 1 gives the exact change
+ * of the MDL; logH (optional, nv doubles) receives each move's log Hastings
+ * ratio ln(p(s->r)/p(r->s)) of GSAP's proposal (0 for a vertex without
+ * edges).  No reference counterpart. */
+sbp_status sbp_delta_mdl_nodal_mode(const sbp_graph_csr* g, const int32_t* part, int32_t B,
+                                    int32_t nv, const int32_t* verts, const int32_t* props,
+                                    int32_t exact, double* dS, double* logH);
+
 /* Merge dS of B*np proposals (props[r*np+k] = target of block r's k-th
  * proposal; kernels.hpp:143-449) and each block's best proposal and its dS
  * (find_best_warp, kernels.hpp:452-491). */
 sbp_status sbp_delta_mdl_merge(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
                                const int32_t* props, double* dS, int32_t* best, double* best_dS);
+
+/* sbp_delta_mdl_merge in a scoring mode (exact = 1: the exact change of the
+ * MDL of each merge; 0 (r = s) for a block proposed to itself).  No
+ * reference counterpart. */
+sbp_status sbp_delta_mdl_merge_mode(const sbp_graph_csr* g, const int32_t* part, int32_t B,
+                                    int32_t np, const int32_t* props, int32_t exact, double* dS,
+                                    int32_t* best, double* best_dS);
 
 /* Merge proposals (kernels.hpp:726-856) from the Philox stream (seed, seq). */
 sbp_status sbp_merge_proposals(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t np,
@@ -241,6 +265,14 @@ sbp_status sbp_merge_proposals(const sbp_graph_csr* g, const int32_t* part, int3
 sbp_status sbp_nodal_batch(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
                            uint32_t seq, int32_t lo, int32_t hi, double* dS_rec, int32_t* props,
                            double* sum);
+
+/* sbp_nodal_batch in a scoring mode (exact, mh, beta as in sbp_options; the
+ * MH uniform of vertex v is the third word of its Philox draw).  dS_rec[i]
+ * is the dS of an accepted move (positive ones included under MH).  No
+ * reference counterpart. */
+sbp_status sbp_nodal_batch_mode(const sbp_graph_csr* g, int32_t* part, int32_t B, uint64_t seed,
+                                uint32_t seq, int32_t lo, int32_t hi, int32_t exact, int32_t mh,
+                                double beta, double* dS_rec, int32_t* props, double* sum);
 
 /* `sweeps` nodal sweeps of `num_batches` Jacobi batches each, as the nodal
  * phase of partition() runs them (partition.hpp:912-916): batch k uses the

@@ -32,6 +32,8 @@ def test_default_options_are_gsaps(sbp):
     assert o.num_proposals == 10 and abs(o.reduction_rate - 0.35) < 1e-7
     assert o.max_nodal_itr == 100 and o.num_batches == 4 and o.window == 3
     assert abs(o.threshold1 - 5e-4) < 1e-10 and abs(o.threshold2 - 1e-4) < 1e-10
+    # GSAP's scoring: its dS terms, accept iff dS < 0
+    assert o.exact == 0 and o.mh == 0 and o.beta == 3.0
 
 
 def _sha(a):
@@ -116,3 +118,14 @@ def test_partition_validates_before_device_use(sbp):
         sbp.build_blockmodel(g, np.full(g.N, 11, np.int32), 11)
     with pytest.raises(sbp.SbpError, match="invalid argument"):
         sbp.delta_mdl_nodal(g, g.true_partitions, 11, [0], [11])
+    # scoring modes
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.partition(g, exact=2)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.partition(g, mh=1, beta=-1.0)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.nodal_batch_mode(g, g.true_partitions, 11, 0, 0, 0, 10, exact=3)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.delta_mdl_nodal_mode(g, g.true_partitions, 11, [0], [1], exact=-1)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.delta_mdl_merge_mode(g, g.true_partitions, 11, np.zeros(110, np.int32), exact=2)
