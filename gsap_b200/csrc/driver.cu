@@ -368,10 +368,15 @@ int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
   return next;
 }
 
-double model_S(int32_t B, int32_t N, int32_t E) {
-  // partition.hpp:696-699 (Q6)
+double model_S(int32_t B, int32_t N, int32_t E, int32_t exact) {
   double b = (double)B;
   double x = b * b / (double)E;
+  // the standard description length's model term, in bits:
+  // (E h(x) + N ln B) / ln 2, h(x) = (1+x) ln(1+x) - x ln x
+  if (exact)
+    return ((double)E * ((1.0 + x) * std::log(1.0 + x) - x * std::log(x)) +
+            (double)N * std::log(b)) / 0.6931471805599453;
+  // partition.hpp:696-699 (Q6)
   return (double)E * (1.0 + x) * std::log(1.0 + x) - x * std::log(x) + (double)N * std::log(b);
 }
 
@@ -805,6 +810,12 @@ sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int3
 
 sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, double* S,
                    double* data_S) {
+  return sbp_mdl_mode(g, part, B, 0, S, data_S);
+}
+
+sbp_status sbp_mdl_mode(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t exact,
+                        double* S, double* data_S) {
+  if (exact != 0 && exact != 1) return fail(SBP_ERR_INVALID, "exact must be 0 or 1");
   Job J;
   sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
@@ -815,7 +826,7 @@ sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, doubl
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());
   if (data_S) *data_S = ds;
-  if (S) *S = model_S(B, g->N, g->E) - ds;
+  if (S) *S = model_S(B, g->N, g->E, exact) - ds;
   return SBP_OK;
 }
 

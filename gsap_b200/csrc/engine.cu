@@ -89,7 +89,7 @@ void Run::after_sweep(double dsum, double dataS, long long acc) {
   ++R.nodal_itrs;
   itr_dS[itr] = dsum;
   R.accepted_moves += acc;
-  S = model_S(B, J->N, J->E) - dataS;
+  S = model_S(B, J->N, J->E, o.exact) - dataS;
   bool stop = false;
   if (itr >= o.window - 1) {
     bool isf = std::isfinite(large.S) && std::isfinite(med.S) && std::isfinite(small.S);
@@ -312,7 +312,7 @@ void Engine::add_run_work(Run& r) {
     const int32_t* ctl = J.ctl;
     const bool isf = std::isfinite(r.large.S) && std::isfinite(r.med.S) && std::isfinite(r.small.S);
     const double thr = isf ? (double)r.o.threshold2 : (double)r.o.threshold1;
-    const double mS = model_S(r.B, J.N, J.E);
+    const double mS = model_S(r.B, J.N, J.E, r.o.exact);
     const ScoreMode md = score_mode(r.o);
     for (int32_t k = 0; k < r.sweep_k; ++k) {
       for (int32_t b = 0; b < nb; ++b) {

@@ -91,7 +91,9 @@ sbp_status device_xlx_table(int device, const double** out);
 // Returns the new block count, or -1 when a target lies outside [0, B).
 int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
                           const double* best_dS, int32_t* map_out);
-double model_S(int32_t B, int32_t N, int32_t E);
+// Model term of the MDL: GSAP's (partition.hpp:696-699, Q6) or, exact = 1,
+// the standard description length's in bits (exact mode searches B on it).
+double model_S(int32_t B, int32_t N, int32_t E, int32_t exact = 0);
 
 inline ScoreMode score_mode(const sbp_options& o) {
   ScoreMode m;

@@ -5,6 +5,7 @@ prints the run report and the quality against the planted labels as JSON.
     python -m gsap_b200.run --synthetic HH --N 20000 --B 32 [--seed 0]
     python -m gsap_b200.run --tsv graph.tsv [--truth graph_truePartition.tsv]
     python -m gsap_b200.run --dataset /path/to/Dataset/static --cat LL --size 5k
+    python -m gsap_b200.run --synthetic HH --N 20000 --B 32 --exact --mh [--beta 3]
 """
 import argparse
 import json
@@ -31,6 +32,12 @@ def main(argv=None):
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--dense-max", type=int, default=None,
                     help="largest B kept in the dense blockmodel form")
+    ap.add_argument("--exact", action="store_true",
+                    help="score moves and merges by the exact change of the MDL")
+    ap.add_argument("--mh", action="store_true",
+                    help="accept nodal moves by Metropolis-Hastings")
+    ap.add_argument("--beta", type=float, default=3.0,
+                    help="inverse temperature of the Metropolis-Hastings test, per bit")
     a = ap.parse_args(argv)
     if a.synthetic:
         g = sbp.dcsbm_variant(a.synthetic, a.N, a.B, seed=a.graph_seed)
@@ -43,9 +50,14 @@ def main(argv=None):
     for i in range(a.repeat):
         t0 = time.perf_counter()
         kw = {} if a.dense_max is None else {"dense_max": a.dense_max}
+        kw.update(exact=int(a.exact), mh=int(a.mh), beta=a.beta)
         rep = sbp.partition(g, seed=a.seed + i, device=a.device, verbose=int(a.verbose), **kw)
         rep["wall_ms"] = (time.perf_counter() - t0) * 1000.0
         rep["N"], rep["E"] = g.N, g.E
+        # the final labels under both objectives: GSAP's MDL formula and the
+        # standard description length (exact mode's)
+        rep["S_gsap_formula"] = sbp.mdl(g, g.partitions, rep["B"])[0]
+        rep["S_standard"] = sbp.mdl(g, g.partitions, rep["B"], exact=1)[0]
         if g.true_partitions is not None and g.true_partitions.min() >= 0:
             r, p, n = sbp.evaluate(g.true_partitions, g.partitions)
             rep.update(recall=r, precision=p, nmi=n)

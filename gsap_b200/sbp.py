@@ -144,6 +144,8 @@ _sig("sbp_merge_step", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32,
      C.c_uint64, C.c_uint32, _vp, _vp, C.POINTER(C.c_int32))
 _sig("sbp_mdl", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.POINTER(C.c_double),
      C.POINTER(C.c_double))
+_sig("sbp_mdl_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32,
+     C.POINTER(C.c_double), C.POINTER(C.c_double))
 _sig("sbp_mdl_device_static", C.c_int, C.c_int32, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp,
      _vp, _vp, _vp)
 _sig("sbp_partition_batch", C.c_int, _vp, C.c_int32, C.POINTER(Options), _vp, C.c_uint64, _vp,
@@ -537,10 +539,12 @@ def merge_step(g: Graph, part, B, B_to_merge, seed, seq, np_=10):
     return part, nb.value, best, best_dS
 
 
-def mdl(g: Graph, part, B):
+def mdl(g: Graph, part, B, exact=0):
+    """(S, data_S): GSAP's MDL (exact = 0) or the standard description
+    length in bits (exact = 1, the objective of exact mode)."""
     part = np.ascontiguousarray(part, dtype=np.int32)
     S, dS = C.c_double(), C.c_double()
-    _check(_lib.sbp_mdl(C.byref(g.csr()), _p(part), B, C.byref(S), C.byref(dS)))
+    _check(_lib.sbp_mdl_mode(C.byref(g.csr()), _p(part), B, exact, C.byref(S), C.byref(dS)))
     return S.value, dS.value
 
 

@@ -75,12 +75,14 @@ typedef struct sbp_options {
   /* Scoring mode (no reference counterpart; defaults reproduce GSAP):
    * exact = 1 scores nodal moves and merges by the exact change of the MDL
    * (merged columns folded, new column degrees, self loops moved with the
-   * vertex) instead of GSAP's dS terms; mh = 1 accepts nodal moves by
-   * Metropolis-Hastings, u < 2^(-beta dS) p(s->r)/p(r->s) with the Hastings
-   * ratio of GSAP's proposal, instead of dS < 0. */
+   * vertex) instead of GSAP's dS terms, and compares partitions (stop test,
+   * golden section, sbp_report.S) by the standard description length
+   * (sbp_mdl_mode) instead of GSAP's formula; mh = 1 accepts nodal moves by
+   * Metropolis-Hastings, u < exp(-beta dS_nats) p(s->r)/p(r->s) with the
+   * Hastings ratio of GSAP's proposal, instead of dS < 0. */
   int32_t exact;           /* 0 (default) or 1 */
   int32_t mh;              /* 0 (default) or 1 */
-  double beta;             /* inverse temperature of the MH test, per bit (default 3) */
+  double beta;             /* inverse temperature of the MH test, per nat (default 3) */
 } sbp_options;
 
 /* What one partition run did.  Timings are CUDA-event milliseconds on the
@@ -294,6 +296,14 @@ sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int3
 /* The MDL of a partition (compute_overall_entropy_cuda, partition.hpp:665-704). */
 sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, double* S,
                    double* data_S);
+
+/* sbp_mdl with exact = 1: the standard description length of the
+ * degree-corrected SBP in bits, (E h(B^2/E) + N ln B) / ln 2 - data_S with
+ * h(x) = (1+x) ln(1+x) - x ln x, the objective exact mode searches B on
+ * (GSAP's formula scales only part of h by E and mixes nats with bits).
+ * exact = 0 is sbp_mdl.  No reference counterpart. */
+sbp_status sbp_mdl_mode(const sbp_graph_csr* g, const int32_t* part, int32_t B, int32_t exact,
+                        double* S, double* data_S);
 
 /* The MDL of a blockmodel already in device memory (out CSR with B+1 row
  * pointers, block degrees), written to the device doubles *S and *data_S on

@@ -62,6 +62,7 @@ _sig("orc_build_blockmodel", C.c_int64, _GP, _vp, C.c_int32, _vp, _vp, _vp, _vp,
 _sig("orc_nodal_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
 _sig("orc_merge_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
 _sig("orc_mdl", C.c_double, _GP, _vp, C.c_int32, C.POINTER(C.c_double))
+_sig("orc_mdl_mode", C.c_double, _GP, _vp, C.c_int32, C.c_int32, C.POINTER(C.c_double))
 _sig("orc_nodal_delta_mode", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, C.c_int32, _vp, _vp)
 _sig("orc_merge_delta_mode", None, _GP, _vp, C.c_int32, C.c_int32, _vp, C.c_int32, _vp, _vp, _vp)
 _sig("orc_nodal_batch_mode", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_uint32, C.c_int32,
@@ -169,6 +170,14 @@ def mdl(g, part, B):
     part = np.ascontiguousarray(part, dtype=np.int32)
     d = C.c_double()
     S = _lib.orc_mdl(C.byref(_g(g)), _p(part), B, C.byref(d))
+    return S, d.value
+
+
+def mdl_mode(g, part, B, exact=1):
+    """exact = 1: the standard description length in bits; 0: GSAP's (Q6)."""
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    d = C.c_double()
+    S = _lib.orc_mdl_mode(C.byref(_g(g)), _p(part), B, exact, C.byref(d))
     return S, d.value
 
 

@@ -222,6 +222,8 @@ double dS_in_block_excl(const BM& m, int32_t r, int32_t x, int32_t y) {
 // in proportion to edge weight, then, with t = b(u), block s with
 // probability (M[t][s] + M[s][t] + 1) / (d[t] + B), d = d_out + d_in; this
 // is the standard SBP sampler (Peixoto, Phys. Rev. E 89, 012804, 2014).
+// The outer loop of exact mode compares partitions (stop test, golden
+// section) by the standard description length (mdl with exact = 1).
 struct Mode {
   int exact = 0;     // 0: GSAP's dS terms; 1: the exact change of the MDL
   int mh = 0;        // 0: accept iff dS < 0 (GSAP); 1: Metropolis-Hastings
@@ -669,12 +671,19 @@ void merge_deltas(const BM& m, const int32_t* props, int np, double* dS, int32_t
 
 // kernels.hpp:1034-1093 + partition.hpp:665-704: the MDL.  data_S uses log2,
 // the model term natural logs, and only its first part is scaled by E (Q6).
-double mdl(const BM& m, int32_t N, int32_t E, double* data_S_out) {
+// exact = 1: the standard description length of the degree-corrected SBP,
+// in bits: (E h(B^2/E) + N ln B) / ln 2 - data_S with
+// h(x) = (1+x) ln(1+x) - x ln x, every term in one base and the whole of
+// h scaled by E.  Exact mode searches B on this objective.
+double mdl(const BM& m, int32_t N, int32_t E, double* data_S_out, int exact = 0) {
   double data_S = 0.0;
   for (int32_t r = 0; r < m.B; ++r) data_S += dS_out_block(m, r);
   double B = (double)m.B;
   double x = B * B / (double)E;
-  double model = (double)E * (1.0 + x) * std::log(1.0 + x) - x * std::log(x) + (double)N * std::log(B);
+  double model = exact ? ((double)E * ((1.0 + x) * std::log(1.0 + x) - x * std::log(x)) +
+                          (double)N * std::log(B)) / 0.6931471805599453
+                       : (double)E * (1.0 + x) * std::log(1.0 + x) - x * std::log(x) +
+                             (double)N * std::log(B);
   if (data_S_out) *data_S_out = data_S;
   return model - data_S;
 }
@@ -933,7 +942,7 @@ int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep
         R.ms_rebuild += ms_since(t0);
       }
       ++R.nodal_itrs;
-      S = mdl(m, N, g.E, nullptr);
+      S = mdl(m, N, g.E, nullptr, o.mode.exact);
       if (itr >= o.window - 1) {
         bool isf = std::isfinite(large.S) && std::isfinite(med.S) && std::isfinite(small.S);
         double mean = 0.0;
@@ -1113,6 +1122,13 @@ double orc_mdl(const orc_graph* xg, const int32_t* part, int32_t B, double* data
   Graph g = to_graph(xg);
   BM m = build_bm(g, part, B);
   return mdl(m, g.N, g.E, data_S);
+}
+
+double orc_mdl_mode(const orc_graph* xg, const int32_t* part, int32_t B, int32_t exact,
+                    double* data_S) {
+  Graph g = to_graph(xg);
+  BM m = build_bm(g, part, B);
+  return mdl(m, g.N, g.E, data_S, exact);
 }
 
 void orc_merge_proposals(const orc_graph* xg, const int32_t* part, int32_t B, int32_t np,

@@ -116,6 +116,16 @@ def test_exact_moves_are_mdl_differences(sbp, gs):
 
 
 @pytest.mark.parametrize("name", GRAPHS)
+def test_standard_mdl(sbp, orc, gs, name):
+    g = gs[name]
+    for B in (1, 7, 90):
+        p = _partition(g, B, B)
+        S, d = sbp.mdl(g, p, B, exact=1)
+        S_o, d_o = orc.mdl_mode(g, p, B, exact=1)
+        assert close(S, S_o) and close(d, d_o)
+
+
+@pytest.mark.parametrize("name", GRAPHS)
 @pytest.mark.parametrize("B", [6, 60])
 def test_exact_merge_dS(sbp, orc, gs, name, B):
     g = gs[name]
@@ -169,6 +179,8 @@ def test_partition_exact_mode_matches_oracle(sbp, orc, variant, seed, exact, mh)
     rep = sbp.partition(g, seed=seed, exact=exact, mh=mh)
     lab_o, rep_o, st = orc.partition(g, seed=seed, exact=exact, mh=mh)
     assert st == 0 and rep["status"] == 0
+    # both report the standard description length of their final labels
+    assert close(rep["S"], sbp.mdl(g, g.partitions, rep["B"], exact=1)[0])
     assert abs(rep["S"] - rep_o["S"]) <= 0.01 * abs(rep_o["S"])
 
 

@@ -130,3 +130,25 @@ def test_mh_batch_accepts_uphill_moves_and_quirk_mode_does_not(sbp, orc):
     p_m, _, props, _ = orc.nodal_batch_mode(g, part, B, 3, 0, 0, g.N, exact=1, mh=1, beta=1.0)
     moved = p_m != part
     assert np.array_equal(p_m[moved], props[moved])
+
+
+def test_standard_mdl_formula(sbp, orc):
+    # exact mode's objective: (E h(B^2/E) + N ln B) / ln 2 - data_S, in bits
+    g = graphs.dcsbm("LH", 1500, 9, seed=3)
+    rng = np.random.default_rng(1)
+    for B in (1, 9, 40):
+        p = rng.integers(0, B, g.N).astype(np.int32)
+        p[:B] = np.arange(B, dtype=np.int32)
+        M = _block_matrix(g, p, B)
+        dout, din = M.sum(axis=1), M.sum(axis=0)
+        nz = M > 0
+        data = (M[nz] * np.log2(M[nz])).sum() - (dout[dout > 0] * np.log2(dout[dout > 0])).sum() \
+            - (din[din > 0] * np.log2(din[din > 0])).sum()
+        x = B * B / g.E
+        model = (g.E * ((1 + x) * np.log(1 + x) - x * np.log(x)) + g.N * np.log(B)) / np.log(2)
+        S, d = orc.mdl_mode(g, p, B, exact=1)
+        assert abs(d - data) <= 1e-9 * abs(data)
+        assert abs(S - (model - data)) <= 1e-9 * abs(S)
+        # GSAP's formula (exact = 0) keeps its own model term and the same data_S
+        S6, d6 = orc.mdl_mode(g, p, B, exact=0)
+        assert d6 == d and (S6, d6) == orc.mdl(g, p, B)
