@@ -347,24 +347,62 @@ constexpr size_t kBigSmem = 65536;
 
 struct RbRowsBigBody {
   using Args = RbArgs;
-  static constexpr int kThreads = kBigThreads, kMinBlocks = 1;
+  static constexpr int kThreads = kBigThreads, kMinBlocks = 2;
   static constexpr size_t kSmem = kBigSmem;
   static __device__ void run(const Args& a, int vb, int vg) {
   if (ctl_stopped(a.ctl)) return;
   extern __shared__ unsigned long long big_sm[];
   __shared__ int sh[33];
+  __shared__ uint32_t touched[kHistCap / 32];  // bitmap of the histogram's nonzero columns
   const RbSide& d = a.s[vb & 1];
   vb >>= 1;
   vg >>= 1;
   uint32_t* hist = (uint32_t*)big_sm;
   int nbig = *d.big_count;
   int T = blockDim.x, tid = threadIdx.x;
+  const int nwords = (a.B + 31) >> 5;
+  if (a.B <= kHistCap && vb < nbig) {
+    // every row fits one histogram: it and the bitmap start zero and each
+    // row's extraction clears what the row touched
+    for (int i = tid; i < a.B; i += T) hist[i] = 0u;
+    for (int i = tid; i < nwords; i += T) touched[i] = 0u;
+    __syncthreads();
+  }
   for (int idx = vb; idx < nbig; idx += vg) {
     int b = d.big[idx];
     int base = d.seg[b];
     int n = d.seg[b + 1] - base;
     int running = 0;
-    if (a.B <= kHistCap || n > kSortCap) {
+    if (a.B <= kHistCap) {
+      // histogram of the row plus a bitmap of its columns; the extraction
+      // walks B/32 bitmap words, not B bins, so a row costs O(n + B/32)
+      for (int i = tid; i < n; i += T) {
+        const int c = d.tcol[base + i];
+        atomicAdd(hist + c, d.tw[base + i]);
+        atomicOr(touched + (c >> 5), 1u << (c & 31));
+      }
+      __syncthreads();
+      const int per = (nwords + T - 1) / T;
+      const int x0 = min(nwords, tid * per), x1 = min(nwords, x0 + per);
+      int nz = 0;
+      for (int x = x0; x < x1; ++x) nz += __popc(touched[x]);
+      int tot;
+      int pos = cta_excl_scan(nz, sh, &tot);
+      for (int x = x0; x < x1; ++x) {
+        uint32_t m = touched[x];
+        touched[x] = 0u;
+        while (m) {
+          const int c = (x << 5) + __ffs(m) - 1;
+          m &= m - 1;
+          d.ucol[base + pos] = c;
+          d.uw[base + pos] = hist[c];
+          hist[c] = 0u;
+          ++pos;
+        }
+      }
+      running = tot;
+      __syncthreads();
+    } else if (n > kSortCap) {
       // histogram over column windows of kHistCap
       for (int w0 = 0; w0 < a.B; w0 += kHistCap) {
         int W = min(kHistCap, a.B - w0);

@@ -256,7 +256,7 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
   J.dsum = A.take<double>(max_itr);
   J.dataS = A.take<double>(max_itr);
   J.acc = (long long*)A.take<double>(max_itr);
-  J.heavy = A.take<int32_t>((size_t)N);
+  J.lists = A.take<int32_t>((size_t)N);
   J.err = A.take<int32_t>(2);
   J.ctl = A.take<int32_t>(2);
   if (J.dense_cap > 0) {
@@ -400,10 +400,32 @@ bool heavy_vertex(const Job& J, int32_t v) {
   return J.h_optr[v + 1] - J.h_optr[v] > t || J.h_iptr[v + 1] - J.h_iptr[v] > t;
 }
 
-static NodalAux aux_for(Job& J, const int32_t* heavy, int32_t n) {
+void classify_batch(const Job& J, const int32_t* verts, int32_t lo, int32_t count,
+                    std::vector<int32_t>& out, int32_t n[3]) {
+  const size_t at = out.size();
+  out.resize(at + (size_t)std::max(count, 0));
+  int32_t* o = out.data() + at;
+  n[0] = n[1] = n[2] = 0;
+  for (int pass = 0; pass < 3; ++pass)
+    for (int32_t i = 0; i < count; ++i) {
+      const int32_t v = verts ? verts[i] : lo + i;
+      const int32_t e = (J.h_optr[v + 1] - J.h_optr[v]) + (J.h_iptr[v + 1] - J.h_iptr[v]);
+      const int cls = heavy_vertex(J, v) ? 2 : e <= kSmallEntries ? 0 : 1;
+      if (cls == pass) {
+        o[n[0] + n[1] + n[2]] = i;
+        ++n[pass];
+      }
+    }
+}
+
+NodalAux nodal_lists(Job& J, const int32_t* dev, const int32_t n[3]) {
   NodalAux a;
-  a.heavy = heavy;
-  a.nheavy = n;
+  a.small = dev;
+  a.nsmall = n[0];
+  a.mid = dev + n[0];
+  a.nmid = n[1];
+  a.heavy = dev + n[0] + n[1];
+  a.nheavy = n[2];
   a.err = J.err;
   a.side = J.side;
   a.fork = J.fork;
@@ -663,14 +685,14 @@ sbp_status sbp_delta_mdl_nodal_mode(const sbp_graph_csr* g, const int32_t* part,
   md.mh = logH ? 1 : 0;
   cudaMemcpyAsync(dv, verts, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
   cudaMemcpyAsync(dp, props, 4 * (size_t)nv, cudaMemcpyHostToDevice, J.st);
-  std::vector<int32_t> hv;
-  for (int32_t i = 0; i < nv; ++i)
-    if (heavy_vertex(J, verts[i])) hv.push_back(i);
-  if (!hv.empty())
-    cudaMemcpyAsync(J.heavy, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice, J.st);
+  std::vector<int32_t> lists;
+  int32_t ln[3];
+  classify_batch(J, verts, 0, nv, lists, ln);
+  if (!lists.empty())
+    cudaMemcpyAsync(J.lists, lists.data(), 4 * lists.size(), cudaMemcpyHostToDevice, J.st);
   block_terms_any(J, B, 0, 0, 0, J.st);
   nodal_delta_given(J.g, J.part, J.m, B, is_dense(J, B), nv, dv, dp, dd,
-                    aux_for(J, J.heavy, (int32_t)hv.size()), J.st, md, dl);
+                    nodal_lists(J, J.lists, ln), J.st, md, dl);
   cudaStreamSynchronize(J.st);
   int32_t err_h = 0;
   cudaMemcpy(&err_h, J.err, 4, cudaMemcpyDeviceToHost);
@@ -747,17 +769,18 @@ sbp_status sbp_nodal_batch_mode(const sbp_graph_csr* g, int32_t* part, int32_t B
   sbp_status s = prepare(J, g, part, B, 1, 1);
   if (s != SBP_OK) return s;
   int32_t cnt = hi - lo;
-  std::vector<int32_t> hv;
-  for (int32_t v = lo; v < hi; ++v)
-    if (heavy_vertex(J, v)) hv.push_back(v - lo);
-  if (!hv.empty())
-    SBP_CUDA(cudaMemcpyAsync(J.heavy, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice, J.st));
+  std::vector<int32_t> lists;
+  int32_t ln[3];
+  classify_batch(J, nullptr, lo, cnt, lists, ln);
+  if (!lists.empty())
+    SBP_CUDA(cudaMemcpyAsync(J.lists, lists.data(), 4 * lists.size(), cudaMemcpyHostToDevice,
+                             J.st));
   const bool dense = is_dense(J, B);
   block_terms_any(J, B, 1, seed, seq, J.st);
   SBP_CUDA(cudaMemsetAsync(J.dsum, 0, 8, J.st));
   SBP_CUDA(cudaMemsetAsync(J.acc, 0, 8, J.st));
   nodal_batch_sample(J.g, J.part, J.m, B, dense, seed, seq, lo, cnt, J.newlab, J.rec, J.props,
-                     aux_for(J, J.heavy, (int32_t)hv.size()), J.st, md);
+                     nodal_lists(J, J.lists, ln), J.st, md);
   nodal_commit(J.part, lo, cnt, J.newlab, J.rec, J.dsum, J.acc, nullptr, 0, J.cs, J.st);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());

@@ -41,15 +41,15 @@ void Run::setup_batches() {
   const int nb = o.num_batches;
   BS = J->N / nb;
   batch_entries.assign(nb, 0.0);
-  heavy_all.clear();
-  heavy_off.assign(nb + 1, 0);
+  lists_all.clear();
+  list_off.assign(nb + 1, 0);
+  list_n.assign(3 * (size_t)nb, 0);
   for (int32_t b = 0; b < nb; ++b) {
     int32_t lo = b * BS, hi = (b + 1) * BS;
     batch_entries[b] = (double)(J->h_optr[hi] - J->h_optr[lo]) +
                        (double)(J->h_iptr[hi] - J->h_iptr[lo]);
-    for (int32_t v = lo; v < hi; ++v)
-      if (heavy_vertex(*J, v)) heavy_all.push_back(v - lo);
-    heavy_off[b + 1] = (int32_t)heavy_all.size();
+    classify_batch(*J, nullptr, lo, BS, lists_all, &list_n[3 * (size_t)b]);
+    list_off[b + 1] = (int32_t)lists_all.size();
   }
 }
 
@@ -63,7 +63,7 @@ void Run::start_partition() {
   setup_batches();
   stage = kMerge;
   init = true;
-  upload_heavy = !heavy_all.empty();
+  upload_lists = !lists_all.empty();
 }
 
 void Run::start_sweeps(int32_t B0, uint32_t seq0, int32_t sweeps) {
@@ -78,7 +78,7 @@ void Run::start_sweeps(int32_t B0, uint32_t seq0, int32_t sweeps) {
   init = false;
   build = true;
   zero_itr = true;
-  upload_heavy = !heavy_all.empty();
+  upload_lists = !lists_all.empty();
 }
 
 bool Run::dense() const { return B <= J->dense_eff; }
@@ -223,7 +223,7 @@ void Engine::ensure_slots(int K, int nb) {
 }
 
 void Engine::clear_slots() {
-  for (Slot* s : {&s_iota, &s_heavy, &s_snap, &s_restore, &s_relabel, &s_zero, &m_bt, &m_props,
+  for (Slot* s : {&s_iota, &s_lists, &s_snap, &s_restore, &s_relabel, &s_zero, &m_bt, &m_props,
                   &m_delta, &s_gather})
     s->clear();
   pre_dense.clear();
@@ -278,8 +278,8 @@ void Engine::add_run_work(Run& r) {
   Job& J = *r.J;
   const int32_t N = J.N;
   if (r.init) add_iota(s_iota, J.part, N);
-  if (r.upload_heavy)
-    add_copy(s_heavy, J.heavy, up_dev_ptr(r.up_heavy), r.heavy_all.size());
+  if (r.upload_lists)
+    add_copy(s_lists, J.lists, up_dev_ptr(r.up_lists), r.lists_all.size());
   if (r.snap_slot >= 0) add_copy(s_snap, J.snap[r.snap_slot], J.part, (size_t)N);
   if (r.restore_slot >= 0) add_copy(s_restore, J.part, J.snap[r.restore_slot], (size_t)N);
   if (r.relabel) add_relabel(s_relabel, J.part, N, (const int32_t*)up_dev_ptr(r.up_map));
@@ -326,9 +326,8 @@ void Engine::add_run_work(Run& r) {
         else add_block_terms(s.bt_csr, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
         const int ms = md.slot(dense);
         add_nodal(s.nodal[ms], s.heavy[ms], dense, md, J.g, J.part, J.m, r.B, r.o.seed, seq, lo,
-                  r.BS, J.newlab, J.rec,
-                  nullptr, J.heavy + r.heavy_off[b], r.heavy_off[b + 1] - r.heavy_off[b], J.err,
-                  ctl, nb);
+                  r.BS, J.newlab, J.rec, nullptr,
+                  nodal_lists(J, J.lists + r.list_off[b], &r.list_n[3 * (size_t)b]), ctl, nb);
         if (dense) {
           // the moved vertices' edges, applied to the dense form before the
           // labels change (it reads old and new labels)
@@ -426,7 +425,7 @@ sbp_status Engine::tick() {
   use_graphs = true;
   for (Run* r : runs)
     if (r->stage != Run::kDone && !r->o.use_graphs) use_graphs = false;
-  // pass 1: sweeps to queue, uploads (maps, heavy lists) and readbacks
+  // pass 1: sweeps to queue, uploads (maps, batch lists) and readbacks
   size_t up = 0, rd = 0;
   int nb_max = 0, k_max = 0;
   for (Run* r : runs) {
@@ -442,9 +441,9 @@ sbp_status Engine::tick() {
       r->up_map = up;
       up += align256(4 * r->map.size());
     }
-    if (r->upload_heavy) {
-      r->up_heavy = up;
-      up += align256(4 * r->heavy_all.size());
+    if (r->upload_lists) {
+      r->up_lists = up;
+      up += align256(4 * r->lists_all.size());
     }
     r->rd_off = rd;
     rd += rd_bytes(*r);
@@ -461,12 +460,12 @@ sbp_status Engine::tick() {
     if (r->stage == Run::kDone) continue;
     if (r->relabel)
       std::memcpy((char*)up_host + r->up_map, r->map.data(), 4 * r->map.size());
-    if (r->upload_heavy)
-      std::memcpy((char*)up_host + r->up_heavy, r->heavy_all.data(), 4 * r->heavy_all.size());
+    if (r->upload_lists)
+      std::memcpy((char*)up_host + r->up_lists, r->lists_all.data(), 4 * r->lists_all.size());
     add_run_work(*r);
   }
   // pass 3: pack the slots' records and offsets
-  std::vector<Slot*> order = {&s_iota, &s_heavy, &s_snap, &s_restore, &s_relabel, &s_zero};
+  std::vector<Slot*> order = {&s_iota, &s_lists, &s_snap, &s_restore, &s_relabel, &s_zero};
   for (Slot* x : pre_dense.all()) order.push_back(x);
   for (Slot* x : pre_rebuild.all()) order.push_back(x);
   for (Slot* x : {&m_bt, &m_props, &m_delta}) order.push_back(x);
@@ -692,7 +691,7 @@ sbp_status Engine::tick() {
     r->R.ms_rebuild += ms_pre;
     const char* rdp = (const char*)rd_host + r->rd_off;
     r->init = false;
-    r->upload_heavy = false;
+    r->upload_lists = false;
     r->snap_slot = -1;
     r->restore_slot = -1;
     r->relabel = false;

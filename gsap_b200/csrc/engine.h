@@ -52,16 +52,18 @@ struct Run {
   Bracket large, med, small;
   double S = 0.0;
   std::vector<double> itr_dS;
-  std::vector<int32_t> heavy_all, heavy_off;
+  // per batch b, vertices by nodal kernel path (classify_batch): groups of
+  // sizes list_n[3b .. 3b+2] starting at list_off[b] in lists_all
+  std::vector<int32_t> lists_all, list_off, list_n;
   std::vector<double> batch_entries;
   double nnz_now = 0.0;
   // device work left pending by the last host decision
-  bool init = false, upload_heavy = false, relabel = false, build = false, zero_itr = false;
+  bool init = false, upload_lists = false, relabel = false, build = false, zero_itr = false;
   bool csr_fresh = false;
   int snap_slot = -1, restore_slot = -1;
   std::vector<int32_t> map;  // merge map, uploaded for the relabel
   // this tick's offsets in the upload and readback buffers
-  size_t up_map = 0, up_heavy = 0, rd_off = 0;
+  size_t up_map = 0, up_lists = 0, rd_off = 0;
   cudaEvent_t ev_begin = nullptr;
   // scheduler / server bookkeeping
   double admit_bytes = 0.0;
@@ -121,7 +123,7 @@ class Engine {
   void reset();
 
  private:
-  Slot s_iota, s_heavy, s_snap, s_restore, s_relabel, s_zero;
+  Slot s_iota, s_lists, s_snap, s_restore, s_relabel, s_zero;
   DenseBuildSlots pre_dense;
   RebuildSlots pre_rebuild;
   Slot m_bt, m_props, m_delta;

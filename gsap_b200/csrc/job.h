@@ -53,7 +53,7 @@ struct Job {
   int32_t *part = nullptr, *newlab = nullptr, *props = nullptr, *best = nullptr, *map = nullptr;
   int32_t* snap[3] = {nullptr, nullptr, nullptr};
   double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
-  int32_t* heavy = nullptr;     // batch indices of the CTA-per-vertex kernel
+  int32_t* lists = nullptr;     // batch indices by nodal kernel path (classify_batch)
   int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
   int32_t* ctl = nullptr;       // sweep control: sweeps done in the outer step, stop flag
   CommitScratch cs;
@@ -103,6 +103,13 @@ inline ScoreMode score_mode(const sbp_options& o) {
   return m;
 }
 bool heavy_vertex(const Job& J, int32_t v);
+// Appends the batch indices i in [0, count) of vertices lo + i (verts[i]
+// when verts is given) to `out`, grouped by nodal kernel path: small, mid,
+// heavy (NodalAux); n[k] receives the group sizes.
+void classify_batch(const Job& J, const int32_t* verts, int32_t lo, int32_t count,
+                    std::vector<int32_t>& out, int32_t n[3]);
+// The NodalAux of groups of sizes n[3] stored back to back at `dev`.
+NodalAux nodal_lists(Job& J, const int32_t* dev, const int32_t n[3]);
 sbp_status check_options(const sbp_options* o);
 
 struct Timer {

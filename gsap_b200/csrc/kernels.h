@@ -173,11 +173,12 @@ void add_iota(Slot& s, int32_t* p, int32_t n);
 // CTA-per-vertex kernel's (heavy vertices) to `heavy`.  Use separate slots
 // per md.slot(dense): dense and CSR jobs, GSAP-mode and general-mode jobs
 // run different kernels.
+struct NodalAux;
 void add_nodal(Slot& warp, Slot& heavy, bool dense, const ScoreMode& md, const DevGraph& g,
                const int32_t* part,
                const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
-               int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
-               int32_t nheavy, int32_t* err, const int32_t* ctl = nullptr, uint32_t seq_mul = 0);
+               int32_t* newlab, double* rec, int32_t* props, const NodalAux& lists,
+               const int32_t* ctl = nullptr, uint32_t seq_mul = 0);
 void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                 const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
                 int32_t B, const CommitScratch& cs, const int32_t* ctl = nullptr,
@@ -232,9 +233,17 @@ cudaError_t init_nodal_attributes();
 // CTA-per-vertex kernel.
 int nodal_heavy_threshold();
 
-// Heavy-vertex list of a batch (indices into the batch) and the side stream
-// it runs on; err counts hash-table overflows (should stay 0).
+// A batch's vertices (indices into the batch) by kernel path: small ones
+// (at most kSmallEntries neighbour entries) go two to a warp, mid ones one to
+// a warp, heavy ones (more than nodal_heavy_threshold() entries in a
+// direction) one to a CTA on the side stream.  err counts hash-table
+// overflows (should stay 0).
+constexpr int32_t kSmallEntries = 16;
 struct NodalAux {
+  const int32_t* small = nullptr;
+  int32_t nsmall = 0;
+  const int32_t* mid = nullptr;
+  int32_t nmid = 0;
   const int32_t* heavy = nullptr;
   int32_t nheavy = 0;
   int32_t* err = nullptr;

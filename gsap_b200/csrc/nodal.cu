@@ -72,6 +72,8 @@ struct NodalArgs {
   double* dS_raw;
   const int32_t* heavy;     // batch indices handled by the CTA kernel
   int32_t nheavy;
+  const int32_t *small, *mid;  // batch indices of the warp kernel: two small ones per warp,
+  int32_t nsmall, nmid;        // one mid one per warp
   int32_t* err;             // error counter (hash table overflow)
   const int32_t* ctl;       // sweep control: gate, and seq += ctl[0] * seq_mul
   uint32_t seq_mul;
@@ -177,18 +179,20 @@ __device__ __forceinline__ void entry(const NodalArgs& a, const Rows<DENSE>& R, 
 }
 
 // Adds the corner cells (r,r), (r,s), (s,r), (s,s) of M and the row-degree
-// terms to lanes 0..12 of the calling warp (call it from one warp of the
-// group, after m4..m7 hold the group totals).  kernels.hpp:1506-1510,
-// 1573-1578, 1663-1669, 1718-1723 give the new corner counts.
+// terms to lanes 0..12 of the calling lane group (lane `lane` of the group
+// starting at warp lane hb; a warp, or a half-warp with its own vertex; call
+// it from one warp of a CTA group, after m4..m7 hold the group totals).
+// kernels.hpp:1506-1510, 1573-1578, 1663-1669, 1718-1723 give the new
+// corner counts.
 template <bool DENSE>
 __device__ __forceinline__ void corner_terms(const NodalArgs& a, const Rows<DENSE>& R, int v,
                                              int r, int s, uint32_t koR, uint32_t koS,
-                                             uint32_t niR, uint32_t niS, Acc& q) {
-  const int lane = threadIdx.x & 31;
+                                             uint32_t niR, uint32_t niS, Acc& q, int lane,
+                                             int hb) {
   // lane 0: M[r][r], 1: M[r][s], 2: M[s][r], 3: M[s][s]
   const uint32_t mm = lane < 4 ? R.out_at((lane & 2) != 0, (lane & 1) ? s : r) : 0u;
-  const uint32_t Mrr = __shfl_sync(kFull, mm, 0), Mrs = __shfl_sync(kFull, mm, 1);
-  const uint32_t Msr = __shfl_sync(kFull, mm, 2), Mss = __shfl_sync(kFull, mm, 3);
+  const uint32_t Mrr = __shfl_sync(kFull, mm, hb), Mrs = __shfl_sync(kFull, mm, hb + 1);
+  const uint32_t Msr = __shfl_sync(kFull, mm, hb + 2), Mss = __shfl_sync(kFull, mm, hb + 3);
   const uint32_t xrr = Mrr - koR - niR;
   const uint32_t xrs = Mrs != 0u ? Mrs - koS + niR : niR;
   const uint32_t xsr = Msr + koR - niS;
@@ -313,7 +317,8 @@ __device__ double finish(const NodalArgs& a, const Rows<DENSE>& R, int v, int r,
   q.m5 = (int)grp.sum_ll(q.m5);
   q.m6 = (int)grp.sum_ll(q.m6);
   q.m7 = (int)grp.sum_ll(q.m7);
-  if (G == 32 || threadIdx.x < 32) corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
+  if (G == 32 || threadIdx.x < 32)
+    corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q, threadIdx.x & 31, 0);
   return grp.sum(q.acc);
 }
 
@@ -390,7 +395,7 @@ __device__ __forceinline__ double delta_from_entries(const NodalArgs& a, const R
   q.m5 = __reduce_add_sync(kFull, q.m5);
   q.m6 = __reduce_add_sync(kFull, q.m6);
   q.m7 = __reduce_add_sync(kFull, q.m7);
-  corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
+  corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q, lane, 0);
   return warp_sum(q.acc);
 }
 
@@ -600,9 +605,93 @@ __device__ __forceinline__ void write_result(const NodalArgs& a, bool given, int
   }
 }
 
-__device__ __forceinline__ bool is_heavy(int no, int ni) {
-  return no > kWarpList || ni > kWarpList;
+// Sum over a lane group of W lanes (32: the warp, 16: each half-warp).
+template <int W>
+__device__ __forceinline__ double group_sum(double x) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
 }
+
+// dS of a vertex whose entries fit one lane group of W lanes (entry c, wt,
+// direction `in` on lane hl of the group; delta_from_entries for one pass).
+// The group's masks keep the two half-warps' vertices apart.
+template <bool DENSE, int W>
+__device__ __forceinline__ double delta_group(const NodalArgs& a, const Rows<DENSE>& R, int v,
+                                              int r, int s, int32_t c, uint32_t wt, bool in,
+                                              bool valid, int lane) {
+  const int hl = lane & (W - 1), hb = lane & (32 - W);
+  const unsigned gm = W == 32 ? kFull : (0xFFFFu << hb);
+  const bool o = valid && !in, i = valid && in;
+  RsWeights w;
+  w.koR = __reduce_add_sync(gm, o && c == r ? wt : 0u);
+  w.koS = __reduce_add_sync(gm, o && c == s ? wt : 0u);
+  w.niR = __reduce_add_sync(gm, i && c == r ? wt : 0u);
+  w.niS = __reduce_add_sync(gm, i && c == s ? wt : 0u);
+  // direction in the top bit, unique keys for idle lanes
+  const unsigned key = valid ? ((unsigned)c | (in ? 0x80000000u : 0u)) : (0x7fffffe0u + (unsigned)lane);
+  const unsigned peers = __match_any_sync(gm, key);
+  const uint32_t kc = __reduce_add_sync(peers, wt);
+  Acc q;
+  if (valid) entry<DENSE>(a, R, r, s, w.niS, in, c, wt, lane == __ffs(peers) - 1, kc, q);
+  q.m4 = __reduce_add_sync(gm, q.m4);
+  q.m5 = __reduce_add_sync(gm, q.m5);
+  q.m6 = __reduce_add_sync(gm, q.m6);
+  q.m7 = __reduce_add_sync(gm, q.m7);
+  corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q, hl, hb);
+  return group_sum<W>(q.acc);
+}
+
+// Proposal, dS and accept of batch vertex i when its entries fit one lane
+// group of W lanes: one entry per lane, loaded once for the neighbour pick
+// (out- then in-entries, pick_neighbour's order) and for the dS.  With
+// W = 16 each half-warp takes a vertex of at most 16 entries; both halves
+// run every warp-wide step, and a half without a vertex of its own
+// (active = false) repeats its partner's and writes nothing.
+template <bool DENSE, int W>
+__device__ __forceinline__ void fused_group(const NodalArgs& a, int i, bool active, int lane) {
+  const int hl = lane & (W - 1), hb = lane & (32 - W);
+  const unsigned gm = W == 32 ? kFull : (0xFFFFu << hb);
+  const int v = a.lo + i;
+  const int32_t o0 = a.optr[v], no = a.optr[v + 1] - o0;
+  const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
+  const P4 x = draw(a.seed, kRngNodalVertex, a.seq + ctl_itr(a.ctl) * a.seq_mul, (uint32_t)v);
+  const int rnd = (int)(x.v[0] % (uint32_t)a.B);
+  const bool in = hl >= no;
+  const bool valid = hl < no + ni;
+  const int k = in ? hl - no : hl;
+  int32_t c = -1;
+  uint32_t w = 0u;
+  if (valid) {
+    const int32_t u = in ? __ldg(a.iidx + i0 + k) : __ldg(a.oidx + o0 + k);
+    w = in ? __ldg(a.iw + i0 + k) : __ldg(a.ow + o0 + k);
+    c = __ldg(a.part + u);
+  }
+  const int r = a.part[v];
+  const uint64_t deg = (uint64_t)a.kdo[v] + a.kdi[v];
+  const uint64_t t = scale_draw(x.v[1], deg);
+  uint64_t incl = w;
+#pragma unroll
+  for (int o = 1; o < W; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(kFull, incl, o);
+    if (hl >= o) incl += y;
+  }
+  const unsigned hit = __ballot_sync(kFull, valid && incl > t) & gm;
+  const int ch = __shfl_sync(kFull, c, hit ? __ffs(hit) - 1 : lane);
+  int s = rnd;
+  if (deg != 0) {
+    const int cu = hit ? ch : a.part[0];
+    s = a.use_rand[cu] ? rnd : a.nbr_s[cu];
+  }
+  double d = 0.0;
+  if (__any_sync(kFull, r != s)) {
+    const Rows<DENSE> R(a, r, s);
+    d = delta_group<DENSE, W>(a, R, v, r, s, c, w, in, valid, lane);
+  }
+  if (hl == 0 && active) write_result(a, false, i, r, s, r != s ? d : 0.0);
+  __syncwarp();
+}
+
 
 // ------------------------------------------------------------ general mode --
 // Kernels instantiated with GEN = true score a move by the exact change of
@@ -731,7 +820,7 @@ __device__ double finish_gen(const NodalArgs& a, const Rows<DENSE>& R, int v, in
     q.m6 = (int)grp.sum_ll(q.m6);
     q.m7 = (int)grp.sum_ll(q.m7);
     if (G == 32 || threadIdx.x < 32)
-      corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q);
+      corner_terms<DENSE>(a, R, v, r, s, w.koR, w.koS, w.niR, w.niS, q, threadIdx.x & 31, 0);
   }
   logH = 0.0;
   if (a.mh) {
@@ -966,6 +1055,63 @@ __device__ __forceinline__ void write_result_gen(const NodalArgs& a, bool given,
   if (a.props_out) a.props_out[i] = s;
 }
 
+// One vertex (batch index i) on the whole warp: the fused path when its
+// entries fit the warp (sampled proposals, GSAP scoring), else the proposal
+// by pick_neighbour and the dS from registers (both lists within a warp)
+// or from sorted shared-memory lists.
+template <bool GIVEN, bool DENSE, bool GEN>
+__device__ __forceinline__ void warp_vertex(const NodalArgs& a, int i, int lane,
+                                            unsigned long long* sko, unsigned long long* ski) {
+  const Group<32> grp{nullptr};
+  const int vv = GIVEN ? a.verts[i] : a.lo + i;
+  const int32_t o0 = a.optr[vv], no = a.optr[vv + 1] - o0;
+  const int32_t i0 = a.iptr[vv], ni = a.iptr[vv + 1] - i0;
+  if constexpr (GEN) {
+    int v, s;
+    uint32_t u2;
+    item<GIVEN>(a, i, lane, v, s, u2);
+    const int r = a.part[v];
+    double d = 0.0, lh = 0.0;
+    if (r != s) {
+      if (no + ni <= 32) {
+        d = delta_registers_gen<DENSE>(a, v, r, s, o0, no, i0, ni, lane, lh);
+      } else {
+        stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, sko, grp);
+        stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, ski, grp);
+        d = delta_sorted_gen<DENSE, 32>(a, v, r, s, sko, no, ski, ni, grp, lh);
+      }
+    }
+    if (lane == 0) write_result_gen(a, GIVEN, i, r, s, d, lh, u2);
+    __syncwarp();
+    return;
+  }
+  if (!GIVEN && no + ni <= 32) {
+    fused_group<DENSE, 32>(a, i, true, lane);
+    return;
+  }
+  int v, s;
+  uint32_t u2;
+  item<GIVEN>(a, i, lane, v, s, u2);
+  const int r = a.part[v];
+  double d = 0.0;
+  if (r != s) {
+    if (no <= 32 && ni <= 32) {
+      d = delta_registers<DENSE>(a, v, r, s, o0, no, i0, ni, lane);
+    } else {
+      stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, sko, grp);
+      stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, ski, grp);
+      d = delta_sorted<DENSE, 32>(a, v, r, s, sko, no, ski, ni, grp);
+    }
+  }
+  if (lane == 0) write_result(a, GIVEN, i, r, s, d);
+  __syncwarp();
+}
+
+// Warp work items of a batch: pairs of small vertices, then mid vertices.
+__host__ __device__ __forceinline__ int nodal_items(int nsmall, int nmid) {
+  return (nsmall + 1) / 2 + nmid;
+}
+
 template <bool GIVEN, bool DENSE, bool GEN>
 struct NodalBody {
   using Args = NodalArgs;
@@ -976,90 +1122,25 @@ struct NodalBody {
   __shared__ unsigned long long s_ko[kNodalWarps][kWarpList], s_ki[kNodalWarps][kWarpList];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = vg * kNodalWarps;
-  Group<32> grp{nullptr};
-  for (int i = vb * kNodalWarps + wid; i < a.count; i += nw) {
-    const int vv = GIVEN ? a.verts[i] : a.lo + i;
-    const int32_t o0 = a.optr[vv], no = a.optr[vv + 1] - o0;
-    const int32_t i0 = a.iptr[vv], ni = a.iptr[vv + 1] - i0;
-    if (is_heavy(no, ni)) continue;  // the CTA kernel's
-    if constexpr (GEN) {
-      int v, s;
-      uint32_t u2;
-      item<GIVEN>(a, i, lane, v, s, u2);
-      const int r = a.part[v];
-      double d = 0.0, lh = 0.0;
-      if (r != s) {
-        if (no + ni <= 32) {
-          d = delta_registers_gen<DENSE>(a, v, r, s, o0, no, i0, ni, lane, lh);
-        } else {
-          stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, s_ko[wid], grp);
-          stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, s_ki[wid], grp);
-          d = delta_sorted_gen<DENSE, 32>(a, v, r, s, s_ko[wid], no, s_ki[wid], ni, grp, lh);
-        }
-      }
-      if (lane == 0) write_result_gen(a, GIVEN, i, r, s, d, lh, u2);
-      __syncwarp();
-      continue;
-    }
-    if (!GIVEN && no + ni <= 32) {
-      // one entry per lane, loaded once: the proposal's neighbour pick (out-
-      // then in-entries, pick_neighbour's order) and the dS both read it
-      const int v = vv;
-      const P4 x = draw(a.seed, kRngNodalVertex, a.seq + ctl_itr(a.ctl) * a.seq_mul, (uint32_t)v);
-      const int rnd = (int)(x.v[0] % (uint32_t)a.B);
-      const bool in = lane >= no;
-      const bool valid = lane < no + ni;
-      const int k = in ? lane - no : lane;
-      int32_t c = -1;
-      uint32_t w = 0u;
-      if (valid) {
-        const int32_t u = in ? __ldg(a.iidx + i0 + k) : __ldg(a.oidx + o0 + k);
-        w = in ? __ldg(a.iw + i0 + k) : __ldg(a.ow + o0 + k);
-        c = __ldg(a.part + u);
-      }
-      const int r = a.part[v];
-      const uint64_t deg = (uint64_t)a.kdo[v] + a.kdi[v];
-      int s = rnd;
-      if (deg != 0) {
-        const uint64_t t = scale_draw(x.v[1], deg);
-        uint64_t incl = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint64_t y = __shfl_up_sync(kFull, incl, o);
-          if (lane >= o) incl += y;
-        }
-        const unsigned hit = __ballot_sync(kFull, valid && incl > t);
-        const int cu = hit ? __shfl_sync(kFull, c, __ffs(hit) - 1) : a.part[0];
-        s = a.use_rand[cu] ? rnd : a.nbr_s[cu];
-      }
-      double d = 0.0;
-      if (r != s) {
-        const Rows<DENSE> R(a, r, s);
-        const int32_t cs[2] = {c, -1};
-        const uint32_t ws[2] = {w, 0u};
-        const bool ins[2] = {in, false}, valids[2] = {valid, false};
-        d = delta_from_entries<DENSE>(a, R, v, r, s, 1, cs, ws, ins, valids, lane);
-      }
-      if (lane == 0) write_result(a, false, i, r, s, d);
-      __syncwarp();
-      continue;
-    }
-    int v, s;
-    uint32_t u2;
-    item<GIVEN>(a, i, lane, v, s, u2);
-    const int r = a.part[v];
-    double d = 0.0;
-    if (r != s) {
-      if (no <= 32 && ni <= 32) {
-        d = delta_registers<DENSE>(a, v, r, s, o0, no, i0, ni, lane);
-      } else {
-        stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, s_ko[wid], grp);
-        stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, s_ki[wid], grp);
-        d = delta_sorted<DENSE, 32>(a, v, r, s, s_ko[wid], no, s_ki[wid], ni, grp);
+  const int npairs = (a.nsmall + 1) / 2;
+  const int items = npairs + a.nmid;
+  for (int it = vb * kNodalWarps + wid; it < items; it += nw) {
+    int ia, ib = -1;
+    if (it >= npairs) {
+      ia = a.mid[it - npairs];
+    } else {
+      ia = a.small[2 * it];
+      const bool two = 2 * it + 1 < a.nsmall;
+      ib = two ? a.small[2 * it + 1] : -1;
+      if constexpr (!GIVEN && !GEN) {
+        // two vertices of at most 16 entries, one per half-warp
+        fused_group<DENSE, 16>(a, lane < 16 || !two ? ia : ib, lane < 16 || two, lane);
+        continue;
       }
     }
-    if (lane == 0) write_result(a, GIVEN, i, r, s, d);
-    __syncwarp();
+    // one call site, so that the body stays inline
+    for (int q = 0; q < (ib >= 0 ? 2 : 1); ++q)
+      warp_vertex<GIVEN, DENSE, GEN>(a, q ? ib : ia, lane, s_ko[wid], s_ki[wid]);
   }
   }
 };
@@ -1249,12 +1330,17 @@ NodalArgs make_args(const DevGraph& g, const int32_t* part, const DevBM& m, int3
   a.B = B;
   a.heavy = aux.heavy;
   a.nheavy = aux.nheavy;
+  a.small = aux.small;
+  a.nsmall = aux.nsmall;
+  a.mid = aux.mid;
+  a.nmid = aux.nmid;
   a.err = aux.err;
   return a;
 }
 
-int nodal_grid(int count) {
-  int g = (count + kNodalWarps - 1) / kNodalWarps;
+// CTAs of the warp kernel: one warp per work item.
+int nodal_grid(const NodalArgs& a) {
+  int g = (nodal_items(a.nsmall, a.nmid) + kNodalWarps - 1) / kNodalWarps;
   return g < 1 ? 1 : (g > 148 * 64 ? 148 * 64 : g);
 }
 
@@ -1267,7 +1353,7 @@ void launch_pair(const NodalArgs& a, const NodalAux& aux, cudaStream_t st) {
     launch_single<NodalHeavyBody<GIVEN, DENSE, GEN>>(a, std::min(a.nheavy, 2 * 148), aux.side);
     cudaEventRecord(aux.join, aux.side);
   }
-  launch_single<NodalBody<GIVEN, DENSE, GEN>>(a, nodal_grid(a.count), st);
+  launch_single<NodalBody<GIVEN, DENSE, GEN>>(a, nodal_grid(a), st);
   if (a.nheavy > 0) cudaStreamWaitEvent(st, aux.join, 0);
 }
 
@@ -1367,13 +1453,9 @@ void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newla
 void add_nodal(Slot& warp, Slot& heavy, bool dense, const ScoreMode& md, const DevGraph& g,
                const int32_t* part,
                const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
-               int32_t* newlab, double* rec, int32_t* props, const int32_t* heavy_list,
-               int32_t nheavy, int32_t* err, const int32_t* ctl, uint32_t seq_mul) {
+               int32_t* newlab, double* rec, int32_t* props, const NodalAux& aux,
+               const int32_t* ctl, uint32_t seq_mul) {
   if (count <= 0) return;
-  NodalAux aux;
-  aux.heavy = heavy_list;
-  aux.nheavy = nheavy;
-  aux.err = err;
   NodalArgs a = make_args(g, part, m, B, aux);
   a.seed = seed;
   a.seq = seq;
@@ -1385,8 +1467,9 @@ void add_nodal(Slot& warp, Slot& heavy, bool dense, const ScoreMode& md, const D
   a.ctl = ctl;
   a.seq_mul = seq_mul;
   set_mode(a, md);
-  slot_push(slot_bind(warp, kmNodal[md.slot(dense)]), a, ceil_div(count, kNodalWarps));
-  slot_push(slot_bind(heavy, kmNodalHeavy[md.slot(dense)]), a, nheavy);
+  slot_push(slot_bind(warp, kmNodal[md.slot(dense)]), a,
+            ceil_div(nodal_items(aux.nsmall, aux.nmid), kNodalWarps));
+  slot_push(slot_bind(heavy, kmNodalHeavy[md.slot(dense)]), a, aux.nheavy);
 }
 
 void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
