@@ -623,11 +623,20 @@ struct DenseArgs {
   const uint32_t *ow, *iw, *kdo, *kdi;
   const int32_t* part;
   const int32_t* newlab;  // update: new labels of vertices lo..lo+count-1
-  uint32_t *Md, *MTd, *d_out, *d_in;
+  uint32_t *Md, *MTd, *Sd, *d_out, *d_in;
   double *ld_out, *ld_in;
   const int32_t* ctl;
   int32_t N, E, B, lo, count, pad;
 };
+
+// Chunk sums of a dense cell (r, c): out-row r's chunk of column c and
+// in-row c's chunk of row r (DevBM::Sd).
+__device__ __forceinline__ uint32_t* sd_out(uint32_t* Sd, int K, int r, int c) {
+  return Sd + (size_t)r * 2 * K + (c >> 5);
+}
+__device__ __forceinline__ uint32_t* sd_in(uint32_t* Sd, int K, int r, int c) {
+  return Sd + (size_t)c * 2 * K + K + (r >> 5);
+}
 
 // Build step 1: every edge adds its weight to M[r][c] (and the transpose).
 struct DenseEdgesBody {
@@ -639,8 +648,11 @@ struct DenseEdgesBody {
     if (j >= a.E) return;
     int r = __ldg(a.part + __ldg(a.osrc + j)), c = __ldg(a.part + __ldg(a.oidx + j));
     uint32_t w = __ldg(a.ow + j);
+    const int K = (a.B + 31) >> 5;
     atomicAdd(a.Md + (size_t)r * a.B + c, w);
     atomicAdd(a.MTd + (size_t)c * a.B + r, w);
+    atomicAdd(sd_out(a.Sd, K, r, c), w);
+    atomicAdd(sd_in(a.Sd, K, r, c), w);
   }
 };
 
@@ -692,7 +704,8 @@ struct DenseUpdateBody {
   const int32_t* __restrict__ part = a.part;
   const int32_t* __restrict__ newlab = a.newlab;
   const int32_t lo = a.lo, count = a.count, B = a.B;
-  uint32_t *Md = a.Md, *MTd = a.MTd, *d_out = a.d_out, *d_in = a.d_in;
+  uint32_t *Md = a.Md, *MTd = a.MTd, *Sd = a.Sd, *d_out = a.d_out, *d_in = a.d_in;
+  const int K = (B + 31) >> 5;
   const int lane = threadIdx.x & 31;
   const int w0 = (vb * blockDim.x + threadIdx.x) >> 5;
   const int nw = (vg * blockDim.x) >> 5;
@@ -715,6 +728,10 @@ struct DenseUpdateBody {
       atomicSub(MTd + (size_t)bo * B + r, wt);
       atomicAdd(Md + (size_t)s * B + bn, wt);
       atomicAdd(MTd + (size_t)bn * B + s, wt);
+      atomicSub(sd_out(Sd, K, r, bo), wt);
+      atomicSub(sd_in(Sd, K, r, bo), wt);
+      atomicAdd(sd_out(Sd, K, s, bn), wt);
+      atomicAdd(sd_in(Sd, K, s, bn), wt);
     }
     for (int j = iptr[v] + lane; j < iptr[v + 1]; j += 32) {
       const int u = __ldg(iidx + j);
@@ -725,6 +742,10 @@ struct DenseUpdateBody {
       atomicSub(MTd + (size_t)r * B + bu, wt);
       atomicAdd(Md + (size_t)bu * B + s, wt);
       atomicAdd(MTd + (size_t)s * B + bu, wt);
+      atomicSub(sd_out(Sd, K, bu, r), wt);
+      atomicSub(sd_in(Sd, K, bu, r), wt);
+      atomicAdd(sd_out(Sd, K, bu, s), wt);
+      atomicAdd(sd_in(Sd, K, bu, s), wt);
     }
   }
   }
@@ -732,24 +753,38 @@ struct DenseUpdateBody {
 
 // First column k of dense out-row ++ in-row of block b whose running count
 // exceeds t (zero columns never advance the count, so this is the same
-// entry as in the CSR rows); the whole warp returns it, or -1.
-__device__ int warp_pick_dense(const uint32_t* orow, const uint32_t* irow, int B, uint64_t t,
-                               int lane) {
+// entry as in the CSR rows); the whole warp returns it, or -1.  Found
+// through the rows' chunk sums (DevBM::Sd, 2K of them: the out-row's K
+// chunks, then the in-row's): the chunk whose running count first exceeds
+// t, then the column inside it, reading 2K + 32 words instead of up to 2B.
+__device__ int warp_pick_chunked(const uint32_t* orow, const uint32_t* irow,
+                                 const uint32_t* srow, int B, int K, uint64_t t, int lane) {
   uint64_t acc = 0;
-  for (int k0 = 0; k0 < 2 * B; k0 += 32) {
-    int k = k0 + lane;
-    uint64_t w = 0;
-    if (k < 2 * B) w = k < B ? orow[k] : irow[k - B];
+  for (int k0 = 0; k0 < 2 * K; k0 += 32) {
+    const int k = k0 + lane;
+    const uint64_t w = k < 2 * K ? __ldg(srow + k) : 0u;
     uint64_t incl = w;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      uint64_t y = __shfl_up_sync(kFull, incl, o);
+      const uint64_t y = __shfl_up_sync(kFull, incl, o);
       if (lane >= o) incl += y;
     }
-    unsigned hit = __ballot_sync(kFull, k < 2 * B && acc + incl > t);
+    const unsigned hit = __ballot_sync(kFull, k < 2 * K && acc + incl > t);
     if (hit) {
-      int kk = k0 + __ffs(hit) - 1;
-      return kk < B ? kk : kk - B;
+      const int j = __ffs(hit) - 1;
+      const uint64_t base = acc + __shfl_sync(kFull, incl - w, j);  // count before chunk k0+j
+      const int kc = k0 + j;
+      const int c0 = (kc < K ? kc : kc - K) * 32;
+      const uint32_t* row = kc < K ? orow : irow;
+      const int c = c0 + lane;
+      uint64_t in2 = c < B ? __ldg(row + c) : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(kFull, in2, o);
+        if (lane >= o) in2 += y;
+      }
+      const unsigned h2 = __ballot_sync(kFull, c < B && base + in2 > t);
+      return h2 ? c0 + __ffs(h2) - 1 : -1;
     }
     acc += __shfl_sync(kFull, incl, 31);
   }
@@ -783,7 +818,7 @@ __device__ __forceinline__ double dense_row_sum(const double* tab, const uint32_
 
 struct BtDenseArgs {
   const double* xlx;
-  const uint32_t *Md, *MTd, *d_out, *d_in;
+  const uint32_t *Md, *MTd, *Sd, *d_out, *d_in;
   const double *ld_out, *ld_in;
   double *dSout, *ambout, *ambin, *sinfull;
   int32_t* nbr_s;
@@ -826,7 +861,9 @@ struct BlockTermsDenseBody {
       uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
       int nb = 0;
       if (deg > 0) {
-        int c = warp_pick_dense(orow, irow, B, scale_draw(x.v[1], deg), lane);
+        const int K = (B + 31) >> 5;
+        int c = warp_pick_chunked(orow, irow, a.Sd + (size_t)b * 2 * K, B, K,
+                                  scale_draw(x.v[1], deg), lane);
         nb = c >= 0 ? c : 0;
       }
       if (lane == 0) {
@@ -1020,7 +1057,7 @@ BtArgs bt_args(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq) {
 BtDenseArgs bt_dense_args(DevBM& m, int32_t B, int draws, uint64_t seed, uint32_t seq) {
   BtDenseArgs a{};
   a.xlx = m.xlx;
-  a.Md = m.Md; a.MTd = m.MTd; a.d_out = m.d_out; a.d_in = m.d_in;
+  a.Md = m.Md; a.MTd = m.MTd; a.Sd = m.Sd; a.d_out = m.d_out; a.d_in = m.d_in;
   a.ld_out = m.ld_out; a.ld_in = m.ld_in;
   a.dSout = m.dSout; a.ambout = m.ambout; a.ambin = m.ambin; a.sinfull = m.sinfull;
   a.nbr_s = m.nbr_s; a.use_rand = m.use_rand;
@@ -1033,7 +1070,7 @@ DenseArgs dense_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m
   a.osrc = g.osrc; a.optr = g.optr; a.oidx = g.oidx; a.iptr = g.iptr; a.iidx = g.iidx;
   a.ow = g.ow; a.iw = g.iw; a.kdo = g.kdo; a.kdi = g.kdi;
   a.part = part;
-  a.Md = m.Md; a.MTd = m.MTd; a.d_out = m.d_out; a.d_in = m.d_in;
+  a.Md = m.Md; a.MTd = m.MTd; a.Sd = m.Sd; a.d_out = m.d_out; a.d_in = m.d_in;
   a.ld_out = m.ld_out; a.ld_in = m.ld_in;
   a.N = g.N; a.E = g.E; a.B = B;
   return a;
@@ -1154,6 +1191,7 @@ void dense_build(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m, cu
   size_t bb = (size_t)B * B;
   cudaMemsetAsync(m.Md, 0, bb * sizeof(uint32_t), st);
   cudaMemsetAsync(m.MTd, 0, bb * sizeof(uint32_t), st);
+  cudaMemsetAsync(m.Sd, 0, (size_t)2 * B * ((B + 31) / 32) * sizeof(uint32_t), st);
   cudaMemsetAsync(m.d_out, 0, (size_t)B * sizeof(uint32_t), st);
   cudaMemsetAsync(m.d_in, 0, (size_t)B * sizeof(uint32_t), st);
   DenseArgs a = dense_args(g, part, B, m);
@@ -1298,6 +1336,7 @@ void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part,
   const size_t bb = (size_t)B * B;
   add_zero(s.zero, m.Md, bb);
   add_zero(s.zero, m.MTd, bb);
+  add_zero(s.zero, m.Sd, (size_t)2 * B * ((B + 31) / 32));
   add_zero(s.zero, m.d_out, (size_t)B);
   add_zero(s.zero, m.d_in, (size_t)B);
   DenseArgs a = dense_args(g, part, B, m);

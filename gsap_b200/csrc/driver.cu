@@ -116,6 +116,7 @@ size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t dens
   add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
   add((size_t)N, 4); add(2, 4); add(2, 4);
   add((size_t)dense_cap * dense_cap, 4); add((size_t)dense_cap * dense_cap, 4);
+  add((size_t)2 * dense_cap * ((dense_cap + 31) / 32), 4);
   add(kCommitCtas, 8); add(kCommitCtas, 8); add(1, 4);
   return b + 4096;
 }
@@ -262,12 +263,13 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
   if (J.dense_cap > 0) {
     m.Md = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
     m.MTd = A.take<uint32_t>((size_t)J.dense_cap * J.dense_cap);
+    m.Sd = A.take<uint32_t>((size_t)2 * J.dense_cap * ((J.dense_cap + 31) / 32));
   }
   m.xlx = const_cast<double*>(xlx);
   J.cs.part_sum = A.take<double>(kCommitCtas);
   J.cs.part_cnt = A.take<long long>(kCommitCtas);
   J.cs.ticket = A.take<unsigned>(1);
-  if (!J.cs.ticket || (J.dense_cap > 0 && !m.MTd)) return fail(SBP_ERR_INTERNAL, "arena sizing");
+  if (!J.cs.ticket || (J.dense_cap > 0 && !m.Sd)) return fail(SBP_ERR_INTERNAL, "arena sizing");
   SBP_CUDA(cudaMemsetAsync(J.err, 0, 8, J.st));
   SBP_CUDA(cudaMemsetAsync(J.cs.ticket, 0, 4, J.st));
   return SBP_OK;

@@ -38,6 +38,10 @@ struct DevBM {
   // dense form for small B: Md[r*B + c] = M[r][c], MTd[c*B + r] = M[r][c]
   uint32_t* Md = nullptr;
   uint32_t* MTd = nullptr;
+  // chunk sums of the dense rows, 32 columns a chunk, K = ceil(B/32):
+  // Sd[b*2K + j] = sum of Md[b][32j..32j+31], Sd[b*2K + K + j] the same
+  // over MTd[b] (the in-row); kept with Md and MTd by the same atomics
+  uint32_t* Sd = nullptr;
   // xlx[x] = x log2 x and xlx[kXlxTable + x] = log2 x for x < kXlxTable
   // (filled by fill_xlx_table)
   double* xlx = nullptr;

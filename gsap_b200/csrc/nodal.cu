@@ -1055,14 +1055,107 @@ __device__ __forceinline__ void write_result_gen(const NodalArgs& a, bool given,
   if (a.props_out) a.props_out[i] = s;
 }
 
+// Mid vertices (more entries than the warp's registers hold, at most
+// kWarpHashEntries in both directions): the entries' (direction, block) keys
+// are grouped in a per-warp shared-memory hash table (open addressing, at
+// most half full), which gives each group its total weight and its first
+// entry, the one that adds the group's terms.  One pass, no sort.
+constexpr int kWarpHashEntries = 128;
+constexpr int kWarpHashSlots = 256;
+constexpr uint32_t kEmptyKey = 0xffffffffu;
+
+struct WarpHash {
+  uint32_t* key;  // kWarpHashSlots each
+  uint32_t* sum;
+  int32_t* first;
+};
+
+__device__ __forceinline__ uint32_t wh_slot(uint32_t key) {
+  return (key * 2654435761u) >> 24;  // 8 bits: kWarpHashSlots = 256
+}
+
+template <bool DENSE>
+__device__ double delta_whash(const NodalArgs& a, int v, int r, int s, int32_t o0, int no,
+                              int32_t i0, int ni, int lane, const WarpHash& h) {
+  constexpr int kPer = kWarpHashEntries / 32;  // entries per lane
+  constexpr uint32_t kMask = kWarpHashSlots - 1;
+  const Rows<DENSE> R(a, r, s);
+  const int n = no + ni;
+  for (int i = lane; i < kWarpHashSlots; i += 32) {
+    h.key[i] = kEmptyKey;
+    h.sum[i] = 0u;
+    h.first[i] = 0x7fffffff;
+  }
+  __syncwarp();
+  int32_t cs[kPer];
+  uint32_t ws[kPer];
+  bool ins[kPer];
+  uint32_t koR = 0, koS = 0, niR = 0, niS = 0;
+#pragma unroll
+  for (int p = 0; p < kPer; ++p) {
+    const int k = lane + 32 * p;
+    cs[p] = -1;
+    ws[p] = 0u;
+    ins[p] = false;
+    if (k < n) {
+      const bool in = k >= no;
+      const int j = in ? i0 + k - no : o0 + k;
+      const int32_t c = __ldg(a.part + __ldg((in ? a.iidx : a.oidx) + j));
+      const uint32_t w = __ldg((in ? a.iw : a.ow) + j);
+      cs[p] = c;
+      ws[p] = w;
+      ins[p] = in;
+      koR += !in && c == r ? w : 0u;
+      koS += !in && c == s ? w : 0u;
+      niR += in && c == r ? w : 0u;
+      niS += in && c == s ? w : 0u;
+      const uint32_t key = (uint32_t)c | (in ? 0x80000000u : 0u);
+      uint32_t sl = wh_slot(key);
+      // at most n <= kWarpHashSlots / 2 keys: a free or matching slot is
+      // found within the table
+      for (int probe = 0; probe < kWarpHashSlots; ++probe, sl = (sl + 1) & kMask) {
+        const uint32_t prev = atomicCAS(h.key + sl, kEmptyKey, key);
+        if (prev == kEmptyKey || prev == key) {
+          atomicAdd(h.sum + sl, w);
+          atomicMin(h.first + sl, k);
+          break;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  const RsWeights w{__reduce_add_sync(kFull, koR), __reduce_add_sync(kFull, koS),
+                    __reduce_add_sync(kFull, niR), __reduce_add_sync(kFull, niS)};
+  Acc q;
+#pragma unroll
+  for (int p = 0; p < kPer; ++p) {
+    const int k = lane + 32 * p;
+    if (k < n) {
+      const uint32_t key = (uint32_t)cs[p] | (ins[p] ? 0x80000000u : 0u);
+      uint32_t sl = wh_slot(key);
+      for (int probe = 0; probe < kWarpHashSlots && h.key[sl] != key; ++probe)
+        sl = (sl + 1) & kMask;
+      entry<DENSE>(a, R, r, s, w.niS, ins[p], cs[p], ws[p], h.first[sl] == k, h.sum[sl], q);
+    }
+  }
+  const double d = finish<DENSE, 32>(a, R, v, r, s, w, q, Group<32>{nullptr});
+  __syncwarp();  // the warp's next vertex reuses the table
+  return d;
+}
+
 // One vertex (batch index i) on the whole warp: the fused path when its
 // entries fit the warp (sampled proposals, GSAP scoring), else the proposal
-// by pick_neighbour and the dS from registers (both lists within a warp)
-// or from sorted shared-memory lists.
+// by pick_neighbour and the dS from registers (both lists within a warp),
+// from the warp's hash table (GSAP scoring, up to kWarpHashEntries) or from
+// sorted shared-memory lists.  buf: the warp's kWarpBufWords words of
+// shared memory.
+constexpr int kWarpBufWords = 384;  // 3 KB: the hash table, or the two sorted lists
 template <bool GIVEN, bool DENSE, bool GEN>
 __device__ __forceinline__ void warp_vertex(const NodalArgs& a, int i, int lane,
-                                            unsigned long long* sko, unsigned long long* ski) {
+                                            unsigned long long* buf) {
   const Group<32> grp{nullptr};
+  unsigned long long* sko = buf;
+  unsigned long long* ski = buf + kWarpList;
   const int vv = GIVEN ? a.verts[i] : a.lo + i;
   const int32_t o0 = a.optr[vv], no = a.optr[vv + 1] - o0;
   const int32_t i0 = a.iptr[vv], ni = a.iptr[vv + 1] - i0;
@@ -1097,6 +1190,10 @@ __device__ __forceinline__ void warp_vertex(const NodalArgs& a, int i, int lane,
   if (r != s) {
     if (no <= 32 && ni <= 32) {
       d = delta_registers<DENSE>(a, v, r, s, o0, no, i0, ni, lane);
+    } else if (no + ni <= kWarpHashEntries) {
+      uint32_t* t = reinterpret_cast<uint32_t*>(buf);
+      const WarpHash h{t, t + kWarpHashSlots, reinterpret_cast<int32_t*>(t + 2 * kWarpHashSlots)};
+      d = delta_whash<DENSE>(a, v, r, s, o0, no, i0, ni, lane, h);
     } else {
       stage_sorted<32>(a.oidx, a.ow, a.part, o0, no, sko, grp);
       stage_sorted<32>(a.iidx, a.iw, a.part, i0, ni, ski, grp);
@@ -1119,7 +1216,9 @@ struct NodalBody {
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
   if (ctl_stopped(a.ctl)) return;
-  __shared__ unsigned long long s_ko[kNodalWarps][kWarpList], s_ki[kNodalWarps][kWarpList];
+  __shared__ unsigned long long s_buf[kNodalWarps][kWarpBufWords];
+  static_assert(2 * kWarpList <= kWarpBufWords && 3 * kWarpHashSlots <= 2 * kWarpBufWords,
+                "per-warp shared buffer");
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = vg * kNodalWarps;
   const int npairs = (a.nsmall + 1) / 2;
@@ -1140,7 +1239,7 @@ struct NodalBody {
     }
     // one call site, so that the body stays inline
     for (int q = 0; q < (ib >= 0 ? 2 : 1); ++q)
-      warp_vertex<GIVEN, DENSE, GEN>(a, q ? ib : ia, lane, s_ko[wid], s_ki[wid]);
+      warp_vertex<GIVEN, DENSE, GEN>(a, q ? ib : ia, lane, s_buf[wid]);
   }
   }
 };
