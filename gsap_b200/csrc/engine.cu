@@ -412,6 +412,10 @@ std::mutex& cuda_submit_mutex() {
 
 sbp_status Engine::tick() {
   std::unique_lock<std::mutex> submit(cuda_submit_mutex());
+  const double t_start = now_ms();
+  int trace = 0;  // verbose >= 2: one line per tick on stderr
+  for (Run* r : runs)
+    if (r->stage != Run::kDone) trace = std::max(trace, r->o.verbose);
   SBP_CUDA(cudaSetDevice(device));
   // runs that reach the outer-step limit stop at their next merge
   for (Run* r : runs) {
@@ -664,9 +668,11 @@ sbp_status Engine::tick() {
   if (s != SBP_OK) return s;
   if (rd) SBP_CUDA(cudaMemcpyAsync(rd_host, rd_dev, rd, cudaMemcpyDeviceToHost, st));
   SBP_CUDA(cudaEventRecord(ev[3], st));
+  const double t_issued = now_ms();
   submit.unlock();
   const cudaError_t waited = cudaEventSynchronize(ev[3]);
   submit.lock();
+  const double t_waited = now_ms();
   SBP_CUDA(waited);
   SBP_CUDA(cudaGetLastError());
   ++ticks;
@@ -794,6 +800,15 @@ sbp_status Engine::tick() {
       // a server request is published (Run::finished) by its lane, under
       // the server's lock, once the engine no longer touches it
     }
+  }
+  if (trace >= 2) {
+    float dev = 0.f;
+    cudaEventElapsedTime(&dev, ev[0], ev[3]);
+    std::fprintf(stderr,
+                 "[sbp] tick %lld runs %zu sweeps %d: host issue %.3f ms, wait %.3f ms, host after "
+                 "%.3f ms, device %.3f ms\n",
+                 ticks, runs.size(), k_max, t_issued - t_start, t_waited - t_issued,
+                 now_ms() - t_waited, (double)dev);
   }
   return SBP_OK;
 }
