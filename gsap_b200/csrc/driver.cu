@@ -22,6 +22,7 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -31,6 +32,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace sbp {
@@ -321,12 +323,100 @@ int resolve_device(int32_t d) {
 // that label is itself.  Union-find gives the same labels as the reference's
 // relabel-all loop.  Surviving labels are renumbered in ascending order
 // (std::set, :58-68).  Returns the new block count.
+// Block ids 0..n-1 in ascending order of key[id], equal keys by id: an LSD
+// radix sort of (key, id) pairs with 8-bit digits (stable, so ids stay
+// ascending within equal keys), skipping digits that all keys share.  Large
+// inputs are split over up to 8 host threads: each counts the digits of its
+// contiguous slice, then writes the slice to the offsets that the counts of
+// the slices before it leave, which keeps the pass stable.
+static void rank_by_key(std::vector<uint64_t> key, std::vector<int32_t>& order) {
+  const size_t n = key.size();
+  order.resize(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::vector<uint64_t> k2(n);
+  std::vector<int32_t> o2(n);
+  constexpr int kDigits = 256;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int T = (int)std::min<size_t>({8, (size_t)hw, std::max<size_t>(1, n / 32768)});
+  std::vector<uint32_t> cnt((size_t)T * kDigits);
+  auto slice = [&](int t, size_t& lo, size_t& hi) {
+    lo = n * (size_t)t / (size_t)T;
+    hi = n * (size_t)(t + 1) / (size_t)T;
+  };
+  auto count_pass = [&](int t, int shift) {
+    size_t lo, hi;
+    slice(t, lo, hi);
+    uint32_t* c = cnt.data() + (size_t)t * kDigits;
+    std::fill(c, c + kDigits, 0u);
+    for (size_t i = lo; i < hi; ++i) ++c[(key[i] >> shift) & 0xff];
+  };
+  auto scatter_pass = [&](int t, int shift) {
+    size_t lo, hi;
+    slice(t, lo, hi);
+    // start of each digit for this slice: all smaller digits, then this
+    // digit in the slices before
+    size_t at[kDigits];
+    size_t run = 0;
+    for (int d = 0; d < kDigits; ++d) {
+      size_t before = 0;
+      for (int u = 0; u < T; ++u) {
+        if (u == t) before = run;
+        run += cnt[(size_t)u * kDigits + d];
+      }
+      at[d] = before;
+    }
+    for (size_t i = lo; i < hi; ++i) {
+      const size_t q = at[(key[i] >> shift) & 0xff]++;
+      k2[q] = key[i];
+      o2[q] = order[i];
+    }
+  };
+  // every thread runs the same passes; a pass's phases are separated by a
+  // barrier (all T threads arrive at each one, so every wait ends)
+  std::atomic<int> arrived{0};
+  std::atomic<int> phase{0};
+  auto barrier = [&](int& my_phase) {
+    ++my_phase;
+    if (arrived.fetch_add(1) + 1 == T * my_phase) phase.store(my_phase);
+    while (phase.load() < my_phase) std::this_thread::yield();
+  };
+  auto worker = [&](int t) {
+    int my_phase = 0;
+    for (int shift = 0; shift < 64; shift += 8) {
+      count_pass(t, shift);
+      barrier(my_phase);
+      bool one = false;
+      for (int d = 0; d < kDigits && !one; ++d) {
+        size_t tot = 0;
+        for (int u = 0; u < T; ++u) tot += cnt[(size_t)u * kDigits + d];
+        one = tot == n;
+      }
+      if (one) {
+        barrier(my_phase);  // counts are read before the next pass clears them
+        continue;
+      }
+      scatter_pass(t, shift);
+      barrier(my_phase);
+      if (t == 0) {
+        key.swap(k2);
+        order.swap(o2);
+      }
+      barrier(my_phase);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) th.emplace_back(worker, t);
+  worker(0);
+  for (auto& x : th) x.join();
+}
+
 int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
                                  const double* best_dS, int32_t* map_out) {
   // the targets come from the device: never index with one out of range
   for (int32_t b = 0; b < B; ++b)
     if (best[b] < 0 || best[b] >= B) return -1;
-  std::vector<std::pair<uint64_t, int32_t>> key(B);
+  // order-preserving integer keys of the dS values (NaN last)
+  std::vector<uint64_t> key(B);
   for (int32_t b = 0; b < B; ++b) {
     double x = best_dS[b];
     uint64_t k;
@@ -338,9 +428,10 @@ int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
       std::memcpy(&u, &x, 8);
       k = (u >> 63) ? ~u : (u | (1ull << 63));
     }
-    key[b] = {k, b};
+    key[b] = k;
   }
-  std::sort(key.begin(), key.end());
+  std::vector<int32_t> ranked;
+  rank_by_key(key, ranked);
   std::vector<int32_t> parent(B);
   std::iota(parent.begin(), parent.end(), 0);
   auto find = [&](int32_t x) {
@@ -355,17 +446,18 @@ int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
   };
   int32_t merged = 0;
   for (int32_t c = 0; c < B && merged < B_to_merge; ++c) {
-    int32_t from = key[c].second;
+    int32_t from = ranked[c];
     int32_t to = find(best[from]);
     if (to != from) {
       parent[from] = to;
       ++merged;
     }
   }
+  // a block is a root iff it never merged away (roots keep parent == self)
   std::vector<int32_t> rootid(B, -1);
   int32_t next = 0;
   for (int32_t b = 0; b < B; ++b)
-    if (find(b) == b) rootid[b] = next++;
+    if (parent[b] == b) rootid[b] = next++;
   for (int32_t b = 0; b < B; ++b) map_out[b] = rootid[find(b)];
   return next;
 }
