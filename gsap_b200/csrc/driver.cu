@@ -181,7 +181,7 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
                       int32_t dense_max, bool lean, cudaStream_t engine_stream) {
   J.device = device;
   J.lean = lean;
-  J.dense_cap = std::max(0, std::min(N, dense_max));
+  J.dense_cap = dense_limit(N, E, dense_max);
   J.dense_eff = J.dense_cap;
   J.N = N;
   J.E = E;
@@ -462,6 +462,12 @@ int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
   return next;
 }
 
+int32_t dense_limit(int32_t N, int32_t E, int32_t dense_max) {
+  int64_t d = dense_max;
+  if (dense_max < 0) d = std::max<int64_t>(4096, (int64_t)std::sqrt(32.0 * (double)E));
+  return (int32_t)std::max<int64_t>(0, std::min<int64_t>(N, d));
+}
+
 double model_S(int32_t B, int32_t N, int32_t E, int32_t exact) {
   double b = (double)B;
   double x = b * b / (double)E;
@@ -635,7 +641,7 @@ void sbp_default_options(sbp_options* o) {
   o->device = -1;
   o->use_graphs = 1;
   o->verbose = 0;
-  o->dense_max = 4096;
+  o->dense_max = -1;
   o->exact = 0;
   o->mh = 0;
   o->beta = 3.0;
@@ -664,7 +670,7 @@ sbp_status sbp_graph_upload(const sbp_graph_csr* g, int32_t device, sbp_graph_de
   *out = nullptr;
   sbp_graph_dev* h = new (std::nothrow) sbp_graph_dev();
   if (!h) return fail(SBP_ERR_NOMEM, "host allocation");
-  sbp_status s = job_for(h->job, g, device, 10, 100, 4096);
+  sbp_status s = job_for(h->job, g, device, 10, 100, -1);
   if (s != SBP_OK) {
     delete h;
     return s;
@@ -690,7 +696,7 @@ sbp_status sbp_partition_resident(sbp_graph_dev* gd, const sbp_options* o, int32
   sbp_status s = check_options(o);
   if (s != SBP_OK) return s;
   Job& J = gd->job;
-  const int32_t want_dense = std::min(gd->shape.N, std::max(0, o->dense_max));
+  const int32_t want_dense = dense_limit(gd->shape.N, gd->shape.E, o->dense_max);
   if (o->num_proposals > J.np || o->max_nodal_itr > J.max_itr || want_dense > J.dense_cap) {
     // grow the job's arena for these options; the graph is uploaded again
     int dev = J.device;

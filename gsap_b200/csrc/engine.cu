@@ -55,7 +55,7 @@ void Run::setup_batches() {
 
 void Run::start_partition() {
   const int32_t N = J->N;
-  J->dense_eff = std::min(J->dense_cap, std::max(0, o.dense_max));
+  J->dense_eff = std::min(J->dense_cap, dense_limit(J->N, J->E, o.dense_max));
   B = N;
   B_to_merge = (int32_t)((float)B * o.reduction_rate);
   itr_dS.assign(o.max_nodal_itr, 0.0);
@@ -890,7 +890,7 @@ sbp_status Scheduler::init(int device, uint64_t hbm_budget, int32_t max_active_j
 static size_t run_bytes(const Run& r) {
   const sbp_graph_csr& g = *r.graph;
   return job_bytes(g.N, g.E, r.o.num_proposals, r.o.max_nodal_itr,
-                   std::max(0, std::min(g.N, r.o.dense_max)));
+                   dense_limit(g.N, g.E, r.o.dense_max));
 }
 
 sbp_status Scheduler::admit(std::vector<Run*>& done) {
@@ -1081,7 +1081,7 @@ using namespace sbp;
 
 extern "C" uint64_t sbp_job_bytes(int32_t N, int32_t E, const sbp_options* o) {
   if (N < 1 || E < 0 || !o) return 0;
-  return job_bytes(N, E, o->num_proposals, o->max_nodal_itr, std::max(0, std::min(N, o->dense_max)));
+  return job_bytes(N, E, o->num_proposals, o->max_nodal_itr, dense_limit(N, E, o->dense_max));
 }
 
 extern "C" sbp_status sbp_partition_batch(const sbp_graph_csr* graphs, int32_t count,

@@ -95,6 +95,13 @@ int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
 // the standard description length's in bits (exact mode searches B on it).
 double model_S(int32_t B, int32_t N, int32_t E, int32_t exact = 0);
 
+// Largest B kept in the dense B x B form: dense_max when it is >= 0, else
+// (the default) max(4096, sqrt(32 E)), so that above B = 4096 the two
+// matrices take at most about 256 bytes per edge; never more than N.  A
+// rebuild of the CSR form after every batch costs O(E); the dense form's
+// per-sweep terms cost O(B^2), so the crossover grows with E.
+int32_t dense_limit(int32_t N, int32_t E, int32_t dense_max);
+
 inline ScoreMode score_mode(const sbp_options& o) {
   ScoreMode m;
   m.exact = o.exact;

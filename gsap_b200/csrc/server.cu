@@ -176,7 +176,7 @@ sbp_status sbp_server_submit(sbp_server* srv, const sbp_graph_csr* g, uint64_t s
   if (s != SBP_OK) return s;
   const sbp_options& po = srv->opt.partition;
   const double bytes = (double)job_bytes(g->N, g->E, po.num_proposals, po.max_nodal_itr,
-                                         std::max(0, std::min(g->N, po.dense_max)));
+                                         dense_limit(g->N, g->E, po.dense_max));
   if (bytes > srv->hbm->cap) return fail(SBP_ERR_BUDGET, "job arena exceeds the HBM budget");
   std::unique_ptr<Run> r(new Run());
   r->graph_copy.assign(*g);

@@ -71,7 +71,8 @@ typedef struct sbp_options {
   int32_t use_graphs;      /* ticks of queued nodal sweeps as CUDA graphs (default 1) */
   int32_t verbose;         /* 1: one line per outer step on stderr; 2: also one per engine tick */
   int32_t dense_max;       /* keep M as dense B x B matrices while B <= dense_max
-                              (default 4096; 0 = always CSR) */
+                              (0 = always CSR); default -1 = automatic:
+                              max(4096, sqrt(32 E)), at most N */
   /* Scoring mode (no reference counterpart; defaults reproduce GSAP):
    * exact = 1 scores nodal moves and merges by the exact change of the MDL
    * (merged columns folded, new column degrees, self loops moved with the
