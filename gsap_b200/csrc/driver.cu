@@ -55,26 +55,57 @@ sbp_status validate_graph(const sbp_graph_csr* g) {
     return fail(SBP_ERR_INVALID, "graph arrays are NULL");
   if (g->E > 0 && (!g->out_idx || !g->out_w || !g->in_idx || !g->in_w))
     return fail(SBP_ERR_INVALID, "graph arrays are NULL");
+  const int32_t N = g->N;
   const int32_t* ptrs[2] = {g->out_ptr, g->in_ptr};
   const int32_t* idxs[2] = {g->out_idx, g->in_idx};
   const uint32_t* ws[2] = {g->out_w, g->in_w};
   const uint32_t* degs[2] = {g->deg_out, g->deg_in};
-  for (int d = 0; d < 2; ++d) {
-    if (ptrs[d][0] != 0 || ptrs[d][g->N] != g->E)
+  // row pointers first: once they run from 0 to E without decreasing, every
+  // entry index below is in [0, E)
+  for (int d = 0; d < 2; ++d)
+    if (ptrs[d][0] != 0 || ptrs[d][N] != g->E)
       return fail(SBP_ERR_INVALID, "row pointers must start at 0 and end at E");
-    for (int32_t v = 0; v < g->N; ++v) {
+  for (int d = 0; d < 2; ++d)
+    for (int32_t v = 0; v < N; ++v)
       if (ptrs[d][v + 1] < ptrs[d][v]) return fail(SBP_ERR_INVALID, "row pointers decrease");
-      uint64_t s = 0;
-      for (int32_t j = ptrs[d][v]; j < ptrs[d][v + 1]; ++j) {
-        if (idxs[d][j] < 0 || idxs[d][j] >= g->N)
-          return fail(SBP_ERR_INVALID, "vertex id out of range");
-        if (ws[d][j] == 0u) return fail(SBP_ERR_INVALID, "edge weights must be >= 1");
-        s += ws[d][j];
+  // the entries, split by vertex over up to 8 threads for large graphs;
+  // the error reported is the first in (direction, vertex, entry) order
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int T = (int)std::min<int64_t>({8, (int64_t)hw, std::max<int64_t>(1, g->E / 262144)});
+  struct Bad {
+    int32_t v = -1;
+    const char* msg = nullptr;
+  };
+  std::vector<Bad> bad((size_t)T * 2);
+  auto check = [&](int t) {
+    const int32_t v0 = (int32_t)((int64_t)N * t / T), v1 = (int32_t)((int64_t)N * (t + 1) / T);
+    for (int d = 0; d < 2; ++d) {
+      Bad& b = bad[(size_t)t * 2 + d];
+      for (int32_t v = v0; v < v1 && !b.msg; ++v) {
+        uint64_t s = 0;
+        for (int32_t j = ptrs[d][v]; j < ptrs[d][v + 1]; ++j) {
+          if (idxs[d][j] < 0 || idxs[d][j] >= N) {
+            b = Bad{v, "vertex id out of range"};
+            break;
+          }
+          if (ws[d][j] == 0u) {
+            b = Bad{v, "edge weights must be >= 1"};
+            break;
+          }
+          s += ws[d][j];
+        }
+        if (!b.msg && s != degs[d][v]) b = Bad{v, "node degree differs from the sum of its edge weights"};
       }
-      if (s != degs[d][v])
-        return fail(SBP_ERR_INVALID, "node degree differs from the sum of its edge weights");
+      if (b.msg) break;  // a direction-0 error precedes every direction-1 error
     }
-  }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) th.emplace_back(check, t);
+  check(0);
+  for (auto& x : th) x.join();
+  for (int d = 0; d < 2; ++d)
+    for (int t = 0; t < T; ++t)  // threads hold ascending vertex ranges
+      if (bad[(size_t)t * 2 + d].msg) return fail(SBP_ERR_INVALID, bad[(size_t)t * 2 + d].msg);
   return SBP_OK;
 }
 

@@ -129,3 +129,33 @@ def test_partition_validates_before_device_use(sbp):
         sbp.delta_mdl_nodal_mode(g, g.true_partitions, 11, [0], [1], exact=-1)
     with pytest.raises(sbp.SbpError, match="invalid argument"):
         sbp.delta_mdl_merge_mode(g, g.true_partitions, 11, np.zeros(110, np.int32), exact=2)
+
+
+def test_validation_reports_the_first_error_in_order(sbp):
+    # large enough that the entries are checked by several host threads; the
+    # error reported is still the first in (direction, vertex) order
+    g = sbp.dcsbm_variant("HH", 120000, 20, seed=1)
+    assert g.E > 4 * 262144
+
+    def bad(**arrays):
+        fields = {**g.__dict__}
+        for k, v in arrays.items():
+            fields[k] = v
+        with pytest.raises(sbp.SbpError) as e:
+            sbp.partition(sbp.Graph(**fields))
+        return str(e.value)
+
+    late_out = g.out_idx.copy()
+    late_out[-1] = g.N + 5  # direction 0, last vertex
+    early_in_w = g.in_w.copy()
+    early_in_w[0] = 0  # direction 1, first vertex
+    msg = bad(out_idx=late_out, in_w=early_in_w)
+    assert "vertex id out of range" in msg
+    msg = bad(in_w=early_in_w)
+    assert "edge weights must be >= 1" in msg
+    deg = g.deg_in.copy()
+    deg[-1] += 1
+    assert "node degree differs" in bad(deg_in=deg)
+    ptr = g.out_ptr.copy()
+    ptr[g.N // 2] = ptr[g.N // 2 + 1] + 1
+    assert "row pointers decrease" in bad(out_ptr=ptr, in_w=early_in_w)
