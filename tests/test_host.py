@@ -159,3 +159,20 @@ def test_validation_reports_the_first_error_in_order(sbp):
     ptr = g.out_ptr.copy()
     ptr[g.N // 2] = ptr[g.N // 2 + 1] + 1
     assert "row pointers decrease" in bad(out_ptr=ptr, in_w=early_in_w)
+
+
+def test_dense_crossover_grows_with_the_edge_count(sbp):
+    # the default dense_max (-1) keeps the dense B x B form while
+    # B <= max(4096, sqrt(32 E)), at most N; the job arena holds two B x B
+    # uint32 matrices and their row chunk sums at that cap
+    def dense_bytes(cap):
+        r = lambda b: (b + 255) // 256 * 256
+        return 2 * r(cap * cap * 4) + r(2 * cap * ((cap + 31) // 32) * 4)
+
+    def extra(N, E, **kw):
+        return sbp.job_bytes(N, E, **kw) - sbp.job_bytes(N, E, dense_max=0)
+
+    assert extra(200000, 2000000) == dense_bytes(8000)  # sqrt(32 * 2e6) = 8000
+    assert extra(200000, 2000000, dense_max=4096) == dense_bytes(4096)
+    assert extra(20000, 200000) == dense_bytes(4096)    # small graphs keep 4096
+    assert extra(3000, 40000) == dense_bytes(3000)      # never above N
