@@ -7,10 +7,11 @@
 // Differences in how it runs on the device:
 //   * one device arena per job (GSAP: four slabs plus separate buffers and
 //     per-call allocations inside bb_segsort / mgpu / thrust);
-//   * every kernel on one stream; the host synchronises once per nodal sweep
-//     (to read the sweep's dS sum and the MDL) and once per merge step (to
-//     apply the merges), where GSAP synchronises after every batch and inside
-//     every rebuild;
+//   * every kernel on one stream, issued by the engine (engine.cu) in ticks:
+//     the host synchronises once per tick of queued nodal sweeps (ended on
+//     the device by the stop test; the host reads their dS sums and MDLs)
+//     and once per merge step (to apply the merges), where GSAP synchronises
+//     after every batch and inside every rebuild;
 //   * golden-section snapshots keep only the labels; the blockmodel of a
 //     restored point is rebuilt from them (exactly the same matrix);
 //   * merges are applied with a union-find pass over the ranked blocks, the

@@ -5,15 +5,20 @@
 // thread walk a whole blockmodel row in a serial sorted merge with the
 // vertex's sorted neighbour-block list (kernels.hpp:494-597, 1153-1726).
 //
-// Here a group of threads owns one vertex: a warp for ordinary vertices, a
-// whole CTA for the few with more than kWarpList neighbours in a direction
-// (a static per-batch list, run on a second stream next to the warp kernel).
+// Here a group of threads owns one vertex: half a warp for vertices of at
+// most kSmallEntries neighbour entries (two per warp), a warp for the other
+// ordinary vertices, a whole CTA for the few with more than kWarpList
+// neighbours in a direction (run on a second stream next to the warp
+// kernel).  The host sorts each batch's vertices into these three lists
+// once per job.
 //   * proposal: Philox draws, an exact integer inverse-CDF pick of a
-//     neighbour (a warp prefix scan over its out- then in-entries), then the
-//     per-block draws of the batch (kernels.hpp:877-1032);
+//     neighbour (a prefix scan over the group's lanes, out- then
+//     in-entries), then the per-block draws of the batch
+//     (kernels.hpp:877-1032);
 //   * neighbour blocks grouped per distinct block: in registers with
-//     __match_any_sync / __reduce_add_sync when a list fits a warp, else
-//     sorted in shared memory (bitonic), else hashed in shared memory in
+//     __match_any_sync / __reduce_add_sync when a list fits the lane group,
+//     else in a per-warp shared-memory hash table (up to kWarpHashEntries),
+//     else sorted in shared memory (bitonic), else hashed in shared memory in
 //     passes; GSAP sorts all E entries every batch;
 //   * dS: GSAP's seven terms rewritten as "changed cells + row degrees".
 //     A row term  sum_c f(x_c)  with  f(x) = x (log2 x - log2 dcol[c] - L)
@@ -27,7 +32,8 @@
 //     (kernels.hpp:1648-1652, 1314-1318), the r/s in-weight corrections and
 //     the conditional extra column term (kernels.hpp:1506-1510, 1573-1578,
 //     1663-1669, 1718-1723), unsigned count arithmetic.
-//   * accept iff dS < 0 (kernels.hpp:634-640); the new label goes to a side
+//   * accept iff dS < 0 (kernels.hpp:634-640), or by the general-mode rules
+//     (exact MDL, Metropolis-Hastings) below; the new label goes to a side
 //     buffer so every vertex of the batch sees the same old labels.
 // All entropy arithmetic is FP64.
 #include "common.cuh"
