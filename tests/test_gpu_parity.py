@@ -167,8 +167,8 @@ def test_partition_matches_oracle(sbp, orc, variant, seed):
     # Same seed, same draws; merge proposals whose dS tie exactly in exact
     # arithmetic may be ranked differently by FP64 rounding (the GPU sums in
     # another order), after which the runs may take different paths.  So the
-    # bar is the north star's: MDL within 1%; on LL, where both runs find the
-    # planted blocks, the same partition up to relabelling.
+    # bar is the end-to-end quality bar: MDL within 1%; on LL, where both runs
+    # find the planted blocks, the same partition up to relabelling.
     g = graphs.dcsbm(variant, 1000, 11, seed)
     rep = sbp.partition(g, seed=seed)
     lab_o, rep_o, st = orc.partition(g, seed=seed)
