@@ -58,17 +58,22 @@ def dist_env():
 
 
 class Dist:
-    """torch.distributed plumbing for the barrier and the max over ranks."""
+    """torch.distributed plumbing for the barrier and the max over ranks:
+    NCCL with one GPU per rank, gloo on hosts without a GPU (the CPU tests
+    of the multi-rank path)."""
 
-    def __init__(self, world, local):
+    def __init__(self, world, local, backend=None):
         self.world = world
         self.pg = None
         if world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            self.device = "cuda" if backend == "nccl" else "cpu"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.dist, self.torch = dist, torch
 
     def barrier(self):
@@ -78,7 +83,7 @@ class Dist:
     def max(self, x):
         if self.world == 1:
             return x
-        t = self.torch.tensor([float(x)], device="cuda")
+        t = self.torch.tensor([float(x)], device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 

@@ -1,0 +1,59 @@
+"""The multi-rank plumbing of bench.py on CPU: two gloo ranks (one process
+each, as torchrun starts them) take the barrier and agree on the max over
+ranks; the reference arm runs on rank 0 alone."""
+import os
+import socket
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+RANK_SCRIPT = r"""
+import sys
+sys.path.insert(0, {root!r})
+import bench
+rank, world, local = bench.dist_env()
+d = bench.Dist(world, local, backend="gloo")
+d.barrier()
+m = d.max(10.0 * (rank + 1))
+d.barrier()
+d.close()
+print("rank", rank, "max", m)
+"""
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _run_ranks(code, world=2, extra=()):
+    port = _free_port()
+    procs = []
+    for rank in range(world):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(world),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, *code, *extra], env=env, cwd=ROOT,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    out = []
+    for p in procs:
+        o, e = p.communicate(timeout=300)
+        out.append((p.returncode, o, e))
+    return out
+
+
+def test_two_gloo_ranks_barrier_and_max():
+    res = _run_ranks(["-c", RANK_SCRIPT.format(root=ROOT)])
+    for rank, (rc, o, e) in enumerate(res):
+        assert rc == 0, e[-2000:]
+        assert f"rank {rank} max 20.0" in o
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    # rank 1 of the reference arm exits 0 without work and prints nothing
+    res = _run_ranks(["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1",
+                      "--warmup", "1"])
+    rc, o, e = res[1]
+    assert rc == 0, e[-2000:]
+    assert o.strip() == ""
