@@ -188,6 +188,20 @@ def cpu_baseline(g, seconds=20.0):
             "cpu": _os.uname().machine, "nproc": _os.cpu_count()}
 
 
+def phase_rates(tot, ms_device, steps):
+    """Algorithmic GB/s of each phase (its bytes over its CUDA-event time)
+    and end to end (the bytes of all phases over the whole device time),
+    from totals over `steps` steps."""
+    def gbs(b, ms):
+        return b / ms / 1e6 if ms > 0 else None
+    total = tot["bytes_nodal"] + tot["bytes_rebuild"] + tot["bytes_merge"]
+    return {"nodal": gbs(tot["bytes_nodal"], tot["ms_nodal"]),
+            "rebuild": gbs(tot["bytes_rebuild"], tot["ms_rebuild"]),
+            "merge": gbs(tot["bytes_merge"], tot["ms_merge"]),
+            "end_to_end": gbs(total, ms_device),
+            "bytes_per_step": total / max(1, steps)}
+
+
 def run_ours(args, rank, world, local, dist):
     from gsap_b200 import sbp
     g = make_graph(sbp)
@@ -228,7 +242,8 @@ def run_ours(args, rank, world, local, dist):
     rec, prec, nmi = sbp.evaluate(g.true_partitions, labels)
     tot = {k: sum(r[k] for r in reports) for k in (
         "ms_merge", "ms_nodal", "ms_rebuild", "ms_nodal_kernel", "nodal_launches",
-        "nodal_proposals", "bytes_nodal", "kernel_launches", "accepted_moves")}
+        "nodal_proposals", "bytes_nodal", "bytes_rebuild", "bytes_merge", "kernel_launches",
+        "accepted_moves")}
     peak, peak_kind = measured_peak()
     achieved = tot["bytes_nodal"] / (tot["ms_nodal_kernel"] / 1000.0) / 1e9
     traffic = None
@@ -259,6 +274,7 @@ def run_ours(args, rank, world, local, dist):
                      "ms_per_launch": tot["ms_nodal_kernel"] / max(tot["nodal_launches"], 1),
                      "traffic": traffic},
         "gpu_launches": int(tot["kernel_launches"]),
+        "algorithmic_gbs": phase_rates(tot, ms_max, K),
         "phases_ms_per_step": {k: tot[k] / K for k in ("ms_merge", "ms_nodal", "ms_rebuild",
                                                         "ms_nodal_kernel")},
         "cuda_graphs": {"captures": int(sum(r.get("graph_captures", 0) for r in reports)),

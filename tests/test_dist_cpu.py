@@ -57,3 +57,15 @@ def test_reference_arm_runs_on_rank_zero_only():
     rc, o, e = res[1]
     assert rc == 0, e[-2000:]
     assert o.strip() == ""
+
+
+def test_phase_rates():
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    tot = {"bytes_nodal": 2e9, "bytes_rebuild": 1e9, "bytes_merge": 5e8, "ms_nodal": 100.0,
+           "ms_rebuild": 50.0, "ms_merge": 0.0}
+    r = bench.phase_rates(tot, 250.0, 2)
+    assert abs(r["nodal"] - 20.0) < 1e-12 and abs(r["rebuild"] - 20.0) < 1e-12
+    assert r["merge"] is None
+    assert abs(r["end_to_end"] - 14.0) < 1e-12 and r["bytes_per_step"] == 1.75e9
