@@ -945,6 +945,16 @@ sbp_status sbp_nodal_sweeps(const sbp_graph_csr* g, int32_t* part, int32_t B, ui
   return SBP_OK;
 }
 
+sbp_status sbp_apply_merges(int32_t B, int32_t B_to_merge, const int32_t* best,
+                            const double* best_dS, int32_t* map, int32_t* B_new) {
+  if (B < 1 || B_to_merge < 0 || !best || !best_dS || !map || !B_new)
+    return fail(SBP_ERR_INVALID, "bad merge arguments");
+  const int32_t nb = apply_merges_host(B, B_to_merge, best, best_dS, map);
+  if (nb < 0) return fail(SBP_ERR_INVALID, "merge target out of [0, B)");
+  *B_new = nb;
+  return SBP_OK;
+}
+
 sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int32_t B_to_merge,
                           int32_t np, uint64_t seed, uint32_t seq, int32_t* best, double* best_dS,
                           int32_t* B_new) {

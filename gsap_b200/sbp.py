@@ -134,6 +134,7 @@ _sig("sbp_delta_mdl_merge_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, 
 _sig("sbp_nodal_batch_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint64,
      C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, _vp, _vp,
      C.POINTER(C.c_double))
+_sig("sbp_apply_merges", C.c_int, C.c_int32, C.c_int32, _vp, _vp, _vp, C.POINTER(C.c_int32))
 _sig("sbp_merge_proposals", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, C.c_uint64,
      C.c_uint32, _vp)
 _sig("sbp_nodal_batch", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint64, C.c_uint32,
@@ -177,7 +178,8 @@ EXPORTED = [
     "sbp_edges_free", "sbp_csr_from_edges", "sbp_load_tsv", "sbp_evaluate",
     "sbp_mdl_device_static", "sbp_job_bytes", "sbp_partition_batch", "sbp_server_default_options",
     "sbp_server_create", "sbp_server_submit", "sbp_server_poll", "sbp_server_stats_get",
-    "sbp_server_destroy",
+    "sbp_server_destroy", "sbp_delta_mdl_nodal_mode", "sbp_delta_mdl_merge_mode",
+    "sbp_nodal_batch_mode", "sbp_mdl_mode", "sbp_apply_merges",
 ]
 
 
@@ -488,6 +490,17 @@ def delta_mdl_merge_mode(g: Graph, part, B, props, np_=10, exact=1):
     _check(_lib.sbp_delta_mdl_merge_mode(C.byref(g.csr()), _p(part), B, np_, _p(props), exact,
                                          _p(dS), _p(best), _p(best_dS)))
     return dS, best, best_dS
+
+
+def apply_merges(B, B_to_merge, best, best_dS):
+    """carry_out_best_merges on the host: (map from old to new block labels,
+    new block count)."""
+    best = np.ascontiguousarray(best, dtype=np.int32)
+    best_dS = np.ascontiguousarray(best_dS, dtype=np.float64)
+    m = np.zeros(max(B, 1), np.int32)
+    nb = C.c_int32()
+    _check(_lib.sbp_apply_merges(B, B_to_merge, _p(best), _p(best_dS), _p(m), C.byref(nb)))
+    return m[:B], nb.value
 
 
 def merge_proposals(g: Graph, part, B, seed, seq, np_=10):

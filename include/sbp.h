@@ -290,6 +290,15 @@ sbp_status sbp_nodal_sweeps(const sbp_graph_csr* g, int32_t* part, int32_t B, ui
 /* One merge step (propose_block_merge + carry_out_best_merges,
  * partition.hpp:26-78, 324-454): labels updated in place; *B_new receives the
  * new block count. */
+/* carry_out_best_merges (partition.hpp:26-78) alone, on the host (no GPU
+ * is touched): blocks merge in ascending order of best_dS (equal values by
+ * block id, NaN last), each into the current label of best[b] unless that
+ * label is its own, until B_to_merge merges are made; map[b] receives the
+ * new label of block b (surviving blocks renumbered in ascending order) and
+ * *B_new the new block count. */
+sbp_status sbp_apply_merges(int32_t B, int32_t B_to_merge, const int32_t* best,
+                            const double* best_dS, int32_t* map, int32_t* B_new);
+
 sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int32_t B_to_merge,
                           int32_t np, uint64_t seed, uint32_t seq, int32_t* best, double* best_dS,
                           int32_t* B_new);

@@ -176,3 +176,26 @@ def test_dense_crossover_grows_with_the_edge_count(sbp):
     assert extra(200000, 2000000, dense_max=4096) == dense_bytes(4096)
     assert extra(20000, 200000) == dense_bytes(4096)    # small graphs keep 4096
     assert extra(3000, 40000) == dense_bytes(3000)      # never above N
+
+
+@pytest.mark.parametrize("B", [1, 7, 300, 5000, 70000])
+def test_apply_merges_matches_oracle(sbp, orc, B):
+    # carry_out_best_merges on the host (radix-ranked, threaded for large B)
+    # against the oracle's literal loop, with tied, signed-zero and NaN dS
+    rng = np.random.default_rng(B)
+    for trial in range(4):
+        best = rng.integers(0, B, B).astype(np.int32)
+        kind = rng.integers(0, 6, B)
+        ds = np.ldexp(rng.integers(-10**6, 10**6, B).astype(np.float64), -rng.integers(0, 40, B))
+        ds[kind == 0] = 0.0
+        ds[kind == 1] = -0.0
+        ds[kind == 2] = np.nan
+        ds[kind == 3] = rng.integers(0, 4, int((kind == 3).sum()))
+        k = int(rng.integers(0, B + 1))
+        part = rng.integers(0, B, 4 * B).astype(np.int32)
+        m, nb = sbp.apply_merges(B, k, best, ds)
+        want, nb_o = orc.apply_merges(part, B, k, best, ds)
+        assert nb == nb_o
+        assert np.array_equal(m[part], want)
+    with pytest.raises(sbp.SbpError, match="invalid argument"):
+        sbp.apply_merges(B, 1, np.full(B, B, np.int32), np.zeros(B))
