@@ -33,6 +33,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -101,7 +102,13 @@ sbp_status validate_graph(const sbp_graph_csr* g) {
     }
   };
   std::vector<std::thread> th;
-  for (int t = 1; t < T; ++t) th.emplace_back(check, t);
+  int spawned = 1;
+  try {
+    for (; spawned < T; ++spawned) th.emplace_back(check, spawned);
+  } catch (const std::system_error&) {
+    // no more threads: the remaining slices run here
+  }
+  for (int t = spawned; t < T; ++t) check(t);
   check(0);
   for (auto& x : th) x.join();
   for (int d = 0; d < 2; ++d)
@@ -348,13 +355,6 @@ int resolve_device(int32_t d) {
 }
 
 // ------------------------------------------------------------ merge apply --
-// carry_out_best_merges (partition.hpp:26-78).  Blocks are ranked by their
-// best dS (ascending, ties by block id: thrust::sort_by_key's stable radix
-// sort over an id sequence, partition.hpp:442-447; NaN last); then in that
-// order each block merges into the current label of its best target unless
-// that label is itself.  Union-find gives the same labels as the reference's
-// relabel-all loop.  Surviving labels are renumbered in ascending order
-// (std::set, :58-68).  Returns the new block count.
 // Block ids 0..n-1 in ascending order of key[id], equal keys by id: an LSD
 // radix sort of (key, id) pairs with 8-bit digits (stable, so ids stay
 // ascending within equal keys), skipping digits that all keys share.  Large
@@ -369,7 +369,7 @@ static void rank_by_key(std::vector<uint64_t> key, std::vector<int32_t>& order) 
   std::vector<int32_t> o2(n);
   constexpr int kDigits = 256;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const int T = (int)std::min<size_t>({8, (size_t)hw, std::max<size_t>(1, n / 32768)});
+  int T = (int)std::min<size_t>({8, (size_t)hw, std::max<size_t>(1, n / 32768)});
   std::vector<uint32_t> cnt((size_t)T * kDigits);
   auto slice = [&](int t, size_t& lo, size_t& hi) {
     lo = n * (size_t)t / (size_t)T;
@@ -436,12 +436,34 @@ static void rank_by_key(std::vector<uint64_t> key, std::vector<int32_t>& order) 
       barrier(my_phase);
     }
   };
+  // the helpers wait at a gate until all of them exist; if one cannot be
+  // started, the others are released without work and the sort runs here
+  std::atomic<int> gate{0};  // 0: wait, 1: run, -1: cancelled
+  auto start = [&](int t) {
+    while (gate.load() == 0) std::this_thread::yield();
+    if (gate.load() > 0) worker(t);
+  };
   std::vector<std::thread> th;
-  for (int t = 1; t < T; ++t) th.emplace_back(worker, t);
+  try {
+    for (int t = 1; t < T; ++t) th.emplace_back(start, t);
+    gate.store(1);
+  } catch (const std::system_error&) {
+    gate.store(-1);
+    for (auto& x : th) x.join();
+    th.clear();
+    T = 1;
+  }
   worker(0);
   for (auto& x : th) x.join();
 }
 
+// carry_out_best_merges (partition.hpp:26-78).  Blocks are ranked by their
+// best dS (ascending, ties by block id: thrust::sort_by_key's stable radix
+// sort over an id sequence, partition.hpp:442-447; NaN last); then in that
+// order each block merges into the current label of its best target unless
+// that label is itself.  Union-find gives the same labels as the reference's
+// relabel-all loop.  Surviving labels are renumbered in ascending order
+// (std::set, :58-68).  Returns the new block count.
 int32_t apply_merges_host(int32_t B, int32_t B_to_merge, const int32_t* best,
                                  const double* best_dS, int32_t* map_out) {
   // the targets come from the device: never index with one out of range
