@@ -243,3 +243,64 @@ def evaluate(truth, given):
     o = np.zeros(3)
     _lib.orc_evaluate(t.size, _p(t), _p(g), _p(o))
     return tuple(o)
+
+
+# ------------------------------------------------------- benchmark graphs --
+_sig("orc_dcsbm", C.c_int64, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32,
+     C.c_double, C.c_uint64, _vp, _vp, C.c_int64, _vp)
+
+# (p_in, Dirichlet alpha) of the GraphChallenge-style variants
+VARIANTS = {"LL": (0.8, 20.0), "LH": (0.8, 1.0), "HL": (0.5, 20.0), "HH": (0.5, 1.0)}
+
+
+class Graph:
+    """Both CSR directions of a directed graph, N+1 row pointers, the way
+    GSAP/load.hpp:86-117 orders them (each row in edge order), weighted
+    degrees, and the planted labels."""
+
+    def __init__(self, N, src, dst, w=None, truth=None):
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        dst = np.ascontiguousarray(dst, dtype=np.int32)
+        w = np.ones(src.size, np.uint32) if w is None else np.ascontiguousarray(w, np.uint32)
+        self.N, self.E = int(N), int(src.size)
+        o = np.argsort(src, kind="stable")
+        i = np.argsort(dst, kind="stable")
+        self.out_ptr = np.zeros(N + 1, np.int32)
+        self.out_ptr[1:] = np.cumsum(np.bincount(src, minlength=N))
+        self.in_ptr = np.zeros(N + 1, np.int32)
+        self.in_ptr[1:] = np.cumsum(np.bincount(dst, minlength=N))
+        self.out_idx, self.out_w = dst[o].copy(), w[o].copy()
+        self.in_idx, self.in_w = src[i].copy(), w[i].copy()
+        self.deg_out = np.bincount(src, weights=w, minlength=N).astype(np.uint32)
+        self.deg_in = np.bincount(dst, weights=w, minlength=N).astype(np.uint32)
+        self.true_partitions = None if truth is None else np.ascontiguousarray(truth, np.int32)
+
+
+def dcsbm(N, B, alpha, p_in, seed=0, deg_min=5, deg_max=50, exponent=2.5):
+    """The seeded DCSBM graph of the benchmarks (orc_dcsbm)."""
+    cap = N * deg_max
+    src = np.zeros(cap, np.int32)
+    dst = np.zeros(cap, np.int32)
+    truth = np.zeros(N, np.int32)
+    E = _lib.orc_dcsbm(N, B, float(alpha), float(p_in), deg_min, deg_max, float(exponent), seed,
+                       _p(src), _p(dst), cap, _p(truth))
+    if E < 0:
+        raise ValueError("bad DCSBM parameters")
+    return Graph(N, src[:E], dst[:E], truth=truth)
+
+
+def dcsbm_variant(variant, N, B, seed=0):
+    p_in, alpha = VARIANTS[variant]
+    return dcsbm(N, B, alpha, p_in, seed=seed)
+
+
+def write_graph_bin(g, path):
+    """The graph file oracle/gsap_ref_main.cu reads: int32 magic 0x53425047,
+    N, E, 0, then out_ptr (N+1), out_idx, out_w, in_ptr (N+1), in_idx, in_w,
+    deg_out, deg_in."""
+    import struct
+    with open(path, "wb") as f:
+        f.write(struct.pack("<4i", 0x53425047, g.N, g.E, 0))
+        for a in (g.out_ptr, g.out_idx, g.out_w, g.in_ptr, g.in_idx, g.in_w, g.deg_out,
+                  g.deg_in):
+            f.write(np.ascontiguousarray(a).tobytes())

@@ -1005,10 +1005,162 @@ int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep
   return R.status;
 }
 
+// ------------------------------------------------------------ generator ---
+// The seeded directed DCSBM graph of the benchmarks and tests, restated from
+// its definition so that the reference arm of the benchmark and the tests
+// can build the same graph without the product library:
+//   * block proportions ~ Dirichlet(alpha): Gamma(alpha, 1) per block by
+//     Marsaglia & Tsang, "A simple method for generating gamma variables"
+//     (ACM TOMS 26(3), 2000), the normal by Box-Muller, alpha < 1 through
+//     Gamma(alpha + 1) * U^(1/alpha);
+//   * sizes floor(N p_b), the remainder one vertex each to the largest
+//     fractional parts (equal parts: lower block first), every block >= 1
+//     (taken from the first largest block);
+//   * planted labels block by block, then a Fisher-Yates shuffle;
+//   * out-degree k on [deg_min, deg_max] with P(k) ~ k^-exponent, by the
+//     first k whose running weight reaches U * total;
+//   * each out-edge stays in the source's block with probability p_in,
+//     else goes to a uniform other block; the destination is drawn in
+//     proportion to degree within that block; self loops and repeated
+//     edges are redrawn (64 attempts per edge).
+// Philox counter layout (idx, 4, stream, k), key = seed; streams 1 gamma,
+// 2 shuffle, 3 degrees, 4 edges.
+struct Dcsbm {
+  int32_t N, B;
+  double alpha, p_in;
+  int32_t deg_min, deg_max;
+  double exponent;
+  uint64_t seed;
+};
+
+inline P4 gen(uint64_t seed, uint32_t stream, uint32_t idx, uint32_t k) {
+  return philox(idx, 4u, stream, k, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+inline double open01(uint32_t x) { return ((double)x + 0.5) * (1.0 / 4294967296.0); }
+
+double gamma_variate(uint64_t seed, uint32_t block, double alpha) {
+  uint32_t k = 0;
+  double scale = 1.0;
+  if (alpha < 1.0) {
+    scale = std::pow(open01(gen(seed, 1, block, k++).v[2]), 1.0 / alpha);
+    alpha += 1.0;
+  }
+  const double d = alpha - 1.0 / 3.0;
+  const double c = 1.0 / std::sqrt(9.0 * d);
+  while (true) {
+    const P4 x = gen(seed, 1, block, k++);
+    const double z = std::sqrt(-2.0 * std::log(open01(x.v[0]))) *
+                     std::cos(6.283185307179586 * open01(x.v[1]));
+    double v = 1.0 + c * z;
+    if (!(v > 0.0)) continue;
+    v = v * v * v;
+    if (std::log(open01(x.v[2])) < 0.5 * z * z + d - d * v + d * std::log(v)) return d * v * scale;
+  }
+}
+
+// Fills src/dst (capacity cap) and truth (N); returns E, or -1 on bad
+// parameters or too small a capacity.
+int64_t dcsbm(const Dcsbm& p, int32_t* src, int32_t* dst, int64_t cap, int32_t* truth) {
+  const int32_t N = p.N, B = p.B;
+  if (N < 2 || B < 1 || B > N || !(p.alpha > 0.0) || p.p_in < 0.0 || p.p_in > 1.0 ||
+      p.deg_min < 1 || p.deg_max < p.deg_min || p.deg_max >= N)
+    return -1;
+  std::vector<double> w(B);
+  double wsum = 0.0;
+  for (int32_t b = 0; b < B; ++b) wsum += (w[b] = gamma_variate(p.seed, (uint32_t)b, p.alpha));
+  std::vector<int64_t> cnt(B);
+  std::vector<int32_t> order(B);
+  std::vector<double> rest(B);
+  int64_t placed = 0;
+  for (int32_t b = 0; b < B; ++b) {
+    const double share = (double)N * w[b] / wsum;
+    cnt[b] = (int64_t)std::floor(share);
+    rest[b] = share - (double)cnt[b];
+    placed += cnt[b];
+    order[b] = b;
+  }
+  std::sort(order.begin(), order.end(), [&](int32_t a, int32_t c) {
+    return rest[a] != rest[c] ? rest[a] > rest[c] : a < c;
+  });
+  for (int64_t i = 0; placed < N; ++i, ++placed) ++cnt[order[i % B]];
+  for (int32_t b = 0; b < B; ++b)
+    while (cnt[b] == 0) {
+      int32_t big = 0;
+      for (int32_t c = 1; c < B; ++c)
+        if (cnt[c] > cnt[big]) big = c;
+      --cnt[big];
+      ++cnt[b];
+    }
+  int32_t at = 0;
+  for (int32_t b = 0; b < B; ++b)
+    for (int64_t i = 0; i < cnt[b]; ++i) truth[at++] = b;
+  for (int32_t i = N - 1; i > 0; --i) {
+    const int32_t j = (int32_t)scale_draw(gen(p.seed, 2, (uint32_t)i, 0).v[0], (uint64_t)i + 1);
+    std::swap(truth[i], truth[j]);
+  }
+  // running weights of the degree law
+  std::vector<double> run;
+  double acc = 0.0;
+  for (int32_t k = p.deg_min; k <= p.deg_max; ++k) run.push_back(acc += std::pow((double)k, -p.exponent));
+  std::vector<int32_t> deg(N);
+  for (int32_t v = 0; v < N; ++v) {
+    const double u = open01(gen(p.seed, 3, (uint32_t)v, 0).v[0]) * run.back();
+    int32_t k = 0;
+    while (k + 1 < (int32_t)run.size() && run[k] < u) ++k;
+    deg[v] = p.deg_min + k;
+  }
+  std::vector<std::vector<int32_t>> members(B);
+  std::vector<std::vector<uint64_t>> upto(B);
+  for (int32_t v = 0; v < N; ++v) {
+    const int32_t b = truth[v];
+    const uint64_t prev = upto[b].empty() ? 0 : upto[b].back();
+    members[b].push_back(v);
+    upto[b].push_back(prev + (uint64_t)deg[v]);
+  }
+  const uint64_t stay = (uint64_t)std::llround(p.p_in * 4294967296.0);
+  int64_t E = 0;
+  std::vector<int32_t> mine;
+  for (int32_t u = 0; u < N; ++u) {
+    mine.clear();
+    for (int32_t k = 0; k < deg[u]; ++k) {
+      for (uint32_t att = 0; att < 64; ++att) {
+        const P4 x = gen(p.seed, 4, (uint32_t)u, ((uint32_t)k << 8) | att);
+        int32_t b = truth[u];
+        if (B > 1 && (uint64_t)x.v[0] >= stay) {
+          const int32_t c = (int32_t)(x.v[1] % (uint32_t)(B - 1));
+          b = c < b ? c : c + 1;
+        }
+        const uint64_t t = scale_draw(x.v[2], upto[b].back());
+        const int32_t i = (int32_t)(std::upper_bound(upto[b].begin(), upto[b].end(), t) -
+                                    upto[b].begin());
+        const int32_t v = members[b][i];
+        if (v == u || std::find(mine.begin(), mine.end(), v) != mine.end()) continue;
+        if (E >= cap) return -1;
+        mine.push_back(v);
+        src[E] = u;
+        dst[E] = v;
+        ++E;
+        break;
+      }
+    }
+  }
+  return E;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI ---
 extern "C" {
+
+// The benchmark DCSBM graph (see dcsbm above): edges into src/dst (capacity
+// cap, N * deg_max always suffices), planted labels into truth (N).
+// Returns E, or -1 on bad parameters.
+int64_t orc_dcsbm(int32_t N, int32_t B, double alpha, double p_in, int32_t deg_min,
+                  int32_t deg_max, double exponent, uint64_t seed, int32_t* src, int32_t* dst,
+                  int64_t cap, int32_t* truth) {
+  Dcsbm p{N, B, alpha, p_in, deg_min, deg_max, exponent, seed};
+  return dcsbm(p, src, dst, cap, truth);
+}
 
 typedef struct orc_graph {
   int32_t N, E;
