@@ -2,22 +2,25 @@
 // memory, computed without allocating anything.
 //
 // Some callers cannot allocate device memory at the point where they need
-// the objective: code that records its work into a CUDA graph, where a
-// cudaMalloc/cudaFree would break or synchronise the capture; serving loops
-// that forbid the implicit device-wide synchronisation a cudaFree costs; and
-// hosts that own all device memory through their own pool and do not let a
-// library allocate behind their back.  For them this entry point keeps its
-// scratch (the log2 of the block degrees and the per-CTA partial sums) in
-// one file-scope device array of fixed size, allocated once when the library
-// is loaded and held by every GPU that loads it until the process exits.
+// the objective: hosts that own all device memory through their own pool and
+// do not let a library allocate behind their back, and serving loops that
+// forbid the device-wide synchronisation a cudaMalloc or cudaFree can cost.
+// For them this entry point keeps its scratch (the log2 of the block degrees
+// and the per-CTA partial sums) in one file-scope device array of fixed size,
+// created when the library is loaded and held by every GPU that loads it
+// until the process exits.  The caller passes the inputs and the outputs.
 //
 // Limits and rules of use:
-//   * at most kStaticMaxBlocks blocks; larger B is rejected;
-//   * the first call on a device looks the array up (cudaGetSymbolAddress)
-//     and caches its address; make that first call before any stream capture;
-//   * every call on a device shares the one array: calls that overlap on the
-//     GPU (different streams, or work still running) race on it.  The call
-//     clears what must start at zero (the CTA ticket) itself.
+//   * at most kStaticMaxBlocks (65,536) blocks; larger B is rejected;
+//   * the first call on a device looks the array's device address up
+//     (cudaGetSymbolAddress, with that device current) and caches it for the
+//     process; make that first call before any stream capture.  A
+//     cudaDeviceReset ends the context the cached address belongs to, and
+//     the entry point must not be called on that device afterwards;
+//   * every call on a device shares the one array, and the array keeps the
+//     last call's contents: calls that overlap on the GPU (different
+//     streams, or work still running) race on it.  Each call clears what
+//     must start at zero (the CTA ticket of the reduction) itself.
 #include "../../include/sbp.h"
 #include "common.cuh"
 
@@ -130,7 +133,8 @@ extern "C" sbp_status sbp_mdl_device_static(int32_t N, int32_t E, int32_t B,
                                             const uint32_t* d_in, double* S, double* data_S,
                                             void* stream) {
   using namespace sbp;
-  if (N < 1 || E < 1 || B < 1 || !out_ptr || !d_out || !d_in || !S || !data_S)
+  if (N < 1 || E < 1 || B < 1 || !out_ptr || !out_col || !out_cnt || !d_out || !d_in || !S ||
+      !data_S)
     return host_fail(SBP_ERR_INVALID, "sbp_mdl_device_static: bad arguments");
   if (B > kStaticMaxBlocks)
     return host_fail(SBP_ERR_INVALID,
@@ -142,6 +146,10 @@ extern "C" sbp_status sbp_mdl_device_static(int32_t N, int32_t E, int32_t B,
   const double b = (double)B, x = b * b / (double)E;
   const double model =
       (double)E * (1.0 + x) * std::log(1.0 + x) - x * std::log(x) + (double)N * std::log(b);
+  // A launch error left pending by earlier, unrelated work is cleared first
+  // so that the status below belongs to these two launches (a sticky error,
+  // which ends the context, is reported again by the check after them).
+  (void)cudaGetLastError();
   static_logs_kernel<<<(B + kStaticThreads - 1) / kStaticThreads, kStaticThreads, 0, st>>>(
       sc, B, d_out, d_in);
   static_mdl_kernel<<<kStaticCtas, kStaticThreads, 0, st>>>(sc, B, out_ptr, out_col, out_cnt,

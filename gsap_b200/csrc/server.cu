@@ -207,17 +207,26 @@ sbp_status sbp_server_poll(sbp_server* srv, int64_t id, int32_t timeout_ms, int3
                            sbp_report* rep, sbp_job_times* times) {
   if (!srv) return fail(SBP_ERR_INVALID, "server is NULL");
   std::unique_lock<std::mutex> lk(srv->mu);
-  auto it = srv->live.find(id);
-  if (it == srv->live.end()) return fail(SBP_ERR_NOT_FOUND, "unknown request id");
-  // the Run stays put while the map may rehash (submits during the wait
-  // below): keep the pointer, never the iterator
-  Run* r = it->second.get();
+  // Another thread polling the same id may collect (and free) the request
+  // while this one waits, so the request is looked up afresh after every
+  // wake-up and never held across the wait.
+  auto lookup = [&]() -> Run* {
+    auto it = srv->live.find(id);
+    return it == srv->live.end() ? nullptr : it->second.get();
+  };
+  Run* r = lookup();
+  if (!r) return fail(SBP_ERR_NOT_FOUND, "unknown request id");
   if (!r->finished) {
     if (timeout_ms == 0) return fail(SBP_ERR_BUSY, "request still running");
-    auto ready = [&] { return r->finished; };
+    auto ready = [&] {
+      Run* q = lookup();
+      return !q || q->finished;
+    };
     if (timeout_ms < 0) srv->cv_done.wait(lk, ready);
     else if (!srv->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
       return fail(SBP_ERR_BUSY, "request still running");
+    r = lookup();
+    if (!r) return fail(SBP_ERR_NOT_FOUND, "request collected by another poll");
   }
   if (labels_out) std::memcpy(labels_out, r->labels_store.data(), 4 * r->labels_store.size());
   if (rep) *rep = r->R;
@@ -230,6 +239,8 @@ sbp_status sbp_server_poll(sbp_server* srv, int64_t id, int32_t timeout_ms, int3
   const sbp_status st = r->status;
   const std::string msg = r->error;
   srv->live.erase(id);
+  // a second poller of this id waits on cv_done: wake it to see it gone
+  srv->cv_done.notify_all();
   if (st != SBP_OK) return fail(st, msg);
   return SBP_OK;
 }

@@ -84,6 +84,16 @@ typedef struct sbp_options {
   int32_t exact;           /* 0 (default) or 1 */
   int32_t mh;              /* 0 (default) or 1 */
   double beta;             /* inverse temperature of the MH test, per nat (default 3) */
+  /* GSAP's merge grid (partition.hpp:335-336): GSAP launches every merge
+   * kernel on nnz threads (nnz = entries of the out CSR) rounded up to 256,
+   * so when B * num_proposals is larger (the first merge step, where
+   * nnz ~ E < 10 N) the proposals of the last blocks are never drawn: their
+   * slots keep what the buffers held, zeros in a fresh process, so those
+   * blocks all propose block 0 with dS 0 and merge into it first.  1 does
+   * the same (slots start at zero and keep earlier steps' values), 0 draws
+   * and scores every proposal; -1 (default) = 1 with GSAP's scoring
+   * (exact = 0), 0 in exact mode. */
+  int32_t ref_grid;
 } sbp_options;
 
 /* What one partition run did.  Timings are CUDA-event milliseconds on the
@@ -318,13 +328,17 @@ sbp_status sbp_mdl_mode(const sbp_graph_csr* g, const int32_t* part, int32_t B, 
 /* The MDL of a blockmodel already in device memory (out CSR with B+1 row
  * pointers, block degrees), written to the device doubles *S and *data_S on
  * `stream` (a cudaStream_t; NULL = default stream), without allocating
- * anything: for callers that cannot call cudaMalloc where they need the
- * objective (inside a CUDA graph capture, in serving loops that forbid
- * allocation syncs, or under a host-owned memory pool).  Its scratch is a
- * fixed ~1 MB device array of the library; B <= 65536.  The first call on a
- * device looks that array up, so make it before any stream capture; calls
- * that overlap on the GPU share the array and race.  This entry point has no
- * counterpart in the reference. */
+ * anything: for callers that cannot let a library allocate device memory,
+ * such as hosts that own all device memory through their own pool, or
+ * serving loops that forbid the synchronisation a cudaMalloc or cudaFree can
+ * cost.  The caller passes inputs and outputs; the scratch is a fixed ~1 MB
+ * device array of the library, held by every GPU that loads it until the
+ * process exits, so B <= 65536 (larger B returns SBP_ERR_INVALID).  The first
+ * call on a device looks that array's address up (once per device, with the
+ * device current), so make it before any stream capture; the address is not
+ * valid after a cudaDeviceReset.  All calls share the array, which keeps the
+ * last call's contents: calls that overlap on the GPU race.  This entry
+ * point has no counterpart in the reference. */
 sbp_status sbp_mdl_device_static(int32_t N, int32_t E, int32_t B, const int32_t* out_ptr,
                                  const int32_t* out_col, const uint32_t* out_cnt,
                                  const uint32_t* d_out, const uint32_t* d_in, double* S,

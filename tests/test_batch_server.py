@@ -164,3 +164,31 @@ def test_graph_replay_same_bits(sbp, solo):
     labs, reps, _ = sbp.partition_batch(gs, seeds=seeds, use_graphs=0)
     for i in range(len(gs)):
         _same(labs[i], reps[i], *ref[i])
+
+
+def test_server_two_pollers_one_request(sbp, solo):
+    # two threads wait on the same request: one collects it, the other is
+    # told it is gone (never a freed request)
+    import threading
+    gs, seeds, ref = solo
+    i = int(np.argmax([g.N for g in gs]))
+    with sbp.Server() as srv:
+        for _ in range(3):
+            j = srv.submit(gs[i], seeds[i])
+            got, errs = [], []
+
+            def poll():
+                try:
+                    got.append(srv.poll(j, timeout_ms=-1))
+                except sbp.SbpError as e:
+                    errs.append(str(e))
+
+            ths = [threading.Thread(target=poll) for _ in range(2)]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join(timeout=120)
+            assert not any(t.is_alive() for t in ths)
+            assert len(got) == 1 and len(errs) == 1, (got, errs)
+            assert "collected" in errs[0] or "unknown request" in errs[0]
+            _same(got[0][0], got[0][1], *ref[i])

@@ -1,7 +1,10 @@
 """sbp_mdl_device_static: the MDL of a device-resident blockmodel computed
-with no allocation inside the call, checked against sbp_mdl (the allocating
-entry point) on the same partitions, twice in a row so that the scratch left
-by one call cannot leak into the next.  Named to be collected last."""
+with no allocation inside the call, for callers that cannot let a library
+allocate device memory (a host-owned memory pool, a serving loop that
+forbids allocation syncs).  Checked against sbp_mdl (the allocating entry
+point) and the CPU oracle on the same partitions, twice in a row so that the
+scratch left by one call cannot leak into the next.  Named to be collected
+last."""
 import numpy as np
 import pytest
 
@@ -20,7 +23,7 @@ def _device_blockmodel(sbp, g, part, B):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant,N,B", [("LL", 1000, 11), ("HH", 4000, 64), ("LH", 4000, 4000)])
-def test_mdl_device_static_matches_mdl(sbp, variant, N, B):
+def test_mdl_device_static_matches_mdl(sbp, orc, variant, N, B):
     import torch
     g = dcsbm(variant, N, seed=7)
     rng = np.random.default_rng(3)
@@ -29,6 +32,7 @@ def test_mdl_device_static_matches_mdl(sbp, variant, N, B):
     for part in parts:
         Bp = int(part.max()) + 1
         S_ref, data_ref = sbp.mdl(g, part, Bp)
+        S_orc, data_orc = orc.mdl(g, part, Bp)
         dev = _device_blockmodel(sbp, g, part, Bp)
         out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
         for _ in range(2):
@@ -42,6 +46,8 @@ def test_mdl_device_static_matches_mdl(sbp, variant, N, B):
             S, data_S = out.cpu().tolist()
             assert abs(S - S_ref) <= REL * abs(S_ref), (S, S_ref)
             assert abs(data_S - data_ref) <= REL * abs(data_ref), (data_S, data_ref)
+            assert abs(S - S_orc) <= REL * abs(S_orc), (S, S_orc)
+            assert abs(data_S - data_orc) <= REL * abs(data_orc), (data_S, data_orc)
 
 
 @pytest.mark.gpu
@@ -52,3 +58,6 @@ def test_mdl_device_static_rejects_too_many_blocks(sbp):
     with pytest.raises(sbp.SbpError, match="static scratch"):
         sbp.mdl_device_static(10, 10, 65537, z.data_ptr(), z.data_ptr(), z.data_ptr(),
                               z.data_ptr(), z.data_ptr(), d[0:1].data_ptr(), d[1:2].data_ptr(), 0)
+    with pytest.raises(sbp.SbpError, match="bad arguments"):
+        sbp.mdl_device_static(10, 10, 4, z.data_ptr(), 0, z.data_ptr(), z.data_ptr(),
+                              z.data_ptr(), d[0:1].data_ptr(), d[1:2].data_ptr(), 0)
