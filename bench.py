@@ -87,6 +87,13 @@ class Dist:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
+    def sum(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([float(x)], device=self.device, dtype=self.torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
     def close(self):
         if self.world > 1:
             self.dist.destroy_process_group()
@@ -170,22 +177,48 @@ def make_graph(sbp):
     return sbp.dcsbm_variant(w["variant"], w["N"], w["B"], seed=w["seed"])
 
 
-def cpu_baseline(g, seconds=20.0):
-    """CPU oracle nodal moves/s: Jacobi batches at the planted labels (B=71)
-    of the same graph, single thread, FP64; as many batches as fit in about
-    `seconds`."""
-    import os as _os
+CPU_SAMPLE = dict(variant="HH", N=20000, B=32, seed=0)
+
+
+def cpu_baseline(local):
+    """The CPU oracle (the sequential FP64 restatement of partition(), one
+    thread) partitioning the 20k-vertex HH DCSBM graph end to end, in
+    partitions/s with its phase times; beside it the GPU's time on the same
+    graph and seed, and the oracle's nodal moves/s over the run.  A full
+    200k partition takes the oracle tens of minutes, so the 20k graph of the
+    same generator is the bounded sample."""
+    import platform
     from oracle import oracle as orc
-    B = int(g.true_partitions.max()) + 1
-    ms1, _ = orc.time_nodal(g, g.true_partitions, B, 7, 1)
-    nb = max(1, min(40, int(seconds * 1000.0 / max(ms1, 1.0))))
-    ms, _ = orc.time_nodal(g, g.true_partitions, B, 7, nb)
-    BS = g.N // 4
-    return {"value": nb * BS / (ms / 1000.0), "unit": "nodal moves/s", "cores": 1,
-            "kind": "port",
-            "sample": f"{nb} Jacobi batches of {BS} vertices at the planted labels (B={B}) of "
-                      f"the benchmark graph, CPU oracle (FP64, 1 thread), {ms / 1000:.1f} s",
-            "cpu": _os.uname().machine, "nproc": _os.cpu_count()}
+    from gsap_b200 import sbp
+    c = CPU_SAMPLE
+    g = orc.dcsbm_variant(c["variant"], c["N"], c["B"], seed=c["seed"])
+    t0 = time.perf_counter()
+    lab, rep, st = orc.partition(g, seed=c["seed"])
+    wall = time.perf_counter() - t0
+    gg = sbp.dcsbm_variant(c["variant"], c["N"], c["B"], seed=c["seed"])
+    sbp.partition(gg, seed=c["seed"], device=local)  # warm
+    grep = sbp.partition(gg, seed=c["seed"], device=local)
+    cpu = platform.processor() or platform.machine()
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                cpu = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"value": 1.0 / wall, "unit": "partitions/s", "cores": 1, "kind": "port",
+            "sample": f"one full partition of the 20k-vertex HH DCSBM graph (N={g.N}, "
+                      f"E={g.E}, {c['B']} planted blocks, seed {c['seed']}) by the CPU oracle "
+                      f"(FP64, 1 thread): {wall:.1f} s",
+            "seconds": wall,
+            "phases_s": {"merge": rep["ms_merge"] / 1e3, "nodal": rep["ms_nodal"] / 1e3,
+                         "rebuild": rep["ms_rebuild"] / 1e3},
+            "nodal_moves_per_s": rep["nodal_proposals"] / max(rep["ms_nodal"] / 1e3, 1e-9),
+            "result": {"B": rep["B"], "S": rep["S"], "status": st},
+            "gpu_same_sample": {"ms_total": grep["ms_total"], "B": grep["B"], "S": grep["S"],
+                                "identical_B_and_S": grep["B"] == rep["B"] and
+                                abs(grep["S"] - rep["S"]) <= 1e-9 * abs(rep["S"])},
+            "cpu": cpu, "nproc": os.cpu_count()}
 
 
 def phase_rates(tot, ms_device, steps):
@@ -284,7 +317,7 @@ def run_ours(args, rank, world, local, dist):
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(g, args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(local)
     return line
 
 
@@ -308,10 +341,17 @@ def quality(sbp, g, lab, S):
 
 
 def run_batched(args, rank, world, local, dist):
+    """One list of `batch_count` graphs.  With N ranks the list is sharded
+    (gsap_b200.shard: balanced by edges), each rank partitions its share in
+    one sbp_partition_batch call on its GPU, and labels and reports are
+    gathered on rank 0: total work is fixed, so scaling is strong."""
     from gsap_b200 import sbp
+    from gsap_b200.shard import gather_results, shard_jobs
     count = args.batch_count
-    gs = batched_graphs(sbp, count, 7 + rank)
-    seeds = list(range(count))
+    every = batched_graphs(sbp, count, 7)
+    mine = shard_jobs([g.E for g in every], world)[rank]
+    gs = [every[i] for i in mine]
+    seeds = list(mine)
     opts = dict(device=local)
     # warm-up: a small batch (kernels, pools)
     for _ in range(max(1, args.warmup)):
@@ -325,39 +365,42 @@ def run_batched(args, rank, world, local, dist):
     dev_max = dist.max(br["ms_device"])
     # the plain form, one graph at a time, same graphs and seeds
     t0 = time.perf_counter()
-    seq_S, same = [], 0
+    same = 0
     for i, g in enumerate(gs):
         rep = sbp.partition(g, seed=seeds[i], **opts)
-        seq_S.append(rep["S"])
         same += int(np.array_equal(g.partitions, labs[i]) and rep["S"] == reps[i]["S"])
     seq = (time.perf_counter() - t0) * 1000.0
     seq_max = dist.max(seq)
+    same_all = int(dist.sum(same))
+    all_labs, all_reps = gather_results(mine, labs, reps, world, rank)
+    launches = int(dist.sum(br["kernel_launches"]))
     if rank != 0:
         return None
-    q = [quality(sbp, g, labs[i], reps[i]["S"]) for i, g in enumerate(gs)]
-    Ns = [g.N for g in gs]
+    q = [quality(sbp, g, all_labs[i], all_reps[i]["S"]) for i, g in enumerate(every)]
+    Ns = [g.N for g in every]
     h2d = sum(sum(a.nbytes for a in (g.out_ptr, g.out_idx, g.out_w, g.in_ptr, g.in_idx,
-                                     g.in_w, g.deg_out, g.deg_in)) for g in gs)
+                                     g.in_w, g.deg_out, g.deg_in)) for g in every)
     return {
         "metric": "batched SBP graphs/s (256 DCSBM graphs, N log-uniform on [1k,50k])",
-        "value": world * count / (dev_max / 1000.0), "unit": "graphs/s", "n_gpus": world,
+        "value": count / (dev_max / 1000.0), "unit": "graphs/s", "n_gpus": world,
         "steps": 1, "warmup": max(1, args.warmup), "ms_per_step": dev_max,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": "batched-256", "graphs": count, "N_min": min(Ns),
                    "N_max": max(Ns), "N_total": int(sum(Ns)),
-                   "E_total": int(sum(g.E for g in gs)), "parallelism": f"replicas x{world}"},
-        "e2e": {"value": world * count / (wall_max / 1000.0), "unit": "graphs/s",
+                   "E_total": int(sum(g.E for g in every)),
+                   "parallelism": f"job list sharded over {world} rank(s)"},
+        "e2e": {"value": count / (wall_max / 1000.0), "unit": "graphs/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(4 * sum(Ns))},
-        "sequential_plain": {"value": world * count / (seq_max / 1000.0), "unit": "graphs/s",
+        "sequential_plain": {"value": count / (seq_max / 1000.0), "unit": "graphs/s",
                              "note": "the same graphs and seeds through sbp_partition, one at a "
                                      "time (host buffers, end to end)"},
         "speedup_vs_sequential_e2e": seq_max / wall_max,
-        "identical_results": f"{same}/{count}",
+        "identical_results": f"{same_all}/{count}",
         "quality": {"mean_S": float(np.mean([x[0] for x in q])),
                     "mean_recall": float(np.mean([x[1] for x in q])),
                     "mean_precision": float(np.mean([x[2] for x in q]))},
-        "batch": br, "gpu_launches": int(br["kernel_launches"]), "clocks": clk.summary(),
+        "batch": br, "gpu_launches": launches, "clocks": clk.summary(),
     }
 
 
@@ -535,7 +578,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain mode: skip the batched and served records")
     ap.add_argument("--ref-steps", type=int, default=None)
     ap.add_argument("--ref-warmup", type=int, default=None)
     ap.add_argument("--ref-timeout", type=float, default=500.0)
@@ -565,6 +609,19 @@ def main():
     runner = {"plain": run_ours, "batched": run_batched, "served": run_served}[args.mode]
     try:
         line = runner(args, rank, world, local, dist)
+        if args.mode == "plain" and world == 1 and not args.no_extras:
+            # the batched and served forms, bounded, in the same record
+            b = run_batched(args, rank, world, local, dist)
+            line["batched"] = {k: b[k] for k in (
+                "metric", "value", "unit", "ms_per_step", "e2e", "sequential_plain",
+                "speedup_vs_sequential_e2e", "identical_results", "quality", "config",
+                "gpu_launches", "clocks")}
+            import copy
+            sa = copy.copy(args)
+            sa.rates, sa.served_max = [5.0, 20.0, 100.0], 200
+            sv = run_served(sa, rank, world, local, dist)
+            line["served"] = {k: sv[k] for k in ("metric", "value", "unit", "config", "rates",
+                                                 "clocks")}
     finally:
         dist.close()
     if line is not None:

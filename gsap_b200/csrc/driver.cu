@@ -153,6 +153,7 @@ size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t dens
   add(N, 8);
   add((size_t)N * np, 4);
   add((size_t)N * np, 8);
+  add((size_t)N * np, 8);
   add(N, 8);
   add((size_t)max_itr, 8); add((size_t)max_itr, 8); add((size_t)max_itr, 8);
   add((size_t)N, 4); add(2, 4); add(2, 4);
@@ -293,6 +294,7 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
   J.rec = A.take<double>(N);
   J.props = A.take<int32_t>((size_t)N * np);
   J.mdS = A.take<double>((size_t)N * np);
+  J.mdsin = A.take<double>((size_t)N * np);
   J.best = J.newlab;  // merge and nodal phases never overlap
   J.best_dS = A.take<double>(N);
   J.dsum = A.take<double>(max_itr);
@@ -588,7 +590,7 @@ NodalAux nodal_lists(Job& J, const int32_t* dev, const int32_t n[3]) {
 }
 
 static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t seed, uint32_t seq,
-                             bool keep_dS) {
+                             bool keep_dS, int32_t ref_grid = 0) {
   cudaStream_t st = J.st;
   if (!J.h_best) {
     SBP_CUDA(cudaMallocHost(&J.h_best, sizeof(int32_t) * (size_t)J.N));
@@ -598,8 +600,19 @@ static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t se
   // the merge kernels read the CSR form, stale after dense nodal sweeps
   if (is_dense(J, B)) rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
   block_terms(J.m, B, 0, seed, 0, st);
-  merge_proposals(J.m, B, J.np, seed, seq, J.props, st);
-  merge_delta(J.m, B, J.np, J.props, keep_dS ? J.mdS : nullptr, J.best, J.best_dS, st);
+  MergeGrid grid;
+  if (ref_grid) {
+    // a fresh run's merge buffers: the slots GSAP's grid leaves out read zeros
+    const size_t slots = (size_t)J.N * J.np;
+    SBP_CUDA(cudaMemsetAsync(J.props, 0, 4 * slots, st));
+    SBP_CUDA(cudaMemsetAsync(J.mdS, 0, 8 * slots, st));
+    SBP_CUDA(cudaMemsetAsync(J.mdsin, 0, 8 * slots, st));
+    grid.on = 1;
+    grid.dS = J.mdS;
+    grid.dsin = J.mdsin;
+  }
+  merge_proposals(J.m, B, J.np, seed, seq, J.props, st, grid);
+  merge_delta(J.m, B, J.np, J.props, keep_dS ? J.mdS : nullptr, J.best, J.best_dS, st, 0, grid);
   SBP_CUDA(cudaMemcpyAsync(J.h_best, J.best, 4 * (size_t)B, cudaMemcpyDeviceToHost, st));
   SBP_CUDA(cudaMemcpyAsync(J.h_best_dS, J.best_dS, 8 * (size_t)B, cudaMemcpyDeviceToHost, st));
   SBP_CUDA(cudaStreamSynchronize(st));
@@ -666,6 +679,7 @@ sbp_status check_options(const sbp_options* o) {
     return fail(SBP_ERR_INVALID, "exact and mh must be 0 or 1");
   if (o->mh && !(o->beta >= 0.0 && o->beta < 1e300))
     return fail(SBP_ERR_INVALID, "beta must be finite and >= 0");
+  if (o->ref_grid < -1 || o->ref_grid > 1) return fail(SBP_ERR_INVALID, "ref_grid must be -1, 0 or 1");
   return SBP_OK;
 }
 
@@ -699,6 +713,7 @@ void sbp_default_options(sbp_options* o) {
   o->exact = 0;
   o->mh = 0;
   o->beta = 3.0;
+  o->ref_grid = -1;
 }
 
 const char* sbp_status_string(sbp_status s) {
@@ -980,12 +995,19 @@ sbp_status sbp_apply_merges(int32_t B, int32_t B_to_merge, const int32_t* best,
 sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int32_t B_to_merge,
                           int32_t np, uint64_t seed, uint32_t seq, int32_t* best, double* best_dS,
                           int32_t* B_new) {
+  return sbp_merge_step_mode(g, part, B, B_to_merge, np, seed, seq, 0, best, best_dS, B_new);
+}
+
+sbp_status sbp_merge_step_mode(const sbp_graph_csr* g, int32_t* part, int32_t B,
+                               int32_t B_to_merge, int32_t np, uint64_t seed, uint32_t seq,
+                               int32_t ref_grid, int32_t* best, double* best_dS, int32_t* B_new) {
   if (np < 1 || np > 32) return fail(SBP_ERR_INVALID, "bad np");
+  if (ref_grid != 0 && ref_grid != 1) return fail(SBP_ERR_INVALID, "ref_grid must be 0 or 1");
   Job J;
   sbp_status s = prepare(J, g, part, B, np, 1);
   if (s != SBP_OK) return s;
   int32_t b = B;
-  s = merge_step(J, b, B_to_merge, seed, seq, false);
+  s = merge_step(J, b, B_to_merge, seed, seq, false, ref_grid);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaStreamSynchronize(J.st));
   if (best) std::memcpy(best, J.h_best, 4 * (size_t)B);

@@ -278,6 +278,14 @@ void Engine::add_run_work(Run& r) {
   Job& J = *r.J;
   const int32_t N = J.N;
   if (r.init) add_iota(s_iota, J.part, N);
+  if (r.init && ref_grid_on(r.o)) {
+    // GSAP's merge buffers start at zero in a fresh process; the slots its
+    // grid leaves out read them (MergeGrid)
+    const size_t slots = (size_t)N * J.np;
+    add_zero(s_zero, J.props, slots);
+    add_zero(s_zero, J.mdS, 2 * slots);
+    add_zero(s_zero, J.mdsin, 2 * slots);
+  }
   if (r.upload_lists)
     add_copy(s_lists, J.lists, up_dev_ptr(r.up_lists), r.lists_all.size());
   if (r.snap_slot >= 0) add_copy(s_snap, J.snap[r.snap_slot], J.part, (size_t)N);
@@ -295,8 +303,10 @@ void Engine::add_run_work(Run& r) {
     // the merge kernels read the CSR form
     if (!r.csr_fresh) add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
     add_block_terms(m_bt, J.m, r.B, 0, r.o.seed, 0);
-    add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props);
-    add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS, r.o.exact);
+    const MergeGrid grid = merge_grid(J, r.o);
+    add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props, grid);
+    add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS, r.o.exact,
+                    grid);
     add_copy(s_gather, rd_dev_ptr(r.rd_off), J.best, (size_t)r.B);
     add_copy(s_gather, rd_dev_ptr(r.rd_off + align256(4 * (size_t)r.B)), J.best_dS,
              2 * (size_t)r.B);

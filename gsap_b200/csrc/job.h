@@ -53,6 +53,7 @@ struct Job {
   int32_t *part = nullptr, *newlab = nullptr, *props = nullptr, *best = nullptr, *map = nullptr;
   int32_t* snap[3] = {nullptr, nullptr, nullptr};
   double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
+  double* mdsin = nullptr;      // merge in-row terms by proposal slot (MergeGrid)
   int32_t* lists = nullptr;     // batch indices by nodal kernel path (classify_batch)
   int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
   int32_t* ctl = nullptr;       // sweep control: sweeps done in the outer step, stop flag
@@ -101,6 +102,19 @@ double model_S(int32_t B, int32_t N, int32_t E, int32_t exact = 0);
 // rebuild of the CSR form after every batch costs O(E); the dense form's
 // per-sweep terms cost O(B^2), so the crossover grows with E.
 int32_t dense_limit(int32_t N, int32_t E, int32_t dense_max);
+
+// Whether GSAP's merge grid is reproduced (sbp_options.ref_grid).
+inline bool ref_grid_on(const sbp_options& o) {
+  return o.ref_grid < 0 ? o.exact == 0 : o.ref_grid != 0;
+}
+// The persistent merge buffers of a job as a MergeGrid.
+inline MergeGrid merge_grid(const Job& J, const sbp_options& o) {
+  MergeGrid g;
+  g.on = ref_grid_on(o) ? 1 : 0;
+  g.dS = J.mdS;
+  g.dsin = J.mdsin;
+  return g;
+}
 
 inline ScoreMode score_mode(const sbp_options& o) {
   ScoreMode m;

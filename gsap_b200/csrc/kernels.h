@@ -187,10 +187,22 @@ void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t
                 const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
                 int32_t B, const CommitScratch& cs, const int32_t* ctl = nullptr,
                 int32_t slot_mul = 0);
+// GSAP's merge grid (Q16, partition.hpp:335-336): when `on`, only the
+// proposal slots below the nnz of the out CSR, rounded up to 256, are drawn
+// and scored; the others keep the targets, dS (dS) and in-row terms (dsin)
+// their slots hold from earlier merge steps of the run (zero at its start).
+// Arrays of N * np entries that persist over the run.
+struct MergeGrid {
+  int32_t on = 0;
+  double* dS = nullptr;
+  double* dsin = nullptr;
+};
+
 void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
-                     int32_t* props);
+                     int32_t* props, const MergeGrid& grid = MergeGrid());
 void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
-                     double* dS, int32_t* best, double* best_dS, int32_t exact = 0);
+                     double* dS, int32_t* best, double* best_dS, int32_t exact = 0,
+                     const MergeGrid& grid = MergeGrid());
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map);
 
 // Tuned shape for a device and a blockmodel size class, if known.
@@ -278,9 +290,10 @@ void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newla
 // Merge proposals (kernels.hpp:726-856) and their dS with the per-block best
 // (kernels.hpp:143-491).
 void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
-                     int32_t* props, cudaStream_t st);
+                     int32_t* props, cudaStream_t st, const MergeGrid& grid = MergeGrid());
 void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
-                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact = 0);
+                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact = 0,
+                 const MergeGrid& grid = MergeGrid());
 // part[v] = map[part[v]] (update_partitions, kernels.hpp:1728-1740).
 void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st);
 

@@ -35,7 +35,23 @@ struct MergeArgs {
   int32_t* best;
   double* best_dS;
   int32_t exact;  // 1: exact merge dS (merge_one_exact)
+  // GSAP's merge grid (Q16, partition.hpp:335-336): with ref_grid set, only
+  // proposals t < T = (nnz of the out CSR, rounded up to 256) are drawn and
+  // scored; slots t >= T keep the target (props) and dS (keep_dS) their
+  // buffers hold, and a proposal whose partner slot s*np+k lies at or past T
+  // reads that slot's in-row term from keep_dsin.
+  int32_t ref_grid;
+  double* keep_dS;
+  double* keep_dsin;
 };
+
+// First proposal slot GSAP's merge grid leaves out (B*np when none is).
+__device__ __forceinline__ long long merge_grid_end(const MergeArgs& a) {
+  const long long n = (long long)a.B * a.np;
+  if (!a.ref_grid) return n;
+  const long long T = ((long long)a.optr[a.B] + 255) / 256 * 256;
+  return T < n ? T : n;
+}
 
 // First index k of out-row ++ in-row of block b with running count > t.
 __device__ int pick_serial(const MergeArgs& a, int b, uint64_t t) {
@@ -68,7 +84,7 @@ struct MergePropsBody {
 
 __device__ void MergePropsBody::run(const MergeArgs& a, int vb, int) {
   long long t = (long long)vb * kThreads + threadIdx.x;
-  if (t >= (long long)a.B * a.np) return;
+  if (t >= merge_grid_end(a)) return;
   int r = (int)(t / a.np);
   P4 x = draw(a.seed, kRngMerge, a.seq, (uint32_t)t);
   uint32_t B = (uint32_t)a.B;
@@ -104,8 +120,11 @@ __device__ __forceinline__ double fterm(const double* tab, uint32_t m, double a,
 }
 
 // Merge dS of block r with s (calculate_dS_overall, kernels.hpp:417-449),
-// s2 = the k-th proposal of block s (its in-term leaves out s2, Q1).
-__device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) {
+// s2 = the k-th proposal of block s (its in-term leaves out s2, Q1).  With
+// in_s_given, block s's in-term is *in_s_given (a slot GSAP's grid left
+// out); in_r_out receives block r's in-term.
+__device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane,
+                            const double* in_s_given = nullptr, double* in_r_out = nullptr) {
   // merged out-rows (calculate_dS_new_out, kernels.hpp:233-320)
   double acc_o = 0.0, acc_i = 0.0;
   const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s], ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
@@ -162,8 +181,14 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane) 
   // old in-rows (calculate_dS_in, kernels.hpp:185-231): row r without r, s;
   // row s without s, s2
   double in_r = a.sinfull[r] - fterm(a.xlx, Mrr, ldo_r, ldi_r) - (s != r ? fterm(a.xlx, Msr, ldo_s, ldi_r) : 0.0);
-  uint32_t Ms2s = s2 == s ? 0u : row_lookup(a.ocol, a.ocnt, a.optr[s2], a.optr[s2 + 1], s);
-  double in_s = a.sinfull[s] - fterm(a.xlx, Mss, ldo_s, ldi_s) - fterm(a.xlx, Ms2s, a.ld_out[s2], ldi_s);
+  double in_s;
+  if (in_s_given) {
+    in_s = *in_s_given;
+  } else {
+    uint32_t Ms2s = s2 == s ? 0u : row_lookup(a.ocol, a.ocnt, a.optr[s2], a.optr[s2 + 1], s);
+    in_s = a.sinfull[s] - fterm(a.xlx, Mss, ldo_s, ldi_s) - fterm(a.xlx, Ms2s, a.ld_out[s2], ldi_s);
+  }
+  if (in_r_out) *in_r_out = in_r;
   return a.dSout[r] + a.dSout[s] + in_r + in_s + new_out + new_in;
 }
 
@@ -217,18 +242,37 @@ struct MergeDeltaBody {
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long T = merge_grid_end(a);
   for (int r = vb * kMergeWarps + wid; r < a.B; r += vg * kMergeWarps) {
     double mine = DBL_MAX;
     int who = 0;
     for (int k = 0; k < a.np; ++k) {
-      int s = a.props_in[(long long)r * a.np + k];
-      int s2 = a.props_in[(long long)s * a.np + k];
-      double d = a.exact ? merge_one_exact(a, r, s, lane) : merge_one(a, r, s, s2, lane);
+      const long long t = (long long)r * a.np + k;
+      int s = a.props_in[t];
+      double d;
+      if (t >= T) {
+        d = a.keep_dS[t];  // a slot GSAP's grid leaves out keeps its old values
+      } else if (a.exact) {
+        d = merge_one_exact(a, r, s, lane);
+      } else {
+        const long long sid = (long long)s * a.np + k;
+        double in_r = 0.0;
+        if (sid >= T) {
+          d = merge_one(a, r, s, 0, lane, a.keep_dsin + sid, &in_r);
+        } else {
+          int s2 = a.props_in[sid];
+          d = merge_one(a, r, s, s2, lane, nullptr, &in_r);
+        }
+        if (a.ref_grid && lane == 0) a.keep_dsin[t] = in_r;
+      }
       if (lane == k) {
         mine = d;
         who = s;
       }
-      if (lane == 0 && a.dS) a.dS[(long long)r * a.np + k] = d;
+      if (lane == 0 && t < T) {
+        if (a.dS) a.dS[t] = d;
+        if (a.ref_grid) a.keep_dS[t] = d;
+      }
     }
     // find_best_warp's reduction
 #pragma unroll
@@ -268,7 +312,7 @@ const MultiKernel kmMergeProps = multi_kernel_desc<MergePropsBody>("merge_props"
 const MultiKernel kmMergeDelta = multi_kernel_desc<MergeDeltaBody>("merge_delta");
 const MultiKernel kmRelabel = multi_kernel_desc<RelabelBody>("relabel");
 
-MergeArgs make_args(const DevBM& m, int32_t B, int32_t np) {
+MergeArgs make_args(const DevBM& m, int32_t B, int32_t np, const MergeGrid& grid) {
   MergeArgs a{};
   a.xlx = m.xlx;
   a.optr = m.optr; a.ocol = m.ocol; a.iptr = m.iptr; a.icol = m.icol;
@@ -277,14 +321,17 @@ MergeArgs make_args(const DevBM& m, int32_t B, int32_t np) {
   a.ambin = m.ambin; a.sinfull = m.sinfull;
   a.B = B;
   a.np = np;
+  a.ref_grid = grid.on;
+  a.keep_dS = grid.dS;
+  a.keep_dsin = grid.dsin;
   return a;
 }
 
 }  // namespace
 
 void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
-                     int32_t* props, cudaStream_t st) {
-  MergeArgs a = make_args(m, B, np);
+                     int32_t* props, cudaStream_t st, const MergeGrid& grid) {
+  MergeArgs a = make_args(m, B, np, grid);
   a.seed = seed;
   a.seq = seq;
   a.props = props;
@@ -293,8 +340,9 @@ void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint3
 }
 
 void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
-                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact) {
-  MergeArgs a = make_args(m, B, np);
+                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact,
+                 const MergeGrid& grid) {
+  MergeArgs a = make_args(m, B, np, grid);
   a.exact = exact;
   a.props_in = props;
   a.dS = dS;
@@ -309,8 +357,8 @@ void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st) {
 }
 
 void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
-                     int32_t* props) {
-  MergeArgs a = make_args(m, B, np);
+                     int32_t* props, const MergeGrid& grid) {
+  MergeArgs a = make_args(m, B, np, grid);
   a.seed = seed;
   a.seq = seq;
   a.props = props;
@@ -318,8 +366,9 @@ void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t se
 }
 
 void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
-                     double* dS, int32_t* best, double* best_dS, int32_t exact) {
-  MergeArgs a = make_args(m, B, np);
+                     double* dS, int32_t* best, double* best_dS, int32_t exact,
+                     const MergeGrid& grid) {
+  MergeArgs a = make_args(m, B, np, grid);
   a.exact = exact;
   a.props_in = props;
   a.dS = dS;

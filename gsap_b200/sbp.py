@@ -51,7 +51,7 @@ class Options(C.Structure):
                 ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32),
                 ("device", C.c_int32), ("use_graphs", C.c_int32), ("verbose", C.c_int32),
                 ("dense_max", C.c_int32), ("exact", C.c_int32), ("mh", C.c_int32),
-                ("beta", C.c_double)]
+                ("beta", C.c_double), ("ref_grid", C.c_int32)]
 
 
 class Report(C.Structure):
@@ -143,6 +143,8 @@ _sig("sbp_nodal_sweeps", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint
      C.c_int32, C.c_int32, C.c_int32, _vp)
 _sig("sbp_merge_step", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, C.c_int32,
      C.c_uint64, C.c_uint32, _vp, _vp, C.POINTER(C.c_int32))
+_sig("sbp_merge_step_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, C.c_int32,
+     C.c_uint64, C.c_uint32, C.c_int32, _vp, _vp, C.POINTER(C.c_int32))
 _sig("sbp_mdl", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.POINTER(C.c_double),
      C.POINTER(C.c_double))
 _sig("sbp_mdl_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32,
@@ -542,13 +544,15 @@ def nodal_sweeps(g: Graph, part, B, seed, seq0, num_batches=4, sweeps=1, dense_m
     return part, sums
 
 
-def merge_step(g: Graph, part, B, B_to_merge, seed, seq, np_=10):
+def merge_step(g: Graph, part, B, B_to_merge, seed, seq, np_=10, ref_grid=0):
+    """One merge step (sbp_merge_step_mode); ref_grid = 1 makes it the first
+    merge step of a run that reproduces GSAP's merge grid."""
     part = np.array(part, dtype=np.int32, copy=True)
     best = np.zeros(B, np.int32)
     best_dS = np.zeros(B, np.float64)
     nb = C.c_int32()
-    _check(_lib.sbp_merge_step(C.byref(g.csr()), _p(part), B, B_to_merge, np_, seed, seq,
-                               _p(best), _p(best_dS), C.byref(nb)))
+    _check(_lib.sbp_merge_step_mode(C.byref(g.csr()), _p(part), B, B_to_merge, np_, seed, seq,
+                                    ref_grid, _p(best), _p(best_dS), C.byref(nb)))
     return part, nb.value, best, best_dS
 
 

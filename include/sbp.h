@@ -313,6 +313,14 @@ sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int3
                           int32_t np, uint64_t seed, uint32_t seq, int32_t* best, double* best_dS,
                           int32_t* B_new);
 
+/* sbp_merge_step as the first merge step of a run with sbp_options.ref_grid
+ * = ref_grid: with 1, the proposal slots past GSAP's merge grid (the nnz of
+ * the out CSR rounded up to 256, partition.hpp:335-336) read the zeros of
+ * fresh merge buffers instead of being drawn and scored. */
+sbp_status sbp_merge_step_mode(const sbp_graph_csr* g, int32_t* part, int32_t B,
+                               int32_t B_to_merge, int32_t np, uint64_t seed, uint32_t seq,
+                               int32_t ref_grid, int32_t* best, double* best_dS, int32_t* B_new);
+
 /* The MDL of a partition (compute_overall_entropy_cuda, partition.hpp:665-704). */
 sbp_status sbp_mdl(const sbp_graph_csr* g, const int32_t* part, int32_t B, double* S,
                    double* data_S);

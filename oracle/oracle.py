@@ -39,7 +39,8 @@ class Options(C.Structure):
                 ("reduction_rate", C.c_float), ("max_nodal_itr", C.c_int32),
                 ("num_batches", C.c_int32), ("threshold1", C.c_float),
                 ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32),
-                ("exact", C.c_int32), ("mh", C.c_int32), ("beta", C.c_double)]
+                ("exact", C.c_int32), ("mh", C.c_int32), ("beta", C.c_double),
+                ("ref_grid", C.c_int32)]
 
 
 class Report(C.Structure):
@@ -72,6 +73,8 @@ _sig("orc_nodal_batch", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_uint32,
      C.c_int32, _vp, _vp)
 _sig("orc_merge_step", C.c_int32, _GP, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
      C.c_uint32, _vp, _vp)
+_sig("orc_merge_step_mode", C.c_int32, _GP, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
+     C.c_uint32, C.c_int32, _vp, _vp)
 _sig("orc_apply_merges", C.c_int32, C.c_int32, _vp, C.c_int32, C.c_int32, _vp, _vp)
 _sig("orc_partition", C.c_int, _GP, C.POINTER(Options), _vp, C.POINTER(Report))
 _sig("orc_time_nodal", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_int32, C.c_int32)
@@ -197,12 +200,12 @@ def nodal_batch(g, part, B, seed, seq, lo, hi):
     return part, dS[:hi - lo], props[:hi - lo], tot
 
 
-def merge_step(g, part, B, B_to_merge, seed, seq, np_=10):
+def merge_step(g, part, B, B_to_merge, seed, seq, np_=10, ref_grid=0):
     part = np.array(part, dtype=np.int32, copy=True)
     best = np.zeros(B, np.int32)
     bds = np.zeros(B)
-    nb = _lib.orc_merge_step(C.byref(_g(g)), _p(part), B, B_to_merge, np_, seed, seq, _p(best),
-                             _p(bds))
+    nb = _lib.orc_merge_step_mode(C.byref(_g(g)), _p(part), B, B_to_merge, np_, seed, seq,
+                                  ref_grid, _p(best), _p(bds))
     return part, nb, best, bds
 
 
@@ -217,7 +220,7 @@ def apply_merges(part, B, B_to_merge, best, best_dS):
 def default_options(**kw):
     o = Options(seed=0, num_proposals=10, reduction_rate=0.35, max_nodal_itr=100, num_batches=4,
                 threshold1=5e-4, threshold2=1e-4, window=3, max_outer=1000, exact=0, mh=0,
-                beta=3.0)
+                beta=3.0, ref_grid=-1)
     for k, v in kw.items():
         setattr(o, k, v)
     return o

@@ -616,23 +616,45 @@ double merge_new_in(const BM& m, int32_t r, int32_t s) {
   return dS;
 }
 
+// The proposals GSAP's merge kernels compute (Q16, partition.hpp:335-336):
+// every merge kernel runs on a grid of nnz threads rounded up to 256 (nnz =
+// entries of the out CSR), so when B*np exceeds that count, proposals t >= T
+// are never drawn or scored; their slots keep what the buffers held (zeros
+// in a fresh process, else an earlier merge step's values), and a proposal
+// whose partner slot s*np+k lies past T reads that slot's stale in-row term.
+// `keep` holds those persistent buffers across the merge steps of one run.
+struct MergeKeep {
+  int64_t T = INT64_MAX;         // proposals [0, T) are computed
+  std::vector<double> dsin;      // in-row terms by proposal slot (dS_in)
+};
+
+inline int64_t merge_grid(const BM& m, int ref_grid) {
+  return ref_grid ? (m.nnz() + 255) / 256 * 256 : INT64_MAX;
+}
+
 // kernels.hpp:417-449 (calculate_dS_overall) for every proposal, then
 // kernels.hpp:452-491 (find_best_warp): per block the minimum over its
 // proposals, reduced over 32 lanes by halving offsets; on equal values the
 // lane further up wins.  Lanes past num_proposals hold (largest finite, 0).
+// With `keep`, proposals t >= keep->T keep the dS and target their slots
+// already hold.
 void merge_deltas(const BM& m, const int32_t* props, int np, double* dS, int32_t* best,
-                  double* best_dS, const Mode& md = Mode()) {
+                  double* best_dS, const Mode& md = Mode(), MergeKeep* keep = nullptr) {
   int32_t B = m.B;
+  const int64_t n = (int64_t)B * np;
+  const int64_t T = keep ? std::min(keep->T, n) : n;
   std::vector<double> dso(B);
   for (int32_t b = 0; b < B; ++b) dso[b] = dS_out_block(m, b);
-  std::vector<double> dsin((size_t)B * np);
-  for (int32_t t = 0; t < B * np; ++t) {
-    int32_t r = t / np;
+  std::vector<double> fresh;
+  std::vector<double>& dsin = keep ? keep->dsin : fresh;
+  if ((int64_t)dsin.size() < n) dsin.resize(n, 0.0);
+  for (int64_t t = 0; t < T; ++t) {
+    int32_t r = (int32_t)(t / np);
     dsin[t] = dS_in_block_excl(m, r, r, props[t]);
   }
-  for (int32_t t = 0; t < B * np; ++t) {
-    int32_t r = t / np, s = props[t], k = t % np;
-    int32_t sid = s * np + k;
+  for (int64_t t = 0; t < T; ++t) {
+    int32_t r = (int32_t)(t / np), s = props[t], k = (int32_t)(t % np);
+    int64_t sid = (int64_t)s * np + k;
     double d = 0.0;
     if (md.exact) {
       d = merge_delta_exact(m, r, s);
@@ -864,6 +886,7 @@ struct Options {
   int32_t window;
   int32_t max_outer;
   Mode mode;
+  int32_t ref_grid;  // 1: GSAP's nnz-sized merge grid (Q16), see MergeKeep
 };
 
 struct Report {
@@ -909,19 +932,23 @@ int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep
   int32_t outer = 0;
   int32_t BS = N / o.num_batches;
   std::vector<double> itr_dS(o.max_nodal_itr);
+  // merge buffers persist over the run and start at zero, like GSAP's
+  // (allocate_device.hpp:31-73 on a fresh stream-ordered pool)
   std::vector<int32_t> props((size_t)N * o.num_proposals);
   std::vector<double> mdS((size_t)N * o.num_proposals);
   std::vector<int32_t> best(N);
   std::vector<double> best_dS(N);
+  MergeKeep keep;
   while (!optimal) {
     if (++outer > o.max_outer) { R.status = 2; break; }
     // merge phase (partition.hpp:900-904)
     t0 = Clock::now();
-    for (int32_t t = 0; t < B * o.num_proposals; ++t)
+    keep.T = std::min<int64_t>(merge_grid(m, o.ref_grid), (int64_t)B * o.num_proposals);
+    for (int32_t t = 0; t < keep.T; ++t)
       props[t] = merge_proposal(m, t / o.num_proposals, o.seed, seq, (uint32_t)t);
     ++seq;
     merge_deltas(m, props.data(), o.num_proposals, mdS.data(), best.data(), best_dS.data(),
-                 o.mode);
+                 o.mode, &keep);
     B = apply_merges(part, B, B_to_merge, best.data(), best_dS.data());
     R.ms_merge += ms_since(t0);
     t0 = Clock::now();
@@ -1303,23 +1330,33 @@ double orc_nodal_batch(const orc_graph* xg, int32_t* part, int32_t B, uint64_t s
 }
 
 // One merge step: proposals, dS, best, merges.  Updates part; returns new B.
-int32_t orc_merge_step(const orc_graph* xg, int32_t* part, int32_t B, int32_t B_to_merge,
-                       int32_t np, uint64_t seed, uint32_t seq, int32_t* best_out,
-                       double* best_dS_out) {
+int32_t orc_merge_step_mode(const orc_graph* xg, int32_t* part, int32_t B, int32_t B_to_merge,
+                            int32_t np, uint64_t seed, uint32_t seq, int32_t ref_grid,
+                            int32_t* best_out, double* best_dS_out) {
   Graph g = to_graph(xg);
   BM m = build_bm(g, part, B);
-  std::vector<int32_t> props((size_t)B * np);
-  for (int32_t t = 0; t < B * np; ++t) props[t] = merge_proposal(m, t / np, seed, seq, (uint32_t)t);
-  std::vector<double> dS((size_t)B * np);
+  // the first merge step of a run: fresh (zero) merge buffers
+  MergeKeep keep;
+  keep.T = std::min<int64_t>(merge_grid(m, ref_grid), (int64_t)B * np);
+  std::vector<int32_t> props((size_t)B * np, 0);
+  for (int64_t t = 0; t < keep.T; ++t)
+    props[t] = merge_proposal(m, (int32_t)(t / np), seed, seq, (uint32_t)t);
+  std::vector<double> dS((size_t)B * np, 0.0);
   std::vector<int32_t> best(B);
   std::vector<double> bds(B);
-  merge_deltas(m, props.data(), np, dS.data(), best.data(), bds.data());
+  merge_deltas(m, props.data(), np, dS.data(), best.data(), bds.data(), Mode(), &keep);
   if (best_out) std::copy(best.begin(), best.end(), best_out);
   if (best_dS_out) std::copy(bds.begin(), bds.end(), best_dS_out);
   std::vector<int32_t> p(part, part + g.N);
   int32_t nb = apply_merges(p, B, B_to_merge, best.data(), bds.data());
   std::copy(p.begin(), p.end(), part);
   return nb;
+}
+
+int32_t orc_merge_step(const orc_graph* xg, int32_t* part, int32_t B, int32_t B_to_merge,
+                       int32_t np, uint64_t seed, uint32_t seq, int32_t* best_out,
+                       double* best_dS_out) {
+  return orc_merge_step_mode(xg, part, B, B_to_merge, np, seed, seq, 0, best_out, best_dS_out);
 }
 
 // Merge application alone (for tests of the host merge loop).
@@ -1344,6 +1381,7 @@ typedef struct orc_options {
   int32_t exact;
   int32_t mh;
   double beta;
+  int32_t ref_grid;
 } orc_options;
 
 typedef struct orc_report {
@@ -1360,7 +1398,8 @@ typedef struct orc_report {
 int orc_partition(const orc_graph* xg, const orc_options* xo, int32_t* labels, orc_report* rep) {
   Graph g = to_graph(xg);
   Options o{xo->seed, xo->num_proposals, xo->reduction_rate, xo->max_nodal_itr, xo->num_batches,
-            xo->threshold1, xo->threshold2, xo->window, xo->max_outer, Mode()};
+            xo->threshold1, xo->threshold2, xo->window, xo->max_outer, Mode(),
+            xo->ref_grid < 0 ? (xo->exact == 0 ? 1 : 0) : xo->ref_grid};
   o.mode.exact = xo->exact;
   o.mode.mh = xo->mh;
   o.mode.beta = xo->beta;

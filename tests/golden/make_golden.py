@@ -1,6 +1,6 @@
 """Generates the golden fixtures of this directory from the reference itself.
 
-Needs the reference tree (REF, default /root/reference) and the checkers
+Needs the reference tree (REF, else the tree oracle/build_ref.sh used) and the checkers
 that oracle/build_ref.sh builds from it into oracle/_ref/:
 
   loader.json       GSAP/load.hpp on the eight bundled 1k/5k GraphChallenge
@@ -26,7 +26,9 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF", "")
+if not REF and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_root")):
+    REF = open(os.path.join(ROOT, "oracle", "_ref", "ref_root")).read().strip()
 REF_HOST = os.path.join(ROOT, "oracle", "_ref", "ref_host")
 CATS = ("LL", "LH", "HL", "HH")
 SIZES = ("1k", "5k")

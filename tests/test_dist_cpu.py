@@ -69,3 +69,58 @@ def test_phase_rates():
     assert abs(r["nodal"] - 20.0) < 1e-12 and abs(r["rebuild"] - 20.0) < 1e-12
     assert r["merge"] is None
     assert abs(r["end_to_end"] - 14.0) < 1e-12 and r["bytes_per_step"] == 1.75e9
+
+
+SHARD_SCRIPT = r"""
+import json, sys
+sys.path.insert(0, {root!r})
+import numpy as np
+import bench
+from gsap_b200.shard import gather_results, shard_jobs
+rank, world, local = bench.dist_env()
+d = bench.Dist(world, local, backend="gloo")
+costs = [int(c) for c in np.random.default_rng(0).integers(1000, 50000, 37)]
+mine = shard_jobs(costs, world)[rank]
+# each rank's stand-in for its partition_batch share
+labels = [np.arange(10 + i, dtype=np.int32) % (i + 2) for i in mine]
+reports = [{{"job": i, "rank": rank, "B": i + 2}} for i in mine]
+tot = d.sum(len(mine))
+labs, reps = gather_results(mine, labels, reports, world, rank)
+d.barrier()
+d.close()
+if rank == 0:
+    ok = all(np.array_equal(labs[i], np.arange(10 + i) % (i + 2)) and reps[i]["job"] == i
+             for i in range(len(costs)))
+    print(json.dumps({{"n": len(labs), "ok": ok, "tot": tot,
+                      "ranks": sorted(set(r["rank"] for r in reps))}}))
+else:
+    print(json.dumps({{"none": labs is None and reps is None}}))
+"""
+
+
+def test_shard_jobs_covers_and_balances():
+    import sys
+    sys.path.insert(0, ROOT)
+    from gsap_b200.shard import shard_jobs
+    costs = [50, 10, 40, 30, 30, 20, 5, 5]
+    for world in (1, 2, 3, 8, 10):
+        plan = shard_jobs(costs, world)
+        assert len(plan) == world
+        flat = sorted(i for p in plan for i in p)
+        assert flat == list(range(len(costs)))
+        assert all(p == sorted(p) for p in plan)
+        loads = [sum(costs[i] for i in p) for p in plan]
+        if world <= len(costs):
+            # greedy longest-first: no rank exceeds the lightest by more than one job
+            assert max(loads) - min(loads) <= max(costs)
+
+
+def test_two_gloo_ranks_shard_and_gather():
+    import json
+    res = _run_ranks(["-c", SHARD_SCRIPT.format(root=ROOT)])
+    for rc, o, e in res:
+        assert rc == 0, e[-2000:]
+    r0 = json.loads(res[0][1].strip().splitlines()[-1])
+    r1 = json.loads(res[1][1].strip().splitlines()[-1])
+    assert r0 == {"n": 37, "ok": True, "tot": 37.0, "ranks": [0, 1]}
+    assert r1 == {"none": True}

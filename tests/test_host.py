@@ -12,7 +12,20 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-DATA = "/root/reference/Dataset/static"
+
+
+def _dataset_dir():
+    """The GraphChallenge graphs bundled with the reference tree: under $REF,
+    else under the tree oracle/build_ref.sh built the checkers from (its
+    oracle/_ref/ref_root).  Empty when neither is on this machine."""
+    ref = os.environ.get("REF", "")
+    marker = os.path.join(ROOT, "oracle", "_ref", "ref_root")
+    if not ref and os.path.exists(marker):
+        ref = open(marker).read().strip()
+    return os.path.join(ref, "Dataset", "static") if ref else ""
+
+
+DATA = _dataset_dir()
 
 
 def test_exports_every_declared_symbol(sbp):
