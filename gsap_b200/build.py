@@ -10,7 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsbp.so")
-SOURCES = ["driver.cu", "engine.cu", "blockmodel.cu", "nodal.cu", "merge.cu", "noalloc.cu", "server.cu", "host.cpp"]
+SOURCES = ["driver.cu", "engine.cu", "blockmodel.cu", "nodal.cu", "merge.cu", "mergeapply.cu",
+           "noalloc.cu", "server.cu", "host.cpp"]
 HEADERS = ["common.cuh", "kernels.h", "multi.cuh", "job.h", "engine.h"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",

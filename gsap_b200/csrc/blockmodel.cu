@@ -1129,6 +1129,10 @@ void add_scan(Slot* sl, const int32_t* in, int32_t* out, int32_t n, int32_t* til
 
 }  // namespace
 
+void add_exclusive_scan(Slot* sl, const int32_t* in, int32_t* out, int32_t n, int32_t* tile) {
+  add_scan(sl, in, out, n, tile, nullptr);
+}
+
 cudaError_t init_kernel_attributes() {
   cudaError_t e = cudaFuncSetAttribute(single_kernel<RbRowsBigBody>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -160,6 +160,9 @@ size_t job_bytes(int32_t N, int32_t E, int32_t np, int32_t max_itr, int32_t dens
   add((size_t)dense_cap * dense_cap, 4); add((size_t)dense_cap * dense_cap, 4);
   add((size_t)2 * dense_cap * ((dense_cap + 31) / 32), 4);
   add(kCommitCtas, 8); add(kCommitCtas, 8); add(1, 4);
+  // merge application on the device
+  b += merge_apply_bytes(N);
+  add(2, 4);
   return b + 4096;
 }
 
@@ -312,7 +315,14 @@ sbp_status job_create(Job& J, int device, int32_t N, int32_t E, int32_t np, int3
   J.cs.part_sum = A.take<double>(kCommitCtas);
   J.cs.part_cnt = A.take<long long>(kCommitCtas);
   J.cs.ticket = A.take<unsigned>(1);
-  if (!J.cs.ticket || (J.dense_cap > 0 && !m.Sd)) return fail(SBP_ERR_INTERNAL, "arena sizing");
+  {
+    const size_t mab = merge_apply_bytes(N);
+    char* base = A.take<char>(mab);
+    if (base) J.ma = merge_apply_carve(base, N);
+    J.ma_out = A.take<int32_t>(2);
+  }
+  if (!J.cs.ticket || !J.ma_out || (J.dense_cap > 0 && !m.Sd))
+    return fail(SBP_ERR_INTERNAL, "arena sizing");
   SBP_CUDA(cudaMemsetAsync(J.err, 0, 8, J.st));
   SBP_CUDA(cudaMemsetAsync(J.cs.ticket, 0, 4, J.st));
   return SBP_OK;
@@ -989,6 +999,49 @@ sbp_status sbp_apply_merges(int32_t B, int32_t B_to_merge, const int32_t* best,
   const int32_t nb = apply_merges_host(B, B_to_merge, best, best_dS, map);
   if (nb < 0) return fail(SBP_ERR_INVALID, "merge target out of [0, B)");
   *B_new = nb;
+  return SBP_OK;
+}
+
+sbp_status sbp_apply_merges_device(int32_t B, int32_t B_to_merge, const int32_t* best,
+                                   const double* best_dS, int32_t device, int32_t* map,
+                                   int32_t* B_new) {
+  if (B < 1 || B_to_merge < 0 || !best || !best_dS || !map || !B_new)
+    return fail(SBP_ERR_INVALID, "bad merge arguments");
+  const int dev = resolve_device(device);
+  SBP_CUDA(cudaSetDevice(dev));
+  const size_t ws = merge_apply_bytes(B);
+  const size_t need = ws + 256 * 5 + (size_t)B * (4 + 8 + 4) + 8;
+  char* mem = nullptr;
+  cudaStream_t st = nullptr;
+  SBP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  if (cudaMalloc(&mem, need) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(st);
+    return fail(SBP_ERR_NOMEM, "device buffers of the merge application");
+  }
+  Arena A{mem, need, 0};
+  MergeApplyBufs w = merge_apply_carve(A.take<char>(ws), B);
+  int32_t* d_best = A.take<int32_t>(B);
+  double* d_bds = A.take<double>(B);
+  int32_t* d_map = A.take<int32_t>(B);
+  int32_t* d_out = A.take<int32_t>(2);
+  int32_t out[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(d_best, best, 4 * (size_t)B, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_bds, best_dS, 8 * (size_t)B, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_out, 0, 8, st);
+  if (e == cudaSuccess) {
+    merge_apply(w, B, B_to_merge, d_best, d_bds, d_map, d_out, st);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(map, d_map, 4 * (size_t)B, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(mem);
+  cudaStreamDestroy(st);
+  if (e != cudaSuccess) return fail(SBP_ERR_CUDA, cudaGetErrorString(e));
+  if (out[1]) return fail(SBP_ERR_INVALID, "merge target out of [0, B)");
+  *B_new = out[0];
   return SBP_OK;
 }
 

@@ -3,17 +3,18 @@
 //
 // Each job is a Run: the loop's host state (block count, golden-section
 // bracket, stop test, RNG sequence) as a state machine that is advanced one
-// step per engine tick.  A step is either one merge step or one nodal sweep
-// (num_batches batches plus the MDL), preceded by the device work the last
-// host decision left pending (golden-section snapshot and restore copies,
-// the relabel after merges, the blockmodel build).
+// step per engine tick.  A step is either one merge step (proposals, dS,
+// the merge application and the relabel, all on the device) or queued nodal
+// sweeps (num_batches batches plus the MDL each), preceded by the device work
+// the last host decision left pending (golden-section snapshot and restore
+// copies, the blockmodel build).
 //
 // A tick gathers the device work of every active Run and issues it as
 // multi-job launches: one launch per kernel body covers all jobs that need
 // it (multi.cuh), so a tick costs about the same number of launches for one
-// job as for hundreds.  Argument records, merge maps and heavy-vertex lists
-// go up in two host-to-device copies per tick, every result the host needs
-// (merge choices, sweep sums, MDL terms, final labels) comes back in one
+// job as for hundreds.  Argument records and heavy-vertex lists go up in two
+// host-to-device copies per tick, every result the host needs (new block
+// counts, sweep sums, MDL terms, final labels) comes back in one
 // device-to-host copy, and the host synchronises once per tick.
 //
 // sbp_partition is a batch of one.  sbp_partition_batch and the server
@@ -223,9 +224,10 @@ void Engine::ensure_slots(int K, int nb) {
 }
 
 void Engine::clear_slots() {
-  for (Slot* s : {&s_iota, &s_lists, &s_snap, &s_restore, &s_relabel, &s_zero, &m_bt, &m_props,
-                  &m_delta, &s_gather})
+  for (Slot* s : {&s_iota, &s_lists, &s_snap, &s_restore, &s_zero, &m_bt, &m_props, &m_delta,
+                  &m_relabel, &s_gather})
     s->clear();
+  m_apply.clear();
   pre_dense.clear();
   pre_rebuild.clear();
   for (auto& b : sw) {
@@ -290,7 +292,6 @@ void Engine::add_run_work(Run& r) {
     add_copy(s_lists, J.lists, up_dev_ptr(r.up_lists), r.lists_all.size());
   if (r.snap_slot >= 0) add_copy(s_snap, J.snap[r.snap_slot], J.part, (size_t)N);
   if (r.restore_slot >= 0) add_copy(s_restore, J.part, J.snap[r.restore_slot], (size_t)N);
-  if (r.relabel) add_relabel(s_relabel, J.part, N, (const int32_t*)up_dev_ptr(r.up_map));
   if (r.zero_itr) {
     const size_t n = r.sweeps_only ? (size_t)r.sweeps_total * r.o.num_batches
                                    : (size_t)r.o.max_nodal_itr;
@@ -307,9 +308,12 @@ void Engine::add_run_work(Run& r) {
     add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props, grid);
     add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS, r.o.exact,
                     grid);
-    add_copy(s_gather, rd_dev_ptr(r.rd_off), J.best, (size_t)r.B);
-    add_copy(s_gather, rd_dev_ptr(r.rd_off + align256(4 * (size_t)r.B)), J.best_dS,
-             2 * (size_t)r.B);
+    // carry_out_best_merges on the device, then the relabel: the host reads
+    // back only the new block count
+    add_zero(s_zero, J.ma_out, 2);
+    add_merge_apply(m_apply, J.ma, r.B, r.B_to_merge, J.best, J.best_dS, J.map, J.ma_out);
+    add_relabel(m_relabel, J.part, N, J.map);
+    add_copy(s_gather, rd_dev_ptr(r.rd_off), J.ma_out, 2);
     return;
   }
   if (r.stage == Run::kSweep) {
@@ -384,7 +388,7 @@ void Engine::add_run_work(Run& r) {
 static size_t rd_bytes(const Run& r) {
   switch (r.stage) {
     case Run::kMerge:
-      return align256(4 * (size_t)r.B) + align256(8 * (size_t)r.B);
+      return 256;
     case Run::kSweep:
       return sweep_rd_bytes(r.sweep_k);
     case Run::kFinish:
@@ -451,10 +455,6 @@ sbp_status Engine::tick() {
       nb_max = std::max(nb_max, r->o.num_batches);
       k_max = std::max(k_max, r->sweep_k);
     }
-    if (r->relabel) {
-      r->up_map = up;
-      up += align256(4 * r->map.size());
-    }
     if (r->upload_lists) {
       r->up_lists = up;
       up += align256(4 * r->lists_all.size());
@@ -472,17 +472,17 @@ sbp_status Engine::tick() {
   clear_slots();
   for (Run* r : runs) {
     if (r->stage == Run::kDone) continue;
-    if (r->relabel)
-      std::memcpy((char*)up_host + r->up_map, r->map.data(), 4 * r->map.size());
     if (r->upload_lists)
       std::memcpy((char*)up_host + r->up_lists, r->lists_all.data(), 4 * r->lists_all.size());
     add_run_work(*r);
   }
   // pass 3: pack the slots' records and offsets
-  std::vector<Slot*> order = {&s_iota, &s_lists, &s_snap, &s_restore, &s_relabel, &s_zero};
+  std::vector<Slot*> order = {&s_iota, &s_lists, &s_snap, &s_restore, &s_zero};
   for (Slot* x : pre_dense.all()) order.push_back(x);
   for (Slot* x : pre_rebuild.all()) order.push_back(x);
   for (Slot* x : {&m_bt, &m_props, &m_delta}) order.push_back(x);
+  for (Slot* x : m_apply.all()) order.push_back(x);
+  order.push_back(&m_relabel);
   for (int k = 0; k < k_max; ++k) {
     for (int b = 0; b < nb_max; ++b) {
       SweepSlots& w = sw[k * nb_max + b];
@@ -554,7 +554,7 @@ sbp_status Engine::tick() {
   s = emit_until(pre_rebuild.all().back());
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaEventRecord(ev[1], st));
-  s = emit_until(&m_delta);
+  s = emit_until(&m_relabel);
   if (s != SBP_OK) return s;
   SBP_CUDA(cudaEventRecord(ev[2], st));
   // the queued sweeps; timing events are external records so that they
@@ -710,17 +710,15 @@ sbp_status Engine::tick() {
     r->upload_lists = false;
     r->snap_slot = -1;
     r->restore_slot = -1;
-    r->relabel = false;
     r->zero_itr = false;
     if (r->stage == Run::kMerge) {
       Job& J = *r->J;
       r->R.ms_merge += ms_merge;
       r->R.bytes_merge += 320.0 * r->nnz_now + 8.0 * J.N;
-      const int32_t* best = (const int32_t*)rdp;
-      const double* best_dS = (const double*)(rdp + align256(4 * (size_t)r->B));
-      r->map.resize(r->B);
-      const int32_t nb = apply_merges_host(r->B, r->B_to_merge, best, best_dS, r->map.data());
-      if (nb < 0) {
+      int32_t res[2] = {0, 0};
+      std::memcpy(res, rdp, 8);
+      const int32_t nb = res[0];
+      if (res[1] != 0 || nb < 1 || nb > r->B) {
         r->set_error(SBP_ERR_INTERNAL, "merge target out of range (B=" + std::to_string(r->B) +
                                            ", N=" + std::to_string(J.N) + ")");
         continue;
@@ -728,7 +726,6 @@ sbp_status Engine::tick() {
       ++r->seq;
       r->B = nb;
       r->csr_fresh = false;
-      r->relabel = true;
       r->build = true;
       r->zero_itr = true;
       r->itr = 0;

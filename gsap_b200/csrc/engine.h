@@ -58,12 +58,11 @@ struct Run {
   std::vector<double> batch_entries;
   double nnz_now = 0.0;
   // device work left pending by the last host decision
-  bool init = false, upload_lists = false, relabel = false, build = false, zero_itr = false;
+  bool init = false, upload_lists = false, build = false, zero_itr = false;
   bool csr_fresh = false;
   int snap_slot = -1, restore_slot = -1;
-  std::vector<int32_t> map;  // merge map, uploaded for the relabel
   // this tick's offsets in the upload and readback buffers
-  size_t up_map = 0, up_lists = 0, rd_off = 0;
+  size_t up_lists = 0, rd_off = 0;
   cudaEvent_t ev_begin = nullptr;
   // scheduler / server bookkeeping
   double admit_bytes = 0.0;
@@ -123,10 +122,12 @@ class Engine {
   void reset();
 
  private:
-  Slot s_iota, s_lists, s_snap, s_restore, s_relabel, s_zero;
+  Slot s_iota, s_lists, s_snap, s_restore, s_zero;
   DenseBuildSlots pre_dense;
   RebuildSlots pre_rebuild;
   Slot m_bt, m_props, m_delta;
+  MergeApplySlots m_apply;  // merge application on the device (mergeapply.cu)
+  Slot m_relabel;
   std::vector<SweepSlots> sw;     // [queued sweep][batch]
   std::vector<SweepEndSlots> ends;  // [queued sweep]
   Slot s_gather;

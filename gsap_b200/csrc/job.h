@@ -54,6 +54,8 @@ struct Job {
   int32_t* snap[3] = {nullptr, nullptr, nullptr};
   double *rec = nullptr, *mdS = nullptr, *best_dS = nullptr;
   double* mdsin = nullptr;      // merge in-row terms by proposal slot (MergeGrid)
+  MergeApplyBufs ma;            // merge application scratch (mergeapply.cu)
+  int32_t* ma_out = nullptr;    // new block count, target-out-of-range flag
   int32_t* lists = nullptr;     // batch indices by nodal kernel path (classify_batch)
   int32_t* err = nullptr;       // nodal error counter (hash-table overflow)
   int32_t* ctl = nullptr;       // sweep control: sweeps done in the outer step, stop flag

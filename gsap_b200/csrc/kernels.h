@@ -205,6 +205,36 @@ void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32
                      const MergeGrid& grid = MergeGrid());
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map);
 
+// Merge application on the device (mergeapply.cu): the scratch of one job
+// (merge_apply_bytes(N) bytes, carved by merge_apply_carve), the launches of
+// one merge application in order, and the one-shot form.  map[b] receives
+// the new label of block b, out[0] the new block count and out[1] = 1 when a
+// target lay outside [0, B) (out[] must start at zero).
+struct MergeApplyBufs {
+  uint64_t *key = nullptr, *mkA = nullptr, *mkB = nullptr;
+  int32_t *jA = nullptr, *jB = nullptr, *miA = nullptr, *miB = nullptr;
+  uint8_t* onc = nullptr;
+  int32_t *pA = nullptr, *pB = nullptr, *root = nullptr, *newid = nullptr, *tile = nullptr;
+  uint32_t* hist = nullptr;
+  int32_t* sel = nullptr;
+};
+constexpr int kMaRounds = 31, kMaSelPasses = 8;
+struct MergeApplySlots {
+  Slot keys, cyc[kMaRounds], mark, hist[kMaSelPasses], pick[kMaSelPasses], parent,
+      rootj[kMaRounds], scan[3], map;
+  void clear();
+  std::vector<Slot*> all();
+};
+size_t merge_apply_bytes(int32_t N);
+MergeApplyBufs merge_apply_carve(void* base, int32_t N);
+void add_merge_apply(MergeApplySlots& s, const MergeApplyBufs& w, int32_t B, int32_t K,
+                     const int32_t* best, const double* best_dS, int32_t* map, int32_t* out);
+void merge_apply(const MergeApplyBufs& w, int32_t B, int32_t K, const int32_t* best,
+                 const double* best_dS, int32_t* map, int32_t* out, cudaStream_t st);
+// Exclusive scan records (three slots: tile sums, one-CTA scan, apply);
+// out[n] receives the total; tile needs 2 * ceil(n / 2048) + 2 entries.
+void add_exclusive_scan(Slot* sl, const int32_t* in, int32_t* out, int32_t n, int32_t* tile);
+
 // Tuned shape for a device and a blockmodel size class, if known.
 bool rebuild_tuned(int device, int32_t E, int32_t B, RebuildTune* out);
 // Times the candidate shapes on this blockmodel (labels `part` must be in

@@ -5,8 +5,10 @@
 // whole rows per proposal thread (kernels.hpp:143-449, grid sized from nnz,
 // Q16) and reduces with find_best_warp (kernels.hpp:452-491).
 //
-// Here: one thread per proposal draws it (Philox, exact integer picks); one
-// warp per block computes its proposals' dS, walking only the shorter of the
+// Here: one warp per block draws its proposals (Philox, exact integer picks
+// by a running prefix over the row in 32-entry chunks, one ballot per
+// proposal per chunk) and one warp per block computes their dS, walking only
+// the shorter of the
 // two rows being merged and looking the other up by binary search, with the
 // unchanged remainder taken from the per-block sums; lanes 0..np-1 then hold
 // the proposals' dS and run the same 32-lane halving argmin as
@@ -20,6 +22,10 @@
 namespace sbp {
 
 namespace {
+
+constexpr int kMergeWarps = 8;
+
+int32_t vg_merge_delta(int32_t B);
 
 struct MergeArgs {
   const double* xlx;
@@ -53,63 +59,116 @@ __device__ __forceinline__ long long merge_grid_end(const MergeArgs& a) {
   return T < n ? T : n;
 }
 
-// First index k of out-row ++ in-row of block b with running count > t.
-__device__ int pick_serial(const MergeArgs& a, int b, uint64_t t) {
-  uint64_t acc = 0;
-  int o0 = a.optr[b], o1 = a.optr[b + 1];
-  for (int i = o0; i < o1; ++i) {
-    acc += a.ocnt[i];
-    if (acc > t) return i - o0;
-  }
-  int i0 = a.iptr[b], i1 = a.iptr[b + 1];
-  for (int i = i0; i < i1; ++i) {
-    acc += a.icnt[i];
-    if (acc > t) return (o1 - o0) + (i - i0);
-  }
-  return -1;
+// Count and column of entry k of out-row ++ in-row of block b (the scan
+// order of kernels.hpp:767-783).
+__device__ __forceinline__ uint32_t cnt_at(const MergeArgs& a, int b, int k, int no) {
+  return k < no ? __ldg(a.ocnt + a.optr[b] + k) : __ldg(a.icnt + a.iptr[b] + k - no);
 }
-
 __device__ __forceinline__ int col_at(const MergeArgs& a, int b, int k) {
   int o0 = a.optr[b], no = a.optr[b + 1] - o0;
-  return k < no ? a.ocol[o0 + k] : a.icol[a.iptr[b] + k - no];
+  return k < no ? __ldg(a.ocol + o0 + k) : __ldg(a.icol + a.iptr[b] + k - no);
 }
 
-// choose_neighbors + propose_blocks (kernels.hpp:726-856) for one proposal.
-struct MergePropsBody {
-  using Args = MergeArgs;
-  static constexpr int kThreads = 256, kMinBlocks = 1;
-  static constexpr size_t kSmem = 0;
-  static __device__ void run(const Args& a, int vb, int);
-};
+// Inclusive scan of 64-bit values over the warp's lanes.
+__device__ __forceinline__ unsigned long long warp_incl_scan_ull(unsigned long long x, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
 
-__device__ void MergePropsBody::run(const MergeArgs& a, int vb, int) {
-  long long t = (long long)vb * kThreads + threadIdx.x;
-  if (t >= merge_grid_end(a)) return;
-  int r = (int)(t / a.np);
-  P4 x = draw(a.seed, kRngMerge, a.seq, (uint32_t)t);
-  uint32_t B = (uint32_t)a.B;
-  int rnd = (int)(x.v[0] % B);
-  uint64_t deg_r = (uint64_t)a.d_out[r] + a.d_in[r];
-  int s;
-  if (deg_r == 0) {
-    s = rnd;
-  } else {
-    int k = pick_serial(a, r, scale_draw(x.v[1], deg_r));
-    int u = k >= 0 ? col_at(a, r, k) : 0;
-    uint64_t deg_u = (uint64_t)a.d_out[u] + a.d_in[u];
-    if (accept_random(x.v[2], deg_u, B)) {
-      s = rnd;
-    } else {
-      s = 0;
-      int k2 = pick_serial(a, u, scale_draw(x.v[3], deg_u));
-      int n = (a.optr[u + 1] - a.optr[u]) + (a.iptr[u + 1] - a.iptr[u]);
-      for (; k2 >= 0 && k2 < n; ++k2) {
-        int c = col_at(a, u, k2);
-        if (c != r) { s = c; break; }
+// The whole warp walks out-row ++ in-row of block b (warp-uniform) in
+// chunks of 32 entries with a running prefix of the counts.  Each lane L
+// with want set looks for the first entry whose running count exceeds its
+// own threshold t; returns that entry's index in the lane that asked, -1
+// where none does.  The same picks as a serial running sum.
+__device__ int warp_pick(const MergeArgs& a, int b, uint64_t t, bool want, int lane) {
+  const int no = a.optr[b + 1] - a.optr[b];
+  const int n = no + (a.iptr[b + 1] - a.iptr[b]);
+  int found = -1;
+  unsigned open = __ballot_sync(kFull, want);
+  unsigned long long base = 0;
+  for (int c0 = 0; c0 < n && open; c0 += 32) {
+    const int k = c0 + lane;
+    const unsigned long long incl =
+        warp_incl_scan_ull(k < n ? cnt_at(a, b, k, no) : 0u, lane) + base;
+    unsigned rest = open;
+    while (rest) {
+      const int L = __ffs(rest) - 1;
+      rest &= rest - 1;
+      const unsigned long long tL = __shfl_sync(kFull, (unsigned long long)t, L);
+      const unsigned m = __ballot_sync(kFull, k < n && incl > tL);
+      if (m) {
+        if (lane == L) found = c0 + __ffs(m) - 1;
+        open &= ~(1u << L);
       }
     }
+    base = __shfl_sync(kFull, incl, 31);
   }
-  a.props[t] = s;
+  return found;
+}
+
+// choose_neighbors + propose_blocks (kernels.hpp:726-856): one warp per
+// block r draws its np proposals, lane k the k-th.  The first hop picks a
+// neighbour u of r by weight (all lanes in r's row at once); lanes that do
+// not propose a random block then pick in u's row, one walk per lane, and
+// take the first entry from there on whose column is not r (block 0 when
+// none is).
+struct MergePropsBody {
+  using Args = MergeArgs;
+  static constexpr int kThreads = kMergeWarps * 32, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg);
+};
+
+__device__ void MergePropsBody::run(const MergeArgs& a, int vb, int vg) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long T = merge_grid_end(a);
+  const uint32_t B = (uint32_t)a.B;
+  for (int r = vb * kMergeWarps + wid; r < a.B; r += vg * kMergeWarps) {
+    const long long t = (long long)r * a.np + lane;
+    const bool mine = lane < a.np && t < T;  // slots GSAP's grid leaves out keep theirs
+    if (!__any_sync(kFull, mine)) continue;
+    P4 x{};
+    if (mine) x = draw(a.seed, kRngMerge, a.seq, (uint32_t)t);
+    const int rnd = (int)(x.v[0] % B);
+    const uint64_t deg_r = (uint64_t)a.d_out[r] + a.d_in[r];
+    int s = rnd;
+    // first hop: a neighbour u of r in proportion to weight
+    const bool hop = mine && deg_r != 0;
+    const int k = warp_pick(a, r, hop ? scale_draw(x.v[1], deg_r) : 0, hop, lane);
+    int u = 0;
+    bool second = false;
+    uint64_t deg_u = 0;
+    if (hop) {
+      u = k >= 0 ? col_at(a, r, k) : 0;
+      deg_u = (uint64_t)a.d_out[u] + a.d_in[u];
+      second = !accept_random(x.v[2], deg_u, B);
+      if (second) s = 0;
+    }
+    // second hop: each lane that needs it walks its own u's row with the warp
+    unsigned need = __ballot_sync(kFull, second && deg_u > 0);
+    while (need) {
+      const int L = __ffs(need) - 1;
+      need &= need - 1;
+      const int uL = __shfl_sync(kFull, u, L);
+      const uint64_t tL = __shfl_sync(kFull, (unsigned long long)scale_draw(x.v[3], deg_u), L);
+      const int k2 = warp_pick(a, uL, tL, lane == L, lane);
+      if (lane == L && k2 >= 0) {
+        const int n = (a.optr[u + 1] - a.optr[u]) + (a.iptr[u + 1] - a.iptr[u]);
+        for (int q = k2; q < n; ++q) {
+          const int c = col_at(a, u, q);
+          if (c != r) {
+            s = c;
+            break;
+          }
+        }
+      }
+    }
+    if (mine) a.props[t] = s;
+  }
 }
 
 __device__ __forceinline__ double gterm(const double* tab, uint32_t x, double ld) {
@@ -234,8 +293,6 @@ __device__ double merge_one_exact(const MergeArgs& a, int r, int s, int lane) {
   return warp_sum(acc);
 }
 
-constexpr int kMergeWarps = 8;
-
 struct MergeDeltaBody {
   using Args = MergeArgs;
   static constexpr int kThreads = kMergeWarps * 32, kMinBlocks = 1;
@@ -306,6 +363,7 @@ struct RelabelBody {
   }
 };
 
+
 int32_t vg_merge_delta(int32_t B) { return std::min(ceil_div(B, kMergeWarps), 148 * 32); }
 
 const MultiKernel kmMergeProps = multi_kernel_desc<MergePropsBody>("merge_props");
@@ -335,8 +393,7 @@ void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint3
   a.seed = seed;
   a.seq = seq;
   a.props = props;
-  long long n = (long long)B * np;
-  if (n > 0) launch_single<MergePropsBody>(a, ceil_div(n, 256), st);
+  if (B > 0 && np > 0) launch_single<MergePropsBody>(a, vg_merge_delta(B), st);
 }
 
 void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
@@ -362,7 +419,7 @@ void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t se
   a.seed = seed;
   a.seq = seq;
   a.props = props;
-  slot_push(slot_bind(s, kmMergeProps), a, ceil_div((long long)B * np, 256));
+  slot_push(slot_bind(s, kmMergeProps), a, B > 0 && np > 0 ? vg_merge_delta(B) : 0);
 }
 
 void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,

@@ -135,6 +135,8 @@ _sig("sbp_nodal_batch_mode", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_
      C.c_uint32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, _vp, _vp,
      C.POINTER(C.c_double))
 _sig("sbp_apply_merges", C.c_int, C.c_int32, C.c_int32, _vp, _vp, _vp, C.POINTER(C.c_int32))
+_sig("sbp_apply_merges_device", C.c_int, C.c_int32, C.c_int32, _vp, _vp, C.c_int32, _vp,
+     C.POINTER(C.c_int32))
 _sig("sbp_merge_proposals", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_int32, C.c_uint64,
      C.c_uint32, _vp)
 _sig("sbp_nodal_batch", C.c_int, C.POINTER(_GraphCSR), _vp, C.c_int32, C.c_uint64, C.c_uint32,
@@ -181,7 +183,8 @@ EXPORTED = [
     "sbp_mdl_device_static", "sbp_job_bytes", "sbp_partition_batch", "sbp_server_default_options",
     "sbp_server_create", "sbp_server_submit", "sbp_server_poll", "sbp_server_stats_get",
     "sbp_server_destroy", "sbp_delta_mdl_nodal_mode", "sbp_delta_mdl_merge_mode",
-    "sbp_nodal_batch_mode", "sbp_mdl_mode", "sbp_apply_merges",
+    "sbp_nodal_batch_mode", "sbp_mdl_mode", "sbp_apply_merges", "sbp_apply_merges_device",
+    "sbp_merge_step_mode",
 ]
 
 
@@ -502,6 +505,17 @@ def apply_merges(B, B_to_merge, best, best_dS):
     m = np.zeros(max(B, 1), np.int32)
     nb = C.c_int32()
     _check(_lib.sbp_apply_merges(B, B_to_merge, _p(best), _p(best_dS), _p(m), C.byref(nb)))
+    return m[:B], nb.value
+
+
+def apply_merges_device(B, B_to_merge, best, best_dS, device=-1):
+    """carry_out_best_merges on the GPU, as the partition loop runs it."""
+    best = np.ascontiguousarray(best, dtype=np.int32)
+    best_dS = np.ascontiguousarray(best_dS, dtype=np.float64)
+    m = np.zeros(max(B, 1), np.int32)
+    nb = C.c_int32()
+    _check(_lib.sbp_apply_merges_device(B, B_to_merge, _p(best), _p(best_dS), device, _p(m),
+                                        C.byref(nb)))
     return m[:B], nb.value
 
 

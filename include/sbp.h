@@ -309,6 +309,13 @@ sbp_status sbp_nodal_sweeps(const sbp_graph_csr* g, int32_t* part, int32_t B, ui
 sbp_status sbp_apply_merges(int32_t B, int32_t B_to_merge, const int32_t* best,
                             const double* best_dS, int32_t* map, int32_t* B_new);
 
+/* sbp_apply_merges computed on the GPU (`device`, -1 = current) the way
+ * the partition loop applies its merges: the same map and block count
+ * (carry_out_best_merges, partition.hpp:26-78), from host arrays. */
+sbp_status sbp_apply_merges_device(int32_t B, int32_t B_to_merge, const int32_t* best,
+                                   const double* best_dS, int32_t device, int32_t* map,
+                                   int32_t* B_new);
+
 sbp_status sbp_merge_step(const sbp_graph_csr* g, int32_t* part, int32_t B, int32_t B_to_merge,
                           int32_t np, uint64_t seed, uint32_t seq, int32_t* best, double* best_dS,
                           int32_t* B_new);
