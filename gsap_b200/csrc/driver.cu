@@ -622,7 +622,8 @@ static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t se
     grid.dsin = J.mdsin;
   }
   merge_proposals(J.m, B, J.np, seed, seq, J.props, st, grid);
-  merge_delta(J.m, B, J.np, J.props, keep_dS ? J.mdS : nullptr, J.best, J.best_dS, st, 0, grid);
+  merge_delta(J.m, B, J.E, J.np, J.props, keep_dS ? J.mdS : nullptr, J.best, J.best_dS, st, 0,
+              grid);
   SBP_CUDA(cudaMemcpyAsync(J.h_best, J.best, 4 * (size_t)B, cudaMemcpyDeviceToHost, st));
   SBP_CUDA(cudaMemcpyAsync(J.h_best_dS, J.best_dS, 8 * (size_t)B, cudaMemcpyDeviceToHost, st));
   SBP_CUDA(cudaStreamSynchronize(st));
@@ -906,7 +907,7 @@ sbp_status sbp_delta_mdl_merge_mode(const sbp_graph_csr* g, const int32_t* part,
   size_t nt = (size_t)B * np;
   SBP_CUDA(cudaMemcpyAsync(J.props, props, 4 * nt, cudaMemcpyHostToDevice, J.st));
   block_terms(J.m, B, 0, 0, 0, J.st);
-  merge_delta(J.m, B, np, J.props, J.mdS, J.best, J.best_dS, J.st, exact);
+  merge_delta(J.m, B, J.E, np, J.props, J.mdS, J.best, J.best_dS, J.st, exact);
   SBP_CUDA(cudaStreamSynchronize(J.st));
   SBP_CUDA(cudaGetLastError());
   if (dS) SBP_CUDA(cudaMemcpy(dS, J.mdS, 8 * nt, cudaMemcpyDeviceToHost));

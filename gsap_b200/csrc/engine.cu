@@ -306,8 +306,8 @@ void Engine::add_run_work(Run& r) {
     add_block_terms(m_bt, J.m, r.B, 0, r.o.seed, 0);
     const MergeGrid grid = merge_grid(J, r.o);
     add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props, grid);
-    add_merge_delta(m_delta, J.m, r.B, J.np, J.props, nullptr, J.best, J.best_dS, r.o.exact,
-                    grid);
+    add_merge_delta(m_delta, J.m, r.B, J.E, J.np, J.props, nullptr, J.best, J.best_dS,
+                    r.o.exact, grid);
     // carry_out_best_merges on the device, then the relabel: the host reads
     // back only the new block count
     add_zero(s_zero, J.ma_out, 2);

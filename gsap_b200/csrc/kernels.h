@@ -200,9 +200,10 @@ struct MergeGrid {
 
 void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
                      int32_t* props, const MergeGrid& grid = MergeGrid());
-void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
-                     double* dS, int32_t* best, double* best_dS, int32_t exact = 0,
-                     const MergeGrid& grid = MergeGrid());
+// E: the graph's edge count (picks the group width of the dS kernel).
+void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t E, int32_t np,
+                     const int32_t* props, double* dS, int32_t* best, double* best_dS,
+                     int32_t exact = 0, const MergeGrid& grid = MergeGrid());
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map);
 
 // Merge application on the device (mergeapply.cu): the scratch of one job
@@ -321,8 +322,8 @@ void nodal_commit(int32_t* part, int32_t lo, int32_t count, const int32_t* newla
 // (kernels.hpp:143-491).
 void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
                      int32_t* props, cudaStream_t st, const MergeGrid& grid = MergeGrid());
-void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
-                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact = 0,
+void merge_delta(const DevBM& m, int32_t B, int32_t E, int32_t np, const int32_t* props,
+                 double* dS, int32_t* best, double* best_dS, cudaStream_t st, int32_t exact = 0,
                  const MergeGrid& grid = MergeGrid());
 // part[v] = map[part[v]] (update_partitions, kernels.hpp:1728-1740).
 void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st);

@@ -178,12 +178,23 @@ __device__ __forceinline__ double fterm(const double* tab, uint32_t m, double a,
   return m == 0u ? 0.0 : xlx(tab, m) - (double)m * (a + b);
 }
 
-// Merge dS of block r with s (calculate_dS_overall, kernels.hpp:417-449),
-// s2 = the k-th proposal of block s (its in-term leaves out s2, Q1).  With
-// in_s_given, block s's in-term is *in_s_given (a slot GSAP's grid left
-// out); in_r_out receives block r's in-term.
-__device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane,
-                            const double* in_s_given = nullptr, double* in_r_out = nullptr) {
+// Sum over a group of G lanes (G = 8 or 32; every lane of the warp calls it).
+template <int G>
+__device__ __forceinline__ double group_sum(double x) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o, G);
+  return x;
+}
+
+// Merge dS of block r with s (calculate_dS_overall, kernels.hpp:417-449) by
+// a group of G lanes (gl = lane in the group), s2 = the k-th proposal of
+// block s (its in-term leaves out s2, Q1).  With given_in_s, block s's
+// in-term is in_s_given (a slot GSAP's grid left out); in_r_out receives
+// block r's in-term.  An inactive group walks nothing but still takes part
+// in the group sums (every lane of the warp must).
+template <int G>
+__device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int gl, bool active,
+                            bool given_in_s, double in_s_given, double* in_r_out) {
   // merged out-rows (calculate_dS_new_out, kernels.hpp:233-320)
   double acc_o = 0.0, acc_i = 0.0;
   const double ldo_r = a.ld_out[r], ldo_s = a.ld_out[s], ldi_r = a.ld_in[r], ldi_s = a.ld_in[s];
@@ -191,10 +202,11 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane,
   const uint32_t Mrs = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], s);
   const uint32_t Msr = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], r);
   const uint32_t Mss = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], s);
-  if (r == s) {
-    for (int i = a.optr[r] + lane; i < a.optr[r + 1]; i += 32)
+  if (!active) {
+  } else if (r == s) {
+    for (int i = a.optr[r] + gl; i < a.optr[r + 1]; i += G)
       acc_o += gterm(a.xlx, 2u * a.ocnt[i], a.ld_in[a.ocol[i]]);
-    for (int i = a.iptr[r] + lane; i < a.iptr[r + 1]; i += 32) {
+    for (int i = a.iptr[r] + gl; i < a.iptr[r + 1]; i += G) {
       int c = a.icol[i];
       if (c != r) acc_i += gterm(a.xlx, 2u * a.icnt[i], a.ld_out[c]);
     }
@@ -202,32 +214,32 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane,
     int x = r, y = s;
     if (a.optr[s + 1] - a.optr[s] < a.optr[r + 1] - a.optr[r]) { x = s; y = r; }
     int y0 = a.optr[y], y1 = a.optr[y + 1];
-    for (int i = a.optr[x] + lane; i < a.optr[x + 1]; i += 32) {
+    for (int i = a.optr[x] + gl; i < a.optr[x + 1]; i += G) {
       int c = a.ocol[i];
       double ld = a.ld_in[c];
       uint32_t my = row_lookup(a.ocol, a.ocnt, y0, y1, c);
       acc_o += gterm(a.xlx, a.ocnt[i] + my, ld) - gterm(a.xlx, my, ld);
     }
-    if (lane == 0) acc_o += a.ambout[y];
+    if (gl == 0) acc_o += a.ambout[y];
     x = r; y = s;
     if (a.iptr[s + 1] - a.iptr[s] < a.iptr[r + 1] - a.iptr[r]) { x = s; y = r; }
     y0 = a.iptr[y]; y1 = a.iptr[y + 1];
-    for (int i = a.iptr[x] + lane; i < a.iptr[x + 1]; i += 32) {
+    for (int i = a.iptr[x] + gl; i < a.iptr[x + 1]; i += G) {
       int c = a.icol[i];
       if (c == r || c == s) continue;
       double ld = a.ld_out[c];
       uint32_t my = row_lookup(a.icol, a.icnt, y0, y1, c);
       acc_i += gterm(a.xlx, a.icnt[i] + my, ld) - gterm(a.xlx, my, ld);
     }
-    if (lane == 0) {
+    if (gl == 0) {
       // in-row y's own terms at columns r and s stay out
       uint32_t yr = y == r ? Mrr : Mrs;  // M[r][y]
       uint32_t ys = y == r ? Msr : Mss;  // M[s][y]
       acc_i += a.ambin[y] - gterm(a.xlx, yr, ldo_r) - gterm(a.xlx, ys, ldo_s);
     }
   }
-  acc_o = warp_sum(acc_o);
-  acc_i = warp_sum(acc_i);
+  acc_o = group_sum<G>(acc_o);
+  acc_i = group_sum<G>(acc_i);
   const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
   long long mass_o = (long long)dor + (long long)dos;
   long long mass_i = r == s ? 2LL * ((long long)dir - (long long)Mrr)
@@ -241,13 +253,13 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane,
   // row s without s, s2
   double in_r = a.sinfull[r] - fterm(a.xlx, Mrr, ldo_r, ldi_r) - (s != r ? fterm(a.xlx, Msr, ldo_s, ldi_r) : 0.0);
   double in_s;
-  if (in_s_given) {
-    in_s = *in_s_given;
+  if (given_in_s) {
+    in_s = in_s_given;
   } else {
     uint32_t Ms2s = s2 == s ? 0u : row_lookup(a.ocol, a.ocnt, a.optr[s2], a.optr[s2 + 1], s);
     in_s = a.sinfull[s] - fterm(a.xlx, Mss, ldo_s, ldi_s) - fterm(a.xlx, Ms2s, a.ld_out[s2], ldi_s);
   }
-  if (in_r_out) *in_r_out = in_r;
+  *in_r_out = in_r;
   return a.dSout[r] + a.dSout[s] + in_r + in_s + new_out + new_in;
 }
 
@@ -255,80 +267,96 @@ __device__ double merge_one(const MergeArgs& a, int r, int s, int s2, int lane,
 // into row s, columns r and s into column s.  Of the sum of M log2 M only
 // the cells present in both rows (both columns) and the four corner cells,
 // which become one, change; of the degree terms the two rows' and the two
-// columns'.  dS = -(change of data_S), B fixed.  Warp-cooperative: the
+// columns'.  dS = -(change of data_S), B fixed.  Group-cooperative: the
 // shorter row is walked, the longer one searched.
-__device__ double merge_one_exact(const MergeArgs& a, int r, int s, int lane) {
-  if (r == s) return 0.0;
+template <int G>
+__device__ double merge_one_exact(const MergeArgs& a, int r, int s, int gl, bool active) {
+  active = active && r != s;
   double acc = 0.0;  // - (change of the off-corner cells)
-  int x = r, y = s;
-  if (a.optr[s + 1] - a.optr[s] < a.optr[r + 1] - a.optr[r]) { x = s; y = r; }
-  int y0 = a.optr[y], y1 = a.optr[y + 1];
-  for (int i = a.optr[x] + lane; i < a.optr[x + 1]; i += 32) {
-    const int c = a.ocol[i];
-    if (c == r || c == s) continue;
-    const uint32_t b = row_lookup(a.ocol, a.ocnt, y0, y1, c);
-    if (b) acc -= xlx(a.xlx, a.ocnt[i] + b) - xlx(a.xlx, a.ocnt[i]) - xlx(a.xlx, b);
+  if (active) {
+    int x = r, y = s;
+    if (a.optr[s + 1] - a.optr[s] < a.optr[r + 1] - a.optr[r]) { x = s; y = r; }
+    int y0 = a.optr[y], y1 = a.optr[y + 1];
+    for (int i = a.optr[x] + gl; i < a.optr[x + 1]; i += G) {
+      const int c = a.ocol[i];
+      if (c == r || c == s) continue;
+      const uint32_t b = row_lookup(a.ocol, a.ocnt, y0, y1, c);
+      if (b) acc -= xlx(a.xlx, a.ocnt[i] + b) - xlx(a.xlx, a.ocnt[i]) - xlx(a.xlx, b);
+    }
+    x = r; y = s;
+    if (a.iptr[s + 1] - a.iptr[s] < a.iptr[r + 1] - a.iptr[r]) { x = s; y = r; }
+    y0 = a.iptr[y]; y1 = a.iptr[y + 1];
+    for (int i = a.iptr[x] + gl; i < a.iptr[x + 1]; i += G) {
+      const int c = a.icol[i];
+      if (c == r || c == s) continue;
+      const uint32_t b = row_lookup(a.icol, a.icnt, y0, y1, c);
+      if (b) acc -= xlx(a.xlx, a.icnt[i] + b) - xlx(a.xlx, a.icnt[i]) - xlx(a.xlx, b);
+    }
+    if (gl == 0) {
+      const uint32_t Mrr = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], r);
+      const uint32_t Mrs = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], s);
+      const uint32_t Msr = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], r);
+      const uint32_t Mss = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], s);
+      const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
+      const double corner = xlx(a.xlx, Mrr + Mrs + Msr + Mss) - xlx(a.xlx, Mrr) -
+                            xlx(a.xlx, Mrs) - xlx(a.xlx, Msr) - xlx(a.xlx, Mss);
+      const double degs = xlx(a.xlx, dor + dos) - xlx(a.xlx, dor) - xlx(a.xlx, dos) +
+                          xlx(a.xlx, dir + dis) - xlx(a.xlx, dir) - xlx(a.xlx, dis);
+      acc += degs - corner;
+    }
   }
-  x = r; y = s;
-  if (a.iptr[s + 1] - a.iptr[s] < a.iptr[r + 1] - a.iptr[r]) { x = s; y = r; }
-  y0 = a.iptr[y]; y1 = a.iptr[y + 1];
-  for (int i = a.iptr[x] + lane; i < a.iptr[x + 1]; i += 32) {
-    const int c = a.icol[i];
-    if (c == r || c == s) continue;
-    const uint32_t b = row_lookup(a.icol, a.icnt, y0, y1, c);
-    if (b) acc -= xlx(a.xlx, a.icnt[i] + b) - xlx(a.xlx, a.icnt[i]) - xlx(a.xlx, b);
-  }
-  if (lane == 0) {
-    const uint32_t Mrr = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], r);
-    const uint32_t Mrs = row_lookup(a.ocol, a.ocnt, a.optr[r], a.optr[r + 1], s);
-    const uint32_t Msr = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], r);
-    const uint32_t Mss = row_lookup(a.ocol, a.ocnt, a.optr[s], a.optr[s + 1], s);
-    const uint32_t dor = a.d_out[r], dos = a.d_out[s], dir = a.d_in[r], dis = a.d_in[s];
-    const double corner = xlx(a.xlx, Mrr + Mrs + Msr + Mss) - xlx(a.xlx, Mrr) -
-                          xlx(a.xlx, Mrs) - xlx(a.xlx, Msr) - xlx(a.xlx, Mss);
-    const double degs = xlx(a.xlx, dor + dos) - xlx(a.xlx, dor) - xlx(a.xlx, dos) +
-                        xlx(a.xlx, dir + dis) - xlx(a.xlx, dir) - xlx(a.xlx, dis);
-    acc += degs - corner;
-  }
-  return warp_sum(acc);
+  return group_sum<G>(acc);
 }
 
+// One warp per block r: groups of G lanes score the block's proposals, 32/G
+// at a time (G = 8 when the blockmodel's rows are short, as at large B;
+// else 32, the whole warp on one proposal); lanes 0..np-1 then hold the
+// proposals' dS and run find_best_warp's 32-lane halving argmin
+// (kernels.hpp:452-491), ties going to the lane further up.
+template <int G>
 struct MergeDeltaBody {
   using Args = MergeArgs;
   static constexpr int kThreads = kMergeWarps * 32, kMinBlocks = 1;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
+  constexpr int NG = 32 / G;  // groups per warp
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int g = lane / G, gl = lane % G;
   const long long T = merge_grid_end(a);
   for (int r = vb * kMergeWarps + wid; r < a.B; r += vg * kMergeWarps) {
     double mine = DBL_MAX;
     int who = 0;
-    for (int k = 0; k < a.np; ++k) {
-      const long long t = (long long)r * a.np + k;
-      int s = a.props_in[t];
-      double d;
-      if (t >= T) {
-        d = a.keep_dS[t];  // a slot GSAP's grid leaves out keeps its old values
-      } else if (a.exact) {
-        d = merge_one_exact(a, r, s, lane);
+    for (int k0 = 0; k0 < a.np; k0 += NG) {
+      const int k = k0 + g;
+      const bool act = k < a.np;
+      const long long t = (long long)r * a.np + (act ? k : 0);
+      const int s = act ? a.props_in[t] : r;
+      const bool stale = act && t >= T;  // a slot GSAP's grid leaves out keeps its values
+      const bool comp = act && !stale;
+      double d, in_r = 0.0;
+      if (a.exact) {
+        d = merge_one_exact<G>(a, r, s, gl, comp);
       } else {
-        const long long sid = (long long)s * a.np + k;
-        double in_r = 0.0;
-        if (sid >= T) {
-          d = merge_one(a, r, s, 0, lane, a.keep_dsin + sid, &in_r);
-        } else {
-          int s2 = a.props_in[sid];
-          d = merge_one(a, r, s, s2, lane, nullptr, &in_r);
-        }
-        if (a.ref_grid && lane == 0) a.keep_dsin[t] = in_r;
+        const long long sid = (long long)s * a.np + (act ? k : 0);
+        const bool given = comp && sid >= T;
+        const int s2 = comp && !given ? a.props_in[sid] : s;
+        d = merge_one<G>(a, r, s, s2, gl, comp, given, given ? a.keep_dsin[sid] : 0.0, &in_r);
       }
-      if (lane == k) {
-        mine = d;
-        who = s;
-      }
-      if (lane == 0 && t < T) {
+      if (stale) d = a.keep_dS[t];
+      if (comp && gl == 0) {
         if (a.dS) a.dS[t] = d;
-        if (a.ref_grid) a.keep_dS[t] = d;
+        if (a.ref_grid) {
+          a.keep_dS[t] = d;
+          if (!a.exact) a.keep_dsin[t] = in_r;
+        }
+      }
+      // proposal k0 + j's dS and target from group j's first lane
+      const int j = (lane - k0) & (NG - 1);
+      const double dj = __shfl_sync(kFull, d, j * G);
+      const int sj = __shfl_sync(kFull, s, j * G);
+      if (lane >= k0 && lane < k0 + NG && lane < a.np) {
+        mine = dj;
+        who = sj;
       }
     }
     // find_best_warp's reduction
@@ -367,7 +395,12 @@ struct RelabelBody {
 int32_t vg_merge_delta(int32_t B) { return std::min(ceil_div(B, kMergeWarps), 148 * 32); }
 
 const MultiKernel kmMergeProps = multi_kernel_desc<MergePropsBody>("merge_props");
-const MultiKernel kmMergeDelta = multi_kernel_desc<MergeDeltaBody>("merge_delta");
+// Groups of 8 lanes score a proposal when rows are short: at most 16
+// entries a row on average (nnz <= E).  A function of the job's sizes only.
+bool short_rows(int32_t B, int32_t E) { return (long long)E <= 16LL * B; }
+
+const MultiKernel kmMergeDelta = multi_kernel_desc<MergeDeltaBody<32>>("merge_delta");
+const MultiKernel kmMergeDelta8 = multi_kernel_desc<MergeDeltaBody<8>>("merge_delta_g8");
 const MultiKernel kmRelabel = multi_kernel_desc<RelabelBody>("relabel");
 
 MergeArgs make_args(const DevBM& m, int32_t B, int32_t np, const MergeGrid& grid) {
@@ -396,8 +429,8 @@ void merge_proposals(const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint3
   if (B > 0 && np > 0) launch_single<MergePropsBody>(a, vg_merge_delta(B), st);
 }
 
-void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, double* dS,
-                 int32_t* best, double* best_dS, cudaStream_t st, int32_t exact,
+void merge_delta(const DevBM& m, int32_t B, int32_t E, int32_t np, const int32_t* props,
+                 double* dS, int32_t* best, double* best_dS, cudaStream_t st, int32_t exact,
                  const MergeGrid& grid) {
   MergeArgs a = make_args(m, B, np, grid);
   a.exact = exact;
@@ -405,7 +438,9 @@ void merge_delta(const DevBM& m, int32_t B, int32_t np, const int32_t* props, do
   a.dS = dS;
   a.best = best;
   a.best_dS = best_dS;
-  if (B > 0) launch_single<MergeDeltaBody>(a, vg_merge_delta(B), st);
+  if (B <= 0) return;
+  if (short_rows(B, E)) launch_single<MergeDeltaBody<8>>(a, vg_merge_delta(B), st);
+  else launch_single<MergeDeltaBody<32>>(a, vg_merge_delta(B), st);
 }
 
 void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st) {
@@ -422,16 +457,17 @@ void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t se
   slot_push(slot_bind(s, kmMergeProps), a, B > 0 && np > 0 ? vg_merge_delta(B) : 0);
 }
 
-void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t np, const int32_t* props,
-                     double* dS, int32_t* best, double* best_dS, int32_t exact,
-                     const MergeGrid& grid) {
+void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t E, int32_t np,
+                     const int32_t* props, double* dS, int32_t* best, double* best_dS,
+                     int32_t exact, const MergeGrid& grid) {
   MergeArgs a = make_args(m, B, np, grid);
   a.exact = exact;
   a.props_in = props;
   a.dS = dS;
   a.best = best;
   a.best_dS = best_dS;
-  slot_push(slot_bind(s, kmMergeDelta), a, B > 0 ? vg_merge_delta(B) : 0);
+  slot_push(slot_bind(s, short_rows(B, E) ? kmMergeDelta8 : kmMergeDelta), a,
+            B > 0 ? vg_merge_delta(B) : 0);
 }
 
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map) {
