@@ -11,6 +11,7 @@ GSAP seeds its RNG from clock64(), so each entry is one draw from its
 run-to-run distribution.  Needs a GPU:
 
     python tests/golden/make_quality.py --out quality_ref.json [--big-runs 2]
+    python tests/golden/make_quality.py --out quality_ref.json --only-big --append --big-runs 5
 """
 import argparse
 import json
@@ -50,7 +51,9 @@ def score(g, lab):
     B = int(lab.max()) + 1
     S, _ = sbp.mdl(g, lab, B)
     rec, prec, nmi = sbp.evaluate(g.true_partitions, lab)
-    return {"B": B, "S": S, "recall": rec, "precision": prec, "nmi": nmi}
+    sizes = np.bincount(lab, minlength=B)
+    return {"B": B, "S": S, "recall": rec, "precision": prec, "nmi": nmi,
+            "largest_block": int(sizes.max()), "block0": int(sizes[0])}
 
 
 def main():
@@ -59,11 +62,17 @@ def main():
     ap.add_argument("--seeds", type=int, default=5)
     ap.add_argument("--big-runs", type=int, default=2)
     ap.add_argument("--timeout", type=float, default=600.0)
+    ap.add_argument("--only-big", action="store_true", help="skip the 20k configs")
+    ap.add_argument("--append", action="store_true",
+                    help="add the new runs to the runs already in --out")
     a = ap.parse_args()
     out = {"generator": "sbp.dcsbm_variant(variant, N, B, seed); GSAP partition(g) via "
                         "oracle/_ref/gsap_ref; MDL and P/R computed on its final labels",
            "runs": []}
-    for v in VARIANTS:
+    if a.append and os.path.exists(a.out):
+        out = json.load(open(a.out))
+    big0 = sum(1 for r in out["runs"] if r["config"] == "200k")
+    for v in (() if a.only_big else VARIANTS):
         for s in range(a.seeds):
             g = sbp.dcsbm_variant(v, 20000, 32, seed=s)
             lab, ms, wall = gsap_run(g, a.timeout)
@@ -74,7 +83,8 @@ def main():
     g = sbp.dcsbm_variant("HH", 200000, 71, seed=0)
     for i in range(a.big_runs):
         lab, ms, wall = gsap_run(g, a.timeout)
-        row = {"config": "200k", "variant": "HH", "graph_seed": 0, "run": i, "N": g.N, "E": g.E,
+        row = {"config": "200k", "variant": "HH", "graph_seed": 0, "run": big0 + i, "N": g.N,
+               "E": g.E,
                "ms": ms, "wall_ms": wall, **score(g, lab)}
         out["runs"].append(row)
         print(json.dumps(row), flush=True)
