@@ -8,6 +8,8 @@
 #   oracle/_ref/ref_host           GSAP/load.hpp + GSAP/evaluate (goldens)
 #   oracle/_ref/gsap_ref           the unmodified GSAP GPU path (sm_100a)
 #                                  driven by oracle/gsap_ref_main.cu
+#   oracle/_ref/gsap_csr           GSAP's blockmodel builder (calculate_new_csr)
+#                                  on given partitions, oracle/gsap_csr_main.cu
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REF="${REF:-/root/reference}"
@@ -49,6 +51,13 @@ if [ "${SKIP_GSAP_GPU:-0}" != "1" ] && command -v "$NVCC" >/dev/null 2>&1; then
     "$NVCC" -std=c++17 -O3 -use_fast_math --expt-relaxed-constexpr --extended-lambda -w \
       -gencode arch=compute_100a,code=sm_100a \
       -I"$REF/GSAP" -I"$REF" "$HERE/gsap_ref_main.cu" -o "$OUT/gsap_ref"
+  fi
+fi
+if [ "${SKIP_GSAP_GPU:-0}" != "1" ] && command -v "$NVCC" >/dev/null 2>&1; then
+  if build_if_stale "$OUT/gsap_csr" "$HERE/gsap_csr_main.cu"; then
+    "$NVCC" -std=c++17 -O3 -use_fast_math --expt-relaxed-constexpr --extended-lambda -w \
+      -gencode arch=compute_100a,code=sm_100a \
+      -I"$REF/GSAP" -I"$REF" "$HERE/gsap_csr_main.cu" -o "$OUT/gsap_csr"
   fi
 fi
 echo "oracle/_ref ready"
