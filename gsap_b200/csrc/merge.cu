@@ -457,7 +457,7 @@ void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t se
   slot_push(slot_bind(s, kmMergeProps), a, B > 0 && np > 0 ? vg_merge_delta(B) : 0);
 }
 
-void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t E, int32_t np,
+void add_merge_delta(Slot& s32, Slot& s8, const DevBM& m, int32_t B, int32_t E, int32_t np,
                      const int32_t* props, double* dS, int32_t* best, double* best_dS,
                      int32_t exact, const MergeGrid& grid) {
   MergeArgs a = make_args(m, B, np, grid);
@@ -466,8 +466,8 @@ void add_merge_delta(Slot& s, const DevBM& m, int32_t B, int32_t E, int32_t np,
   a.dS = dS;
   a.best = best;
   a.best_dS = best_dS;
-  slot_push(slot_bind(s, short_rows(B, E) ? kmMergeDelta8 : kmMergeDelta), a,
-            B > 0 ? vg_merge_delta(B) : 0);
+  if (short_rows(B, E)) slot_push(slot_bind(s8, kmMergeDelta8), a, B > 0 ? vg_merge_delta(B) : 0);
+  else slot_push(slot_bind(s32, kmMergeDelta), a, B > 0 ? vg_merge_delta(B) : 0);
 }
 
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map) {
