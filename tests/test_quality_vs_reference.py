@@ -3,9 +3,16 @@
 tests/golden/quality_ref.json holds GSAP's results (final B, MDL of its
 labels, pairwise recall and precision against the planted labels) on the
 plain configs, written by tests/golden/make_quality.py on a B200.  Our
-partitions of the same graphs, with partition seed = graph seed, must score
-an MDL within 1% of GSAP's and recall / precision within 0.02 of GSAP's,
-each averaged over the config's runs."""
+partitions of the same graphs must score an MDL within 1% of GSAP's and
+pairwise recall / precision within 0.02 of GSAP's.
+
+20k configs: partition seed = graph seed, five graph seeds, means against
+means.  200k HH: five partition seeds of the benchmark graph against every
+GSAP run on record (at least five; GSAP seeds its RNG from clock64(), so
+each run is a fresh draw).  There GSAP's recall has a heavy tail (one draw
+in eight ended with one block holding most vertices, recall 0.61, against
+0.011-0.028 for the others), so the bar compares our mean with GSAP's
+median of each score; the MDL bar also holds against GSAP's mean."""
 import json
 import os
 
@@ -52,5 +59,12 @@ def test_20k_quality_matches_gsap(sbp, variant):
 
 def test_200k_quality_matches_gsap(sbp):
     ref = _ref("200k", "HH")
-    assert len(ref) >= 1
-    _check(_ours(sbp, "HH", 200000, 71, [0, 0], [0, 1]), ref)
+    assert len(ref) >= 5
+    ours = _ours(sbp, "HH", 200000, 71, [0] * 5, [0, 1, 2, 3, 4])
+    S, rec, prec = ours.mean(axis=0)
+    med = {k: float(np.median([r[k] for r in ref])) for k in ("S", "recall", "precision")}
+    mean = {k: float(np.mean([r[k] for r in ref])) for k in ("S", "recall", "precision")}
+    assert abs(S - med["S"]) <= 0.01 * med["S"], (S, med, mean)
+    assert abs(rec - med["recall"]) <= 0.02, (rec, med, mean)
+    assert abs(prec - med["precision"]) <= 0.02, (prec, med, mean)
+    assert abs(S - mean["S"]) <= 0.01 * mean["S"], (S, mean)
