@@ -70,8 +70,14 @@ def test_nodal_batch_at_configs(sbp, orc, cfg):
         pb, db, xb, tb = orc.nodal_batch(g, p, B, 21, 100, 0, BS)
         assert np.array_equal(xa, xb), (name, "proposals differ")
         ok = close(da, db)
-        assert ok.all(), (name, np.flatnonzero(~ok)[:5])
-        assert np.array_equal(pa, pb), (name, "accepted moves differ")
+        bad = np.flatnonzero(~ok)
+        assert ok.all(), (name, bad[:5], da[bad[:5]], db[bad[:5]], p[bad[:5]], xb[bad[:5]])
+        # a move whose dS is zero in exact arithmetic may land on either side
+        # of zero after rounding; every other decision must agree
+        diff = np.flatnonzero(pa != pb)
+        if diff.size:
+            raw, _ = orc.nodal_delta(g, p, B, diff.astype(np.int32), xb[diff])
+            assert (np.abs(raw) <= REL).all(), (name, diff[:5], raw[:5])
         assert abs(ta - tb) <= REL * max(abs(tb), 1.0), name
         if name == "first-merge":
             assert (db < 0).sum() > 0  # the batch does move vertices
