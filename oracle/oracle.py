@@ -60,7 +60,7 @@ _GP = C.POINTER(_G)
 _sig("orc_philox", None, _vp, _vp, _vp)
 _sig("orc_build_blockmodel", C.c_int64, _GP, _vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
      _vp)
-_sig("orc_nodal_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
+_sig("orc_nodal_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp)
 _sig("orc_merge_delta", None, _GP, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp)
 _sig("orc_mdl", C.c_double, _GP, _vp, C.c_int32, C.POINTER(C.c_double))
 _sig("orc_mdl_mode", C.c_double, _GP, _vp, C.c_int32, C.c_int32, C.POINTER(C.c_double))
@@ -122,8 +122,21 @@ def nodal_delta(g, part, B, verts, props):
     dS = np.zeros(max(verts.size, 1))
     q3 = np.zeros(max(verts.size, 1), np.uint8)
     _lib.orc_nodal_delta(C.byref(_g(g)), _p(part), B, verts.size, _p(verts), _p(props), _p(dS),
-                         _p(q3))
+                         _p(q3), None)
     return dS[:verts.size], q3[:verts.size].astype(bool)
+
+
+def nodal_delta_scale(g, part, B, verts, props):
+    """GSAP's dS of the moves and the sum of the magnitudes of the eight row
+    sums each is the difference of (FP64 rounding grows with them)."""
+    part = np.ascontiguousarray(part, dtype=np.int32)
+    verts = np.ascontiguousarray(verts, dtype=np.int32)
+    props = np.ascontiguousarray(props, dtype=np.int32)
+    n = max(verts.size, 1)
+    dS, q3, mag = np.zeros(n), np.zeros(n, np.uint8), np.zeros(n)
+    _lib.orc_nodal_delta(C.byref(_g(g)), _p(part), B, verts.size, _p(verts), _p(props), _p(dS),
+                         _p(q3), _p(mag))
+    return dS[:verts.size], mag[:verts.size]
 
 
 def nodal_delta_exact(g, part, B, verts, props):

@@ -552,21 +552,34 @@ double new_s_in(const BM& m, const std::vector<Entry>& L, int32_t r, int32_t s, 
 }
 
 // kernels.hpp:600-643 (calculate_dS_overall_nodal): dS of moving v from r to s.
+// `mag` (optional) receives the sum of the magnitudes of the eight row sums
+// the value is the difference of: its FP64 rounding error grows with them.
 double nodal_delta(const Graph& g, const BM& m, const double* dS_out, const int32_t* part,
-                   int32_t v, int32_t s, bool* q3) {
+                   int32_t v, int32_t s, bool* q3, double* mag = nullptr) {
   int32_t r = part[v];
+  if (mag) *mag = 0.0;
   if (r == s) return 0.0;
   std::vector<Entry> Lo = nbr_blocks(g.out_ptr, g.out_idx, g.out_w, part, v);
   std::vector<Entry> Li = nbr_blocks(g.in_ptr, g.in_idx, g.in_w, part, v);
   uint32_t ni_r = weight_from_block(Li, r);
   uint32_t ni_s = weight_from_block(Li, s);
+  const double t[8] = {dS_out[r],
+                       dS_out[s],
+                       dS_in_block_excl(m, r, r, s),
+                       dS_in_block_excl(m, s, r, s),
+                       new_r_out(m, Lo, r, s, g.deg_out[v], ni_r),
+                       new_s_out(m, Lo, r, s, g.deg_out[v], ni_s),
+                       new_r_in(m, Li, r, s, g.deg_in[v]),
+                       new_s_in(m, Li, r, s, g.deg_in[v], q3)};
   double d = 0.0;
-  d += dS_out[r] + dS_out[s];
-  d += dS_in_block_excl(m, r, r, s) + dS_in_block_excl(m, s, r, s);
-  d -= new_r_out(m, Lo, r, s, g.deg_out[v], ni_r);
-  d -= new_s_out(m, Lo, r, s, g.deg_out[v], ni_s);
-  d -= new_r_in(m, Li, r, s, g.deg_in[v]);
-  d -= new_s_in(m, Li, r, s, g.deg_in[v], q3);
+  d += t[0] + t[1];
+  d += t[2] + t[3];
+  d -= t[4];
+  d -= t[5];
+  d -= t[6];
+  d -= t[7];
+  if (mag)
+    for (double x : t) *mag += std::fabs(x);
   return d;
 }
 
@@ -1234,14 +1247,15 @@ int64_t orc_build_blockmodel(const orc_graph* xg, const int32_t* part, int32_t B
 
 // dS of moving verts[i] to props[i], every move judged against `part`.
 void orc_nodal_delta(const orc_graph* xg, const int32_t* part, int32_t B, int32_t nv,
-                     const int32_t* verts, const int32_t* props, double* dS, uint8_t* q3_hit) {
+                     const int32_t* verts, const int32_t* props, double* dS, uint8_t* q3_hit,
+                     double* mag) {
   Graph g = to_graph(xg);
   BM m = build_bm(g, part, B);
   std::vector<double> dso(B);
   for (int32_t b = 0; b < B; ++b) dso[b] = dS_out_block(m, b);
   for (int32_t i = 0; i < nv; ++i) {
     bool q3 = false;
-    dS[i] = nodal_delta(g, m, dso.data(), part, verts[i], props[i], &q3);
+    dS[i] = nodal_delta(g, m, dso.data(), part, verts[i], props[i], &q3, mag ? mag + i : nullptr);
     if (q3_hit) q3_hit[i] = q3 ? 1 : 0;
   }
 }

@@ -7,7 +7,11 @@ alone, B = N; after GSAP's first merge step, B = 0.65 N; the planted
 blocks):
   * the blockmodel is bit-exact;
   * one nodal batch (the first quarter of the vertices) draws the same
-    proposals, accepts the same moves and records dS within 1e-9;
+    proposals, accepts the same moves and records dS within 1e-9, relative
+    to the value or, for moves of the giant block GSAP's first merge step
+    makes, to the magnitude of the row sums the oracle's value is the
+    difference of (1e-12 of it: the FP64 rounding of those sums; the GPU's
+    formulation does not subtract them);
   * one merge step gives the same best dS per block within 1e-9 and, where
     the two rankings agree, the same labels.
 The first merge step reproduces GSAP's merge grid (the proposal slots past
@@ -69,7 +73,8 @@ def test_nodal_batch_at_configs(sbp, orc, cfg):
         pa, da, xa, ta = sbp.nodal_batch(g, p, B, 21, 100, 0, BS)
         pb, db, xb, tb = orc.nodal_batch(g, p, B, 21, 100, 0, BS)
         assert np.array_equal(xa, xb), (name, "proposals differ")
-        ok = close(da, db)
+        _, mag = orc.nodal_delta_scale(g, p, B, np.arange(BS, dtype=np.int32), xb)
+        ok = close(da, db) | (np.abs(da - db) <= 1e-12 * mag)
         bad = np.flatnonzero(~ok)
         assert ok.all(), (name, bad[:5], da[bad[:5]], db[bad[:5]], p[bad[:5]], xb[bad[:5]])
         # a move whose dS is zero in exact arithmetic may land on either side
