@@ -343,6 +343,7 @@ struct RbRowsSmallBody {
 constexpr int kBigThreads = 512;
 constexpr int kHistCap = 16384;  // columns counted in shared memory at once
 constexpr int kSortCap = 8192;   // longest segment sorted in shared memory
+constexpr int kMaxWindows = 256; // column windows a long segment is bucketed into
 constexpr size_t kBigSmem = 65536;
 
 struct RbRowsBigBody {
@@ -354,6 +355,7 @@ struct RbRowsBigBody {
   extern __shared__ unsigned long long big_sm[];
   __shared__ int sh[33];
   __shared__ uint32_t touched[kHistCap / 32];  // bitmap of the histogram's nonzero columns
+  __shared__ int wstart[kMaxWindows + 1];      // a long segment's entries by column window
   const RbSide& d = a.s[vb & 1];
   vb >>= 1;
   vg >>= 1;
@@ -402,6 +404,70 @@ struct RbRowsBigBody {
       }
       running = tot;
       __syncthreads();
+    } else if (n > kSortCap && (a.B + kHistCap - 1) / kHistCap <= kMaxWindows) {
+      // Long segment, many columns: bucket the entries by column window of
+      // kHistCap (a counting sort into the segment's own output range), then
+      // one histogram pass per window over that window's entries only, with
+      // the touched-column bitmap.  Window w's results start at or before
+      // its bucket (every result consumes an entry of an earlier or the
+      // same window) and end at or before the next bucket, and are written
+      // after the window's entries are read: the range serves as both.
+      const int W = (a.B + kHistCap - 1) / kHistCap;
+      uint32_t* cursor = hist;  // W counters, before the histogram use
+      for (int i = tid; i < W; i += T) cursor[i] = 0u;
+      __syncthreads();
+      for (int i = tid; i < n; i += T) atomicAdd(cursor + d.tcol[base + i] / kHistCap, 1u);
+      __syncthreads();
+      if (tid == 0) {
+        int acc = 0;
+        for (int w = 0; w < W; ++w) {
+          wstart[w] = acc;
+          acc += (int)cursor[w];
+          cursor[w] = (uint32_t)wstart[w];
+        }
+        wstart[W] = acc;
+      }
+      __syncthreads();
+      for (int i = tid; i < n; i += T) {
+        const int c = d.tcol[base + i];
+        const int at = (int)atomicAdd(cursor + c / kHistCap, 1u);
+        d.ucol[base + at] = c;
+        d.uw[base + at] = d.tw[base + i];
+      }
+      __syncthreads();
+      for (int i = tid; i < kHistCap; i += T) hist[i] = 0u;
+      for (int i = tid; i < kHistCap / 32; i += T) touched[i] = 0u;
+      __syncthreads();
+      for (int w = 0; w < W; ++w) {
+        const int w0 = w * kHistCap, e0 = wstart[w], e1 = wstart[w + 1];
+        const int nwords_w = (min(kHistCap, a.B - w0) + 31) >> 5;
+        for (int i = e0 + tid; i < e1; i += T) {
+          const int c = d.ucol[base + i] - w0;
+          atomicAdd(hist + c, d.uw[base + i]);
+          atomicOr(touched + (c >> 5), 1u << (c & 31));
+        }
+        __syncthreads();
+        const int per = (nwords_w + T - 1) / T;
+        const int x0 = min(nwords_w, tid * per), x1 = min(nwords_w, x0 + per);
+        int nz = 0;
+        for (int x = x0; x < x1; ++x) nz += __popc(touched[x]);
+        int tot;
+        int pos = cta_excl_scan(nz, sh, &tot) + running;
+        for (int x = x0; x < x1; ++x) {
+          uint32_t m = touched[x];
+          touched[x] = 0u;
+          while (m) {
+            const int c = (x << 5) + __ffs(m) - 1;
+            m &= m - 1;
+            d.ucol[base + pos] = w0 + c;
+            d.uw[base + pos] = hist[c];
+            hist[c] = 0u;
+            ++pos;
+          }
+        }
+        running += tot;
+        __syncthreads();
+      }
     } else if (n > kSortCap) {
       // histogram over column windows of kHistCap
       for (int w0 = 0; w0 < a.B; w0 += kHistCap) {

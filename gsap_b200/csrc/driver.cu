@@ -611,6 +611,8 @@ static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t se
   if (is_dense(J, B)) rebuild_blockmodel(J.g, J.part, B, J.m, J.rs, st);
   block_terms(J.m, B, 0, seed, 0, st);
   MergeGrid grid;
+  grid.dS = J.mdS;  // per-proposal scratch, and the slots' kept dS
+  grid.dsin = J.mdsin;
   if (ref_grid) {
     // a fresh run's merge buffers: the slots GSAP's grid leaves out read zeros
     const size_t slots = (size_t)J.N * J.np;
@@ -618,8 +620,6 @@ static sbp_status merge_step(Job& J, int32_t& B, int32_t B_to_merge, uint64_t se
     SBP_CUDA(cudaMemsetAsync(J.mdS, 0, 8 * slots, st));
     SBP_CUDA(cudaMemsetAsync(J.mdsin, 0, 8 * slots, st));
     grid.on = 1;
-    grid.dS = J.mdS;
-    grid.dsin = J.mdsin;
   }
   merge_proposals(J.m, B, J.np, seed, seq, J.props, st, grid);
   merge_delta(J.m, B, J.E, J.np, J.props, keep_dS ? J.mdS : nullptr, J.best, J.best_dS, st, 0,

@@ -225,7 +225,7 @@ void Engine::ensure_slots(int K, int nb) {
 
 void Engine::clear_slots() {
   for (Slot* s : {&s_iota, &s_lists, &s_snap, &s_restore, &s_zero, &m_bt, &m_props, &m_delta,
-                  &m_delta8, &m_relabel, &s_gather})
+                  &m_delta8, &m_best, &m_relabel, &s_gather})
     s->clear();
   m_apply.clear();
   pre_dense.clear();
@@ -306,7 +306,7 @@ void Engine::add_run_work(Run& r) {
     add_block_terms(m_bt, J.m, r.B, 0, r.o.seed, 0);
     const MergeGrid grid = merge_grid(J, r.o);
     add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props, grid);
-    add_merge_delta(m_delta, m_delta8, J.m, r.B, J.E, J.np, J.props, nullptr, J.best,
+    add_merge_delta(m_delta, m_delta8, m_best, J.m, r.B, J.E, J.np, J.props, nullptr, J.best,
                     J.best_dS, r.o.exact, grid);
     // carry_out_best_merges on the device, then the relabel: the host reads
     // back only the new block count
@@ -480,7 +480,7 @@ sbp_status Engine::tick() {
   std::vector<Slot*> order = {&s_iota, &s_lists, &s_snap, &s_restore, &s_zero};
   for (Slot* x : pre_dense.all()) order.push_back(x);
   for (Slot* x : pre_rebuild.all()) order.push_back(x);
-  for (Slot* x : {&m_bt, &m_props, &m_delta, &m_delta8}) order.push_back(x);
+  for (Slot* x : {&m_bt, &m_props, &m_delta, &m_delta8, &m_best}) order.push_back(x);
   for (Slot* x : m_apply.all()) order.push_back(x);
   order.push_back(&m_relabel);
   for (int k = 0; k < k_max; ++k) {

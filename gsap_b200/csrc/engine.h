@@ -125,7 +125,7 @@ class Engine {
   Slot s_iota, s_lists, s_snap, s_restore, s_zero;
   DenseBuildSlots pre_dense;
   RebuildSlots pre_rebuild;
-  Slot m_bt, m_props, m_delta, m_delta8;
+  Slot m_bt, m_props, m_delta, m_delta8, m_best;
   MergeApplySlots m_apply;  // merge application on the device (mergeapply.cu)
   Slot m_relabel;
   std::vector<SweepSlots> sw;     // [queued sweep][batch]

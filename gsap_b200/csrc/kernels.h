@@ -202,10 +202,12 @@ struct MergeGrid {
 
 void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t seed, uint32_t seq,
                      int32_t* props, const MergeGrid& grid = MergeGrid());
-// E: the graph's edge count, which picks the group width of the dS kernel:
-// jobs with short blockmodel rows go to slot s8 (groups of 8 lanes), the
-// others to s32 (the whole warp on a proposal).
-void add_merge_delta(Slot& s32, Slot& s8, const DevBM& m, int32_t B, int32_t E, int32_t np,
+// E: the graph's edge count, which picks the dS kernel: jobs with short
+// blockmodel rows go to slot s8 (a warp per block, groups of 8 lanes per
+// proposal), the others to s32 (a warp per proposal, into grid.dS) and
+// sbest (each block's best).  Without grid.dS, dS is the scratch.
+void add_merge_delta(Slot& s32, Slot& s8, Slot& sbest, const DevBM& m, int32_t B, int32_t E,
+                     int32_t np,
                      const int32_t* props, double* dS, int32_t* best, double* best_dS,
                      int32_t exact = 0, const MergeGrid& grid = MergeGrid());
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map);

@@ -49,6 +49,7 @@ struct MergeArgs {
   int32_t ref_grid;
   double* keep_dS;
   double* keep_dsin;
+  double* pdS;  // per-proposal dS (B * np) between the warp-per-proposal kernels
 };
 
 // First proposal slot GSAP's merge grid leaves out (B*np when none is).
@@ -375,6 +376,65 @@ struct MergeDeltaBody {
   }
 };
 
+// Long rows (E > 16 B): one warp per proposal, so that the few blocks of a
+// small B still fill the GPU; each proposal's dS goes to pdS (slots GSAP's
+// grid leaves out keep theirs: pdS is then the persistent keep_dS), and
+// MergeBestBody reduces each block's proposals.
+struct MergePropDeltaBody {
+  using Args = MergeArgs;
+  static constexpr int kThreads = kMergeWarps * 32, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const long long n = (long long)a.B * a.np, T = merge_grid_end(a);
+    for (long long t = (long long)vb * kMergeWarps + wid; t < n && t < T;
+         t += (long long)vg * kMergeWarps) {
+      const int r = (int)(t / a.np), k = (int)(t % a.np);
+      const int s = a.props_in[t];
+      double d, in_r = 0.0;
+      if (a.exact) {
+        d = merge_one_exact<32>(a, r, s, lane, true);
+      } else {
+        const long long sid = (long long)s * a.np + k;
+        const bool given = sid >= T;
+        const int s2 = given ? s : a.props_in[sid];
+        d = merge_one<32>(a, r, s, s2, lane, true, given, given ? a.keep_dsin[sid] : 0.0, &in_r);
+      }
+      if (lane == 0) {
+        a.pdS[t] = d;
+        if (a.dS && a.dS != a.pdS) a.dS[t] = d;
+        if (a.ref_grid && !a.exact) a.keep_dsin[t] = in_r;
+      }
+    }
+  }
+};
+
+// find_best_warp (kernels.hpp:452-491) over each block's proposals in pdS.
+struct MergeBestBody {
+  using Args = MergeArgs;
+  static constexpr int kThreads = kMergeWarps * 32, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int r = vb * kMergeWarps + wid; r < a.B; r += vg * kMergeWarps) {
+      const long long t = (long long)r * a.np + lane;
+      double mine = lane < a.np ? a.pdS[t] : DBL_MAX;
+      int who = lane < a.np ? a.props_in[t] : 0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_down_sync(kFull, mine, o);
+        int ow = __shfl_down_sync(kFull, who, o);
+        mine = fmin(mine, ov);
+        if (mine == ov) who = ow;
+      }
+      if (lane == 0) {
+        a.best[r] = who;
+        a.best_dS[r] = mine;
+      }
+    }
+  }
+};
+
 struct RelabelArgs {
   int32_t* part;
   const int32_t* map;
@@ -398,8 +458,12 @@ const MultiKernel kmMergeProps = multi_kernel_desc<MergePropsBody>("merge_props"
 // Groups of 8 lanes score a proposal when rows are short: at most 16
 // entries a row on average (nnz <= E).  A function of the job's sizes only.
 bool short_rows(int32_t B, int32_t E) { return (long long)E <= 16LL * B; }
+int32_t vg_merge_prop(int32_t B, int32_t np) {
+  return std::max(1, std::min(ceil_div((long long)B * np, kMergeWarps), 148 * 32));
+}
 
-const MultiKernel kmMergeDelta = multi_kernel_desc<MergeDeltaBody<32>>("merge_delta");
+const MultiKernel kmMergeDelta = multi_kernel_desc<MergePropDeltaBody>("merge_delta");
+const MultiKernel kmMergeBest = multi_kernel_desc<MergeBestBody>("merge_best");
 const MultiKernel kmMergeDelta8 = multi_kernel_desc<MergeDeltaBody<8>>("merge_delta_g8");
 const MultiKernel kmRelabel = multi_kernel_desc<RelabelBody>("relabel");
 
@@ -415,6 +479,7 @@ MergeArgs make_args(const DevBM& m, int32_t B, int32_t np, const MergeGrid& grid
   a.ref_grid = grid.on;
   a.keep_dS = grid.dS;
   a.keep_dsin = grid.dsin;
+  a.pdS = grid.dS;
   return a;
 }
 
@@ -438,9 +503,16 @@ void merge_delta(const DevBM& m, int32_t B, int32_t E, int32_t np, const int32_t
   a.dS = dS;
   a.best = best;
   a.best_dS = best_dS;
+  if (!a.pdS) a.pdS = dS;
   if (B <= 0) return;
-  if (short_rows(B, E)) launch_single<MergeDeltaBody<8>>(a, vg_merge_delta(B), st);
-  else launch_single<MergeDeltaBody<32>>(a, vg_merge_delta(B), st);
+  if (short_rows(B, E)) {
+    launch_single<MergeDeltaBody<8>>(a, vg_merge_delta(B), st);
+  } else if (!a.pdS) {
+    launch_single<MergeDeltaBody<32>>(a, vg_merge_delta(B), st);
+  } else {
+    launch_single<MergePropDeltaBody>(a, vg_merge_prop(B, np), st);
+    launch_single<MergeBestBody>(a, vg_merge_delta(B), st);
+  }
 }
 
 void relabel(int32_t* part, int32_t N, const int32_t* map, cudaStream_t st) {
@@ -457,7 +529,8 @@ void add_merge_props(Slot& s, const DevBM& m, int32_t B, int32_t np, uint64_t se
   slot_push(slot_bind(s, kmMergeProps), a, B > 0 && np > 0 ? vg_merge_delta(B) : 0);
 }
 
-void add_merge_delta(Slot& s32, Slot& s8, const DevBM& m, int32_t B, int32_t E, int32_t np,
+void add_merge_delta(Slot& s32, Slot& s8, Slot& sbest, const DevBM& m, int32_t B, int32_t E,
+                     int32_t np,
                      const int32_t* props, double* dS, int32_t* best, double* best_dS,
                      int32_t exact, const MergeGrid& grid) {
   MergeArgs a = make_args(m, B, np, grid);
@@ -466,8 +539,14 @@ void add_merge_delta(Slot& s32, Slot& s8, const DevBM& m, int32_t B, int32_t E, 
   a.dS = dS;
   a.best = best;
   a.best_dS = best_dS;
-  if (short_rows(B, E)) slot_push(slot_bind(s8, kmMergeDelta8), a, B > 0 ? vg_merge_delta(B) : 0);
-  else slot_push(slot_bind(s32, kmMergeDelta), a, B > 0 ? vg_merge_delta(B) : 0);
+  if (!a.pdS) a.pdS = dS;
+  if (B <= 0) return;
+  if (short_rows(B, E) || !a.pdS) {
+    slot_push(slot_bind(s8, kmMergeDelta8), a, vg_merge_delta(B));
+  } else {
+    slot_push(slot_bind(s32, kmMergeDelta), a, vg_merge_prop(B, np));
+    slot_push(slot_bind(sbest, kmMergeBest), a, vg_merge_delta(B));
+  }
 }
 
 void add_relabel(Slot& s, int32_t* part, int32_t N, const int32_t* map) {
