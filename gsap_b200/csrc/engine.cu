@@ -498,16 +498,21 @@ sbp_status Engine::tick() {
     for (Slot* x : {&e.bt_csr, &e.bt_dense, &e.mdl, &e.ctl}) order.push_back(x);
   }
   order.push_back(&s_gather);
+  // Only multi-job launches read their records from device memory (a
+  // one-job launch takes its record as the kernel argument), so a tick of
+  // one-job slots packs and uploads nothing.
+  bool multi = false;
+  for (const Slot* x : order) multi = multi || x->njobs() > 1;
   size_t desc = 0;
   std::vector<size_t> off(order.size(), 0);
-  for (size_t i = 0; i < order.size(); ++i) {
+  for (size_t i = 0; i < order.size() && multi; ++i) {
     if (order[i]->empty()) continue;
     off[i] = desc;
     desc += align256(order[i]->recs.size()) + align256(4 * order[i]->cta0.size());
   }
   s = grow(desc, desc_cap, desc_host, desc_dev);
   if (s != SBP_OK) return s;
-  for (size_t i = 0; i < order.size(); ++i) {
+  for (size_t i = 0; i < order.size() && multi; ++i) {
     Slot* x = order[i];
     if (x->empty()) continue;
     std::memcpy((char*)desc_host + off[i], x->recs.data(), x->recs.size());
@@ -615,10 +620,12 @@ sbp_status Engine::tick() {
     s = issue_sweeps();
     if (s != SBP_OK) return s;
   } else {
-    uint64_t key = 1469598103934665603ull;  // FNV-1a over the sweeps' launches
+    // the sweeps' launches, byte for byte: kernels, records, grids, offsets
+    std::vector<unsigned char>& key = key_scratch;
+    key.clear();
     auto mix = [&](const void* p, size_t n) {
       const unsigned char* c = (const unsigned char*)p;
-      for (size_t x = 0; x < n; ++x) key = (key ^ c[x]) * 1099511628211ull;
+      key.insert(key.end(), c, c + n);
     };
     mix(&k_max, sizeof(k_max));
     mix(&nb_max, sizeof(nb_max));
@@ -632,7 +639,8 @@ sbp_status Engine::tick() {
       mix(&off[q], sizeof(off[q]));
     }
     mix(&desc_dev, sizeof(desc_dev));
-    if (graph_exec && key == graph_key) {
+    if (graph_exec && key.size() == graph_key.size() &&
+        std::memcmp(key.data(), graph_key.data(), key.size()) == 0) {
       // replay: skip the slots the graph holds
       i = sweep_first;
       while (i < order.size() && order[i] != &s_gather) ++i;
@@ -669,7 +677,7 @@ sbp_status Engine::tick() {
         }
       }
       cudaGraphDestroy(g);
-      graph_key = key;
+      graph_key.swap(key);
       ++graph_captures;
     }
     SBP_CUDA(cudaGraphLaunch(graph_exec, st));
@@ -680,27 +688,31 @@ sbp_status Engine::tick() {
   SBP_CUDA(cudaEventRecord(ev[3], st));
   const double t_issued = now_ms();
   submit.unlock();
-  const cudaError_t waited = cudaEventSynchronize(ev[3]);
+  // phase times of this tick (shared by the runs that took part), each
+  // batch's read as soon as its last event has passed, so that the queries
+  // overlap the later batches instead of following the tick
+  float ms_pre = 0.f, ms_merge = 0.f;
+  float t_nodal = 0.f, t_kernel = 0.f, t_rebuild = 0.f;
+  cudaError_t waited = cudaEventSynchronize(ev[2]);
+  if (waited == cudaSuccess) waited = cudaEventElapsedTime(&ms_pre, ev[0], ev[1]);
+  if (waited == cudaSuccess) waited = cudaEventElapsedTime(&ms_merge, ev[1], ev[2]);
+  for (int q = 0; q < nbatch && waited == cudaSuccess; ++q) {
+    cudaEvent_t* be = &ev[4 + 5 * q];
+    float a = 0.f, b = 0.f, c = 0.f;
+    waited = cudaEventSynchronize(be[4]);
+    if (waited == cudaSuccess) waited = cudaEventElapsedTime(&a, be[0], be[3]);
+    if (waited == cudaSuccess) waited = cudaEventElapsedTime(&b, be[1], be[2]);
+    if (waited == cudaSuccess) waited = cudaEventElapsedTime(&c, be[3], be[4]);
+    t_nodal += a;
+    t_kernel += b;
+    t_rebuild += c;
+  }
+  if (waited == cudaSuccess) waited = cudaEventSynchronize(ev[3]);
   submit.lock();
   const double t_waited = now_ms();
   SBP_CUDA(waited);
   SBP_CUDA(cudaGetLastError());
   ++ticks;
-  // phase times of this tick (shared by the runs that took part)
-  float ms_pre = 0.f, ms_merge = 0.f;
-  SBP_CUDA(cudaEventElapsedTime(&ms_pre, ev[0], ev[1]));
-  SBP_CUDA(cudaEventElapsedTime(&ms_merge, ev[1], ev[2]));
-  float t_nodal = 0.f, t_kernel = 0.f, t_rebuild = 0.f;
-  for (int q = 0; q < nbatch; ++q) {
-    cudaEvent_t* be = &ev[4 + 5 * q];
-    float a = 0.f, b = 0.f, c = 0.f;
-    SBP_CUDA(cudaEventElapsedTime(&a, be[0], be[3]));
-    SBP_CUDA(cudaEventElapsedTime(&b, be[1], be[2]));
-    SBP_CUDA(cudaEventElapsedTime(&c, be[3], be[4]));
-    t_nodal += a;
-    t_kernel += b;
-    t_rebuild += c;
-  }
   // host side of each run
   for (Run* r : runs) {
     if (r->stage == Run::kDone) continue;

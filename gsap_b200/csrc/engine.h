@@ -136,7 +136,8 @@ class Engine {
   void *rd_host = nullptr, *rd_dev = nullptr;
   size_t up_cap = 0, desc_cap = 0, rd_cap = 0;
   cudaGraphExec_t graph_exec = nullptr;  // the last captured sweep tick
-  uint64_t graph_key = 0;
+  std::vector<unsigned char> graph_key;    // what the graph's launches were made from
+  std::vector<unsigned char> key_scratch;
   long long graph_kernels = 0;            // kernel launches the graph holds
   int nb_slots_ = 0;  // batch positions per queued sweep in this tick's slots
 

@@ -47,13 +47,9 @@ namespace {
 constexpr int kNodalWarps = 8;
 constexpr int kWarpList = 128;     // entries per direction a warp sorts in shared memory
 constexpr int kHeavyThreads = 256;
-constexpr int kHeavyList = 4096;   // entries per direction a CTA sorts in shared memory
 constexpr int kHashSlotsCfg = 8192;
-// sorted lists (two directions) or the hash table (key, sum, first)
-constexpr size_t kHeavySmem =
-    2 * kHeavyList * sizeof(unsigned long long) > 3 * kHashSlotsCfg * sizeof(int32_t)
-        ? 2 * kHeavyList * sizeof(unsigned long long)
-        : 3 * kHashSlotsCfg * sizeof(int32_t);
+// the heavy path's hash table: key, sum, first
+constexpr size_t kHeavySmem = 3 * kHashSlotsCfg * sizeof(int32_t);
 
 struct NodalArgs {
   const double* xlx;        // x log2 x table
@@ -450,7 +446,7 @@ __device__ double delta_registers(const NodalArgs& a, int v, int r, int s, int32
 }
 
 
-// Lists too long for shared memory: per-block totals from a shared-memory
+// Lists of more than kWarpList entries: per-block totals from a shared-memory
 // hash table, built in passes that each take the blocks of one hash class,
 // so the table never holds more than a few thousand blocks.  Costs
 // O(n * passes) with passes ~ n / 2048.
@@ -1251,8 +1247,10 @@ struct NodalBody {
 };
 
 // Vertices with more than kWarpList entries in a direction: one CTA each,
-// lists sorted in shared memory up to kHeavyList entries, longer ones
-// through the hashed passes.
+// per-block totals from the shared-memory hash table (one pass up to a few
+// thousand distinct blocks, more passes beyond).  Sorting both lists in
+// shared memory instead (the warp path's method) made the nodal kernels of a
+// 200k-vertex partition about 6 ms slower, for the same dS.
 template <bool GIVEN, bool DENSE, bool GEN>
 struct NodalHeavyBody {
   using Args = NodalArgs;
@@ -1265,8 +1263,6 @@ struct NodalHeavyBody {
   __shared__ int flag, sh_v, sh_s;
   __shared__ uint32_t sh_u2;
   Group<kHeavyThreads> grp{red};
-  unsigned long long* ko = hsm;
-  unsigned long long* ki = hsm + kHeavyList;
   HashTab ht{(int32_t*)hsm, (uint32_t*)hsm + kHashSlots, (int32_t*)hsm + 2 * kHashSlots};
   for (int h = vb; h < a.nheavy; h += vg) {
     const int i = a.heavy[h];
@@ -1287,20 +1283,11 @@ struct NodalHeavyBody {
     const int32_t i0 = a.iptr[v], ni = a.iptr[v + 1] - i0;
     double d = 0.0, lh = 0.0;
     if (r != s) {
-      if (no <= kHeavyList && ni <= kHeavyList) {
-        stage_sorted<kHeavyThreads>(a.oidx, a.ow, a.part, o0, no, ko, grp);
-        stage_sorted<kHeavyThreads>(a.iidx, a.iw, a.part, i0, ni, ki, grp);
-        if constexpr (GEN)
-          d = delta_sorted_gen<DENSE, kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp, lh);
-        else
-          d = delta_sorted<DENSE, kHeavyThreads>(a, v, r, s, ko, no, ki, ni, grp);
-      } else {
-        if constexpr (GEN)
-          d = delta_hashed_gen<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp, lh);
-        else
-          d = delta_hashed<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp);
-        if (threadIdx.x == 0 && d != d) atomicAdd(a.err, 1);
-      }
+      if constexpr (GEN)
+        d = delta_hashed_gen<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp, lh);
+      else
+        d = delta_hashed<DENSE, kHeavyThreads>(a, v, r, s, ht, &flag, grp);
+      if (threadIdx.x == 0 && d != d) atomicAdd(a.err, 1);
     }
     if (threadIdx.x == 0) {
       if constexpr (GEN) write_result_gen(a, GIVEN, i, r, s, d, lh, sh_u2);
