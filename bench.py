@@ -318,10 +318,44 @@ def run_ours(args, rank, world, local, dist):
     }
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(local)
+    if world == 1 and not args.no_extras:
+        line["ingest"] = ingest_times(sbp, g, local)
     return line
 
 
-def batched_graphs(sbp, count, seed):
+def ingest_times(sbp, g, local, reps=3):
+    """The plain workload's graph made on the host (sbp_dcsbm_generate then
+    sbp_csr_from_edges) and on the device (sbp_dcsbm_generate_device: labels
+    on the host, degrees, members, edges and the CSR pair on the device, into
+    a resident graph), wall ms each, and whether the device graph equals the
+    host one in every CSR array."""
+    w = WORKLOAD
+    p_in, alpha = sbp.VARIANTS[w["variant"]]
+    host, dev = [], []
+    same = True
+    for i in range(reps + 1):
+        t0 = time.perf_counter()
+        gh = sbp.dcsbm_variant(w["variant"], w["N"], w["B"], seed=w["seed"])
+        t1 = time.perf_counter()
+        dg = sbp.dcsbm_variant_device(w["variant"], w["N"], w["B"], seed=w["seed"], device=local)
+        t2 = time.perf_counter()
+        if i == 0:  # warm-up (kernels, pools); checked once
+            gd = dg.download()
+            same = all(np.array_equal(getattr(gd, k), getattr(g, k)) for k in (
+                "out_ptr", "out_idx", "out_w", "in_ptr", "in_idx", "in_w", "deg_out", "deg_in"))
+            same = same and np.array_equal(dg.true_partitions, g.true_partitions)
+        else:
+            host.append((t1 - t0) * 1000.0)
+            dev.append((t2 - t1) * 1000.0)
+        dg.close()
+        del gh
+    return {"graph": w["name"], "N": g.N, "E": g.E, "host_generate_ms": float(np.median(host)),
+            "device_generate_ms": float(np.median(dev)), "device_equals_host": bool(same),
+            "note": "wall ms, median of 3; device = sbp_dcsbm_generate_device to a resident "
+                    "graph, host = sbp_dcsbm_generate + sbp_csr_from_edges"}
+
+
+def batched_specs(count, seed):
     """The batched workload: graph i has N log-uniform on [1k, 50k],
     B = round(2.6 N^0.34), p_in in {0.5, 0.8}, alpha in {1, 20}."""
     rng = np.random.default_rng(seed)
@@ -331,7 +365,21 @@ def batched_graphs(sbp, count, seed):
         B = int(round(2.6 * N ** 0.34))
         p_in = float(rng.choice([0.5, 0.8]))
         alpha = float(rng.choice([1.0, 20.0]))
-        out.append(sbp.dcsbm(N, B, alpha, p_in, seed=seed * 100000 + i))
+        out.append((N, B, alpha, p_in, seed * 100000 + i))
+    return out
+
+
+def batched_graphs(sbp, count, seed, device=None):
+    """The batched graphs, from the host generator, or (device given) from
+    the device generator downloaded to host CSRs (the batch API's input)."""
+    out = []
+    for N, B, alpha, p_in, s in batched_specs(count, seed):
+        if device is None:
+            out.append(sbp.dcsbm(N, B, alpha, p_in, seed=s))
+        else:
+            dg = sbp.dcsbm_device(N, B, alpha, p_in, seed=s, device=device)
+            out.append(dg.download())
+            dg.close()
     return out
 
 
@@ -348,7 +396,18 @@ def run_batched(args, rank, world, local, dist):
     from gsap_b200 import sbp
     from gsap_b200.shard import gather_results, shard_jobs
     count = args.batch_count
+    # the load generator on the host and on the device: the same graphs
+    t0 = time.perf_counter()
     every = batched_graphs(sbp, count, 7)
+    gen_host = (time.perf_counter() - t0) * 1000.0
+    batched_graphs(sbp, 4, 7, device=local)  # warm-up
+    t0 = time.perf_counter()
+    every_dev = batched_graphs(sbp, count, 7, device=local)
+    gen_dev = (time.perf_counter() - t0) * 1000.0
+    gen_same = sum(int(all(np.array_equal(getattr(a, k), getattr(b, k)) for k in (
+        "out_ptr", "out_idx", "out_w", "in_ptr", "in_idx", "in_w", "deg_out", "deg_in",
+        "true_partitions"))) for a, b in zip(every, every_dev))
+    del every_dev
     mine = shard_jobs([g.E for g in every], world)[rank]
     gs = [every[i] for i in mine]
     seeds = list(mine)
@@ -401,6 +460,10 @@ def run_batched(args, rank, world, local, dist):
                     "mean_recall": float(np.mean([x[1] for x in q])),
                     "mean_precision": float(np.mean([x[2] for x in q]))},
         "batch": br, "gpu_launches": launches, "clocks": clk.summary(),
+        "load_generator": {"host_ms": gen_host, "device_ms": gen_dev,
+                           "device_equals_host": f"{gen_same}/{count}",
+                           "note": "wall ms for all graphs; device = sbp_dcsbm_generate_device "
+                                   "plus sbp_graph_download to host CSRs"},
     }
 
 
@@ -615,7 +678,7 @@ def main():
             line["batched"] = {k: b[k] for k in (
                 "metric", "value", "unit", "ms_per_step", "e2e", "sequential_plain",
                 "speedup_vs_sequential_e2e", "identical_results", "quality", "config",
-                "gpu_launches", "clocks")}
+                "gpu_launches", "clocks", "load_generator")}
             import copy
             sa = copy.copy(args)
             sa.rates, sa.served_max = [5.0, 20.0, 100.0], 200

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsbp.so")
 SOURCES = ["driver.cu", "engine.cu", "blockmodel.cu", "nodal.cu", "merge.cu", "mergeapply.cu",
-           "noalloc.cu", "server.cu", "host.cpp"]
+           "noalloc.cu", "server.cu", "ingest.cu", "host.cpp"]
 HEADERS = ["common.cuh", "kernels.h", "multi.cuh", "job.h", "engine.h"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",

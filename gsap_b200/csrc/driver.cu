@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <memory>
 #include <cstring>
 #include <limits>
 #include <mutex>
@@ -698,8 +699,71 @@ sbp_status check_options(const sbp_options* o) {
 
 struct sbp_graph_dev {
   sbp::Job job;
-  sbp_graph_csr shape;
+  sbp_graph_csr shape;  // host arrays of an uploaded graph (null for device-built ones)
+  // a graph built on the device keeps its edges there, to build the CSR
+  // pair again when the job's arena has to grow
+  int32_t *d_src = nullptr, *d_dst = nullptr;
+  uint32_t* d_w = nullptr;
+  int dev = -1;
+  ~sbp_graph_dev() {
+    if (d_src || d_dst || d_w) {
+      int cur = 0;
+      cudaGetDevice(&cur);
+      cudaSetDevice(dev);
+      cudaFree(d_src);
+      cudaFree(d_dst);
+      cudaFree(d_w);
+      cudaSetDevice(cur);
+    }
+  }
 };
+
+namespace sbp {
+
+// Creates the job's arena and builds its CSR pair from edges in device
+// memory (csr_from_device_edges), with the host row pointers the engine
+// reads.
+static sbp_status job_from_device_edges(Job& J, int device, int32_t N, int32_t E,
+                                        const int32_t* src, const int32_t* dst,
+                                        const uint32_t* w, int32_t np, int32_t max_itr,
+                                        int32_t dense_max) {
+  sbp_status s = job_create(J, device, N, E, np, max_itr, dense_max);
+  if (s != SBP_OK) return s;
+  const size_t sb = csr_build_scratch_bytes(N, E) + 256;
+  char* scratch = nullptr;
+  SBP_CUDA(cudaMallocAsync((void**)&scratch, sb, J.st));
+  int32_t* err = (int32_t*)(scratch + sb - 256);
+  cudaError_t e = csr_from_device_edges(N, E, src, dst, w, J.g, err, scratch, J.st);
+  int32_t herr = 0;
+  J.h_optr.resize((size_t)N + 1);
+  J.h_iptr.resize((size_t)N + 1);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, J.st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(J.h_optr.data(), J.g.optr, 4 * ((size_t)N + 1), cudaMemcpyDeviceToHost,
+                        J.st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(J.h_iptr.data(), J.g.iptr, 4 * ((size_t)N + 1), cudaMemcpyDeviceToHost,
+                        J.st);
+  const cudaError_t f = cudaFreeAsync(scratch, J.st);
+  const cudaError_t q = cudaStreamSynchronize(J.st);
+  SBP_CUDA(e);
+  SBP_CUDA(f);
+  SBP_CUDA(q);
+  if (herr & 1) return fail(SBP_ERR_INVALID, "edge endpoint out of range");
+  if (herr & 2) return fail(SBP_ERR_INVALID, "edge weights must be >= 1");
+  if (herr & 4) return fail(SBP_ERR_INVALID, "node degree does not fit 32 bits");
+  return SBP_OK;
+}
+
+// A resident-graph handle over edges in device memory that the handle owns.
+static sbp_status graph_from_owned_edges(sbp_graph_dev* h, int32_t N, int32_t E) {
+  h->shape = sbp_graph_csr{};
+  h->shape.N = N;
+  h->shape.E = E;
+  return job_from_device_edges(h->job, h->dev, N, E, h->d_src, h->d_dst, h->d_w, 10, 100, -1);
+}
+
+}  // namespace sbp
 
 using namespace sbp;
 
@@ -770,6 +834,115 @@ sbp_status sbp_graph_release(sbp_graph_dev* g) {
   return SBP_OK;
 }
 
+sbp_status sbp_graph_from_device_edges(int32_t N, int32_t E, const int32_t* src,
+                                       const int32_t* dst, const uint32_t* w, int32_t device,
+                                       sbp_graph_dev** out) {
+  if (!out) return fail(SBP_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (N < 1 || E < 0) return fail(SBP_ERR_INVALID, "need N >= 1 and E >= 0");
+  if (E > 0 && (!src || !dst)) return fail(SBP_ERR_INVALID, "edge arrays are NULL");
+  std::unique_ptr<sbp_graph_dev> h(new (std::nothrow) sbp_graph_dev());
+  if (!h) return fail(SBP_ERR_NOMEM, "host allocation");
+  h->dev = resolve_device(device);
+  SBP_CUDA(cudaSetDevice(h->dev));
+  const size_t n = (size_t)std::max(E, 1);
+  SBP_CUDA(cudaMalloc(&h->d_src, 4 * n));
+  SBP_CUDA(cudaMalloc(&h->d_dst, 4 * n));
+  if (w) SBP_CUDA(cudaMalloc(&h->d_w, 4 * n));
+  if (E > 0) {
+    SBP_CUDA(cudaMemcpy(h->d_src, src, 4 * (size_t)E, cudaMemcpyDeviceToDevice));
+    SBP_CUDA(cudaMemcpy(h->d_dst, dst, 4 * (size_t)E, cudaMemcpyDeviceToDevice));
+    if (w) SBP_CUDA(cudaMemcpy(h->d_w, w, 4 * (size_t)E, cudaMemcpyDeviceToDevice));
+  }
+  sbp_status s = graph_from_owned_edges(h.get(), N, E);
+  if (s != SBP_OK) return s;
+  *out = h.release();
+  return SBP_OK;
+}
+
+sbp_status sbp_dcsbm_generate_device(const sbp_dcsbm_params* p, int32_t device,
+                                     int32_t* truth_out, sbp_graph_dev** out) {
+  if (!p || !out) return fail(SBP_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  std::vector<int32_t> truth;
+  std::vector<double> cdf;
+  sbp_status s = dcsbm_labels(p, truth, cdf);
+  if (s != SBP_OK) return s;
+  const long long slots = (long long)p->N * p->deg_max;
+  if (slots >= (1ll << 31))
+    return fail(SBP_ERR_INVALID, "N * deg_max must be below 2^31 for the device generator");
+  std::unique_ptr<sbp_graph_dev> h(new (std::nothrow) sbp_graph_dev());
+  if (!h) return fail(SBP_ERR_NOMEM, "host allocation");
+  h->dev = resolve_device(device);
+  SBP_CUDA(cudaSetDevice(h->dev));
+  cudaStream_t st = nullptr;
+  SBP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int32_t *src = nullptr, *dst = nullptr;
+  int32_t E = 0;
+  cudaError_t e = cudaMalloc(&src, 4 * (size_t)std::max(slots, 1ll));
+  if (e == cudaSuccess) e = cudaMalloc(&dst, 4 * (size_t)std::max(slots, 1ll));
+  if (e == cudaSuccess) {
+    DcsbmDeviceIn in{};
+    in.truth = truth.data();
+    in.cdf = cdf.data();
+    in.seed = p->seed;
+    in.pin_scaled = (uint64_t)std::llround(p->p_in * 4294967296.0);
+    in.N = p->N;
+    in.B = p->B;
+    in.ncdf = (int32_t)cdf.size();
+    in.deg_min = p->deg_min;
+    in.max_edges = slots;
+    DcsbmDeviceOut o{src, dst, &E};
+    e = dcsbm_device_edges(in, o, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  // the handle keeps the edges at their exact size
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_src, 4 * (size_t)std::max(E, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&h->d_dst, 4 * (size_t)std::max(E, 1));
+  if (e == cudaSuccess && E > 0)
+    e = cudaMemcpyAsync(h->d_src, src, 4 * (size_t)E, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess && E > 0)
+    e = cudaMemcpyAsync(h->d_dst, dst, 4 * (size_t)E, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(src);
+  cudaFree(dst);
+  cudaStreamDestroy(st);
+  SBP_CUDA(e);
+  if (truth_out) std::memcpy(truth_out, truth.data(), 4 * (size_t)p->N);
+  s = graph_from_owned_edges(h.get(), p->N, E);
+  if (s != SBP_OK) return s;
+  *out = h.release();
+  return SBP_OK;
+}
+
+sbp_status sbp_graph_shape(const sbp_graph_dev* g, int32_t* N, int32_t* E) {
+  if (!g) return fail(SBP_ERR_INVALID, "graph handle is NULL");
+  if (N) *N = g->shape.N;
+  if (E) *E = g->shape.E;
+  return SBP_OK;
+}
+
+sbp_status sbp_graph_download(const sbp_graph_dev* g, int32_t* out_ptr, int32_t* out_idx,
+                              uint32_t* out_w, int32_t* in_ptr, int32_t* in_idx, uint32_t* in_w,
+                              uint32_t* deg_out, uint32_t* deg_in) {
+  if (!g) return fail(SBP_ERR_INVALID, "graph handle is NULL");
+  const Job& J = g->job;
+  const size_t n1 = (size_t)J.N + 1, E = (size_t)J.E, N = (size_t)J.N;
+  SBP_CUDA(cudaSetDevice(J.device));
+  struct Copy {
+    void* dst;
+    const void* src;
+    size_t bytes;
+  } copies[] = {{out_ptr, J.g.optr, 4 * n1}, {out_idx, J.g.oidx, 4 * E}, {out_w, J.g.ow, 4 * E},
+                {in_ptr, J.g.iptr, 4 * n1},  {in_idx, J.g.iidx, 4 * E},  {in_w, J.g.iw, 4 * E},
+                {deg_out, J.g.kdo, 4 * N},   {deg_in, J.g.kdi, 4 * N}};
+  for (const Copy& c : copies)
+    if (c.dst && c.bytes)
+      SBP_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, J.st));
+  SBP_CUDA(cudaStreamSynchronize(J.st));
+  return SBP_OK;
+}
+
 sbp_status sbp_partition_resident(sbp_graph_dev* gd, const sbp_options* o, int32_t* labels_out,
                                   sbp_report* report) {
   if (!gd) return fail(SBP_ERR_INVALID, "graph handle is NULL");
@@ -778,12 +951,17 @@ sbp_status sbp_partition_resident(sbp_graph_dev* gd, const sbp_options* o, int32
   Job& J = gd->job;
   const int32_t want_dense = dense_limit(gd->shape.N, gd->shape.E, o->dense_max);
   if (o->num_proposals > J.np || o->max_nodal_itr > J.max_itr || want_dense > J.dense_cap) {
-    // grow the job's arena for these options; the graph is uploaded again
+    // grow the job's arena for these options; the graph is uploaded (or
+    // built from its device edges) again
     int dev = J.device;
     int32_t np = std::max(o->num_proposals, J.np), mi = std::max(o->max_nodal_itr, J.max_itr);
     int32_t dm = std::max(want_dense, J.dense_cap);
     J.release();
-    s = job_for(J, &gd->shape, dev, np, mi, dm);
+    if (gd->d_src)
+      s = job_from_device_edges(J, dev, gd->shape.N, gd->shape.E, gd->d_src, gd->d_dst, gd->d_w,
+                                np, mi, dm);
+    else
+      s = job_for(J, &gd->shape, dev, np, mi, dm);
     if (s != SBP_OK) return s;
   }
   SBP_CUDA(cudaSetDevice(J.device));

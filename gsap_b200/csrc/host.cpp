@@ -64,19 +64,19 @@ double gamma_draw(uint64_t seed, uint32_t idx, double alpha) {
 
 }  // namespace
 
-extern "C" {
+namespace sbp {
 
-sbp_status sbp_dcsbm_generate(const sbp_dcsbm_params* p, sbp_edges** out) {
-  if (!p || !out) return sbp::host_fail(SBP_ERR_INVALID, "NULL argument");
-  *out = nullptr;
+// The generator's first stages, shared by the host generator and the device
+// one: the planted labels (block proportions ~ Dirichlet(alpha), sizes, a
+// Fisher-Yates shuffle) and the running weights k^-exponent of the
+// out-degrees on [deg_min, deg_max].
+sbp_status dcsbm_labels(const sbp_dcsbm_params* p, std::vector<int32_t>& truth,
+                        std::vector<double>& cdf) {
   const int32_t N = p->N, B = p->B;
   if (N < 2 || B < 1 || B > N || !(p->alpha > 0.0) || p->p_in < 0.0 || p->p_in > 1.0 ||
       p->deg_min < 1 || p->deg_max < p->deg_min || p->deg_max >= N)
     return sbp::host_fail(SBP_ERR_INVALID, "bad DCSBM parameters");
   const uint64_t seed = p->seed;
-  sbp_edges* g = new (std::nothrow) sbp_edges();
-  if (!g) return sbp::host_fail(SBP_ERR_NOMEM, "host allocation");
-  g->N = N;
   // block proportions ~ Dirichlet(alpha)
   std::vector<double> prop(B);
   double tot = 0.0;
@@ -103,21 +103,41 @@ sbp_status sbp_dcsbm_generate(const sbp_dcsbm_params* p, sbp_edges** out) {
     }
   }
   // labels, shuffled (Fisher-Yates)
-  g->truth.resize(N);
+  truth.resize(N);
   {
     int32_t v = 0;
     for (int32_t b = 0; b < B; ++b)
-      for (int64_t i = 0; i < size[b]; ++i) g->truth[v++] = b;
+      for (int64_t i = 0; i < size[b]; ++i) truth[v++] = b;
     for (int32_t i = N - 1; i > 0; --i) {
       P4 x = gen_draw(seed, 2, (uint32_t)i, 0);
       int32_t j = (int32_t)sbp::scale_draw(x.v[0], (uint64_t)i + 1);
-      std::swap(g->truth[i], g->truth[j]);
+      std::swap(truth[i], truth[j]);
     }
   }
   // out-degrees ~ k^-exponent on [deg_min, deg_max]
-  std::vector<double> cdf;
+  cdf.clear();
   for (int32_t k = p->deg_min; k <= p->deg_max; ++k)
     cdf.push_back((cdf.empty() ? 0.0 : cdf.back()) + std::pow((double)k, -p->exponent));
+  return SBP_OK;
+}
+
+}  // namespace sbp
+
+extern "C" {
+
+sbp_status sbp_dcsbm_generate(const sbp_dcsbm_params* p, sbp_edges** out) {
+  if (!p || !out) return sbp::host_fail(SBP_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  std::vector<int32_t> truth;
+  std::vector<double> cdf;
+  sbp_status st = sbp::dcsbm_labels(p, truth, cdf);
+  if (st != SBP_OK) return st;
+  const int32_t N = p->N, B = p->B;
+  const uint64_t seed = p->seed;
+  sbp_edges* g = new (std::nothrow) sbp_edges();
+  if (!g) return sbp::host_fail(SBP_ERR_NOMEM, "host allocation");
+  g->N = N;
+  g->truth.swap(truth);
   std::vector<int32_t> deg(N);
   for (int32_t v = 0; v < N; ++v) {
     P4 x = gen_draw(seed, 3, (uint32_t)v, 0);

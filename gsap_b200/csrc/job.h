@@ -81,6 +81,10 @@ struct Job {
 };
 
 sbp_status validate_graph(const sbp_graph_csr* g);
+// The DCSBM generator's planted labels and out-degree CDF (host.cpp), the
+// stages the host and device generators share.
+sbp_status dcsbm_labels(const sbp_dcsbm_params* p, std::vector<int32_t>& truth,
+                        std::vector<double>& cdf);
 sbp_status validate_part(const int32_t* part, int32_t N, int32_t B);
 int resolve_device(int32_t d);
 // Device arena bytes of a job (the engine's HBM admission test uses it).

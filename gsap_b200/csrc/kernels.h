@@ -255,6 +255,37 @@ cudaError_t init_kernel_attributes();
 // Exclusive scan of n int32 counts into out[0..n] (out[n] = total).
 void scan_exclusive(const int32_t* in, int32_t* out, int32_t n, int32_t* tile, cudaStream_t st);
 
+// ---------------------------------------------------------------- ingest --
+// Stable sort of n non-negative keys (at most max_key): keys_out ascending,
+// vals_out[p] = input position of the p-th key, equal keys in input order.
+// scratch: sort_scratch_bytes(n).
+size_t sort_scratch_bytes(int32_t n);
+cudaError_t sort_by_key_stable(const int32_t* keys, int32_t n, int32_t max_key,
+                               int32_t* keys_out, int32_t* vals_out, void* scratch,
+                               cudaStream_t st);
+// The CSR pair of an edge list in device memory, as sbp_csr_from_edges
+// builds it (rows in input edge order, w == nullptr for unit weights), into
+// g's arrays (row pointers, entries, weights, degrees, owners).  Bits of
+// *err (device): 1 endpoint outside [0, N), 2 weight 0, 4 degree above
+// 2^32 - 1.  scratch: csr_build_scratch_bytes(N, E).
+size_t csr_build_scratch_bytes(int32_t N, int32_t E);
+cudaError_t csr_from_device_edges(int32_t N, int32_t E, const int32_t* src, const int32_t* dst,
+                                  const uint32_t* w, DevGraph& g, int32_t* err, void* scratch,
+                                  cudaStream_t st);
+// The device stages of the DCSBM generator: degrees, block members, edges.
+struct DcsbmDeviceIn {
+  const int32_t* truth;  // host: the N planted labels (dcsbm_labels)
+  const double* cdf;     // host: ncdf running out-degree weights
+  uint64_t seed, pin_scaled;
+  int32_t N, B, ncdf, deg_min;
+  long long max_edges;   // N * deg_max: the edge slots the sources may fill
+};
+struct DcsbmDeviceOut {
+  int32_t *src, *dst;  // device, max_edges entries each: the edges, source-major
+  int32_t* E_host;     // the edge count, once the stream has run
+};
+cudaError_t dcsbm_device_edges(const DcsbmDeviceIn& in, DcsbmDeviceOut& out, cudaStream_t st);
+
 // calculate_new_csr (partition.hpp:707-849): rebuild M from the labels.
 void rebuild_blockmodel(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
                         RebuildScratch& rs, cudaStream_t st,

@@ -1214,7 +1214,7 @@ __host__ __device__ __forceinline__ int nodal_items(int nsmall, int nmid) {
 template <bool GIVEN, bool DENSE, bool GEN>
 struct NodalBody {
   using Args = NodalArgs;
-  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = GEN ? 2 : DENSE ? 5 : 3;
+  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = GEN ? 2 : DENSE ? 6 : 3;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
   if (ctl_stopped(a.ctl)) return;

@@ -10,6 +10,7 @@ missing library is an ImportError.
 from __future__ import annotations
 
 import ctypes as C
+import types
 import os
 import struct
 from dataclasses import dataclass, field
@@ -172,6 +173,12 @@ _sig("sbp_csr_from_edges", C.c_int, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _v
 _sig("sbp_load_tsv", C.c_int, C.c_char_p, C.c_char_p, C.POINTER(_vp))
 _sig("sbp_evaluate", C.c_int, C.c_int32, _vp, _vp, C.POINTER(C.c_double),
      C.POINTER(C.c_double), C.POINTER(C.c_double))
+_sig("sbp_graph_from_device_edges", C.c_int, C.c_int32, C.c_int32, _vp, _vp, _vp, C.c_int32,
+     C.POINTER(_vp))
+_sig("sbp_dcsbm_generate_device", C.c_int, C.POINTER(_DcsbmParams), C.c_int32, _vp,
+     C.POINTER(_vp))
+_sig("sbp_graph_shape", C.c_int, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32))
+_sig("sbp_graph_download", C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
 
 LIB_PATH = _LIB_PATH
 EXPORTED = [
@@ -184,7 +191,8 @@ EXPORTED = [
     "sbp_server_create", "sbp_server_submit", "sbp_server_poll", "sbp_server_stats_get",
     "sbp_server_destroy", "sbp_delta_mdl_nodal_mode", "sbp_delta_mdl_merge_mode",
     "sbp_nodal_batch_mode", "sbp_mdl_mode", "sbp_apply_merges", "sbp_apply_merges_device",
-    "sbp_merge_step_mode",
+    "sbp_merge_step_mode", "sbp_graph_from_device_edges", "sbp_dcsbm_generate_device",
+    "sbp_graph_shape", "sbp_graph_download",
 ]
 
 
@@ -431,6 +439,60 @@ class ResidentGraph:
             self.close()
         except Exception:
             pass
+
+
+class DeviceGraph(ResidentGraph):
+    """A resident graph built on the device, with no host CSR: from an edge
+    list in device memory (sbp_graph_from_device_edges) or by the device
+    DCSBM generator (sbp_dcsbm_generate_device)."""
+
+    def __init__(self, handle, truth=None):
+        self.h = handle
+        N, E = C.c_int32(), C.c_int32()
+        _check(_lib.sbp_graph_shape(self.h, C.byref(N), C.byref(E)))
+        self.N, self.E = N.value, E.value
+        self.true_partitions = truth
+        self.g = types.SimpleNamespace(N=self.N, E=self.E)  # what partition() reads
+
+    @staticmethod
+    def from_edges(N, src_ptr, dst_ptr, E, w_ptr=None, device=-1) -> "DeviceGraph":
+        """src_ptr, dst_ptr, w_ptr: device addresses of E int32 / uint32
+        entries (w_ptr None for unit weights)."""
+        h = _vp()
+        _check(_lib.sbp_graph_from_device_edges(N, E, _vp(src_ptr), _vp(dst_ptr),
+                                                _vp(w_ptr) if w_ptr else None, device,
+                                                C.byref(h)))
+        return DeviceGraph(h)
+
+    def download(self) -> Graph:
+        """A host copy of the CSR pair."""
+        N, E = self.N, self.E
+        arrs = dict(out_ptr=np.zeros(N + 1, np.int32), out_idx=np.zeros(max(E, 1), np.int32),
+                    out_w=np.zeros(max(E, 1), np.uint32), in_ptr=np.zeros(N + 1, np.int32),
+                    in_idx=np.zeros(max(E, 1), np.int32), in_w=np.zeros(max(E, 1), np.uint32),
+                    deg_out=np.zeros(N, np.uint32), deg_in=np.zeros(N, np.uint32))
+        _check(_lib.sbp_graph_download(self.h, *[_p(arrs[k]) for k in (
+            "out_ptr", "out_idx", "out_w", "in_ptr", "in_idx", "in_w", "deg_out", "deg_in")]))
+        for k in ("out_idx", "out_w", "in_idx", "in_w"):
+            arrs[k] = arrs[k][:E].copy()
+        return Graph(N=N, E=E, true_partitions=self.true_partitions, **arrs)
+
+
+def dcsbm_device(N, B, alpha, p_in, seed=0, deg_min=5, deg_max=50, exponent=2.5,
+                 device=-1) -> DeviceGraph:
+    """The graph of :func:`dcsbm` with the same arguments, generated on the
+    device (sbp_dcsbm_generate_device); planted labels in true_partitions."""
+    p = _DcsbmParams(N=N, B=B, alpha=float(alpha), p_in=float(p_in), deg_min=deg_min,
+                     deg_max=deg_max, exponent=float(exponent), seed=seed)
+    truth = np.empty(N, np.int32)
+    h = _vp()
+    _check(_lib.sbp_dcsbm_generate_device(C.byref(p), device, _p(truth), C.byref(h)))
+    return DeviceGraph(h, truth)
+
+
+def dcsbm_variant_device(variant, N, B, seed=0, device=-1) -> DeviceGraph:
+    p_in, alpha = VARIANTS[variant]
+    return dcsbm_device(N, B, alpha, p_in, seed=seed, device=device)
 
 
 # ------------------------------------------------------------ path pieces ---

@@ -141,6 +141,39 @@ sbp_status sbp_graph_release(sbp_graph_dev* g);
 sbp_status sbp_partition_resident(sbp_graph_dev* g, const sbp_options* o, int32_t* labels_out,
                                   sbp_report* report);
 
+/* ------------------------------------------------------------ device ingest
+ * Resident graphs made on the device, without a host CSR.  GSAP builds the
+ * CSR pair on the host (load.hpp:86-117) and uploads it
+ * (allocate_device.hpp:184-191); these have no counterpart there.
+ *
+ * sbp_graph_from_device_edges: the CSR pair of an edge list already in the
+ * memory of `device` (src, dst, w: E entries each; w NULL for unit
+ * weights), the same arrays sbp_csr_from_edges builds on the host (rows in
+ * input edge order).  The handle keeps its own copy of the edges; the
+ * caller's arrays may be freed after the call.  SBP_ERR_INVALID for an
+ * endpoint outside [0, N), a weight of 0 or a weighted degree above
+ * 2^32 - 1.
+ *
+ * sbp_dcsbm_generate_device: the graph of sbp_dcsbm_generate with the same
+ * parameters, edge for edge, generated on `device` (the planted labels and
+ * the degree CDF on the host, degrees, block members and edges on the
+ * device).  truth_out (N labels, may be NULL) receives the planted labels.
+ * Requires N * deg_max < 2^31.
+ *
+ * sbp_graph_shape / sbp_graph_download: sizes and a host copy of a resident
+ * graph's CSR pair (arrays sized as sbp_graph_csr; any pointer may be
+ * NULL). */
+struct sbp_dcsbm_params; /* defined with the host utilities below */
+sbp_status sbp_graph_from_device_edges(int32_t N, int32_t E, const int32_t* src,
+                                       const int32_t* dst, const uint32_t* w, int32_t device,
+                                       sbp_graph_dev** out);
+sbp_status sbp_dcsbm_generate_device(const struct sbp_dcsbm_params* p, int32_t device,
+                                     int32_t* truth_out, sbp_graph_dev** out);
+sbp_status sbp_graph_shape(const sbp_graph_dev* g, int32_t* N, int32_t* E);
+sbp_status sbp_graph_download(const sbp_graph_dev* g, int32_t* out_ptr, int32_t* out_idx,
+                              uint32_t* out_w, int32_t* in_ptr, int32_t* in_idx, uint32_t* in_w,
+                              uint32_t* deg_out, uint32_t* deg_in);
+
 /* ----------------------------------------------------------------- batched
  * Partitions `count` independent graphs in one call (no GSAP counterpart:
  * GSAP partitions one graph per process).  A multi-job engine advances every
