@@ -23,6 +23,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
+#include "dense.cuh"
 
 #include <algorithm>
 #include <map>
@@ -749,10 +750,12 @@ struct DenseLogsBody {
   }
 };
 
-// One warp per batch vertex that moves: its out-edges move from
-// (r, old block of w) to (s, new block of w); its in-edges from unmoved
-// sources move from (b(u), r) to (b(u), s).  Edges between two moved vertices
-// are handled once, from the source's out-edges.
+// The moved vertices of a batch: its out-edges move from (r, old block of
+// w) to (s, new block of w); its in-edges from unmoved sources move from
+// (b(u), r) to (b(u), s).  Edges between two moved vertices are handled
+// once, from the source's out-edges.  A lane per batch vertex finds the
+// moved ones (about a tenth of a batch once the first sweeps are done);
+// the warp then applies each moved vertex's entries together, lane-strided.
 struct DenseUpdateBody {
   using Args = DenseArgs;
   static constexpr int kThreads = 256, kMinBlocks = 1;
@@ -773,89 +776,58 @@ struct DenseUpdateBody {
   uint32_t *Md = a.Md, *MTd = a.MTd, *Sd = a.Sd, *d_out = a.d_out, *d_in = a.d_in;
   const int K = (B + 31) >> 5;
   const int lane = threadIdx.x & 31;
-  const int w0 = (vb * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (vg * blockDim.x) >> 5;
-  for (int i = w0; i < count; i += nw) {
-    const int v = lo + i;
-    const int r = part[v], s = newlab[i];
-    if (r == s) continue;
-    if (lane == 0) {
-      atomicSub(d_out + r, kdo[v]);
-      atomicAdd(d_out + s, kdo[v]);
-      atomicSub(d_in + r, kdi[v]);
-      atomicAdd(d_in + s, kdi[v]);
+  const int nw = (vg * kThreads) >> 5;
+  for (int w0 = ((vb * kThreads + threadIdx.x) >> 5) * 32; w0 < count; w0 += nw * 32) {
+    const int i = w0 + lane;
+    int32_t r0 = 0, s0 = 0;
+    if (i < count) {
+      r0 = part[lo + i];
+      s0 = newlab[i];
     }
-    for (int j = optr[v] + lane; j < optr[v + 1]; j += 32) {
-      const int x = __ldg(oidx + j);
-      const uint32_t wt = __ldg(ow + j);
-      const int bo = __ldg(part + x);
-      const int bn = (x >= lo && x < lo + count) ? newlab[x - lo] : bo;
-      atomicSub(Md + (size_t)r * B + bo, wt);
-      atomicSub(MTd + (size_t)bo * B + r, wt);
-      atomicAdd(Md + (size_t)s * B + bn, wt);
-      atomicAdd(MTd + (size_t)bn * B + s, wt);
-      atomicSub(sd_out(Sd, K, r, bo), wt);
-      atomicSub(sd_in(Sd, K, r, bo), wt);
-      atomicAdd(sd_out(Sd, K, s, bn), wt);
-      atomicAdd(sd_in(Sd, K, s, bn), wt);
-    }
-    for (int j = iptr[v] + lane; j < iptr[v + 1]; j += 32) {
-      const int u = __ldg(iidx + j);
-      const int bu = __ldg(part + u);
-      if (u >= lo && u < lo + count && newlab[u - lo] != bu) continue;  // moved source
-      const uint32_t wt = __ldg(iw + j);
-      atomicSub(Md + (size_t)bu * B + r, wt);
-      atomicSub(MTd + (size_t)r * B + bu, wt);
-      atomicAdd(Md + (size_t)bu * B + s, wt);
-      atomicAdd(MTd + (size_t)s * B + bu, wt);
-      atomicSub(sd_out(Sd, K, bu, r), wt);
-      atomicSub(sd_in(Sd, K, bu, r), wt);
-      atomicAdd(sd_out(Sd, K, bu, s), wt);
-      atomicAdd(sd_in(Sd, K, bu, s), wt);
+    unsigned moved = __ballot_sync(kFull, i < count && r0 != s0);
+    while (moved) {
+      const int src = __ffs(moved) - 1;
+      moved &= moved - 1;
+      const int v = lo + w0 + src;
+      const int r = __shfl_sync(kFull, r0, src), s = __shfl_sync(kFull, s0, src);
+      if (lane == 0) {
+        atomicSub(d_out + r, kdo[v]);
+        atomicAdd(d_out + s, kdo[v]);
+        atomicSub(d_in + r, kdi[v]);
+        atomicAdd(d_in + s, kdi[v]);
+      }
+      for (int j = optr[v] + lane; j < optr[v + 1]; j += 32) {
+        const int x = __ldg(oidx + j);
+        const uint32_t wt = __ldg(ow + j);
+        const int bo = __ldg(part + x);
+        const int bn = (x >= lo && x < lo + count) ? newlab[x - lo] : bo;
+        atomicSub(Md + (size_t)r * B + bo, wt);
+        atomicSub(MTd + (size_t)bo * B + r, wt);
+        atomicAdd(Md + (size_t)s * B + bn, wt);
+        atomicAdd(MTd + (size_t)bn * B + s, wt);
+        atomicSub(sd_out(Sd, K, r, bo), wt);
+        atomicSub(sd_in(Sd, K, r, bo), wt);
+        atomicAdd(sd_out(Sd, K, s, bn), wt);
+        atomicAdd(sd_in(Sd, K, s, bn), wt);
+      }
+      for (int j = iptr[v] + lane; j < iptr[v + 1]; j += 32) {
+        const int u = __ldg(iidx + j);
+        const int bu = __ldg(part + u);
+        if (u >= lo && u < lo + count && newlab[u - lo] != bu) continue;  // moved source
+        const uint32_t wt = __ldg(iw + j);
+        atomicSub(Md + (size_t)bu * B + r, wt);
+        atomicSub(MTd + (size_t)r * B + bu, wt);
+        atomicAdd(Md + (size_t)bu * B + s, wt);
+        atomicAdd(MTd + (size_t)s * B + bu, wt);
+        atomicSub(sd_out(Sd, K, bu, r), wt);
+        atomicSub(sd_in(Sd, K, bu, r), wt);
+        atomicAdd(sd_out(Sd, K, bu, s), wt);
+        atomicAdd(sd_in(Sd, K, bu, s), wt);
+      }
     }
   }
   }
 };
-
-// First column k of dense out-row ++ in-row of block b whose running count
-// exceeds t (zero columns never advance the count, so this is the same
-// entry as in the CSR rows); the whole warp returns it, or -1.  Found
-// through the rows' chunk sums (DevBM::Sd, 2K of them: the out-row's K
-// chunks, then the in-row's): the chunk whose running count first exceeds
-// t, then the column inside it, reading 2K + 32 words instead of up to 2B.
-__device__ int warp_pick_chunked(const uint32_t* orow, const uint32_t* irow,
-                                 const uint32_t* srow, int B, int K, uint64_t t, int lane) {
-  uint64_t acc = 0;
-  for (int k0 = 0; k0 < 2 * K; k0 += 32) {
-    const int k = k0 + lane;
-    const uint64_t w = k < 2 * K ? __ldg(srow + k) : 0u;
-    uint64_t incl = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint64_t y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const unsigned hit = __ballot_sync(kFull, k < 2 * K && acc + incl > t);
-    if (hit) {
-      const int j = __ffs(hit) - 1;
-      const uint64_t base = acc + __shfl_sync(kFull, incl - w, j);  // count before chunk k0+j
-      const int kc = k0 + j;
-      const int c0 = (kc < K ? kc : kc - K) * 32;
-      const uint32_t* row = kc < K ? orow : irow;
-      const int c = c0 + lane;
-      uint64_t in2 = c < B ? __ldg(row + c) : 0u;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint64_t y = __shfl_up_sync(kFull, in2, o);
-        if (lane >= o) in2 += y;
-      }
-      const unsigned h2 = __ballot_sync(kFull, c < B && base + in2 > t);
-      return h2 ? c0 + __ffs(h2) - 1 : -1;
-    }
-    acc += __shfl_sync(kFull, incl, 31);
-  }
-  return -1;
-}
 
 // Sum of cell_term over a dense row with the CSR loop's order: each chunk of
 // 32 columns hands its nonzeros, by their rank in the row, to lanes
@@ -922,21 +894,9 @@ struct BlockTermsDenseBody {
       a.sinfull[b] = row_total(ai, a.d_in[b], a.ld_in[b]);
     }
     }
-    if (a.draws) {
-      P4 x = draw(a.seed, kRngNodalBlock, seq, (uint32_t)b);
-      uint64_t deg = (uint64_t)a.d_out[b] + a.d_in[b];
-      int nb = 0;
-      if (deg > 0) {
-        const int K = (B + 31) >> 5;
-        int c = warp_pick_chunked(orow, irow, a.Sd + (size_t)b * 2 * K, B, K,
-                                  scale_draw(x.v[1], deg), lane);
-        nb = c >= 0 ? c : 0;
-      }
-      if (lane == 0) {
-        a.use_rand[b] = accept_random(x.v[0], deg, (uint64_t)B) ? 1 : 0;
-        a.nbr_s[b] = nb;
-      }
-    }
+    if (a.draws)
+      dense_block_draw(a.Md, a.MTd, a.Sd, a.d_out, a.d_in, B, a.seed, seq, b, lane, a.nbr_s,
+                       a.use_rand);
   }
   }
 };
@@ -1143,7 +1103,7 @@ DenseArgs dense_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m
 }
 
 int32_t vg_block_terms(int32_t B) { return grid_for((long long)B * 32, 256, 8192); }
-int32_t vg_dense_update(int32_t count) { return grid_for((long long)count * 32, 256, 148 * 16); }
+int32_t vg_dense_update(int32_t count) { return grid_for((long long)count, 256, 148 * 16); }
 
 const MultiKernel kmScanTile = multi_kernel_desc<ScanTileBody>("scan_tile");
 const MultiKernel kmScanSingle = multi_kernel_desc<ScanSingleBody>("scan_single");

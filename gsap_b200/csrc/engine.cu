@@ -336,8 +336,14 @@ void Engine::add_run_work(Run& r) {
         long long* slot_acc = r.sweeps_only ? J.acc + b : J.acc;
         const int32_t slot_mul = r.sweeps_only ? nb : 1;
         const int32_t lo = b * r.BS;
-        if (dense) add_block_terms_dense(s.bt_dense, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
-        else add_block_terms(s.bt_csr, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
+        // dense form: the tick's first batch draws here, every later one in
+        // the commit of the batch before it (its seq is always one more)
+        if (dense) {
+          if (k == 0 && b == 0)
+            add_block_terms_dense(s.bt_dense, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
+        } else {
+          add_block_terms(s.bt_csr, J.m, r.B, 1, r.o.seed, seq, ctl, nb);
+        }
         const int ms = md.slot(dense);
         add_nodal(s.nodal[ms], s.heavy[ms], dense, md, J.g, J.part, J.m, r.B, r.o.seed, seq, lo,
                   r.BS, J.newlab, J.rec, nullptr,
@@ -346,8 +352,9 @@ void Engine::add_run_work(Run& r) {
           // the moved vertices' edges, applied to the dense form before the
           // labels change (it reads old and new labels)
           add_dense_update(s.dupd, J.g, J.part, lo, r.BS, J.newlab, r.B, J.m, ctl);
+          const bool last = k == r.sweep_k - 1 && b == nb - 1;
           add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, slot_sum, slot_acc, &J.m,
-                     r.B, J.cs, ctl, slot_mul);
+                     r.B, J.cs, ctl, slot_mul, !last, r.o.seed, seq + 1, nb);
         } else {
           add_commit(s.commit, J.part, lo, r.BS, J.newlab, J.rec, slot_sum, slot_acc, nullptr,
                      0, J.cs, ctl, slot_mul);
@@ -696,6 +703,7 @@ sbp_status Engine::tick() {
   cudaError_t waited = cudaEventSynchronize(ev[2]);
   if (waited == cudaSuccess) waited = cudaEventElapsedTime(&ms_pre, ev[0], ev[1]);
   if (waited == cudaSuccess) waited = cudaEventElapsedTime(&ms_merge, ev[1], ev[2]);
+  std::vector<float> seg;  // verbose >= 3: each batch's four segments
   for (int q = 0; q < nbatch && waited == cudaSuccess; ++q) {
     cudaEvent_t* be = &ev[4 + 5 * q];
     float a = 0.f, b = 0.f, c = 0.f;
@@ -706,6 +714,12 @@ sbp_status Engine::tick() {
     t_nodal += a;
     t_kernel += b;
     t_rebuild += c;
+    if (trace >= 3 && waited == cudaSuccess) {
+      float d = 0.f, e = 0.f;
+      waited = cudaEventElapsedTime(&d, be[0], be[1]);
+      if (waited == cudaSuccess) waited = cudaEventElapsedTime(&e, be[2], be[3]);
+      seg.insert(seg.end(), {d, b, e, c});
+    }
   }
   if (waited == cudaSuccess) waited = cudaEventSynchronize(ev[3]);
   submit.lock();
@@ -828,6 +842,11 @@ sbp_status Engine::tick() {
                  "%.3f ms, device %.3f ms\n",
                  ticks, runs.size(), k_max, t_issued - t_start, t_waited - t_issued,
                  now_ms() - t_waited, (double)dev);
+    // per batch: block draws, nodal kernels, dense update + commit, rebuild (us)
+    for (size_t q = 0; q + 3 < seg.size(); q += 4)
+      std::fprintf(stderr, "[sbp]   batch %zu: draws %.1f us, nodal %.1f us, commit %.1f us, rebuild %.1f us\n",
+                   q / 4, 1000.0 * seg[q], 1000.0 * seg[q + 1], 1000.0 * seg[q + 2],
+                   1000.0 * seg[q + 3]);
   }
   return SBP_OK;
 }

@@ -56,7 +56,7 @@ struct CommitScratch {
   long long* part_cnt = nullptr;
   unsigned* ticket = nullptr;  // must be 0 between commits
 };
-constexpr int kCommitCtas = 64;
+constexpr int kCommitCtas = 256;
 
 // Scratch of one rebuild direction.
 struct RebuildDir {
@@ -185,10 +185,14 @@ void add_nodal(Slot& warp, Slot& heavy, bool dense, const ScoreMode& md, const D
                const DevBM& m, int32_t B, uint64_t seed, uint32_t seq, int32_t lo, int32_t count,
                int32_t* newlab, double* rec, int32_t* props, const NodalAux& lists,
                const int32_t* ctl = nullptr, uint32_t seq_mul = 0);
+// With draw_next (dense mode), the commit's extra CTAs also make the next
+// batch's per-block draws (the block-terms kernel's draws == 1 work) with RNG
+// sequence draw_seq + ctl[0] * draw_seq_mul, from M after the batch's moves.
 void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                 const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
                 int32_t B, const CommitScratch& cs, const int32_t* ctl = nullptr,
-                int32_t slot_mul = 0);
+                int32_t slot_mul = 0, bool draw_next = false, uint64_t seed = 0,
+                uint32_t draw_seq = 0, uint32_t draw_seq_mul = 0);
 // GSAP's merge grid (Q16, partition.hpp:335-336): when `on`, only the
 // proposal slots below the nnz of the out CSR, rounded up to 256, are drawn
 // and scored; the others keep the targets, dS (dS) and in-row terms (dsin)

@@ -39,6 +39,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "multi.cuh"
+#include "dense.cuh"
 
 namespace sbp {
 
@@ -1299,11 +1300,15 @@ struct NodalHeavyBody {
 };
 
 // Applies the batch's labels and sums its recorded dS.  Each CTA sums a fixed
-// slice in a fixed order into its own partial; the last CTA to finish (a
-// ticket, no waiting) adds the partials in CTA order, so the result does
-// not depend on scheduling.  In dense mode the CTAs also refresh the log2 of
-// the block degrees that dense_update changed.
-constexpr int kCommitThreads = 512;
+// slice (one vertex a thread) in a fixed order into its own partial; the
+// last CTA to finish (a ticket, no waiting) adds the partials with one warp
+// in a fixed order, so the result does not depend on scheduling.  In dense
+// mode the CTAs also refresh the log2 of the block degrees that
+// dense_update changed, and the virtual blocks past `ncommit` (if any) make
+// the next batch's per-block draws: they read only M, its chunk sums and the
+// block degrees, all final once dense_update has run, so the draws need no
+// launch of their own.
+constexpr int kCommitThreads = 256;
 
 struct CommitArgs {
   int32_t* part;
@@ -1317,7 +1322,15 @@ struct CommitArgs {
   long long* part_cnt;
   unsigned* ticket;
   const int32_t* ctl;  // sweep control: gate, and slots advance ctl[0] * slot_mul
+  // dense mode, draws for the next batch (RNG sequence draw_seq + ctl[0] *
+  // draw_seq_mul) by the virtual blocks past ncommit
+  const uint32_t *Md, *MTd, *Sd;
+  int32_t* nbr_s;
+  uint8_t* use_rand;
+  uint64_t seed;
+  uint32_t draw_seq, draw_seq_mul;
   int32_t lo, count, B, slot_mul;
+  int32_t ncommit, pad;
 };
 
 struct CommitBody {
@@ -1326,61 +1339,79 @@ struct CommitBody {
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
     if (ctl_stopped(a.ctl)) return;
-    __shared__ double sh[kCommitThreads];
-    __shared__ long long shc[kCommitThreads];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (vb >= a.ncommit) {
+      const uint32_t seq = a.draw_seq + ctl_itr(a.ctl) * a.draw_seq_mul;
+      const int nw = ((vg - a.ncommit) * kCommitThreads) >> 5;
+      for (int b = ((vb - a.ncommit) * kCommitThreads + tid) >> 5; b < a.B; b += nw)
+        dense_block_draw(a.Md, a.MTd, a.Sd, a.d_out, a.d_in, a.B, a.seed, seq, b, lane,
+                         a.nbr_s, a.use_rand);
+      return;
+    }
+    const int nc = a.ncommit;
+    __shared__ double sh[kCommitThreads / 32];
+    __shared__ long long shc[kCommitThreads / 32];
     __shared__ bool last;
-    const int tid = threadIdx.x;
     double s = 0.0;
     long long c = 0;
-    for (int i = vb * kCommitThreads + tid; i < a.count; i += vg * kCommitThreads) {
-      int32_t nl = a.newlab[i];
-      if (a.part[a.lo + i] != nl) {
+    for (int i = vb * kCommitThreads + tid; i < a.count; i += nc * kCommitThreads) {
+      const int32_t nl = a.newlab[i];
+      const int32_t old = a.part[a.lo + i];
+      const double x = a.rec[i];
+      if (old != nl) {
         a.part[a.lo + i] = nl;
         ++c;
       }
-      s += a.rec[i];
+      s += x;
     }
     if (a.ld_out)
-      for (int b = vb * kCommitThreads + tid; b < a.B; b += vg * kCommitThreads) {
+      for (int b = vb * kCommitThreads + tid; b < a.B; b += nc * kCommitThreads) {
         a.ld_out[b] = log2((double)a.d_out[b]);
         a.ld_in[b] = log2((double)a.d_in[b]);
       }
-    sh[tid] = s;
-    shc[tid] = c;
-    __syncthreads();
-    for (int o = kCommitThreads / 2; o > 0; o >>= 1) {
-      if (tid < o) {
-        sh[tid] += sh[tid + o];
-        shc[tid] += shc[tid + o];
-      }
-      __syncthreads();
+    s = warp_sum(s);
+    c = warp_sum_ll(c);
+    if (lane == 0) {
+      sh[wid] = s;
+      shc[wid] = c;
     }
+    __syncthreads();
     if (tid == 0) {
-      a.part_sum[vb] = sh[0];
-      a.part_cnt[vb] = shc[0];
+      double t = 0.0;
+      long long n = 0;
+      for (int k = 0; k < kCommitThreads / 32; ++k) {
+        t += sh[k];
+        n += shc[k];
+      }
+      a.part_sum[vb] = t;
+      a.part_cnt[vb] = n;
       __threadfence();
-      last = atomicAdd(a.ticket, 1u) == (unsigned)vg - 1u;
+      last = atomicAdd(a.ticket, 1u) == (unsigned)nc - 1u;
     }
     __syncthreads();
-    if (last && tid == 0) {
+    if (last && wid == 0) {
       __threadfence();
       double t = 0.0;
       long long n = 0;
-      for (int k = 0; k < vg; ++k) {
+      for (int k = lane; k < nc; k += 32) {
         t += ((volatile double*)a.part_sum)[k];
         n += ((volatile long long*)a.part_cnt)[k];
       }
-      const int k = (int)ctl_itr(a.ctl) * a.slot_mul;
-      a.slot_sum[k] += t;
-      a.slot_acc[k] += n;
-      *a.ticket = 0u;
+      t = warp_sum(t);
+      n = warp_sum_ll(n);
+      if (lane == 0) {
+        const int k = (int)ctl_itr(a.ctl) * a.slot_mul;
+        a.slot_sum[k] += t;
+        a.slot_acc[k] += n;
+        *a.ticket = 0u;
+      }
     }
   }
 };
 
 // CTAs of one commit: a function of the batch size only.
 int32_t vg_commit(int32_t count) {
-  return std::max(1, std::min(kCommitCtas, ceil_div(count, kCommitThreads * 4)));
+  return std::max(1, std::min(kCommitCtas, ceil_div(count, kCommitThreads)));
 }
 
 CommitArgs commit_args(int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
@@ -1404,6 +1435,7 @@ CommitArgs commit_args(int32_t* part, int32_t lo, int32_t count, const int32_t* 
   a.ticket = cs.ticket;
   a.lo = lo;
   a.count = count;
+  a.ncommit = vg_commit(count);
   return a;
 }
 
@@ -1566,11 +1598,25 @@ void add_nodal(Slot& warp, Slot& heavy, bool dense, const ScoreMode& md, const D
 
 void add_commit(Slot& s, int32_t* part, int32_t lo, int32_t count, const int32_t* newlab,
                 const double* rec, double* slot_sum, long long* slot_acc, const DevBM* dense_m,
-                int32_t B, const CommitScratch& cs, const int32_t* ctl, int32_t slot_mul) {
+                int32_t B, const CommitScratch& cs, const int32_t* ctl, int32_t slot_mul,
+                bool draw_next, uint64_t seed, uint32_t draw_seq, uint32_t draw_seq_mul) {
   CommitArgs a = commit_args(part, lo, count, newlab, rec, slot_sum, slot_acc, dense_m, B, cs);
   a.ctl = ctl;
   a.slot_mul = slot_mul;
-  slot_push(slot_bind(s, kmCommit), a, vg_commit(count));
+  int32_t vg = a.ncommit;
+  if (draw_next && dense_m) {
+    a.Md = dense_m->Md;
+    a.MTd = dense_m->MTd;
+    a.Sd = dense_m->Sd;
+    a.nbr_s = dense_m->nbr_s;
+    a.use_rand = dense_m->use_rand;
+    a.seed = seed;
+    a.draw_seq = draw_seq;
+    a.draw_seq_mul = draw_seq_mul;
+    // a warp per block, as the block-terms kernel
+    vg += std::max(1, std::min(8192, ceil_div((long long)B * 32, kCommitThreads)));
+  }
+  slot_push(slot_bind(s, kmCommit), a, vg);
 }
 
 }  // namespace sbp

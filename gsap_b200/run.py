@@ -30,7 +30,7 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--verbose", "-v", action="count", default=0,
-                    help="-v: one line per outer step; -vv: also one line per engine tick")
+                    help="-v: one line per outer step; -vv: also one line per engine tick; -vvv: also the event-timed segments of every nodal batch")
     ap.add_argument("--dense-max", type=int, default=None,
                     help="largest B kept in the dense blockmodel form")
     ap.add_argument("--exact", action="store_true",

@@ -69,7 +69,8 @@ typedef struct sbp_options {
   int32_t max_outer;       /* cap on merge/golden-section steps (no reference counterpart) */
   int32_t device;          /* CUDA device ordinal, -1 = current device */
   int32_t use_graphs;      /* ticks of queued nodal sweeps as CUDA graphs (default 1) */
-  int32_t verbose;         /* 1: one line per outer step on stderr; 2: also one per engine tick */
+  int32_t verbose;         /* 1: one line per outer step on stderr; 2: also one per engine tick;
+                              3: also each nodal batch's event-timed segments */
   int32_t dense_max;       /* keep M as dense B x B matrices while B <= dense_max
                               (0 = always CSR); default -1 = automatic:
                               max(4096, sqrt(32 E)), at most N */
