@@ -692,6 +692,8 @@ sbp_status check_options(const sbp_options* o) {
   if (o->mh && !(o->beta >= 0.0 && o->beta < 1e300))
     return fail(SBP_ERR_INVALID, "beta must be finite and >= 0");
   if (o->ref_grid < -1 || o->ref_grid > 1) return fail(SBP_ERR_INVALID, "ref_grid must be -1, 0 or 1");
+  if (o->phase_timing != 0 && o->phase_timing != 1)
+    return fail(SBP_ERR_INVALID, "phase_timing must be 0 or 1");
   return SBP_OK;
 }
 
@@ -789,6 +791,7 @@ void sbp_default_options(sbp_options* o) {
   o->mh = 0;
   o->beta = 3.0;
   o->ref_grid = -1;
+  o->phase_timing = 0;
 }
 
 const char* sbp_status_string(sbp_status s) {

@@ -302,7 +302,10 @@ void Engine::add_run_work(Run& r) {
   const bool dense = r.dense();
   if (r.stage == Run::kMerge) {
     // the merge kernels read the CSR form
-    if (!r.csr_fresh) add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
+    if (!r.csr_fresh) {
+      add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
+      r.pre_bytes += 4.0 * N + 24.0 * J.E + 16.0 * r.nnz_now + 8.0 * r.B;
+    }
     add_block_terms(m_bt, J.m, r.B, 0, r.o.seed, 0);
     const MergeGrid grid = merge_grid(J, r.o);
     add_merge_props(m_props, J.m, r.B, J.np, r.o.seed, r.seq, J.props, grid);
@@ -318,8 +321,13 @@ void Engine::add_run_work(Run& r) {
   }
   if (r.stage == Run::kSweep) {
     if (r.build) {
-      if (dense) add_dense_build(pre_dense, J.g, J.part, r.B, J.m);
-      else add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
+      if (dense) {
+        add_dense_build(pre_dense, J.g, J.part, r.B, J.m);
+        r.pre_bytes += 8.0 * r.B * (double)r.B + 12.0 * J.E;  // zero M, M^T; add the edges
+      } else {
+        add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
+        r.pre_bytes += 4.0 * N + 24.0 * J.E + 16.0 * r.nnz_now + 8.0 * r.B;
+      }
     }
     const int nb = r.o.num_batches;
     const RebuildTune tune = tune_for(J, r.B);
@@ -450,6 +458,11 @@ sbp_status Engine::tick() {
   use_graphs = true;
   for (Run* r : runs)
     if (r->stage != Run::kDone && !r->o.use_graphs) use_graphs = false;
+  // per-batch phase events when any active run asks for them (an event node
+  // costs a few microseconds of device time, five of them every batch)
+  bool timing = trace >= 3;
+  for (Run* r : runs)
+    if (r->stage != Run::kDone && r->o.phase_timing) timing = true;
   // pass 1: sweeps to queue, uploads (maps, batch lists) and readbacks
   size_t up = 0, rd = 0;
   int nb_max = 0, k_max = 0;
@@ -582,10 +595,10 @@ sbp_status Engine::tick() {
       for (int b = 0; b < nb_max; ++b) {
         SweepSlots& w = sw[k * nb_max + b];
         cudaEvent_t* be = &ev[4 + 5 * (k * nb_max + b)];
-        SBP_CUDA(record(be[0]));
+        if (timing) SBP_CUDA(record(be[0]));
         sbp_status q = emit_until(&w.bt_dense);
         if (q != SBP_OK) return q;
-        SBP_CUDA(record(be[1]));
+        if (timing) SBP_CUDA(record(be[1]));
         bool heavy = false;
         for (const Slot& x : w.heavy) heavy = heavy || !x.empty();
         if (heavy) {
@@ -602,13 +615,13 @@ sbp_status Engine::tick() {
         q = emit_until(&w.nodal[3]);
         if (q != SBP_OK) return q;
         if (heavy) SBP_CUDA(cudaStreamWaitEvent(st, join, 0));
-        SBP_CUDA(record(be[2]));
+        if (timing) SBP_CUDA(record(be[2]));
         q = emit_until(&w.commit);
         if (q != SBP_OK) return q;
-        SBP_CUDA(record(be[3]));
+        if (timing) SBP_CUDA(record(be[3]));
         q = emit_until(w.rebuild.all().back());
         if (q != SBP_OK) return q;
-        SBP_CUDA(record(be[4]));
+        if (timing) SBP_CUDA(record(be[4]));
       }
       sbp_status q = emit_until(&ends[k].ctl);
       if (q != SBP_OK) return q;
@@ -636,6 +649,7 @@ sbp_status Engine::tick() {
     };
     mix(&k_max, sizeof(k_max));
     mix(&nb_max, sizeof(nb_max));
+    mix(&timing, sizeof(timing));
     for (size_t q = sweep_first; q < order.size(); ++q) {
       const Slot* x = order[q];
       if (x == &s_gather || x->empty()) continue;
@@ -704,7 +718,7 @@ sbp_status Engine::tick() {
   if (waited == cudaSuccess) waited = cudaEventElapsedTime(&ms_pre, ev[0], ev[1]);
   if (waited == cudaSuccess) waited = cudaEventElapsedTime(&ms_merge, ev[1], ev[2]);
   std::vector<float> seg;  // verbose >= 3: each batch's four segments
-  for (int q = 0; q < nbatch && waited == cudaSuccess; ++q) {
+  for (int q = 0; q < nbatch && waited == cudaSuccess && timing; ++q) {
     cudaEvent_t* be = &ev[4 + 5 * q];
     float a = 0.f, b = 0.f, c = 0.f;
     waited = cudaEventSynchronize(be[4]);
@@ -731,6 +745,8 @@ sbp_status Engine::tick() {
   for (Run* r : runs) {
     if (r->stage == Run::kDone) continue;
     r->R.ms_rebuild += ms_pre;
+    r->R.bytes_rebuild += r->pre_bytes;
+    r->pre_bytes = 0.0;
     const char* rdp = (const char*)rd_host + r->rd_off;
     r->init = false;
     r->upload_lists = false;
@@ -787,8 +803,9 @@ sbp_status Engine::tick() {
           r->R.nodal_launches += 1;
           r->R.bytes_nodal += 28.0 * r->BS + 12.0 * r->batch_entries[b] +
                               16.0 * r->nnz_now + 8.0 * r->B;
-          r->R.bytes_rebuild += dense ? 12.0 * r->batch_entries[b] + 8.0 * (double)r->B * r->B
-                                      : 4.0 * J.N + 24.0 * J.E + 16.0 * r->nnz_now + 8.0 * r->B;
+          // a CSR batch's rebuild; a dense batch's incremental update runs
+          // inside the nodal phase and is not counted
+          if (!dense) r->R.bytes_rebuild += 4.0 * J.N + 24.0 * J.E + 16.0 * r->nnz_now + 8.0 * r->B;
         }
       r->seq = r->seq_sweep0 + (uint32_t)ctl[0] * (uint32_t)nb;
       if (!dense) r->nnz_now = (double)nnz;

@@ -57,6 +57,7 @@ struct Run {
   std::vector<int32_t> lists_all, list_off, list_n;
   std::vector<double> batch_entries;
   double nnz_now = 0.0;
+  double pre_bytes = 0.0;  // algorithmic bytes of this tick's builds before the merge or sweeps
   // device work left pending by the last host decision
   bool init = false, upload_lists = false, build = false, zero_itr = false;
   bool csr_fresh = false;

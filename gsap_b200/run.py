@@ -39,6 +39,8 @@ def main(argv=None):
                     help="accept nodal moves by Metropolis-Hastings")
     ap.add_argument("--beta", type=float, default=3.0,
                     help="inverse temperature of the Metropolis-Hastings test, per nat")
+    ap.add_argument("--no-phase-timing", action="store_true",
+                    help="leave out the per-batch CUDA events that time each phase")
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch the queued sweeps directly instead of as CUDA graphs")
     a = ap.parse_args(argv)
@@ -53,7 +55,8 @@ def main(argv=None):
     for i in range(a.repeat):
         t0 = time.perf_counter()
         kw = {} if a.dense_max is None else {"dense_max": a.dense_max}
-        kw.update(exact=int(a.exact), mh=int(a.mh), beta=a.beta, use_graphs=int(not a.no_graphs))
+        kw.update(exact=int(a.exact), mh=int(a.mh), beta=a.beta, use_graphs=int(not a.no_graphs),
+                  phase_timing=int(not a.no_phase_timing))
         rep = sbp.partition(g, seed=a.seed + i, device=a.device, verbose=int(a.verbose), **kw)
         rep["wall_ms"] = (time.perf_counter() - t0) * 1000.0
         rep["N"], rep["E"] = g.N, g.E

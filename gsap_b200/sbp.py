@@ -52,7 +52,7 @@ class Options(C.Structure):
                 ("threshold2", C.c_float), ("window", C.c_int32), ("max_outer", C.c_int32),
                 ("device", C.c_int32), ("use_graphs", C.c_int32), ("verbose", C.c_int32),
                 ("dense_max", C.c_int32), ("exact", C.c_int32), ("mh", C.c_int32),
-                ("beta", C.c_double), ("ref_grid", C.c_int32)]
+                ("beta", C.c_double), ("ref_grid", C.c_int32), ("phase_timing", C.c_int32)]
 
 
 class Report(C.Structure):
