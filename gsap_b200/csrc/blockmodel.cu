@@ -647,10 +647,13 @@ struct BlockTermsBody {
     if (a.draws != 1) {
     double acc = 0.0;
     // the row's k-th nonzero is added by lane k % 32, in order of k
+    // (unrolled so that several entries' loads are in flight at once)
+#pragma unroll 4
     for (int i = a.optr[b] + lane; i < a.optr[b + 1]; i += 32)
       acc += cell_term(a.xlx, a.ocnt[i], a.ld_in[a.ocol[i]]);
     double ao = warp_sum(acc);
     acc = 0.0;
+#pragma unroll 4
     for (int i = a.iptr[b] + lane; i < a.iptr[b + 1]; i += 32)
       acc += cell_term(a.xlx, a.icnt[i], a.ld_out[a.icol[i]]);
     double ai = warp_sum(acc);
@@ -756,6 +759,10 @@ struct DenseLogsBody {
 // once, from the source's out-edges.  A lane per batch vertex finds the
 // moved ones (about a tenth of a batch once the first sweeps are done);
 // the warp then applies each moved vertex's entries together, lane-strided.
+// A warp covers kDuVerts batch vertices, so that the moved ones (a few per
+// warp at most) are spread over many warps: their dependent loads are the
+// latency of the launch.
+constexpr int kDuVerts = 8;
 struct DenseUpdateBody {
   using Args = DenseArgs;
   static constexpr int kThreads = 256, kMinBlocks = 1;
@@ -777,14 +784,15 @@ struct DenseUpdateBody {
   const int K = (B + 31) >> 5;
   const int lane = threadIdx.x & 31;
   const int nw = (vg * kThreads) >> 5;
-  for (int w0 = ((vb * kThreads + threadIdx.x) >> 5) * 32; w0 < count; w0 += nw * 32) {
+  for (int w0 = ((vb * kThreads + threadIdx.x) >> 5) * kDuVerts; w0 < count;
+       w0 += nw * kDuVerts) {
     const int i = w0 + lane;
     int32_t r0 = 0, s0 = 0;
-    if (i < count) {
+    if (lane < kDuVerts && i < count) {
       r0 = part[lo + i];
       s0 = newlab[i];
     }
-    unsigned moved = __ballot_sync(kFull, i < count && r0 != s0);
+    unsigned moved = __ballot_sync(kFull, lane < kDuVerts && i < count && r0 != s0);
     while (moved) {
       const int src = __ffs(moved) - 1;
       moved &= moved - 1;
@@ -833,23 +841,40 @@ struct DenseUpdateBody {
 // 32 columns hands its nonzeros, by their rank in the row, to lanes
 // (rank % 32) through a 32-slot shared buffer of the warp, so every lane adds
 // the same terms in the same order as over the row's CSR entries.
+// Four chunks at a time: their counts, degrees and cell terms are loaded and
+// computed first (independent loads in flight together), then handed out
+// chunk by chunk in the same order as one chunk at a time.
 __device__ __forceinline__ double dense_row_sum(const double* tab, const uint32_t* row,
                                                 const double* ld, int B, int lane,
                                                 double* buf) {
+  constexpr int U = 4;
   double acc = 0.0;
   int k = 0;  // nonzeros before this chunk
   const unsigned lt = (1u << lane) - 1u;
-  for (int c0 = 0; c0 < B; c0 += 32) {
-    const int c = c0 + lane;
-    const uint32_t m = c < B ? row[c] : 0u;
-    const unsigned nz = __ballot_sync(kFull, m != 0u);
-    if (nz == 0u) continue;
-    const int n = __popc(nz);
-    if (m) buf[(k + __popc(nz & lt)) & 31] = cell_term(tab, m, ld[c]);
-    __syncwarp();
-    if (((lane - k) & 31) < n) acc += buf[lane];
-    __syncwarp();
-    k += n;
+  for (int c0 = 0; c0 < B; c0 += 32 * U) {
+    uint32_t m[U];
+    double t[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int c = c0 + 32 * u + lane;
+      m[u] = c < B ? row[c] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int c = c0 + 32 * u + lane;
+      t[u] = m[u] ? cell_term(tab, m[u], ld[c]) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const unsigned nz = __ballot_sync(kFull, m[u] != 0u);
+      if (nz == 0u) continue;
+      const int n = __popc(nz);
+      if (m[u]) buf[(k + __popc(nz & lt)) & 31] = t[u];
+      __syncwarp();
+      if (((lane - k) & 31) < n) acc += buf[lane];
+      __syncwarp();
+      k += n;
+    }
   }
   return acc;
 }
@@ -1103,7 +1128,9 @@ DenseArgs dense_args(const DevGraph& g, const int32_t* part, int32_t B, DevBM& m
 }
 
 int32_t vg_block_terms(int32_t B) { return grid_for((long long)B * 32, 256, 8192); }
-int32_t vg_dense_update(int32_t count) { return grid_for((long long)count, 256, 148 * 16); }
+int32_t vg_dense_update(int32_t count) {
+  return grid_for((long long)count, 256 / 32 * kDuVerts, 148 * 16);
+}
 
 const MultiKernel kmScanTile = multi_kernel_desc<ScanTileBody>("scan_tile");
 const MultiKernel kmScanSingle = multi_kernel_desc<ScanSingleBody>("scan_single");
