@@ -104,7 +104,7 @@ void Run::after_sweep(double dsum, double dataS, long long acc) {
     return;
   }
   if (o.verbose)
-    std::fprintf(stderr, "[sbp] step %d B=%d S=%.6f itrs=%d\n", R.outer_steps, B, S,
+    std::fprintf(stderr, "[sbp] step %d B=%d S=%.17g itrs=%d\n", R.outer_steps, B, S,
                  R.nodal_itrs);
   Bracket P;
   P.B = B;

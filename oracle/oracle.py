@@ -77,6 +77,7 @@ _sig("orc_merge_step_mode", C.c_int32, _GP, _vp, C.c_int32, C.c_int32, C.c_int32
      C.c_uint32, C.c_int32, _vp, _vp)
 _sig("orc_apply_merges", C.c_int32, C.c_int32, _vp, C.c_int32, C.c_int32, _vp, _vp)
 _sig("orc_partition", C.c_int, _GP, C.POINTER(Options), _vp, C.POINTER(Report))
+_sig("orc_partition_trace", C.c_int, _GP, C.POINTER(Options), _vp, _vp, _vp, _vp, C.c_int32)
 _sig("orc_time_nodal", C.c_double, _GP, _vp, C.c_int32, C.c_uint64, C.c_int32, C.c_int32)
 _sig("orc_evaluate", None, C.c_int32, _vp, _vp, _vp)
 
@@ -245,6 +246,23 @@ def partition(g, **kw):
     r = Report()
     st = _lib.orc_partition(C.byref(_g(g)), C.byref(o), _p(lab), C.byref(r))
     return lab, {k: getattr(r, k) for k, _ in r._fields_}, st
+
+
+def partition_trace(g, max_steps=1000, **kw):
+    """orc_partition with its outer-step trace: labels and a list of (B, S,
+    cumulative sweeps) per outer step, in the order the golden section saw
+    them."""
+    o = default_options(**kw)
+    lab = np.zeros(g.N, np.int32)
+    sb = np.zeros(max_steps, np.int32)
+    ss = np.zeros(max_steps, np.float64)
+    si = np.zeros(max_steps, np.int32)
+    n = _lib.orc_partition_trace(C.byref(_g(g)), C.byref(o), _p(lab), _p(sb), _p(ss), _p(si),
+                                 max_steps)
+    if n < 0:
+        raise RuntimeError("oracle partition failed")
+    n = min(n, max_steps)
+    return lab, [(int(sb[i]), float(ss[i]), int(si[i])) for i in range(n)]
 
 
 def time_nodal(g, part, B, seed, batches, num_batches=4):

@@ -925,9 +925,19 @@ inline double ms_since(Clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
 }
 
+// One outer step as the golden section sees it: the step's B, its MDL after
+// the nodal sweeps, and the sweeps run so far in the whole partition.
+struct TraceStep {
+  int32_t B;
+  double S;
+  int32_t itrs;
+};
+
 // partition.hpp:852-954 (partition) with the golden-section bookkeeping of
-// partition.hpp:80-322 (prepare_for_partition_next).
-int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep) {
+// partition.hpp:80-322 (prepare_for_partition_next).  trace (optional)
+// receives one record per outer step.
+int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep,
+                  std::vector<TraceStep>* trace = nullptr) {
   auto t_all = Clock::now();
   Report R{};
   int32_t N = g.N;
@@ -995,6 +1005,7 @@ int run_partition(const Graph& g, const Options& o, int32_t* labels, Report* rep
         }
       }
     }
+    if (trace) trace->push_back(TraceStep{B, S, R.nodal_itrs});
     // golden section (partition.hpp:80-322)
     Snapshot P;
     P.B = B;
@@ -1426,6 +1437,30 @@ int orc_partition(const orc_graph* xg, const orc_options* xo, int32_t* labels, o
     rep->ms_rebuild = R.ms_rebuild; rep->status = R.status;
   }
   return st;
+}
+
+// orc_partition with the outer-step trace: up to max_steps records of the
+// step's B, MDL and cumulative sweeps; returns the number of steps (or -1
+// on a failed run).
+int orc_partition_trace(const orc_graph* xg, const orc_options* xo, int32_t* labels,
+                        int32_t* steps_B, double* steps_S, int32_t* steps_itrs,
+                        int32_t max_steps) {
+  Graph g = to_graph(xg);
+  Options o{xo->seed, xo->num_proposals, xo->reduction_rate, xo->max_nodal_itr, xo->num_batches,
+            xo->threshold1, xo->threshold2, xo->window, xo->max_outer, Mode(),
+            xo->ref_grid < 0 ? (xo->exact == 0 ? 1 : 0) : xo->ref_grid};
+  o.mode.exact = xo->exact;
+  o.mode.mh = xo->mh;
+  o.mode.beta = xo->beta;
+  std::vector<TraceStep> tr;
+  if (run_partition(g, o, labels, nullptr, &tr) != 0) return -1;
+  const int32_t n = std::min<int32_t>((int32_t)tr.size(), max_steps);
+  for (int32_t i = 0; i < n; ++i) {
+    steps_B[i] = tr[i].B;
+    steps_S[i] = tr[i].S;
+    steps_itrs[i] = tr[i].itrs;
+  }
+  return (int32_t)tr.size();
 }
 
 // Time nodal batches only (the CPU baseline sample): runs `batches` Jacobi

@@ -263,3 +263,4 @@ def test_partition_same_bits_in_both_forms(sbp, variant, N, B, seed):
         assert np.array_equal(lab, out[0][0])
         assert rep["S"] == out[0][1]["S"] and rep["B"] == out[0][1]["B"]
         assert rep["nodal_itrs"] == out[0][1]["nodal_itrs"]
+
