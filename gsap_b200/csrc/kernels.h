@@ -231,6 +231,7 @@ struct MergeApplyBufs {
 };
 constexpr int kMaRounds = 31, kMaSelPasses = 8;
 struct MergeApplySlots {
+  Slot fused;  // the whole application in one CTA (small B)
   Slot keys, cyc[kMaRounds], mark, hist[kMaSelPasses], pick[kMaSelPasses], parent,
       rootj[kMaRounds], scan[3], map;
   void clear();

@@ -315,6 +315,92 @@ struct MaMapBody {
   }
 };
 
+// Rounds of pointer doubling that cover B: 2^L >= B.
+__host__ __device__ __forceinline__ int ma_rounds(int32_t B) {
+  int L = 1;
+  while (L < 31 && (1ll << L) < (long long)B) ++L;
+  return L;
+}
+
+// Every step above in one CTA for B <= kMaFusedMax: the same bodies on a
+// virtual grid of one block, in the order the separate launches take, with
+// a CTA barrier between them instead of a launch (global writes of one
+// body are visible to the whole CTA after the barrier).  At the block counts
+// of the golden-section phase this is one launch per merge step instead of
+// about forty, with the same bits.
+constexpr int kMaFusedMax = 4096;
+struct MaFusedBody {
+  using Args = MaArgs;
+  static constexpr int kThreads = kMaThreads, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a0, int, int) {
+    __shared__ int sh[kMaThreads / 32 + 1];
+    MaArgs a = a0;
+    const int L = ma_rounds(a.B);
+    MaKeysBody::run(a, 0, 1);
+    __syncthreads();
+    for (int r = 0; r < L; ++r) {
+      a.round = r;
+      MaCycleJumpBody::run(a, 0, 1);
+      __syncthreads();
+    }
+    a.round = L;
+    MaMarkBody::run(a, 0, 1);
+    __syncthreads();
+    for (int q = 0; q < kSelPasses; ++q) {
+      a.pass = q;
+      MaSelHistBody::run(a, 0, 1);
+      __syncthreads();
+      MaSelPickBody::run(a, 0, 1);
+      __syncthreads();
+    }
+    MaParentBody::run(a, 0, 1);
+    __syncthreads();
+    for (int r = 0; r < L; ++r) {
+      a.round = r;
+      MaRootJumpBody::run(a, 0, 1);
+      __syncthreads();
+    }
+    // exclusive scan of the root flags into new ids, newid[B] = the count:
+    // each thread a contiguous run of ceil(B / 256) flags
+    {
+      const int per = (a.B + kMaThreads - 1) / kMaThreads;
+      const int b0 = threadIdx.x * per, b1 = min(a.B, b0 + per);
+      int local = 0;
+      for (int b = b0; b < b1; ++b) local += a.w.root[b];
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      int incl = local;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) sh[wid] = incl;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int run = 0;
+        for (int k = 0; k < kMaThreads / 32; ++k) {
+          const int c = sh[k];
+          sh[k] = run;
+          run += c;
+        }
+        sh[kMaThreads / 32] = run;
+      }
+      __syncthreads();
+      int pre = sh[wid] + incl - local;
+      for (int b = b0; b < b1; ++b) {
+        const int f = a.w.root[b];
+        a.w.newid[b] = pre;
+        pre += f;
+      }
+      if (threadIdx.x == 0) a.w.newid[a.B] = sh[kMaThreads / 32];
+      __syncthreads();
+    }
+    a.round = L;
+    MaMapBody::run(a, 0, 1);
+  }
+};
+
 const MultiKernel kmMaKeys = multi_kernel_desc<MaKeysBody>("ma_keys");
 const MultiKernel kmMaCycle = multi_kernel_desc<MaCycleJumpBody>("ma_cycle_jump");
 const MultiKernel kmMaMark = multi_kernel_desc<MaMarkBody>("ma_mark");
@@ -323,15 +409,12 @@ const MultiKernel kmMaPick = multi_kernel_desc<MaSelPickBody>("ma_select_pick");
 const MultiKernel kmMaParent = multi_kernel_desc<MaParentBody>("ma_parent");
 const MultiKernel kmMaRoot = multi_kernel_desc<MaRootJumpBody>("ma_root_jump");
 const MultiKernel kmMaMap = multi_kernel_desc<MaMapBody>("ma_map");
+const MultiKernel kmMaFused = multi_kernel_desc<MaFusedBody>("ma_fused");
 
 int32_t vg_ma(int32_t B) { return std::max(1, std::min(ceil_div(B, kMaThreads), 148 * 8)); }
 
 // Rounds of pointer doubling that cover B: 2^L >= B.
-int rounds_for(int32_t B) {
-  int L = 1;
-  while (L < 31 && (1ll << L) < (long long)B) ++L;
-  return L;
-}
+int rounds_for(int32_t B) { return ma_rounds(B); }
 
 MaArgs ma_args(const MergeApplyBufs& w, int32_t B, int32_t K, const int32_t* best,
                const double* best_dS, int32_t* map, int32_t* out) {
@@ -393,7 +476,7 @@ void MergeApplySlots::clear() {
 }
 
 std::vector<Slot*> MergeApplySlots::all() {
-  std::vector<Slot*> v{&keys};
+  std::vector<Slot*> v{&fused, &keys};
   for (Slot& s : cyc) v.push_back(&s);
   v.push_back(&mark);
   for (int p = 0; p < kMaSelPasses; ++p) {
@@ -411,6 +494,10 @@ void add_merge_apply(MergeApplySlots& s, const MergeApplyBufs& w, int32_t B, int
                      const int32_t* best, const double* best_dS, int32_t* map, int32_t* out) {
   if (B <= 0) return;
   MaArgs a = ma_args(w, B, K, best, best_dS, map, out);
+  if (B <= kMaFusedMax) {
+    slot_push(slot_bind(s.fused, kmMaFused), a, 1);
+    return;
+  }
   const int32_t vg = vg_ma(B);
   const int L = rounds_for(B);
   slot_push(slot_bind(s.keys, kmMaKeys), a, vg);
@@ -439,6 +526,10 @@ void merge_apply(const MergeApplyBufs& w, int32_t B, int32_t K, const int32_t* b
                  const double* best_dS, int32_t* map, int32_t* out, cudaStream_t st) {
   if (B <= 0) return;
   MaArgs a = ma_args(w, B, K, best, best_dS, map, out);
+  if (B <= kMaFusedMax) {
+    launch_single<MaFusedBody>(a, 1, st);
+    return;
+  }
   const int32_t vg = vg_ma(B);
   const int L = rounds_for(B);
   launch_single<MaKeysBody>(a, vg, st);

@@ -16,7 +16,7 @@ def _check(sbp, orc, B, k, best, ds):
     assert np.array_equal(m, want)
 
 
-@pytest.mark.parametrize("B", [1, 2, 7, 300, 5000, 70000, 200000])
+@pytest.mark.parametrize("B", [1, 2, 7, 300, 4096, 4097, 5000, 70000, 200000])
 def test_device_merges_match_oracle(sbp, orc, B):
     rng = np.random.default_rng(B + 1)
     for trial in range(3):
@@ -32,7 +32,7 @@ def test_device_merges_match_oracle(sbp, orc, B):
             _check(sbp, orc, B, k, best, ds)
 
 
-@pytest.mark.parametrize("B", [1000, 100000])
+@pytest.mark.parametrize("B", [1000, 4096, 100000])
 def test_device_merges_chains_and_cycles(sbp, orc, B):
     rng = np.random.default_rng(7)
     ds = rng.standard_normal(B)
