@@ -630,7 +630,13 @@ def run_reference(args, rank, world, local):
                        "B_planted": WORKLOAD["B"], "parallelism": "single GPU"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "cpu_baseline": None,
+            # this run itself, in the record's cpu_baseline form: GSAP's path
+            # runs on the GPU (its host side is one thread issuing kernels)
+            "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 1,
+                             "sample": f"{K} full GSAP partition(s) of the {WORKLOAD['name']} "
+                                       "graph by GSAP's own build, whose path runs on the GPU "
+                                       "(GSAP has no CPU implementation); the CPU oracle's "
+                                       "timing is our arm's cpu_baseline"},
             "same_steps": K == args.steps,
             "steps_note": f"{K} GSAP partitions of {args.steps} requested: one takes 75-190 s "
                           f"on a B200, so the arm runs at most {args.ref_max_steps}",
