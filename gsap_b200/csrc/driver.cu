@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <future>
 #include <memory>
 #include <cstring>
 #include <limits>
@@ -51,7 +52,9 @@ sbp_status host_fail(sbp_status st, const char* msg) { return fail(st, msg); }
 
 
 // ------------------------------------------------------------ validation --
-sbp_status validate_graph(const sbp_graph_csr* g) {
+// Sizes, arrays and row pointers (0 .. E, never decreasing): what an upload
+// needs before the owner-filling kernels write through the row pointers.
+static sbp_status validate_rows(const sbp_graph_csr* g) {
   if (!g) return fail(SBP_ERR_INVALID, "graph is NULL");
   if (g->N < 1 || g->E < 0) return fail(SBP_ERR_INVALID, "need N >= 1 and E >= 0");
   if (!g->out_ptr || !g->in_ptr || !g->deg_out || !g->deg_in)
@@ -71,8 +74,20 @@ sbp_status validate_graph(const sbp_graph_csr* g) {
   for (int d = 0; d < 2; ++d)
     for (int32_t v = 0; v < N; ++v)
       if (ptrs[d][v + 1] < ptrs[d][v]) return fail(SBP_ERR_INVALID, "row pointers decrease");
-  // the entries, split by vertex over up to 8 threads for large graphs;
-  // the error reported is the first in (direction, vertex, entry) order
+  return SBP_OK;
+}
+
+// The entries of a graph whose rows validate_rows accepted: vertex ids in
+// range, weights >= 1, degrees equal to the weight sums.  Split by vertex
+// over up to 8 threads for large graphs; returns the first error in
+// (direction, vertex, entry) order, or nullptr.  Sets no thread's error, so
+// that it can run beside the upload on a helper thread.
+static const char* graph_entry_error(const sbp_graph_csr* g) {
+  const int32_t N = g->N;
+  const int32_t* ptrs[2] = {g->out_ptr, g->in_ptr};
+  const int32_t* idxs[2] = {g->out_idx, g->in_idx};
+  const uint32_t* ws[2] = {g->out_w, g->in_w};
+  const uint32_t* degs[2] = {g->deg_out, g->deg_in};
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const int T = (int)std::min<int64_t>({8, (int64_t)hw, std::max<int64_t>(1, g->E / 262144)});
   struct Bad {
@@ -114,8 +129,15 @@ sbp_status validate_graph(const sbp_graph_csr* g) {
   for (auto& x : th) x.join();
   for (int d = 0; d < 2; ++d)
     for (int t = 0; t < T; ++t)  // threads hold ascending vertex ranges
-      if (bad[(size_t)t * 2 + d].msg) return fail(SBP_ERR_INVALID, bad[(size_t)t * 2 + d].msg);
-  return SBP_OK;
+      if (bad[(size_t)t * 2 + d].msg) return bad[(size_t)t * 2 + d].msg;
+  return nullptr;
+}
+
+sbp_status validate_graph(const sbp_graph_csr* g) {
+  sbp_status s = validate_rows(g);
+  if (s != SBP_OK) return s;
+  const char* bad = graph_entry_error(g);
+  return bad ? fail(SBP_ERR_INVALID, bad) : SBP_OK;
 }
 
 sbp_status validate_part(const int32_t* part, int32_t N, int32_t B) {
@@ -642,13 +664,25 @@ int32_t env_dense_max() {
   return e ? std::atoi(e) : 4096;
 }
 
+// The entries are checked on a helper thread while the host thread creates
+// the arena and uploads (the upload only needs valid row pointers); no
+// kernel reads an entry before the check has passed.
 static sbp_status job_for(Job& J, const sbp_graph_csr* g, int device, int32_t np, int32_t max_itr,
                           int32_t dense_max) {
-  sbp_status s = validate_graph(g);
+  sbp_status s = validate_rows(g);
   if (s != SBP_OK) return s;
+  std::future<const char*> entries;
+  try {
+    entries = std::async(std::launch::async, graph_entry_error, g);
+  } catch (const std::system_error&) {
+    const char* bad = graph_entry_error(g);  // no thread to spare: check first
+    if (bad) return fail(SBP_ERR_INVALID, bad);
+  }
   s = job_create(J, resolve_device(device), g->N, g->E, np, max_itr, dense_max);
-  if (s != SBP_OK) return s;
-  return job_upload(J, g);
+  if (s == SBP_OK) s = job_upload(J, g);
+  const char* bad = entries.valid() ? entries.get() : nullptr;
+  if (bad) return fail(SBP_ERR_INVALID, bad);
+  return s;
 }
 
 // Validates the graph and the labels, then creates the job, uploads both
