@@ -73,7 +73,7 @@ class Dist:
             if backend == "nccl":
                 torch.cuda.set_device(local)
             self.device = "cuda" if backend == "nccl" else "cpu"
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
             self.dist, self.torch = dist, torch
 
     def barrier(self):
