@@ -1207,7 +1207,8 @@ __device__ __forceinline__ void warp_vertex(const NodalArgs& a, int i, int lane,
   __syncwarp();
 }
 
-// Warp work items of a batch: pairs of small vertices, then mid vertices.
+// Warp work items of a batch: the mid vertices (largest first, as the host
+// lists them), then pairs of small vertices.
 __host__ __device__ __forceinline__ int nodal_items(int nsmall, int nmid) {
   return (nsmall + 1) / 2 + nmid;
 }
@@ -1226,11 +1227,12 @@ struct NodalBody {
   const int nw = vg * kNodalWarps;
   const int npairs = (a.nsmall + 1) / 2;
   const int items = npairs + a.nmid;
-  for (int it = vb * kNodalWarps + wid; it < items; it += nw) {
+  for (int it0 = vb * kNodalWarps + wid; it0 < items; it0 += nw) {
     int ia, ib = -1;
-    if (it >= npairs) {
-      ia = a.mid[it - npairs];
+    if (it0 < a.nmid) {
+      ia = a.mid[it0];
     } else {
+      const int it = it0 - a.nmid;
       ia = a.small[2 * it];
       const bool two = 2 * it + 1 < a.nsmall;
       ib = two ? a.small[2 * it + 1] : -1;
