@@ -595,29 +595,42 @@ void classify_batch(const Job& J, const int32_t* verts, int32_t lo, int32_t coun
   out.resize(at + (size_t)std::max(count, 0));
   int32_t* o = out.data() + at;
   n[0] = n[1] = n[2] = 0;
-  for (int pass = 0; pass < 3; ++pass)
-    for (int32_t i = 0; i < count; ++i) {
-      const int32_t v = verts ? verts[i] : lo + i;
-      const int32_t e = (J.h_optr[v + 1] - J.h_optr[v]) + (J.h_iptr[v + 1] - J.h_iptr[v]);
-      const int cls = heavy_vertex(J, v) ? 2 : e <= kSmallEntries ? 0 : 1;
-      if (cls == pass) {
-        o[n[0] + n[1] + n[2]] = i;
-        ++n[pass];
-      }
-    }
+  if (count <= 0) return;
   // The kernels run their items in list order, the larger vertices first: a
   // longest-first schedule, so that a launch does not end on a tail of its
   // slowest items (10% of a 200k partition), and small vertices paired with
-  // ones of about their size.  A stable order: ties by batch index.  Each
-  // vertex's result does not depend on where it runs.
-  auto ent = [&](int32_t i) {
+  // ones of about their size.  Each class is ordered by entry count, largest
+  // first, ties by batch index (a counting sort: the small and mid classes
+  // have at most 2 * kWarpList entries); a vertex's result does not depend on
+  // where it runs.
+  std::vector<int32_t> ent((size_t)count);
+  std::vector<uint8_t> cls((size_t)count);
+  int32_t emax = 0;
+  for (int32_t i = 0; i < count; ++i) {
     const int32_t v = verts ? verts[i] : lo + i;
-    return (J.h_optr[v + 1] - J.h_optr[v]) + (J.h_iptr[v + 1] - J.h_iptr[v]);
-  };
-  auto larger = [&](int32_t x, int32_t y) { return ent(x) > ent(y); };
-  std::stable_sort(o, o + n[0], larger);
-  std::stable_sort(o + n[0], o + n[0] + n[1], larger);
-  std::stable_sort(o + n[0] + n[1], o + n[0] + n[1] + n[2], larger);
+    const int32_t e = (J.h_optr[v + 1] - J.h_optr[v]) + (J.h_iptr[v + 1] - J.h_iptr[v]);
+    ent[i] = e;
+    cls[i] = heavy_vertex(J, v) ? 2 : e <= kSmallEntries ? 0 : 1;
+    ++n[cls[i]];
+    if (cls[i] < 2) emax = std::max(emax, e);
+  }
+  std::vector<int32_t> start((size_t)emax + 2, 0);
+  int32_t base = 0;
+  for (int c = 0; c < 2; ++c) {
+    // descending entry count: bucket emax first
+    std::fill(start.begin(), start.end(), 0);
+    for (int32_t i = 0; i < count; ++i)
+      if (cls[i] == c) ++start[(size_t)(emax - ent[i]) + 1];
+    for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
+    for (int32_t i = 0; i < count; ++i)
+      if (cls[i] == c) o[base + start[(size_t)(emax - ent[i])]++] = i;
+    base += n[c];
+  }
+  int32_t* h = o + base;
+  int32_t nh = 0;
+  for (int32_t i = 0; i < count; ++i)
+    if (cls[i] == 2) h[nh++] = i;
+  std::stable_sort(h, h + nh, [&](int32_t x, int32_t y) { return ent[x] > ent[y]; });
 }
 
 NodalAux nodal_lists(Job& J, const int32_t* dev, const int32_t n[3]) {
