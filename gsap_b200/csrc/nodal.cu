@@ -45,7 +45,7 @@ namespace sbp {
 
 namespace {
 
-constexpr int kNodalWarps = 8;
+constexpr int kNodalWarps = 4;
 constexpr int kWarpList = 128;     // entries per direction a warp sorts in shared memory
 constexpr int kHeavyThreads = 256;
 constexpr int kHashSlotsCfg = 8192;
@@ -1216,7 +1216,7 @@ __host__ __device__ __forceinline__ int nodal_items(int nsmall, int nmid) {
 template <bool GIVEN, bool DENSE, bool GEN>
 struct NodalBody {
   using Args = NodalArgs;
-  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = GEN ? 2 : DENSE ? 6 : 3;
+  static constexpr int kThreads = kNodalWarps * 32, kMinBlocks = GEN ? 4 : DENSE ? 10 : 6;
   static constexpr size_t kSmem = 0;
   static __device__ void run(const Args& a, int vb, int vg) {
   if (ctl_stopped(a.ctl)) return;
