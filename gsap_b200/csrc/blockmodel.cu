@@ -740,6 +740,40 @@ struct DenseDegreesBody {
   }
 };
 
+// Build step 1 after a merge step: the dense form of the merged labels from
+// the CSR blockmodel of the labels before it (rebuilt for the merge) and the
+// merge map: entry (r, c, count) adds count at (map[r], map[c]).  The same
+// integer sums as adding every edge (the counts are the edges' weight sums),
+// from nnz entries instead of E edges; a warp per old block row.
+struct DenseMapArgs {
+  const int32_t *bop, *boc;
+  const uint32_t* bon;
+  const int32_t* map;
+  uint32_t *Md, *MTd, *Sd;
+  int32_t B_old, B;
+};
+
+struct DenseFromCsrBody {
+  using Args = DenseMapArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    const int lane = threadIdx.x & 31;
+    const int K = (a.B + 31) >> 5;
+    for (int r = (vb * kThreads + threadIdx.x) >> 5; r < a.B_old; r += (vg * kThreads) >> 5) {
+      const int R = a.map[r];
+      for (int i = a.bop[r] + lane; i < a.bop[r + 1]; i += 32) {
+        const int C = a.map[a.boc[i]];
+        const uint32_t w = a.bon[i];
+        atomicAdd(a.Md + (size_t)R * a.B + C, w);
+        atomicAdd(a.MTd + (size_t)C * a.B + R, w);
+        atomicAdd(sd_out(a.Sd, K, R, C), w);
+        atomicAdd(sd_in(a.Sd, K, R, C), w);
+      }
+    }
+  }
+};
+
 // Build step 3: log2 of the block degrees.
 struct DenseLogsBody {
   using Args = DenseArgs;
@@ -1143,6 +1177,7 @@ const MultiKernel kmRbCompact = multi_kernel_desc<RbCompactBody>("rb_compact");
 const MultiKernel kmBlockTerms = multi_kernel_desc<BlockTermsBody>("block_terms");
 const MultiKernel kmBlockTermsDense = multi_kernel_desc<BlockTermsDenseBody>("block_terms_dense");
 const MultiKernel kmDenseEdges = multi_kernel_desc<DenseEdgesBody>("dense_edges");
+const MultiKernel kmDenseFromCsr = multi_kernel_desc<DenseFromCsrBody>("dense_from_csr");
 const MultiKernel kmDenseDegrees = multi_kernel_desc<DenseDegreesBody>("dense_degrees");
 const MultiKernel kmDenseLogs = multi_kernel_desc<DenseLogsBody>("dense_logs");
 const MultiKernel kmDenseUpdate = multi_kernel_desc<DenseUpdateBody>("dense_update");
@@ -1386,7 +1421,7 @@ void DenseBuildSlots::clear() {
   for (Slot* x : all()) x->clear();
 }
 
-std::vector<Slot*> DenseBuildSlots::all() { return {&zero, &edges, &degrees, &logs}; }
+std::vector<Slot*> DenseBuildSlots::all() { return {&zero, &edges, &mapped, &degrees, &logs}; }
 
 void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B,
                      DevBM& m) {
@@ -1398,6 +1433,21 @@ void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part,
   add_zero(s.zero, m.d_in, (size_t)B);
   DenseArgs a = dense_args(g, part, B, m);
   slot_push(slot_bind(s.edges, kmDenseEdges), a, g.E > 0 ? ceil_div(g.E, 256) : 0);
+  slot_push(slot_bind(s.degrees, kmDenseDegrees), a, ceil_div(g.N, 256));
+  slot_push(slot_bind(s.logs, kmDenseLogs), a, ceil_div(B, 256));
+}
+
+void add_dense_build_mapped(DenseBuildSlots& s, const DevGraph& g, const int32_t* part,
+                            int32_t B, DevBM& m, int32_t B_old, const int32_t* map) {
+  const size_t bb = (size_t)B * B;
+  add_zero(s.zero, m.Md, bb);
+  add_zero(s.zero, m.MTd, bb);
+  add_zero(s.zero, m.Sd, (size_t)2 * B * ((B + 31) / 32));
+  add_zero(s.zero, m.d_out, (size_t)B);
+  add_zero(s.zero, m.d_in, (size_t)B);
+  DenseMapArgs b{m.optr, m.ocol, m.ocnt, map, m.Md, m.MTd, m.Sd, B_old, B};
+  slot_push(slot_bind(s.mapped, kmDenseFromCsr), b, grid_for((long long)B_old * 32, 256, 148 * 16));
+  DenseArgs a = dense_args(g, part, B, m);
   slot_push(slot_bind(s.degrees, kmDenseDegrees), a, ceil_div(g.N, 256));
   slot_push(slot_bind(s.logs, kmDenseLogs), a, ceil_div(B, 256));
 }

@@ -78,6 +78,7 @@ void Run::start_sweeps(int32_t B0, uint32_t seq0, int32_t sweeps) {
   stage = kSweep;
   init = false;
   build = true;
+  build_from_merge = false;
   zero_itr = true;
   upload_lists = !lists_all.empty();
 }
@@ -321,7 +322,12 @@ void Engine::add_run_work(Run& r) {
   }
   if (r.stage == Run::kSweep) {
     if (r.build) {
-      if (dense) {
+      if (dense && r.build_from_merge) {
+        // from the merge step's CSR blockmodel and its map: nnz entries, not E edges
+        add_dense_build_mapped(pre_dense, J.g, J.part, r.B, J.m, r.B_merged_from, J.map);
+        r.pre_bytes += 8.0 * r.B * (double)r.B +
+                       12.0 * std::min((double)J.E, (double)r.B_merged_from * r.B_merged_from);
+      } else if (dense) {
         add_dense_build(pre_dense, J.g, J.part, r.B, J.m);
         r.pre_bytes += 8.0 * r.B * (double)r.B + 12.0 * J.E;  // zero M, M^T; add the edges
       } else {
@@ -766,9 +772,11 @@ sbp_status Engine::tick() {
         continue;
       }
       ++r->seq;
+      r->B_merged_from = r->B;  // the CSR form holds this B's blockmodel
       r->B = nb;
       r->csr_fresh = false;
       r->build = true;
+      r->build_from_merge = true;
       r->zero_itr = true;
       r->itr = 0;
       r->stage = Run::kSweep;

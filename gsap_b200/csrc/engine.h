@@ -61,6 +61,11 @@ struct Run {
   // device work left pending by the last host decision
   bool init = false, upload_lists = false, build = false, zero_itr = false;
   bool csr_fresh = false;
+  // the pending build follows a merge step: the CSR arrays still hold the
+  // blockmodel of the B_merged_from blocks before it, and the job's map the
+  // merge, so a dense form is built from them rather than from the edges
+  bool build_from_merge = false;
+  int32_t B_merged_from = 0;
   int snap_slot = -1, restore_slot = -1;
   // this tick's offsets in the upload and readback buffers
   size_t up_lists = 0, rd_off = 0;

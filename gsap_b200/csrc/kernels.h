@@ -145,7 +145,7 @@ struct RebuildSlots {
 
 // The launches of a dense-form build, in order.
 struct DenseBuildSlots {
-  Slot zero, edges, degrees, logs;
+  Slot zero, edges, mapped, degrees, logs;
   void clear();
   std::vector<Slot*> all();
 };
@@ -159,6 +159,10 @@ struct DenseBuildSlots {
 void add_rebuild(RebuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
                  RebuildScratch& rs, const int32_t* ctl = nullptr,
                  const RebuildTune& t = RebuildTune{});
+// The dense form right after a merge step: from the CSR blockmodel of the
+// labels before it (B_old blocks, still in m's CSR arrays) and the merge map.
+void add_dense_build_mapped(DenseBuildSlots& s, const DevGraph& g, const int32_t* part,
+                            int32_t B, DevBM& m, int32_t B_old, const int32_t* map);
 void add_dense_build(DenseBuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B,
                      DevBM& m);
 void add_dense_update(Slot& s, const DevGraph& g, const int32_t* part, int32_t lo, int32_t count,
