@@ -774,6 +774,58 @@ struct DenseFromCsrBody {
   }
 };
 
+// The CSR blockmodel from a dense form that holds the current labels' M (a
+// merge step after sweeps that left the labels as they were): a warp per
+// row of M (the out CSR) and of M^T (the in CSR) counts the row's nonzero
+// cells, and after the scan writes them in column order with their counts:
+// the arrays the rebuild from the edges builds.  Degrees and their log2 are
+// the dense form's own.
+struct DenseCsrArgs {
+  const uint32_t *Md, *MTd;
+  int32_t *cnt_o, *cnt_i;  // per row: nonzero cells (the scan's input)
+  const int32_t *optr, *iptr;
+  int32_t *ocol, *icol;
+  uint32_t *ocnt, *icnt;
+  int32_t B, fill;  // fill 0: count, 1: write the rows
+};
+
+struct DenseCsrBody {
+  using Args = DenseCsrArgs;
+  static constexpr int kThreads = 256, kMinBlocks = 1;
+  static constexpr size_t kSmem = 0;
+  static __device__ void run(const Args& a, int vb, int vg) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int B = a.B;
+    for (int t = (vb * kThreads + threadIdx.x) >> 5; t < 2 * B; t += (vg * kThreads) >> 5) {
+      const bool in = t >= B;
+      const int b = in ? t - B : t;
+      const uint32_t* row = (in ? a.MTd : a.Md) + (size_t)b * B;
+      int k = 0;
+      int32_t* col = nullptr;
+      uint32_t* cnt = nullptr;
+      if (a.fill) {
+        k = (in ? a.iptr : a.optr)[b];
+        col = in ? a.icol : a.ocol;
+        cnt = in ? a.icnt : a.ocnt;
+      }
+      int n = 0;
+      for (int c0 = 0; c0 < B; c0 += 32) {
+        const int c = c0 + lane;
+        const uint32_t m = c < B ? row[c] : 0u;
+        const unsigned nz = __ballot_sync(kFull, m != 0u);
+        if (a.fill && m) {
+          const int pos = k + n + __popc(nz & lt);
+          col[pos] = c;
+          cnt[pos] = m;
+        }
+        n += __popc(nz);
+      }
+      if (!a.fill && lane == 0) (in ? a.cnt_i : a.cnt_o)[b] = n;
+    }
+  }
+};
+
 // Build step 3: log2 of the block degrees.
 struct DenseLogsBody {
   using Args = DenseArgs;
@@ -1178,6 +1230,7 @@ const MultiKernel kmBlockTerms = multi_kernel_desc<BlockTermsBody>("block_terms"
 const MultiKernel kmBlockTermsDense = multi_kernel_desc<BlockTermsDenseBody>("block_terms_dense");
 const MultiKernel kmDenseEdges = multi_kernel_desc<DenseEdgesBody>("dense_edges");
 const MultiKernel kmDenseFromCsr = multi_kernel_desc<DenseFromCsrBody>("dense_from_csr");
+const MultiKernel kmDenseCsr = multi_kernel_desc<DenseCsrBody>("dense_csr");
 const MultiKernel kmDenseDegrees = multi_kernel_desc<DenseDegreesBody>("dense_degrees");
 const MultiKernel kmDenseLogs = multi_kernel_desc<DenseLogsBody>("dense_logs");
 const MultiKernel kmDenseUpdate = multi_kernel_desc<DenseUpdateBody>("dense_update");
@@ -1396,7 +1449,20 @@ void RebuildSlots::clear() {
 
 std::vector<Slot*> RebuildSlots::all() {
   return {&zero,     &count,     &scan1[0],   &scan1[1], &scan1[2], &scatter,
-          &rows_small, &rows_big, &scan2[0], &scan2[1], &scan2[2], &compact};
+          &rows_small, &rows_big, &dense_count, &scan2[0], &scan2[1], &scan2[2], &compact,
+          &dense_fill};
+}
+
+void add_csr_from_dense(RebuildSlots& s, int32_t B, DevBM& m, RebuildScratch& rs) {
+  DenseCsrArgs a{m.Md, m.MTd, rs.d[0].uniq, rs.d[1].uniq, m.optr, m.iptr,
+                 m.ocol, m.icol, m.ocnt, m.icnt, B, 0};
+  const int32_t vg = grid_for((long long)2 * B * 32, 256, 148 * 16);
+  slot_push(slot_bind(s.dense_count, kmDenseCsr), a, vg);
+  for (int dir = 0; dir < 2; ++dir)
+    add_scan(s.scan2, rs.d[dir].uniq, dir == 0 ? m.optr : m.iptr, B,
+             rs.tile + dir * (rs.tile_cap / 2), nullptr);
+  a.fill = 1;
+  slot_push(slot_bind(s.dense_fill, kmDenseCsr), a, vg);
 }
 
 void add_rebuild(RebuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,

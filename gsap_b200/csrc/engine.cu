@@ -155,6 +155,10 @@ void Run::after_sweep(double dsum, double dataS, long long acc) {
     return;
   }
   restore_slot = restore->slot;
+  // restoring the snapshot just taken of this step leaves the labels as they
+  // are, and with them a dense form, which the merge step then reads its CSR
+  // form from
+  dense_kept = dense() && restore->slot == snap_slot;
   B = restore->B;
   S = restore->S;
   csr_fresh = false;
@@ -303,7 +307,10 @@ void Engine::add_run_work(Run& r) {
   const bool dense = r.dense();
   if (r.stage == Run::kMerge) {
     // the merge kernels read the CSR form
-    if (!r.csr_fresh) {
+    if (!r.csr_fresh && r.dense_kept && r.dense()) {
+      add_csr_from_dense(pre_rebuild, r.B, J.m, J.rs);
+      r.pre_bytes += 8.0 * r.B * (double)r.B + 8.0 * r.nnz_now + 8.0 * r.B;
+    } else if (!r.csr_fresh) {
       add_rebuild(pre_rebuild, J.g, J.part, r.B, J.m, J.rs, nullptr, tune_for(J, r.B));
       r.pre_bytes += 4.0 * N + 24.0 * J.E + 16.0 * r.nnz_now + 8.0 * r.B;
     }
@@ -773,6 +780,7 @@ sbp_status Engine::tick() {
       }
       ++r->seq;
       r->B_merged_from = r->B;  // the CSR form holds this B's blockmodel
+      r->dense_kept = false;
       r->B = nb;
       r->csr_fresh = false;
       r->build = true;

@@ -66,6 +66,9 @@ struct Run {
   // merge, so a dense form is built from them rather than from the edges
   bool build_from_merge = false;
   int32_t B_merged_from = 0;
+  // the golden section kept the step's labels, so the dense form still holds
+  // their blockmodel (the next merge step reads its CSR form from it)
+  bool dense_kept = false;
   int snap_slot = -1, restore_slot = -1;
   // this tick's offsets in the upload and readback buffers
   size_t up_lists = 0, rd_off = 0;

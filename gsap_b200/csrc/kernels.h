@@ -139,6 +139,7 @@ inline Slot& slot_bind(Slot& s, const MultiKernel& k) {
 // The launches of a blockmodel rebuild, in order.
 struct RebuildSlots {
   Slot zero, count, scan1[3], scatter, rows_small, rows_big, scan2[3], compact;
+  Slot dense_count, dense_fill;  // the CSR form from a fresh dense form instead
   void clear();
   std::vector<Slot*> all();
 };
@@ -159,6 +160,9 @@ struct DenseBuildSlots {
 void add_rebuild(RebuildSlots& s, const DevGraph& g, const int32_t* part, int32_t B, DevBM& m,
                  RebuildScratch& rs, const int32_t* ctl = nullptr,
                  const RebuildTune& t = RebuildTune{});
+// The CSR form of the current labels from their dense form (which must hold
+// them): the rebuild's outputs from O(B^2) cells instead of the edges.
+void add_csr_from_dense(RebuildSlots& s, int32_t B, DevBM& m, RebuildScratch& rs);
 // The dense form right after a merge step: from the CSR blockmodel of the
 // labels before it (B_old blocks, still in m's CSR arrays) and the merge map.
 void add_dense_build_mapped(DenseBuildSlots& s, const DevGraph& g, const int32_t* part,
