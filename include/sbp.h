@@ -97,7 +97,7 @@ typedef struct sbp_options {
   int32_t ref_grid;
   /* 1: time every phase with CUDA events around each nodal batch and
    * rebuild, filling sbp_report.ms_nodal, ms_nodal_kernel and ms_rebuild
-   * (each event node costs a few microseconds of device time, about 5% of
+   * (each event node costs a few microseconds of device time, about 10% of
    * a 200k partition); 0 (default): only ms_device, ms_total and the
    * merge and pre-build parts of ms_merge / ms_rebuild. */
   int32_t phase_timing;
