@@ -1,8 +1,8 @@
 // Drives the unmodified GSAP GPU path (graph.hpp + partition.hpp from the
-// reference tree) on a graph file written by gsap_b200 (sbp.write_graph_bin),
-// for the reference arm of bench.py.  Built by oracle/build_ref.sh into
-// oracle/_ref/gsap_ref; the binary travels to the GPU box, the sources of
-// the reference do not.
+// reference tree) on a graph file written by write_graph_bin (oracle/oracle.py
+// or gsap_b200/sbp.py, the same format), for the reference arm of bench.py.
+// Built by oracle/build_ref.sh into oracle/_ref/gsap_ref; the binary is all
+// that later runs need, not the sources of the reference.
 //
 //   gsap_ref <graph.bin> <runs> <labels_out.bin>
 //
